@@ -1,0 +1,383 @@
+/*
+ * sygraph_b200.h -- C ABI of libsygraph_b200.so, the B200 (sm_100a) frontier
+ * hot path of SYgraph.
+ *
+ * SYgraph is a header-only C++20/SYCL library with no FFI: its boundary is
+ * the template API under include/sygraph/ called in-process on one
+ * sycl::queue.  Each entry point below names the reference interface it
+ * replaces (file:line, relative to the SYgraph project root).  The C++20
+ * header layer in include/sygraph/ (same names as the reference) is built on
+ * these calls; templated advances with user lambdas instantiate the kernels
+ * of include/sygraph/detail/advance_kernels.cuh directly.
+ *
+ * Conventions
+ *   - Every call returns an sg_status; SG_OK is 0.  No C++ exception crosses
+ *     this boundary.  sg_last_error() gives the message of the last failure
+ *     on the calling thread.  Where the reference throws std::runtime_error
+ *     (unsupported combinations, uninitialised instances) these calls return
+ *     SG_ERR_INVALID / SG_ERR_UNSUPPORTED / SG_ERR_NOT_INITIALIZED.
+ *   - Vertex ids, row offsets and column indices are uint32 (the reference's
+ *     index_t; every example and test instantiates uint32, e.g.
+ *     tests/include/test_utils.hpp:63).  Edge weights are float32 or uint32.
+ *   - `stream` is a cudaStream_t passed as void*; NULL means the legacy
+ *     default stream.  Objects remember the stream they were created with,
+ *     as GraphCSR holds its queue (graph/impls/graph_csr.hpp:434).
+ *   - Pointers named host_* are host memory; dev_* are device memory.
+ *   - Device-side persistent loops use bounded waits: a wait that runs out
+ *     returns SG_ERR_TIMEOUT instead of hanging.
+ */
+#ifndef SYGRAPH_B200_H
+#define SYGRAPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status -- */
+typedef int sg_status;
+#define SG_OK 0
+#define SG_ERR_INVALID 1         /* bad argument: std::runtime_error in the reference */
+#define SG_ERR_CUDA 2            /* a CUDA runtime call failed */
+#define SG_ERR_NOMEM 3           /* device or host allocation failed / over budget */
+#define SG_ERR_TIMEOUT 4         /* a bounded device-side wait ran out */
+#define SG_ERR_UNSUPPORTED 5     /* "Load balancer not implemented" (operators/advance/advance.hpp:63,138) */
+#define SG_ERR_NOT_INITIALIZED 6 /* "BFS instance not initialized" (algorithms/bfs.hpp:155) */
+
+/* Message of the last failed call on this thread ("" when none). */
+const char* sg_last_error(void);
+/* Static name of a status code. */
+const char* sg_status_string(sg_status s);
+/* Library version string. */
+const char* sg_version(void);
+
+/* ---------------------------------------------------------------- enums -- */
+/* operators/config.hpp:10-37 */
+#define SG_DIR_PUSH 0
+#define SG_DIR_PULL 1     /* pull with short-circuit after the first successful edge */
+#define SG_DIR_PULL_ALL 2 /* pull without short-circuit */
+
+#define SG_LB_WORKITEM_MAPPED 0  /* one thread per candidate vertex */
+#define SG_LB_SUBGROUP_MAPPED 1  /* one warp per candidate vertex */
+#define SG_LB_WORKGROUP_MAPPED 2 /* CTA-wide degree scan, edge-parallel (the reference default) */
+#define SG_LB_BUCKETING 3        /* lane / warp / CTA buckets by degree */
+
+/* frontier/frontier_settings.hpp:13-27 */
+#define SG_VIEW_GRAPH 0
+#define SG_VIEW_VERTEX 1
+#define SG_VIEW_EDGE 2
+#define SG_VIEW_NONE 3
+
+/* operators/config.hpp:31-32 */
+#define SG_SIZE_FETCH_FROM_MEMORY (-1)
+#define SG_SIZE_INFER_FROM_DEVICE 0
+
+/* algorithms/bfs.hpp:29 */
+#define SG_BFS_PUSH 0
+#define SG_BFS_PULL 1
+#define SG_BFS_HYBRID 2
+
+#define SG_WEIGHT_NONE 0
+#define SG_WEIGHT_F32 1
+#define SG_WEIGHT_U32 2
+
+/* graph/properties.hpp:29-32 and the binary CSR flags (io/read_csr.hpp:22-25) */
+#define SG_GRAPH_DIRECTED 1u
+#define SG_GRAPH_WEIGHTED 2u
+
+/* ------------------------------------------------------ device helpers -- */
+sg_status sg_device_count(int* count);
+sg_status sg_set_device(int device);
+sg_status sg_device_info(int* sm_count, uint64_t* free_bytes, uint64_t* total_bytes);
+/* Plain device memory helpers for callers without a CUDA toolchain. */
+sg_status sg_malloc_device(uint64_t bytes, void** dev_ptr);
+sg_status sg_free_device(void* dev_ptr);
+sg_status sg_malloc_host_pinned(uint64_t bytes, void** host_ptr);
+sg_status sg_free_host_pinned(void* host_ptr);
+/* kind: 0 host->device, 1 device->host, 2 device->device, 3 default (unified addressing) */
+sg_status sg_memcpy(void* dst, const void* src, uint64_t bytes, int kind, void* stream);
+sg_status sg_memset(void* dev_ptr, int value, uint64_t bytes, void* stream);
+sg_status sg_stream_synchronize(void* stream);
+sg_status sg_device_synchronize(void);
+/* Number of kernels this library has launched in this process (all entry
+ * points, all devices); used to report launch counts. */
+uint64_t sg_kernel_launch_count(void);
+
+/* ---------------------------------------------------------------- graph -- */
+typedef struct sg_graph_s* sg_graph;
+
+/* Device view of one CSR direction; pointers are device memory owned by the graph. */
+typedef struct {
+  uint32_t n;
+  uint64_t m;
+  const uint32_t* row_offsets;
+  const uint32_t* column_indices;
+  const void* values; /* float32 or uint32 per value_type; NULL when unweighted */
+  int value_type;
+} sg_graph_view;
+
+/* graph::build::fromCSR<Space>(q, csr, Properties) (graph/build.hpp:31-41),
+ * GraphCSR::initializeGraphStorage (graph/impls/graph_csr.hpp:394-426).
+ * Copies the host CSR to the device.  host_values may be NULL (every weight
+ * is then 1, as fromMM does for pattern matrices).  When flags has
+ * SG_GRAPH_DIRECTED the inverse (incoming-edge) CSR is built as well
+ * (formats/csr.hpp:179-209); otherwise the inverse view aliases the forward
+ * one (graph_csr.hpp:424). */
+sg_status sg_graph_create_csr(const uint32_t* host_row_offsets, const uint32_t* host_column_indices,
+                              const void* host_values, int value_type, uint32_t n, uint64_t m, uint32_t flags,
+                              void* stream, sg_graph* out);
+sg_status sg_graph_destroy(sg_graph g);
+sg_status sg_graph_info(sg_graph g, uint32_t* n, uint64_t* m, uint32_t* flags, int* value_type);
+/* GraphCSR::getDeviceGraph / getInverseDeviceGraph (graph_csr.hpp:300-320). */
+sg_status sg_graph_device_view(sg_graph g, int inverse, sg_graph_view* view);
+sg_status sg_graph_set_stream(sg_graph g, void* stream);
+/* Host copy of row offsets / columns (GraphCSR::getRowOffsets etc.). */
+sg_status sg_graph_copy_csr(sg_graph g, int inverse, uint32_t* host_row_offsets, uint32_t* host_column_indices,
+                            void* host_values);
+/* GraphCSRDevice::getDegree (graph_csr.hpp:64), host query. */
+sg_status sg_graph_degree(sg_graph g, uint32_t v, uint32_t* degree);
+sg_status sg_graph_memory_bytes(sg_graph g, uint64_t* bytes);
+
+/* ------------------------------------------------------------- frontier -- */
+typedef struct sg_frontier_s* sg_frontier;
+
+/* Device view of a two-level bitmap frontier (MLBDevice, frontier/impls/mlb_frontier.hpp:58-153). */
+typedef struct {
+  uint32_t num_elems;
+  uint32_t words0; /* ceil(num_elems/32) */
+  uint32_t words1; /* ceil(words0/32) */
+  uint32_t* level0;
+  uint32_t* level1;
+  int32_t* offsets;       /* compacted active-word indices */
+  uint32_t* offsets_size; /* device scalar */
+} sg_frontier_view;
+
+/* FrontierMLB(q, num_elems) (mlb_frontier.hpp:162-179) / makeFrontier (frontier/frontier.hpp:68-80). */
+sg_status sg_frontier_create(uint32_t num_elems, void* stream, sg_frontier* out);
+sg_status sg_frontier_destroy(sg_frontier f);
+sg_status sg_frontier_device_view(sg_frontier f, sg_frontier_view* view);
+sg_status sg_frontier_num_elems(sg_frontier f, uint32_t* num_elems);
+/* FrontierMLB::clear (mlb:367-380) */
+sg_status sg_frontier_clear(sg_frontier f);
+/* FrontierMLB::insert / remove / check (mlb:248-285) */
+sg_status sg_frontier_insert(sg_frontier f, uint32_t idx);
+sg_status sg_frontier_remove(sg_frontier f, uint32_t idx);
+sg_status sg_frontier_check(sg_frontier f, uint32_t idx, int* present);
+/* Bulk insert of a host list (many FrontierMLB::insert calls in one launch). */
+sg_status sg_frontier_insert_list(sg_frontier f, const uint32_t* host_ids, uint64_t count);
+/* FrontierMLB::empty (mlb:216-246) and size (mlb:287-311). */
+sg_status sg_frontier_empty(sg_frontier f, int* empty);
+sg_status sg_frontier_size(sg_frontier f, uint64_t* size);
+/* FrontierMLB::merge / intersect (mlb:313-337): level-0 OR / AND.  Both
+ * levels are kept consistent here (the reference leaves level 1 stale). */
+sg_status sg_frontier_merge(sg_frontier f, sg_frontier other);
+sg_status sg_frontier_intersect(sg_frontier f, sg_frontier other);
+/* frontier::swap (frontier/frontier.hpp:94-101, mlb:444) */
+sg_status sg_frontier_swap(sg_frontier a, sg_frontier b);
+/* FrontierMLB::computeActiveFrontier(invert) (mlb:388-442): writes the
+ * indices of non-empty level-0 words (invert=0) or of non-full words
+ * (invert=1) into the offsets list, warp-ballot compaction.  When
+ * host_active_words is non-NULL the count is copied back (a blocking read,
+ * as buildAdvanceLaunchConfig does at operators/advance/common.hpp:112-119). */
+sg_status sg_frontier_compact(sg_frontier f, int invert, uint32_t* host_active_words);
+/* FrontierMLB::saveState / loadState (mlb:339-365): both levels to/from host. */
+sg_status sg_frontier_save(sg_frontier f, uint32_t* host_level0, uint32_t* host_level1);
+sg_status sg_frontier_load(sg_frontier f, const uint32_t* host_level0, const uint32_t* host_level1);
+/* Flags of every element (1 byte each), for tests and tools. */
+sg_status sg_frontier_to_flags(sg_frontier f, uint8_t* host_flags);
+
+/* ------------------------------------------------------------- operators -- */
+/* Built-in device functors for sg_advance.  The templated C++ API accepts any
+ * device lambda; through the C ABI a functor is one of these, with its state
+ * in sg_op_args (device pointers p[] and scalars u[] / f[]). */
+#define SG_OP_BFS_PUSH 0     /* bfs.hpp:185-191: p0=uint32 depth, u0=sentinel(n+1), u1=iter */
+#define SG_OP_BFS_PULL 1     /* bfs.hpp:201-207: same args; src = candidate, dst = in-frontier neighbour */
+#define SG_OP_SSSP_RELAX 2   /* sssp.hpp:180-189: p0=distances (f32 or u32 per the graph's value_type) */
+#define SG_OP_CC_MAX 3       /* cc.hpp:137-142 with an atomic max: p0=uint32 labels */
+#define SG_OP_BC_FORWARD 4   /* bc.hpp:144-153: p0=uint32 labels, p1=float sigma, u0=invalid label */
+#define SG_OP_BC_BACKWARD 5  /* bc.hpp:174-186: p0=labels, p1=sigma, p2=delta, p3=bc, u0=source */
+#define SG_OP_COUNT_VISITS 6 /* tests/operators/advance_pull.cpp:29-32: p0=uint32 visits; atomicAdd(visits[src],1); true */
+#define SG_OP_NONZERO_DEGREE 7 /* tests/operators/advance_graph.cpp:19: degree(src) != 0 */
+#define SG_OP_BFS_VISIT_FLAG 8 /* tests/operators/advance.cpp:29-36: p0=uint8 visited, p1=uint64 distances */
+#define SG_OP_TRUE 9           /* always true (pure frontier expansion) */
+
+typedef struct {
+  void* p[4];
+  uint32_t u[4];
+  float f[4];
+} sg_op_args;
+
+/* advance::frontier<Direction, Lb, InView, OutView>(G, in, out, f, expected_size)
+ * (operators/advance/advance.hpp:116-218) and advance::vertices<Lb, OutView>(G, out, f)
+ * (advance.hpp:46-87).
+ *   in_view  : SG_VIEW_VERTEX (needs `in`) or SG_VIEW_GRAPH (every vertex, `in` ignored)
+ *   out_view : SG_VIEW_VERTEX (needs `out`) or SG_VIEW_NONE
+ *   expected_size : SG_SIZE_FETCH_FROM_MEMORY, SG_SIZE_INFER_FROM_DEVICE or a
+ *     positive hint.  The active-word count is always read on the device, so
+ *     none of them costs a host round trip.
+ * Pull directions walk the inverse graph (common.hpp:147). */
+sg_status sg_advance(sg_graph g, sg_frontier in, sg_frontier out, int direction, int load_balancer, int in_view,
+                     int out_view, int op, const sg_op_args* args, int expected_size);
+
+#define SG_PRED_EVEN 0        /* tests/operators/filter_compute.cpp:15: v % 2 == 0 */
+#define SG_PRED_LESS_THAN 1   /* filter_compute.cpp:19: v < u0 */
+#define SG_PRED_ITER_MARK 2   /* sssp.hpp:546-550: p0=int32 visited, u0=iter; false if visited[v]==iter else mark, true */
+#define SG_PRED_FLAG 3        /* p0=uint8 flags: flags[v] != 0 */
+
+/* filter::external(G, in, out, pred) (operators/filter/filter.hpp:41-69):
+ * out.clear(), then out gets every v in `in` with pred(v). */
+sg_status sg_filter_external(sg_graph g, sg_frontier in, sg_frontier out, int pred, const sg_op_args* args);
+/* filter::inplace(G, f, pred): removes every v in f with pred(v). */
+sg_status sg_filter_inplace(sg_graph g, sg_frontier f, int pred, const sg_op_args* args);
+
+#define SG_FN_MARK 0         /* filter_compute.cpp:26: p0=uint32 seen; seen[v] = 1 */
+#define SG_FN_SET_U8 1       /* advance_pull.cpp:36: p0=uint8 flags; flags[v] = 1 */
+#define SG_RED_VERTEX_ID 0   /* filter_compute.cpp:35-36: acc += v */
+#define SG_RED_DEGREE 1      /* bfs.hpp:290-291: acc += degree(v) */
+#define SG_RED_COUNT 2       /* acc += 1 */
+
+/* compute::execute<vertex>(G, f, fn) (operators/for/for.hpp:48-60). */
+sg_status sg_compute_execute(sg_graph g, sg_frontier f, int fn, const sg_op_args* args);
+/* compute::reduce<vertex, plus<R>>(G, f, acc, fn) (for.hpp:62-92); the sum is
+ * returned in *host_result (64-bit). */
+sg_status sg_compute_reduce(sg_graph g, sg_frontier f, int fn, const sg_op_args* args, uint64_t* host_result);
+/* intersection::execute(G, in1, in2, out, f) (operators/intersection/intersection.hpp:44-55):
+ * out = in1 AND in2. */
+sg_status sg_intersection_execute(sg_graph g, sg_frontier in1, sg_frontier in2, sg_frontier out);
+/* GraphCSRDevice::getIntersectionCount (graph_csr.hpp:109-135) for a batch of
+ * vertex pairs: counts[i] = |N(a[i]) n N(b[i])| over sorted adjacency. */
+sg_status sg_segmented_intersection(sg_graph g, const uint32_t* dev_a, const uint32_t* dev_b, uint64_t pairs,
+                                    uint32_t* dev_counts);
+
+/* ------------------------------------------------------------ algorithms -- */
+#define SG_MAX_LOGGED_LEVELS 4096
+
+/* BFSRunDetails (algorithms/bfs.hpp:31-35).  step_is_pull[i] records the
+ * direction of step i for the first SG_MAX_LOGGED_LEVELS steps. */
+typedef struct {
+  uint64_t iterations;
+  uint64_t push_steps;
+  uint64_t pull_steps;
+  uint64_t visited_vertices;
+  uint64_t visited_edges; /* sum of degrees of reached vertices (bfs.hpp:88-99) */
+  uint8_t step_is_pull[SG_MAX_LOGGED_LEVELS];
+} sg_bfs_details;
+
+/* Per-level record kept by the fused traversal engines (one per step). */
+typedef struct {
+  uint32_t level;
+  uint32_t strategy;      /* direction * 2 + load balancer (0 warp-mapped, 1 CTA-mapped) */
+  uint32_t frontier_size; /* |F| processed in this step */
+  uint32_t next_size;     /* |F'| produced */
+  uint64_t frontier_degree;   /* sum of degrees over F */
+  uint64_t next_degree;       /* sum of degrees over F' */
+  uint64_t unexplored_degree; /* sum of degrees over unvisited vertices after the step */
+  uint64_t t_start_ns;        /* device global timer at the step's start */
+  uint64_t t_end_ns;
+} sg_level_record;
+
+typedef struct sg_bfs_s* sg_bfs;
+
+/* BFS(G) + init(source) + run(direction, alpha, beta) + getDistances()
+ * (algorithms/bfs.hpp:129-278), as one fused device-side traversal: frontier
+ * compaction, advance, size / degree bookkeeping, the direction heuristic and
+ * termination run inside one persistent kernel with no host round trip per
+ * level.  Depths are uint32 with n+1 for unreached (bfs.hpp:67). */
+sg_status sg_bfs_create(sg_graph g, sg_bfs* out);
+sg_status sg_bfs_destroy(sg_bfs b);
+sg_status sg_bfs_init(sg_bfs b, uint32_t source);
+sg_status sg_bfs_reset(sg_bfs b);
+sg_status sg_bfs_run(sg_bfs b, int direction, float alpha, float beta, sg_bfs_details* details);
+/* Same as sg_bfs_run but enqueues only: no host synchronisation and no
+ * details; for timing loops and graph capture. */
+sg_status sg_bfs_run_async(sg_bfs b, int direction, float alpha, float beta);
+sg_status sg_bfs_get_distances(sg_bfs b, uint32_t* host_depth);
+sg_status sg_bfs_distances_device(sg_bfs b, const uint32_t** dev_depth);
+sg_status sg_bfs_level_records(sg_bfs b, sg_level_record* host_records, uint32_t cap, uint32_t* count);
+/* One-shot form: host depth out (n entries). */
+sg_status sg_run_bfs(sg_graph g, uint32_t source, int direction, float alpha, float beta, uint32_t* host_depth,
+                 sg_bfs_details* details);
+
+/* SSSP(G) + init + run + getDistance (algorithms/sssp.hpp:109-217): frontier
+ * Bellman-Ford with atomicMin, fused.  Distances have the graph's weight type
+ * (float32 or uint32); unreached = (weight_t)(n+1) (sssp.hpp:43). */
+typedef struct sg_sssp_s* sg_sssp;
+sg_status sg_sssp_create(sg_graph g, sg_sssp* out);
+sg_status sg_sssp_destroy(sg_sssp s);
+sg_status sg_sssp_init(sg_sssp s, uint32_t source);
+sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations);
+sg_status sg_sssp_run_async(sg_sssp s);
+sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist);
+sg_status sg_sssp_distances_device(sg_sssp s, const void** dev_dist);
+sg_status sg_run_sssp(sg_graph g, uint32_t source, void* host_dist, uint64_t* iterations);
+
+/* CC(G) + init + run (algorithms/cc.hpp:82-169): maximum-label propagation
+ * with atomicMax; labels[v] = max id over the vertices reaching v. */
+sg_status sg_cc(sg_graph g, uint32_t* host_labels, uint64_t* iterations);
+
+/* BC(G) + init(source) + run (algorithms/bc.hpp:86-200) for each of k
+ * sources; host_bc[v] = sum over sources of the Brandes dependency
+ * delta_s(v), v != s, float32. */
+sg_status sg_bc(sg_graph g, const uint32_t* host_sources, uint32_t k, float* host_bc);
+
+/* TC(G) + init + run + getNumTriangles (algorithms/tc.hpp:58-138), exact:
+ * degree-ordered DAG and sorted-list segmented intersection, uint64.  When
+ * host_per_vertex is non-NULL it receives getNumTriangles(v): for every edge
+ * (u,v) with u < v, |N(u) n N(v)| added to u. */
+sg_status sg_tc(sg_graph g, uint64_t* total, uint64_t* host_per_vertex);
+
+/* ------------------------------------------------------- host graph I/O -- */
+/* Host CSR owned by the library (malloc'd); free with sg_host_csr_free. */
+typedef struct {
+  uint32_t n;
+  uint64_t m;
+  uint32_t* row_offsets;    /* n+1 */
+  uint32_t* column_indices; /* m */
+  void* values;             /* m entries of value_type, or NULL */
+  int value_type;
+  uint32_t flags; /* SG_GRAPH_DIRECTED / SG_GRAPH_WEIGHTED */
+} sg_host_csr;
+
+typedef struct {
+  uint32_t scale;      /* n = 2^scale */
+  uint32_t edge_factor; /* generated pairs = edge_factor * n */
+  double a, b, c;       /* quadrant probabilities; d = 1-a-b-c */
+  uint64_t seed;        /* edge seed */
+  uint64_t weight_seed; /* weight seed (weights keyed by the unordered pair) */
+  uint64_t perm_seed;   /* 0: no relabelling; else seeded random vertex permutation */
+  int value_type;       /* SG_WEIGHT_NONE / F32 ((0,1]) / U32 ([1,64]) */
+} sg_rmat_params;
+
+/* Seeded RMAT generator: recursive quadrant choice, then symmetrise, drop
+ * self-loops, de-duplicate and sort each adjacency list.  OpenMP host code. */
+sg_status sg_rmat_generate(const sg_rmat_params* params, sg_host_csr* out);
+/* side x side 4-neighbour grid plus long_range_frac * (grid pairs) uniform
+ * random pairs, symmetrised, sorted; weights as in sg_rmat_params. */
+sg_status sg_grid_generate(uint32_t side, double long_range_frac, uint64_t seed, uint64_t weight_seed, int value_type,
+                           sg_host_csr* out);
+/* io::csr::fromCOO (io/read_csr.hpp:260-300) generalised: builds a CSR from
+ * an edge list; symmetrize adds (v,u), dedupe drops repeated pairs (keeping
+ * the first value), self-loops are dropped when drop_self_loops. */
+sg_status sg_csr_from_edges(uint32_t n, const uint32_t* src, const uint32_t* dst, const void* values, int value_type,
+                            uint64_t count, int symmetrize, int dedupe, int drop_self_loops, sg_host_csr* out);
+/* formats::CSR::invert (formats/csr.hpp:179-209). */
+sg_status sg_csr_invert(const sg_host_csr* in, sg_host_csr* out);
+/* io::csr::toBinary / fromBinary (io/read_csr.hpp:316-411): the "SYGRCSR"
+ * binary layout, including the legacy headerless one on read.  The file stores
+ * n+1 row offsets, m column indices and m values (4 bytes each). */
+sg_status sg_csr_write_binary(const sg_host_csr* csr, const char* path);
+sg_status sg_csr_read_binary(const char* path, int value_type, sg_host_csr* out);
+/* io::csr::fromMM (io/read_csr.hpp:88-192): coordinate Matrix Market,
+ * general or symmetric, pattern or real/integer. */
+sg_status sg_csr_read_mm(const char* path, int value_type, sg_host_csr* out);
+void sg_host_csr_free(sg_host_csr* csr);
+/* Uniform random sample of k vertices with degree > 0 (seeded, sorted by draw order). */
+sg_status sg_sample_sources(const sg_host_csr* csr, uint32_t k, uint64_t seed, uint32_t* out_sources);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYGRAPH_B200_H */

@@ -1,0 +1,190 @@
+"""Algorithm classes with the reference's interface (algorithms/*.hpp):
+``BFS(G).init(src); BFS.run(direction, alpha, beta) -> BFSRunDetails;
+getDistances()``, and the same shape for SSSP, CC, BC and TC.  Each run is
+one fused device-side traversal behind the C ABI."""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, lib
+from .core import WEIGHT_F32, Graph, _ptr
+
+
+class bfs_direction:  # noqa: N801 - algorithms::bfs_direction (bfs.hpp:29)
+    push = 0
+    pull = 1
+    hybrid = 2
+
+
+@dataclass
+class BFSRunDetails:
+    """algorithms::BFSRunDetails (bfs.hpp:31-35)."""
+    iterations: int = 0
+    push_steps: set = field(default_factory=set)
+    pull_steps: set = field(default_factory=set)
+    visited_vertices: int = 0
+    visited_edges: int = 0
+
+
+def _details(d: _lib.BfsDetails) -> BFSRunDetails:
+    out = BFSRunDetails(iterations=int(d.iterations), visited_vertices=int(d.visited_vertices),
+                        visited_edges=int(d.visited_edges))
+    for i in range(min(out.iterations, _lib.SG_MAX_LOGGED_LEVELS)):
+        (out.pull_steps if d.step_is_pull[i] else out.push_steps).add(i)
+    return out
+
+
+class BFS:
+    """algorithms::BFS (bfs.hpp:120-351)."""
+
+    def __init__(self, G: Graph):
+        self.G = G
+        h = C.c_void_p()
+        call("sg_bfs_create", G.handle, C.byref(h))
+        self.handle = h
+        self._init = False
+
+    def init(self, source: int) -> None:
+        call("sg_bfs_init", self.handle, int(source))
+        self._init = True
+
+    def reset(self) -> None:
+        call("sg_bfs_reset", self.handle)
+        self._init = False
+
+    def run(self, direction: int = bfs_direction.push, alpha: float = 1.0, beta: float = 1.0) -> BFSRunDetails:
+        d = _lib.BfsDetails()
+        call("sg_bfs_run", self.handle, direction, alpha, beta, C.byref(d))
+        return _details(d)
+
+    def run_async(self, direction: int = bfs_direction.push, alpha: float = 1.0, beta: float = 1.0) -> None:
+        call("sg_bfs_run_async", self.handle, direction, alpha, beta)
+
+    def getDistances(self) -> np.ndarray:
+        out = np.empty(self.G.getVertexCount(), np.uint32)
+        call("sg_bfs_get_distances", self.handle, _ptr(out))
+        return out
+
+    def getDistance(self, v: int) -> int:
+        return int(self.getDistances()[v])
+
+    def level_records(self) -> list[dict]:
+        recs = (_lib.LevelRecord * _lib.SG_MAX_LOGGED_LEVELS)()
+        cnt = C.c_uint32()
+        call("sg_bfs_level_records", self.handle, recs, _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
+        return [{k: getattr(recs[i], k) for k, _ in _lib.LevelRecord._fields_} for i in range(cnt.value)]
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib.sg_bfs_destroy(h)
+            self.handle = None
+
+
+class SSSP:
+    """algorithms::SSSP (sssp.hpp:109-217)."""
+
+    def __init__(self, G: Graph):
+        self.G = G
+        h = C.c_void_p()
+        call("sg_sssp_create", G.handle, C.byref(h))
+        self.handle = h
+        self.iterations = 0
+
+    def init(self, source: int) -> None:
+        call("sg_sssp_init", self.handle, int(source))
+
+    def run(self) -> int:
+        it = C.c_uint64()
+        call("sg_sssp_run", self.handle, C.byref(it))
+        self.iterations = it.value
+        return it.value
+
+    def run_async(self) -> None:
+        call("sg_sssp_run_async", self.handle)
+
+    def getDistances(self) -> np.ndarray:
+        dt = np.float32 if self.G.value_type == WEIGHT_F32 else np.uint32
+        out = np.empty(self.G.getVertexCount(), dt)
+        call("sg_sssp_get_distances", self.handle, C.c_void_p(out.ctypes.data))
+        return out
+
+    def getDistance(self, v: int):
+        return self.getDistances()[v]
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib.sg_sssp_destroy(h)
+            self.handle = None
+
+
+class CC:
+    """algorithms::CC (cc.hpp:74-192): labels[v] = max id over the vertices reaching v."""
+
+    def __init__(self, G: Graph):
+        self.G = G
+        self.labels = None
+        self.iterations = 0
+
+    def init(self, source: int = 0) -> None:
+        self.source = source
+
+    def run(self) -> None:
+        self.labels = np.empty(self.G.getVertexCount(), np.uint32)
+        it = C.c_uint64()
+        call("sg_cc", self.G.handle, _ptr(self.labels), C.byref(it))
+        self.iterations = it.value
+
+    def getLabels(self) -> np.ndarray:
+        return self.labels
+
+
+class BC:
+    """algorithms::BC (bc.hpp:274-419); init accepts one source or a list."""
+
+    def __init__(self, G: Graph):
+        self.G = G
+        self.sources = None
+        self.values = None
+
+    def init(self, source) -> None:
+        self.sources = np.atleast_1d(np.asarray(source, dtype=np.uint32))
+
+    def run(self) -> None:
+        self.values = np.empty(self.G.getVertexCount(), np.float32)
+        call("sg_bc", self.G.handle, _ptr(self.sources), self.sources.size, self.values.ctypes.data_as(
+            C.POINTER(C.c_float)))
+
+    def getBC(self) -> np.ndarray:
+        return self.values
+
+
+class TC:
+    """algorithms::TC (tc.hpp:473-565), exact."""
+
+    def __init__(self, G: Graph):
+        self.G = G
+        self.total = None
+        self.per_vertex = None
+
+    def init(self) -> None:
+        self.total = None
+
+    def run(self, per_vertex: bool = False) -> None:
+        tot = C.c_uint64()
+        pv = np.zeros(self.G.getVertexCount(), np.uint64) if per_vertex else None
+        call("sg_tc", self.G.handle, C.byref(tot), pv.ctypes.data_as(C.POINTER(C.c_uint64)) if pv is not None else None)
+        self.total = tot.value
+        self.per_vertex = pv
+
+    def getNumTriangles(self, v: int | None = None) -> int:
+        if v is None:
+            return int(self.total)
+        if self.per_vertex is None:
+            self.run(per_vertex=True)
+        return int(self.per_vertex[v])
