@@ -1,0 +1,411 @@
+"""Benchmark: direction-optimising BFS (and SSSP) GTEPS on RMAT scale 22.
+
+Workload (one step): a direction-optimising BFS (hybrid heuristic,
+alpha=15, beta=24) from each of 64 sources drawn uniformly among the vertices
+with degree > 0 (seed 3) on RMAT scale 22, edge factor 16,
+(a,b,c,d) = (0.57, 0.19, 0.19, 0.05), symmetrised, self-loops and
+duplicates removed, uint32 CSR, seed 1, float32 weights on (0,1] (seed 2).
+The graph is synthetic (no dataset) and resident in HBM before timing.
+
+value  = GTEPS = sum over the step's traversals of the edges incident to
+         reached vertices / device time (CUDA events), all ranks.
+e2e    = the same metric through the C ABI with host buffers: the source ids
+         are copied from pinned host memory and every depth array is read back
+         to pinned host memory inside the timed region.
+roofline: the BFS kernel against the measured HBM copy bandwidth, with
+         B = 4(n+1) + 4m + 4n algorithmic bytes per traversal.
+cpu_baseline: the oracle's OpenMP frontier BFS on the host cores, a bounded
+         sample of the same workload.
+
+Multi-GPU (torchrun): replicas; each rank holds the graph and runs its own 64
+sources (weak scaling); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SCALE, EDGE_FACTOR, A, B, C = 22, 16, 0.57, 0.19, 0.19
+GRAPH_SEED, WEIGHT_SEED, SOURCE_SEED = 1, 2, 3
+N_SOURCES = 64
+ALPHA, BETA = 15.0, 24.0
+METRIC = "BFS/SSSP GTEPS & %HBM roofline on RMAT-22; learned+batched vs plain speedup"
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(name: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get(name)
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """SM clocks and clock-event (throttle) reasons sampled every 20 ms during
+    the timed region, through NVML (read-only queries); nvidia-smi when NVML
+    is unavailable."""
+
+    # NVML clock-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []  # (sm_mhz, max_mhz, reason bits)
+        self._stop = threading.Event()
+        self._t = None
+        self._nvml = None
+
+    def _sample_nvml(self):
+        p = self._nvml
+        h = p.nvmlDeviceGetHandleByIndex(self.index)
+        mx = p.nvmlDeviceGetMaxClockInfo(h, p.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                sm = p.nvmlDeviceGetClockInfo(h, p.NVML_CLOCK_SM)
+                bits = p.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.rows.append((float(sm), float(mx), int(bits)))
+            except Exception:
+                pass
+            self._stop.wait(0.02)
+
+    def _sample_smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.sw_power_cap,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.hw_thermal_slowdown")
+        bitv = [0x4, 0x8, 0x20, 0x40]
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                f = [x.strip() for x in out.stdout.strip().split(",")]
+                bits = sum(b for b, s in zip(bitv, f[2:]) if s == "Active")
+                self.rows.append((float(f[0]), float(f[1]), bits))
+            except Exception:
+                pass
+            self._stop.wait(0.05)
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            target = self._sample_nvml
+        except Exception:
+            target = self._sample_smi
+        self._t = threading.Thread(target=target, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({name for r in self.rows for b, name in self.REASONS.items() if r[2] & b})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(r[1] for r in self.rows) if self.rows else None,
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml" if self._nvml else "nvidia-smi"}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_graph(sg):
+    t = time.time()
+    g = sg.io.rmat(SCALE, EDGE_FACTOR, A, B, C, seed=GRAPH_SEED, weight_seed=WEIGHT_SEED, perm_seed=0,
+                   value_type=sg.WEIGHT_F32)
+    return g, time.time() - t
+
+
+def run_reference(args, world, rank):
+    """CPU arm: the oracle's OpenMP restatement of BFS::run on the host cores."""
+    if rank != 0:
+        return
+    import sygraph_b200 as sg  # graph generator only (host code)
+    import oracle
+    g, _ = make_graph(sg)
+    srcs = sg.io.sample_sources(g, N_SOURCES, seed=SOURCE_SEED)
+    cores = os.cpu_count() or 1
+    per_step = 2  # bounded sample: two traversals per step
+    k = 0
+
+    def step():
+        nonlocal k
+        edges = 0
+        t = time.perf_counter()
+        for _ in range(per_step):
+            s = int(srcs[k % len(srcs)])
+            k += 1
+            d, _, _ = oracle.bfs_frontier(g, s, 2, ALPHA, BETA, nthreads=cores)
+            edges += oracle.visited_edges(g, d, g.n + 1)
+        return edges, time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        step()
+    tot_e, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        e, dt = step()
+        tot_e += e
+        tot_t += dt
+    val = tot_e / tot_t / 1e9
+    line = {"metric": METRIC, "value": val, "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_t / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "uint32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"DO-BFS RMAT-{SCALE} ef{EDGE_FACTOR}, {per_step} sources per step",
+                       "n": g.n, "m": g.m, "alpha": ALPHA, "beta": BETA},
+            "cpu_baseline": {"value": val, "unit": "GTEPS", "cores": cores, "kind": "port",
+                             "sample": f"{per_step} hybrid BFS traversals per step on RMAT-{SCALE}"},
+            "e2e": {"value": val, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference is SYCL and cannot be compiled here; the oracle's OpenMP restatement "
+                    "of its BFS::run is timed instead"}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(g, srcs, sg):
+    import oracle
+    cores = os.cpu_count() or 1
+    edges, t0 = 0, time.perf_counter()
+    used = 0
+    for s in srcs:
+        d, _, _ = oracle.bfs_frontier(g, int(s), 2, ALPHA, BETA, nthreads=cores)
+        edges += oracle.visited_edges(g, d, g.n + 1)
+        used += 1
+        if time.perf_counter() - t0 > 15.0:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": edges / dt / 1e9, "unit": "GTEPS", "cores": cores, "kind": "port",
+            "sample": f"{used} hybrid BFS traversals (alpha 15, beta 24) on RMAT-{SCALE}, OpenMP oracle"}
+
+
+def profile_case(kind: str) -> None:
+    """Two traversals on the bench graph from the first bench source, for ncu
+    captures: the second launch is the one to capture (-s 1 -c 1 on the
+    traversal kernel)."""
+    import sygraph_b200 as sg
+    g, _ = make_graph(sg)
+    src = int(sg.io.sample_sources(g, 1, seed=SOURCE_SEED)[0])
+    G = sg.graph.build.fromCSR(g)
+    if kind == "bfs":
+        a = sg.algorithms.BFS(G)
+        for _ in range(2):
+            a.init(src)
+            det = a.run(2, ALPHA, BETA)
+        print(json.dumps({"profile": "bfs", "source": src, "iterations": det.iterations,
+                          "levels": a.level_records()}))
+    else:
+        a = sg.algorithms.SSSP(G)
+        for _ in range(2):
+            a.init(src)
+            it = a.run()
+        print(json.dumps({"profile": "sssp", "source": src, "iterations": it}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sygraph_b200", choices=["sygraph_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sssp-sources", type=int, default=8)
+    ap.add_argument("--profile", choices=["bfs", "sssp"], default=None,
+                    help="profiling case: build the graph, run 2 traversals of one kind and exit (few launches)")
+    args = ap.parse_args()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    if args.profile:
+        profile_case(args.profile)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import sygraph_b200 as sg
+    sg._lib.call("sg_set_device", local)
+
+    g, gen_s = make_graph(sg)
+    from sygraph_b200 import replicas
+    srcs_all = sg.io.sample_sources(g, N_SOURCES * world, seed=SOURCE_SEED)
+    srcs = replicas.shard(srcs_all, rank, world, per_rank=N_SOURCES)
+    G = sg.graph.build.fromCSR(g)
+    bfs = sg.algorithms.BFS(G)
+    n, m = g.n, g.m
+    algo_bytes = 4 * (n + 1) + 4 * m + 4 * n
+
+    # reached-edge totals (GTEPS numerator) from one untimed pass
+    reached = {}
+    for s in srcs:
+        bfs.init(int(s))
+        det = bfs.run(2, ALPHA, BETA)
+        reached[int(s)] = det.visited_edges
+    step_edges = sum(reached.values())
+
+    def step():
+        for s in srcs:
+            bfs.init(int(s))
+            bfs.run_async(2, ALPHA, BETA)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    launches0 = sg.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        barrier()
+    launches = sg.launch_count() - launches0
+    t_ms = replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    ms_per_step = t_ms / args.steps
+    value = step_edges * world * args.steps / (t_ms * 1e-3) / 1e9
+
+    # per-launch duration of the BFS kernel (events around each launch)
+    durs = []
+    for s in srcs:
+        bfs.init(int(s))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        bfs.run_async(2, ALPHA, BETA)
+        b.record()
+        b.synchronize()
+        durs.append(a.elapsed_time(b))
+    kern_ms = float(np.mean(durs))
+    peak, peak_kind = peaks()
+    achieved = algo_bytes / (kern_ms * 1e-3) / 1e9
+    traffic = ncu_traffic("bfs_kernel")
+
+    # end to end through the C ABI: sources from pinned host memory, depths back to pinned host memory
+    import ctypes as C
+    hp_src = C.c_void_p()
+    sg._lib.call("sg_malloc_host_pinned", 4 * len(srcs), C.byref(hp_src))
+    hp_dst = C.c_void_p()
+    sg._lib.call("sg_malloc_host_pinned", 4 * n, C.byref(hp_dst))
+    dsrc = C.c_void_p()
+    sg._lib.call("sg_malloc_device", 4 * len(srcs), C.byref(dsrc))
+    np.ctypeslib.as_array(C.cast(hp_src, C.POINTER(C.c_uint32)), shape=(len(srcs),))[:] = srcs
+    host_src = np.ctypeslib.as_array(C.cast(hp_src, C.POINTER(C.c_uint32)), shape=(len(srcs),))
+    out_ptr = C.cast(hp_dst, C.POINTER(C.c_uint32))
+
+    def e2e_step():
+        sg._lib.call("sg_memcpy", dsrc, hp_src, 4 * len(srcs), 0, None)
+        for i in range(len(srcs)):
+            sg._lib.call("sg_bfs_init", bfs.handle, int(host_src[i]))
+            sg._lib.call("sg_bfs_run_async", bfs.handle, 2, ALPHA, BETA)
+            sg._lib.call("sg_bfs_get_distances", bfs.handle, out_ptr)
+
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    e_steps = max(2, args.steps // 2)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(e_steps):
+        e2e_step()
+    b.record()
+    barrier()
+    e2e_ms = replicas.max_over_ranks(a.elapsed_time(b), device="cuda")
+    e2e_val = step_edges * world * e_steps / (e2e_ms * 1e-3) / 1e9
+    sg._lib.call("sg_free_host_pinned", hp_src)
+    sg._lib.call("sg_free_host_pinned", hp_dst)
+    sg._lib.call("sg_free_device", dsrc)
+
+    # SSSP on a subset of the same sources (reported beside the BFS line)
+    sssp = sg.algorithms.SSSP(G)
+    ss_edges, ss_ms = 0, 0.0
+    sssp_bytes = 4 * (n + 1) + 8 * m + 4 * n
+    k_ss = min(args.sssp_sources, len(srcs))
+    for s in srcs[:k_ss]:
+        sssp.init(int(s))
+        sssp.run_async()
+    torch.cuda.synchronize()
+    for s in srcs[:k_ss]:
+        sssp.init(int(s))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        sssp.run_async()
+        b.record()
+        b.synchronize()
+        ss_ms += a.elapsed_time(b)
+        ss_edges += reached[int(s)]
+    sssp_gteps = ss_edges / (ss_ms * 1e-3) / 1e9
+    sssp_kern = ss_ms / k_ss
+    sssp_achieved = sssp_bytes / (sssp_kern * 1e-3) / 1e9
+
+    if rank == 0:
+        base = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(g, srcs[:8], sg)
+        line = {
+            "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "uint32", "data": "synthetic",
+            "config": {"workload": f"DO-BFS (hybrid, alpha {ALPHA:g}, beta {BETA:g}) from {N_SOURCES} random "
+                                   f"sources per GPU, RMAT-{SCALE} ef{EDGE_FACTOR} (0.57,0.19,0.19,0.05) seed 1",
+                       "n": n, "m": m, "sources_per_step": N_SOURCES, "source_seed": SOURCE_SEED,
+                       "graph_bytes": G.memory_bytes(), "l2": "inputs larger than L2 (CSR %.2f GB > 126 MB)"
+                                                             % ((4 * (n + 1) + 8 * m) / 1e9),
+                       "generate_s": round(gen_s, 2)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "bfs_kernel", "bytes_per_launch": algo_bytes, "launch_ms": kern_ms},
+            "e2e": {"value": e2e_val, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
+                    "d2h_bytes_per_step": 4 * n * len(srcs), "ms_per_step": e2e_ms / e_steps},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": base,
+            "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
+                     "roofline": {"bound": "hbm", "achieved": sssp_achieved, "peak": peak, "unit": "GB/s",
+                                  "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,
+                                  "traffic": ncu_traffic("sssp_kernel")}},
+        }
+        print(json.dumps(line), flush=True)
+    del bfs, sssp, G
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

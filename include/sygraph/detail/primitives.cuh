@@ -183,7 +183,9 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
           ok = 0;
           break;
         }
-        __nanosleep(64);
+        // poll back-to-back first (a barrier normally completes within a few
+        // microseconds), then back off
+        if (spins > 512) __nanosleep(spins > 4096 ? 256 : 32);
       }
     }
     __threadfence();

@@ -300,6 +300,27 @@ sg_status sg_bfs_level_records(sg_bfs b, sg_level_record* host_records, uint32_t
 sg_status sg_run_bfs(sg_graph g, uint32_t source, int direction, float alpha, float beta, uint32_t* host_depth,
                  sg_bfs_details* details);
 
+/* Batched multi-source BFS: up to 64 BFS::run traversals of one graph
+ * (algorithms/bfs.hpp:153-238) in one persistent kernel, bit-parallel (one
+ * 64-bit frontier / seen word per vertex).  Per source the depths equal the
+ * single-source ones.  Depths are a source-major k x n uint32 array
+ * (n+1 = unreached). */
+typedef struct sg_msbfs_s* sg_msbfs;
+typedef struct {
+  uint64_t iterations;
+  uint64_t push_steps;
+  uint64_t pull_steps;
+  uint64_t reached_edges; /* sum over sources of the degrees of reached vertices */
+} sg_msbfs_details;
+sg_status sg_msbfs_create(sg_graph g, uint32_t max_sources, sg_msbfs* out);
+sg_status sg_msbfs_destroy(sg_msbfs h);
+sg_status sg_msbfs_run(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int direction, float alpha, float beta,
+                       sg_msbfs_details* details);
+sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int direction, float alpha,
+                             float beta);
+sg_status sg_msbfs_get_depths(sg_msbfs h, uint32_t* host_depth);
+sg_status sg_msbfs_depths_device(sg_msbfs h, const uint32_t** dev_depth);
+
 /* SSSP(G) + init + run + getDistance (algorithms/sssp.hpp:109-217): frontier
  * Bellman-Ford with atomicMin, fused.  Distances have the graph's weight type
  * (float32 or uint32); unreached = (weight_t)(n+1) (sssp.hpp:43). */

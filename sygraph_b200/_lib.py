@@ -55,6 +55,11 @@ class LevelRecord(C.Structure):
                 ("unexplored_degree", C.c_uint64), ("t_start_ns", C.c_uint64), ("t_end_ns", C.c_uint64)]
 
 
+class MsbfsDetails(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("push_steps", C.c_uint64), ("pull_steps", C.c_uint64),
+                ("reached_edges", C.c_uint64)]
+
+
 class HostCSR(C.Structure):
     _fields_ = [("n", C.c_uint32), ("m", C.c_uint64), ("row_offsets", u32p), ("column_indices", u32p),
                 ("values", vp), ("value_type", C.c_int), ("flags", C.c_uint32)]
@@ -130,6 +135,12 @@ SIGNATURES = {
     "sg_bfs_distances_device": (st, [vp, C.POINTER(u32p)]),
     "sg_bfs_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
     "sg_run_bfs": (st, [vp, C.c_uint32, C.c_int, C.c_float, C.c_float, u32p, C.POINTER(BfsDetails)]),
+    "sg_msbfs_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
+    "sg_msbfs_destroy": (st, [vp]),
+    "sg_msbfs_run": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float, C.POINTER(MsbfsDetails)]),
+    "sg_msbfs_run_async": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float]),
+    "sg_msbfs_get_depths": (st, [vp, u32p]),
+    "sg_msbfs_depths_device": (st, [vp, C.POINTER(u32p)]),
     "sg_sssp_create": (st, [vp, C.POINTER(vp)]),
     "sg_sssp_destroy": (st, [vp]),
     "sg_sssp_init": (st, [vp, C.c_uint32]),

@@ -85,6 +85,45 @@ class BFS:
             self.handle = None
 
 
+class MultiBFS:
+    """Batched BFS from up to 64 sources in one launch (bit-parallel); depths
+    per source equal BFS(G).run from that source."""
+
+    def __init__(self, G: Graph, max_sources: int = 64):
+        self.G = G
+        h = C.c_void_p()
+        call("sg_msbfs_create", G.handle, max_sources, C.byref(h))
+        self.handle = h
+        self.k = 0
+        self.details = None
+
+    def run(self, sources, direction: int = bfs_direction.hybrid, alpha: float = 15.0, beta: float = 24.0):
+        src = np.ascontiguousarray(sources, np.uint32)
+        d = _lib.MsbfsDetails()
+        call("sg_msbfs_run", self.handle, _ptr(src), src.size, direction, alpha, beta, C.byref(d))
+        self.k = src.size
+        self.details = {k: int(getattr(d, k)) for k, _ in _lib.MsbfsDetails._fields_}
+        return self.details
+
+    def run_async(self, sources, direction: int = bfs_direction.hybrid, alpha: float = 15.0,
+                  beta: float = 24.0) -> None:
+        src = np.ascontiguousarray(sources, np.uint32)
+        call("sg_msbfs_run_async", self.handle, _ptr(src), src.size, direction, alpha, beta)
+        self.k = src.size
+
+    def getDistances(self) -> np.ndarray:
+        """k x n depths (row s: depths from sources[s])."""
+        out = np.empty((self.k, self.G.getVertexCount()), np.uint32)
+        call("sg_msbfs_get_depths", self.handle, _ptr(out))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib.sg_msbfs_destroy(h)
+            self.handle = None
+
+
 class SSSP:
     """algorithms::SSSP (sssp.hpp:109-217)."""
 

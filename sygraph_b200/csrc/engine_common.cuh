@@ -180,6 +180,21 @@ __device__ __forceinline__ void push_expand(const uint32_t* __restrict__ ro, con
   }
 }
 
+// Position of the k-th (0-based) set bit of x.
+__device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t s = 16; s > 0; s >>= 1) {
+    const uint32_t low = __popc(x & ((1u << s) - 1u));
+    if (k >= low) {
+      k -= low;
+      x >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
 __device__ __forceinline__ uint32_t valid_bits(uint32_t wi, uint32_t w0, uint32_t n) {
   const uint32_t rem = n & 31u;
   return (wi == w0 - 1 && rem) ? ((1u << rem) - 1u) : 0xffffffffu;

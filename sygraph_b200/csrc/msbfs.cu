@@ -1,0 +1,629 @@
+// Batched multi-source BFS: up to 64 traversals of the same graph in one
+// persistent cooperative kernel, bit-parallel (one uint64 word per vertex:
+// bit s = source s).  Each traversal computes exactly the depths of
+// BFS::run from its source (algorithms/bfs.hpp:153-238; depths are unique, so
+// the result per source equals the single-source engine's).
+//
+// State: seen[v] (sources that reached v), frontier masks F[v] in three
+// rotating buffers with an activity bitmap + summary for enumeration, and a
+// "done" bitmap of vertices every source has reached.  Per level:
+//   push: for every active v and edge (v,u): new = F[v] & ~seen[u];
+//         atomicOr on seen[u] claims the bits, atomicOr on F'[u] publishes them
+//   pull: for every u not done: OR the frontier masks of its in-neighbours,
+//         stopping once every missing source is covered; u owns seen[u]
+// Depths land in a source-major k x n array: pull writes for one source are
+// coalesced across the warp's 32 consecutive vertices.  Entries never
+// reached are filled with n+1 at the end.  One grid barrier per level.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "engine_common.cuh"
+
+namespace sgb {
+namespace ms {
+
+using namespace eng;
+
+constexpr uint32_t kHeavy = 256;
+constexpr uint32_t kHeavyBuf = 1024;
+using u64 = unsigned long long;
+
+struct LevelCounters {
+  u64 heavy_packed;
+  u64 new_count;     // vertices that became active
+  u64 new_deg;       // their degree sum
+  u64 reached_edges; // sum over (source, newly reached vertex) of the vertex degree
+  u64 done_deg;      // degree of vertices every source reached at this level
+  u64 pad[3];
+};
+
+struct Params {
+  uint32_t n, w0, w1, k;
+  uint64_t m;
+  const uint32_t* ro;
+  const uint32_t* col;
+  const uint32_t* iro;
+  const uint32_t* icol;
+  const uint32_t* sources;
+  int mode;
+  float alpha, beta;
+  u64 all;
+  u64* seen;
+  u64* F;            // 3 * n
+  uint32_t* fa;      // 3 * w0 activity bitmaps
+  uint32_t* sm;      // 3 * w1 summaries
+  uint32_t* done;    // w0
+  const uint32_t* no_in_edges;
+  uint32_t* heavy_v; // 2 * heavy_cap
+  uint32_t* heavy_s;
+  uint32_t heavy_cap;
+  LevelCounters* cnt;
+  GridBarrier* bar;
+  uint32_t* depth;   // k * n, source-major
+  sg_level_record* log;
+  u64* result;       // [iterations, push, pull, reached_edges]
+};
+
+struct Shared {
+  uint32_t scan[32];
+  u64 red[32];
+  uint32_t hv[kHeavyBuf];
+  uint32_t hd[kHeavyBuf];
+  uint32_t hn;
+  uint32_t base_e, base_c;
+};
+
+struct Level {
+  const Params* P;
+  Shared* S;
+  LevelCounters* C;
+  u64* F_next;
+  uint32_t* fa_next;
+  uint32_t* sm_next;
+  uint32_t* hv_next;
+  uint32_t* hs_next;
+  uint32_t next_depth;
+  uint32_t n_new = 0;
+  u64 deg_new = 0, reached = 0, done_deg = 0;
+
+  __device__ __forceinline__ void add_heavy(uint32_t u, uint32_t du) {
+    const uint32_t i = atomicAdd(&S->hn, 1u);
+    if (i < kHeavyBuf) {
+      S->hv[i] = u;
+      S->hd[i] = du;
+    } else {
+      const u64 old = atomicAdd(&C->heavy_packed, (1ull << 32) | chunks_of(du));
+      hv_next[old >> 32] = u;
+      hs_next[old >> 32] = (uint32_t)old;
+    }
+  }
+  // push: relax edge (v -> u) carrying frontier mask fv
+  __device__ __forceinline__ void visit_push(uint32_t u, u64 fv) {
+    const u64 su = ld_cg(P->seen + u);
+    const u64 nb = fv & ~su;
+    if (!nb) return;
+    const u64 old = atomicOr(P->seen + u, nb);
+    const u64 nw = nb & ~old;
+    if (!nw) return;
+    const uint32_t du = P->ro[u + 1] - P->ro[u];
+    reached += (u64)__popcll(nw) * du;
+    if ((old | nw) == P->all) {
+      done_deg += du;
+      atomicOr(P->done + (u >> 5), 1u << (u & 31));
+    }
+    for (u64 x = nw; x; x &= x - 1) st_cg(P->depth + (size_t)(__ffsll(x) - 1) * P->n + u, next_depth);
+    if (atomicOr(F_next + u, nw) == 0) {
+      const uint32_t b = 1u << (u & 31);
+      if (atomicOr(fa_next + (u >> 5), b) == 0) atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31));
+      n_new++;
+      deg_new += du;
+      if (du >= kHeavy) add_heavy(u, du);
+    }
+  }
+};
+
+__device__ __forceinline__ u64 shfl64(u64 x, uint32_t src) {
+  const uint32_t lo = __shfl_sync(kFullMask, (uint32_t)x, src);
+  const uint32_t hi = __shfl_sync(kFullMask, (uint32_t)(x >> 32), src);
+  return ((u64)hi << 32) | lo;
+}
+
+__device__ __forceinline__ void expand_group(Level& L, uint32_t beg, uint32_t deg, u64 fv) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t incl = warp_inclusive_scan(deg);
+  const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+  const uint32_t excl = incl - deg;
+  for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+    const uint32_t r = r0 + lane;
+    const bool act = r < total;
+    const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+    const uint32_t ob = __shfl_sync(kFullMask, beg, o);
+    const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+    const u64 of = shfl64(fv, o);
+    if (act) L.visit_push(L.P->col[ob + (r - oe)], of);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
+  __shared__ Shared S;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
+  const uint32_t n = P.n, w0 = P.w0, w1 = P.w1;
+
+  // ---- clear state
+  for (uint32_t i = gtid; i < n; i += nthreads) {
+    st_cg(P.seen + i, 0ull);
+    st_cg(P.F + i, 0ull);
+    st_cg(P.F + n + i, 0ull);
+    st_cg(P.F + 2 * (size_t)n + i, 0ull);
+  }
+  for (uint32_t i = gtid; i < w0; i += nthreads) {
+    st_cg(P.fa + i, 0u);
+    st_cg(P.fa + w0 + i, 0u);
+    st_cg(P.fa + 2 * w0 + i, 0u);
+    st_cg(P.done + i, P.no_in_edges[i]);
+  }
+  for (uint32_t i = gtid; i < 3 * w1; i += nthreads) st_cg(P.sm + i, 0u);
+  if (gtid < 3) {
+    LevelCounters z = {};
+    P.cnt[gtid] = z;
+  }
+  if (threadIdx.x == 0) S.hn = 0;
+  if (!grid_sync(P.bar)) return;
+  // ---- sources: F_0, seen, depth 0, and the level-0 heavy list
+  if (gtid == 0) {
+    u64 cnt = 0, deg = 0;
+    uint32_t hn = 0, hc = 0;
+    for (uint32_t i = 0; i < P.k; i++) {
+      const uint32_t s = P.sources[i];
+      const u64 bit = 1ull << i;
+      const u64 before = P.F[s];
+      P.seen[s] |= bit;
+      P.F[s] = before | bit;
+      P.depth[(size_t)i * n + s] = 0;
+      if (before == 0) {
+        const uint32_t d = P.ro[s + 1] - P.ro[s];
+        cnt++;
+        deg += d;
+        P.fa[s >> 5] |= 1u << (s & 31);
+        P.sm[s >> 10] |= 1u << ((s >> 5) & 31);
+        if (d >= kHeavy) {
+          P.heavy_v[hn] = s;
+          P.heavy_s[hn] = hc;
+          hn++;
+          hc += chunks_of(d);
+        }
+      }
+    }
+    LevelCounters c0 = {};
+    c0.heavy_packed = ((u64)hn << 32) | hc;
+    c0.new_count = cnt;
+    c0.new_deg = deg;
+    P.cnt[2] = c0;
+    __threadfence();
+  }
+  if (!grid_sync(P.bar)) return;
+
+  u64 unexplored = P.m;
+  u64 frontier_size = ld_cg(&P.cnt[2].new_count), frontier_deg = ld_cg(&P.cnt[2].new_deg);
+  u64 reached_total = 0;
+  for (uint32_t i = 0; i < P.k; i++) {
+    const uint32_t s = P.sources[i];
+    reached_total += P.ro[s + 1] - P.ro[s];
+  }
+  u64 n_push = 0, n_pull = 0;
+  int pull = P.mode == SG_BFS_PULL;
+  uint32_t level = 0;
+  for (;; level++) {
+    LevelCounters* C = P.cnt + (level % 3);
+    const LevelCounters* Cprev = P.cnt + ((level + 2) % 3);
+    const size_t cur = level % 3, nxt = (level + 1) % 3, zro = (level + 2) % 3;
+    u64* F_cur = P.F + cur * n;
+    u64* F_zero = P.F + zro * n;
+    uint32_t* fa_cur = P.fa + cur * w0;
+    uint32_t* fa_zero = P.fa + zro * w0;
+    uint32_t* sm_cur = P.sm + cur * w1;
+    uint32_t* sm_zero = P.sm + zro * w1;
+    const uint32_t par = level & 1;
+    if (gtid == 0) {
+      LevelCounters z = {};
+      P.cnt[nxt] = z;
+    }
+    const uint64_t t0 = gtid == 0 ? sygraph::detail::global_timer_ns() : 0;
+    Level L{&P, &S, C, P.F + nxt * n, P.fa + nxt * w0, P.sm + nxt * w1,
+            P.heavy_v + (size_t)(par ^ 1) * P.heavy_cap, P.heavy_s + (size_t)(par ^ 1) * P.heavy_cap, level + 1};
+    if (!pull) {
+      n_push++;
+      const u64 hp = ld_cg(&Cprev->heavy_packed);
+      const uint32_t n_heavy = (uint32_t)(hp >> 32), n_chunks = (uint32_t)hp;
+      const uint32_t* hv_cur = P.heavy_v + (size_t)par * P.heavy_cap;
+      const uint32_t* hs_cur = P.heavy_s + (size_t)par * P.heavy_cap;
+      const uint32_t units = w1 + n_chunks;
+      for (uint32_t unit = gwarp; unit < units; unit += nwarps) {
+        if (unit < w1) {
+          const uint32_t s = ld_cg(sm_cur + unit);
+          if (!s) continue;
+          const uint32_t bits = ((s >> lane) & 1u) ? ld_cg(fa_cur + unit * 32 + lane) : 0u;
+          const uint32_t c = __popc(bits);
+          const uint32_t incl = warp_inclusive_scan(c);
+          const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+          const uint32_t excl = incl - c;
+          for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+            const uint32_t r = r0 + lane;
+            const bool act = r < total;
+            const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+            const uint32_t ob = __shfl_sync(kFullMask, bits, o);
+            const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+            uint32_t beg = 0, deg = 0;
+            u64 fv = 0;
+            if (act) {
+              const uint32_t v = (unit * 32 + o) * 32 + select_bit(ob, r - oe);
+              beg = P.ro[v];
+              deg = P.ro[v + 1] - beg;
+              fv = ld_cg(F_cur + v);
+              if (deg >= kHeavy) deg = 0;
+            }
+            expand_group(L, beg, deg, fv);
+          }
+        } else {
+          const uint32_t c = unit - w1;
+          const uint32_t ent = find_chunk_owner(hs_cur, n_heavy, c);
+          const uint32_t v = ld_cg(hv_cur + ent);
+          const uint32_t first = ld_cg(hs_cur + ent);
+          const uint32_t cb = P.ro[v] + (c - first) * kChunk;
+          const uint32_t ce = min(P.ro[v + 1], cb + kChunk);
+          const u64 fv = ld_cg(F_cur + v);
+          for (uint32_t eb = cb; eb < ce; eb += 32) {
+            const uint32_t e = eb + lane;
+            if (e < ce) L.visit_push(P.col[e], fv);
+          }
+        }
+      }
+    } else {
+      n_pull++;
+      const bool same = P.iro == P.ro;
+      for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+        const uint32_t dw = ld_cg(P.done + wi);
+        const uint32_t cand = ~dw & valid_bits(wi, w0, n);
+        if (!cand) continue;
+        const uint32_t u = wi * 32 + lane;
+        const bool mine = (cand >> lane) & 1u;
+        const u64 su = mine ? ld_cg(P.seen + u) : P.all;
+        const uint32_t beg = mine ? P.iro[u] : 0u;
+        const uint32_t end = mine ? P.iro[u + 1] : 0u;
+        u64 acc = 0;
+        uint32_t e = beg;
+        const uint32_t lim = min(end, beg + kPullSerial);
+        while (e < lim && (acc | su) != P.all) {
+          const uint32_t c0 = P.icol[e];
+          const uint32_t c1 = e + 1 < lim ? P.icol[e + 1] : c0;
+          acc |= ld_cg(F_cur + c0) | ld_cg(F_cur + c1);
+          e += 2;
+        }
+        if (e > lim) e = lim;
+        uint32_t left = __ballot_sync(kFullMask, mine && (acc | su) != P.all && e < end);
+        while (left) {
+          const uint32_t j = __ffs(left) - 1;
+          left &= left - 1;
+          const uint32_t jb = __shfl_sync(kFullMask, e, j);
+          const uint32_t je = __shfl_sync(kFullMask, end, j);
+          const u64 sj = shfl64(su | acc, j);
+          u64 part = 0;
+          for (uint32_t eb = jb; eb < je; eb += 32) {
+            const uint32_t ee = eb + lane;
+            if (ee < je) part |= ld_cg(F_cur + P.icol[ee]);
+            // warp OR-reduce, stop once everything missing is covered
+            u64 r = part;
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) r |= ((u64)__shfl_xor_sync(kFullMask, (uint32_t)(r >> 32), d) << 32) |
+                                                   __shfl_xor_sync(kFullMask, (uint32_t)r, d);
+            part = r;
+            if ((part | sj) == P.all) break;
+          }
+          if (lane == j) acc |= part;
+        }
+        const u64 nw = acc & ~su;
+        const bool got = mine && nw != 0;
+        const uint32_t du = got ? (same ? end - beg : P.ro[u + 1] - P.ro[u]) : 0u;
+        if (got) {
+          st_cg(P.seen + u, su | nw);
+          st_cg(L.F_next + u, nw);
+          L.n_new++;
+          L.deg_new += du;
+          L.reached += (u64)__popcll(nw) * du;
+          if ((su | nw) == P.all) L.done_deg += du;
+          if (du >= kHeavy) L.add_heavy(u, du);
+        }
+        // depth of each newly reached (source, vertex): one coalesced row per source
+        u64 any = got ? nw : 0ull;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) any |= ((u64)__shfl_xor_sync(kFullMask, (uint32_t)(any >> 32), d) << 32) |
+                                                __shfl_xor_sync(kFullMask, (uint32_t)any, d);
+        for (u64 x = any; x; x &= x - 1) {
+          const uint32_t s = __ffsll(x) - 1;
+          if (got && ((nw >> s) & 1ull)) st_cg(P.depth + (size_t)s * n + u, level + 1);
+        }
+        const uint32_t gmask = __ballot_sync(kFullMask, got);
+        const uint32_t dmask = __ballot_sync(kFullMask, mine && (su | nw) == P.all);
+        if (lane == 0) {
+          if (gmask) {
+            st_cg(L.fa_next + wi, gmask);
+            atomicOr(L.sm_next + (wi >> 5), 1u << (wi & 31));
+          }
+          if (dmask) st_cg(P.done + wi, dw | dmask);
+        }
+      }
+    }
+    // clear F_{L-1}
+    for (uint32_t j = gwarp; j < w1; j += nwarps) {
+      const uint32_t s = ld_cg(sm_zero + j);
+      if (!s) continue;
+      const uint32_t w = j * 32 + lane;
+      const uint32_t bits = ((s >> lane) & 1u) ? ld_cg(fa_zero + w) : 0u;
+      for (uint32_t b = bits; b; b &= b - 1) st_cg(F_zero + w * 32 + (__ffs(b) - 1), 0ull);
+      if ((s >> lane) & 1u) st_cg(fa_zero + w, 0u);
+      __syncwarp();
+      if (lane == 0) st_cg(sm_zero + j, 0u);
+    }
+    __syncthreads();
+    {
+      const uint32_t nb = min(S.hn, kHeavyBuf);
+      const uint32_t k0 = 2 * threadIdx.x;
+      uint32_t my = 0;
+      if (k0 < nb) my += chunks_of(S.hd[k0]);
+      if (k0 + 1 < nb) my += chunks_of(S.hd[k0 + 1]);
+      uint32_t total;
+      const uint32_t ex = sygraph::detail::block_excl_scan(my, &total, S.scan);
+      if (threadIdx.x == 0 && nb) {
+        const u64 old = atomicAdd(&C->heavy_packed, ((u64)nb << 32) | total);
+        S.base_e = (uint32_t)(old >> 32);
+        S.base_c = (uint32_t)old;
+      }
+      __syncthreads();
+      if (nb) {
+        uint32_t pc = S.base_c + ex;
+        for (uint32_t k = k0; k < k0 + 2 && k < nb; k++) {
+          L.hv_next[S.base_e + k] = S.hv[k];
+          L.hs_next[S.base_e + k] = pc;
+          pc += chunks_of(S.hd[k]);
+        }
+      }
+      if (threadIdx.x == 0) S.hn = 0;
+    }
+    {
+      const u64 c = block_sum<u64>(L.n_new, S.red);
+      const u64 d = block_sum<u64>(L.deg_new, S.red);
+      const u64 r = block_sum<u64>(L.reached, S.red);
+      const u64 dd = block_sum<u64>(L.done_deg, S.red);
+      if (threadIdx.x == 0) {
+        if (c) atomicAdd(&C->new_count, c);
+        if (d) atomicAdd(&C->new_deg, d);
+        if (r) atomicAdd(&C->reached_edges, r);
+        if (dd) atomicAdd(&C->done_deg, dd);
+      }
+    }
+    if (!grid_sync(P.bar)) return;
+    const u64 next_size = ld_cg(&C->new_count);
+    const u64 next_deg = ld_cg(&C->new_deg);
+    reached_total += ld_cg(&C->reached_edges);
+    unexplored -= ld_cg(&C->done_deg);
+    if (gtid == 0 && level < kMaxLog) {
+      sg_level_record rr;
+      rr.level = level;
+      rr.strategy = pull ? 2u : 0u;
+      rr.frontier_size = (uint32_t)frontier_size;
+      rr.next_size = (uint32_t)next_size;
+      rr.frontier_degree = frontier_deg;
+      rr.next_degree = next_deg;
+      rr.unexplored_degree = unexplored;
+      rr.t_start_ns = t0;
+      rr.t_end_ns = sygraph::detail::global_timer_ns();
+      P.log[level] = rr;
+    }
+    if (P.mode == SG_BFS_HYBRID) {
+      if (!pull) {
+        if ((float)next_deg > (float)unexplored / P.alpha) pull = 1;
+      } else {
+        if ((float)next_size < (float)n / P.beta) pull = 0;
+      }
+    }
+    frontier_size = next_size;
+    frontier_deg = next_deg;
+    if (next_size == 0) break;
+  }
+  // entries never reached: n+1 (one coalesced row store per source and warp)
+  for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+    const uint32_t u = wi * 32 + lane;
+    const bool in = u < n;
+    const u64 miss = in ? (P.all & ~ld_cg(P.seen + u)) : 0ull;
+    u64 any = miss;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) any |= ((u64)__shfl_xor_sync(kFullMask, (uint32_t)(any >> 32), d) << 32) |
+                                            __shfl_xor_sync(kFullMask, (uint32_t)any, d);
+    for (u64 x = any; x; x &= x - 1) {
+      const uint32_t s = __ffsll(x) - 1;
+      if ((miss >> s) & 1ull) st_cg(P.depth + (size_t)s * n + u, n + 1);
+    }
+  }
+  if (gtid == 0) {
+    P.result[0] = level + 1;
+    P.result[1] = n_push;
+    P.result[2] = n_pull;
+    P.result[3] = reached_total;
+  }
+}
+
+__global__ void no_in_edges_kernel(const uint32_t* __restrict__ iro, uint32_t n, uint32_t w0, uint32_t* out) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < (uint64_t)w0 * 32;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t v = base + lane;
+    const bool z = v < n && iro[v + 1] == iro[v];
+    const uint32_t msk = __ballot_sync(kFullMask, z);
+    if (lane == 0) out[base >> 5] = msk;
+  }
+}
+
+}  // namespace ms
+}  // namespace sgb
+
+using namespace sgb;
+
+struct sg_msbfs_s {
+  sg_graph g = nullptr;
+  uint32_t k = 0, w0 = 0, w1 = 0, heavy_cap = 0;
+  unsigned long long* seen = nullptr;
+  unsigned long long* F = nullptr;
+  uint32_t *fa = nullptr, *sm = nullptr, *done = nullptr, *no_in = nullptr;
+  uint32_t *heavy_v = nullptr, *heavy_s = nullptr;
+  uint32_t* sources = nullptr;
+  uint32_t* depth = nullptr;
+  ms::LevelCounters* cnt = nullptr;
+  sygraph::detail::GridBarrier* bar = nullptr;
+  sg_level_record* log = nullptr;
+  unsigned long long* result = nullptr;
+  uint32_t last_k = 0;
+};
+
+static void msbfs_release(sg_msbfs h) {
+  if (!h) return;
+  dev_free(h->seen);
+  dev_free(h->F);
+  dev_free(h->fa);
+  dev_free(h->sm);
+  dev_free(h->done);
+  dev_free(h->no_in);
+  dev_free(h->heavy_v);
+  dev_free(h->heavy_s);
+  dev_free(h->sources);
+  dev_free(h->depth);
+  dev_free(h->cnt);
+  dev_free(h->bar);
+  dev_free(h->log);
+  dev_free(h->result);
+  delete h;
+}
+
+extern "C" {
+
+sg_status sg_msbfs_create(sg_graph g, uint32_t max_sources, sg_msbfs* out) {
+  clear_error();
+  SG_REQUIRE(g && out, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(max_sources >= 1 && max_sources <= 64, SG_ERR_INVALID, "a batch holds 1 to 64 sources");
+  SG_REQUIRE(g->n > 0, SG_ERR_INVALID, "graph has no vertices");
+  *out = nullptr;
+  sg_msbfs h = new sg_msbfs_s();
+  h->g = g;
+  h->k = max_sources;
+  h->w0 = div_up(g->n, 32);
+  h->w1 = div_up(h->w0, 32);
+  h->heavy_cap = (uint32_t)std::min<uint64_t>(g->n, g->m / ms::kHeavy + 1);
+  const uint64_t n = g->n;
+  sg_status s;
+  if ((s = dev_alloc(&h->seen, n)) || (s = dev_alloc(&h->F, 3 * n)) || (s = dev_alloc(&h->fa, 3ull * h->w0)) ||
+      (s = dev_alloc(&h->sm, 3ull * h->w1)) || (s = dev_alloc(&h->done, h->w0)) || (s = dev_alloc(&h->no_in, h->w0)) ||
+      (s = dev_alloc(&h->heavy_v, 2ull * h->heavy_cap)) || (s = dev_alloc(&h->heavy_s, 2ull * h->heavy_cap)) ||
+      (s = dev_alloc(&h->sources, 64)) || (s = dev_alloc(&h->depth, (uint64_t)max_sources * n)) ||
+      (s = dev_alloc(&h->cnt, 3)) || (s = dev_alloc(&h->bar, 1)) || (s = dev_alloc(&h->log, SG_MAX_LOGGED_LEVELS)) ||
+      (s = dev_alloc(&h->result, 8))) {
+    msbfs_release(h);
+    return s;
+  }
+  ms::no_in_edges_kernel<<<grid_for((uint64_t)h->w0 * 32, 256), 256, 0, g->stream>>>(g->inv.ro, g->n, h->w0, h->no_in);
+  if (cudaGetLastError() != cudaSuccess) {
+    msbfs_release(h);
+    return fail(SG_ERR_CUDA, "multi-source BFS set-up kernel failed to launch");
+  }
+  count_launch();
+  *out = h;
+  return SG_OK;
+}
+
+sg_status sg_msbfs_destroy(sg_msbfs h) {
+  if (h) {
+    cudaStreamSynchronize(h->g->stream);
+    msbfs_release(h);
+  }
+  return SG_OK;
+}
+
+sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int direction, float alpha,
+                             float beta) {
+  clear_error();
+  SG_REQUIRE(h && host_sources, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(k >= 1 && k <= h->k, SG_ERR_INVALID, "source count exceeds the batch capacity");
+  SG_REQUIRE(direction >= SG_BFS_PUSH && direction <= SG_BFS_HYBRID, SG_ERR_INVALID, "unknown BFS direction");
+  for (uint32_t i = 0; i < k; i++) SG_REQUIRE(host_sources[i] < h->g->n, SG_ERR_INVALID, "source out of range");
+  sg_graph g = h->g;
+  SG_CUDA(cudaMemcpyAsync(h->sources, host_sources, sizeof(uint32_t) * k, cudaMemcpyHostToDevice, g->stream));
+  SG_CUDA(cudaMemsetAsync(h->bar, 0, sizeof(*h->bar), g->stream));
+  ms::Params P;
+  P.n = g->n;
+  P.w0 = h->w0;
+  P.w1 = h->w1;
+  P.k = k;
+  P.m = g->m;
+  P.ro = g->fwd.ro;
+  P.col = g->fwd.col;
+  P.iro = g->inv.ro;
+  P.icol = g->inv.col;
+  P.sources = h->sources;
+  P.mode = direction;
+  P.alpha = alpha;
+  P.beta = beta;
+  P.all = k == 64 ? ~0ull : ((1ull << k) - 1ull);
+  P.seen = h->seen;
+  P.F = h->F;
+  P.fa = h->fa;
+  P.sm = h->sm;
+  P.done = h->done;
+  P.no_in_edges = h->no_in;
+  P.heavy_v = h->heavy_v;
+  P.heavy_s = h->heavy_s;
+  P.heavy_cap = h->heavy_cap;
+  P.cnt = h->cnt;
+  P.bar = h->bar;
+  P.depth = h->depth;
+  P.log = h->log;
+  P.result = h->result;
+  h->last_k = k;
+  return eng::launch_persistent(ms::msbfs_kernel, P, 2, g->stream);
+}
+
+sg_status sg_msbfs_run(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int direction, float alpha, float beta,
+                       sg_msbfs_details* details) {
+  SG_TRY(sg_msbfs_run_async(h, host_sources, k, direction, alpha, beta));
+  unsigned long long r[4];
+  sygraph::detail::GridBarrier b;
+  SG_CUDA(cudaMemcpyAsync(r, h->result, sizeof(r), cudaMemcpyDeviceToHost, h->g->stream));
+  SG_CUDA(cudaMemcpyAsync(&b, h->bar, sizeof(b), cudaMemcpyDeviceToHost, h->g->stream));
+  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  if (b.error) return fail(SG_ERR_TIMEOUT, "multi-source BFS: a grid barrier wait ran out");
+  if (details) {
+    details->iterations = r[0];
+    details->push_steps = r[1];
+    details->pull_steps = r[2];
+    details->reached_edges = r[3];
+  }
+  return SG_OK;
+}
+
+sg_status sg_msbfs_get_depths(sg_msbfs h, uint32_t* host_depth) {
+  SG_REQUIRE(h && host_depth, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(h->last_k, SG_ERR_NOT_INITIALIZED, "no batch has run");
+  SG_CUDA(cudaMemcpyAsync(host_depth, h->depth, sizeof(uint32_t) * (uint64_t)h->last_k * h->g->n,
+                          cudaMemcpyDeviceToHost, h->g->stream));
+  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  return SG_OK;
+}
+
+sg_status sg_msbfs_depths_device(sg_msbfs h, const uint32_t** dev_depth) {
+  SG_REQUIRE(h && dev_depth, SG_ERR_INVALID, "NULL argument");
+  *dev_depth = h->depth;
+  return SG_OK;
+}
+
+}  // extern "C"

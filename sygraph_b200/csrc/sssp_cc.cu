@@ -178,9 +178,30 @@ struct sg_sssp_s {
   sg_graph g = nullptr;
   uint32_t source = 0;
   bool initialised = false;
+  bool fresh = false;  // initialised but not run: distances not written yet
   void* dist = nullptr;
   PushWorkspace ws;
 };
+
+template <typename W>
+__global__ void fill_dist_kernel(W* dist, uint32_t n, uint32_t src) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dist[i] = i == src ? (W)0 : (W)(n + 1);
+}
+
+// SSSPInstance ctor state (sssp.hpp:392-405), written only when distances are
+// read before a run.
+static sg_status sssp_materialise(sg_sssp s) {
+  if (!s->fresh) return SG_OK;
+  sg_graph g = s->g;
+  if (g->value_type == SG_WEIGHT_F32)
+    fill_dist_kernel<float><<<grid_for(g->n, 256), 256, 0, g->stream>>>((float*)s->dist, g->n, s->source);
+  else
+    fill_dist_kernel<uint32_t><<<grid_for(g->n, 256), 256, 0, g->stream>>>((uint32_t*)s->dist, g->n, s->source);
+  SG_CHECK_LAUNCH();
+  s->fresh = false;
+  return SG_OK;
+}
 
 static sg_status sssp_launch(sg_sssp s) {
   sg_graph g = s->g;
@@ -232,6 +253,7 @@ sg_status sg_sssp_init(sg_sssp s, uint32_t source) {
   SG_REQUIRE(source < s->g->n, SG_ERR_INVALID, "source out of range");
   s->source = source;
   s->initialised = true;
+  s->fresh = true;
   return SG_OK;
 }
 
@@ -239,6 +261,7 @@ sg_status sg_sssp_run_async(sg_sssp s) {
   clear_error();
   SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
   SG_REQUIRE(s->initialised, SG_ERR_NOT_INITIALIZED, "SSSP instance not initialized");
+  s->fresh = false;
   return sssp_launch(s);
 }
 
@@ -250,6 +273,7 @@ sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations) {
 sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist) {
   SG_REQUIRE(s && host_dist, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(s->initialised, SG_ERR_NOT_INITIALIZED, "SSSP instance not initialized");
+  SG_TRY(sssp_materialise(s));
   SG_CUDA(cudaMemcpyAsync(host_dist, s->dist, sizeof(uint32_t) * s->g->n, cudaMemcpyDeviceToHost, s->g->stream));
   SG_CUDA(cudaStreamSynchronize(s->g->stream));
   return SG_OK;
@@ -257,6 +281,7 @@ sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist) {
 
 sg_status sg_sssp_distances_device(sg_sssp s, const void** dev_dist) {
   SG_REQUIRE(s && dev_dist, SG_ERR_INVALID, "NULL argument");
+  if (s->initialised) SG_TRY(sssp_materialise(s));
   *dev_dist = s->dist;
   return SG_OK;
 }
