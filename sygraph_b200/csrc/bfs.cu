@@ -21,6 +21,7 @@
 // One grid barrier per level; no host round trip until the traversal ends.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "engine_common.cuh"
@@ -618,6 +619,144 @@ sg_status sg_run_bfs(sg_graph g, uint32_t source, int direction, float alpha, fl
   if (s == SG_OK && host_depth) s = sg_bfs_get_distances(b, host_depth);
   sg_bfs_destroy(b);
   return s;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// BFS without any allocation.
+//
+// Some callers cannot allocate device memory at the moment they need a
+// traversal: host code that runs inside a region where the CUDA allocator must
+// not be entered (cudaMalloc can synchronise the whole device and take
+// milliseconds, which a latency-critical query loop cannot afford), or a
+// plug-in embedded in a host application that owns every byte of device
+// memory and hands the plug-in only its input and output buffers.  For them,
+// sg_bfs_noalloc runs the same traversal kernel as sg_bfs_run with all of its
+// working memory in one statically sized device array of this library.
+//
+// The array is kNoAllocScratchBytes long (about 11 MB) and every GPU that
+// loads the library holds it until the process exits.  It bounds the graphs
+// this entry point accepts: at most kNoAllocMaxVertices vertices and
+// kNoAllocMaxEdges edges; larger graphs are rejected with SG_ERR_INVALID.
+// ---------------------------------------------------------------------------
+namespace sgb {
+namespace bfs_noalloc {
+
+constexpr uint64_t kNoAllocMaxVertices = 1ull << 22;
+constexpr uint64_t kNoAllocMaxEdges = 1ull << 27;
+constexpr uint64_t kMaxW0 = kNoAllocMaxVertices / 32;
+constexpr uint64_t kMaxW1 = kMaxW0 / 32;
+constexpr uint64_t kMaxHeavy = kNoAllocMaxEdges / bfs::kHeavy + 1;
+
+constexpr uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
+// Byte offsets of each region inside the static array.
+constexpr uint64_t kOffVisited = 0;
+constexpr uint64_t kOffNoIn = kOffVisited + align256(4 * kMaxW0);
+constexpr uint64_t kOffFb = kOffNoIn + align256(4 * kMaxW0);
+constexpr uint64_t kOffSm = kOffFb + align256(3 * 4 * kMaxW0);
+constexpr uint64_t kOffHeavyV = kOffSm + align256(3 * 4 * kMaxW1);
+constexpr uint64_t kOffHeavyS = kOffHeavyV + align256(2 * 4 * kMaxHeavy);
+constexpr uint64_t kOffCnt = kOffHeavyS + align256(2 * 4 * kMaxHeavy);
+constexpr uint64_t kOffBar = kOffCnt + align256(3 * sizeof(bfs::LevelCounters));
+constexpr uint64_t kOffLog = kOffBar + align256(sizeof(sygraph::detail::GridBarrier));
+constexpr uint64_t kOffResult = kOffLog + align256(SG_MAX_LOGGED_LEVELS * sizeof(sg_level_record));
+constexpr uint64_t kNoAllocScratchBytes = kOffResult + align256(8 * sizeof(unsigned long long));
+
+// Working memory of sg_bfs_noalloc; shared by every call on a device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once per device.
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_base[64] = {};
+
+static sg_status scratch_base(unsigned char** out) {
+  int dev = 0;
+  SG_CUDA(cudaGetDevice(&dev));
+  SG_REQUIRE(dev >= 0 && dev < 64, SG_ERR_UNSUPPORTED, "device index out of range for the static scratch table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_base[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static BFS scratch)", __FILE__, __LINE__);
+    SG_REQUIRE(p, SG_ERR_CUDA, "cudaGetSymbolAddress returned NULL for the static BFS scratch");
+    g_noalloc_base[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_base[dev]);
+  return SG_OK;
+}
+
+}  // namespace bfs_noalloc
+}  // namespace sgb
+
+extern "C" {
+
+sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_column_indices,
+                         const uint32_t* dev_inv_row_offsets, const uint32_t* dev_inv_column_indices, uint32_t n,
+                         uint64_t m, uint32_t source, int direction, float alpha, float beta, uint32_t* dev_depth,
+                         uint64_t* host_iterations, void* stream) {
+  using namespace sgb::bfs_noalloc;
+  clear_error();
+  SG_REQUIRE(dev_row_offsets && dev_depth, SG_ERR_INVALID, "row offsets and depth output are required");
+  SG_REQUIRE(m == 0 || dev_column_indices, SG_ERR_INVALID, "column indices are required");
+  SG_REQUIRE(n > 0, SG_ERR_INVALID, "graph has no vertices");
+  SG_REQUIRE(n <= kNoAllocMaxVertices, SG_ERR_INVALID,
+             "sg_bfs_noalloc: vertex count exceeds its static scratch limit of 4194304 (2^22) vertices");
+  SG_REQUIRE(m <= kNoAllocMaxEdges, SG_ERR_INVALID,
+             "sg_bfs_noalloc: edge count exceeds its static scratch limit of 134217728 (2^27) edges");
+  SG_REQUIRE(source < n, SG_ERR_INVALID, "source out of range");
+  SG_REQUIRE(direction >= SG_BFS_PUSH && direction <= SG_BFS_HYBRID, SG_ERR_INVALID, "unknown BFS direction");
+  if (!dev_inv_row_offsets) {  // an undirected graph is its own inverse
+    dev_inv_row_offsets = dev_row_offsets;
+    dev_inv_column_indices = dev_column_indices;
+  }
+  unsigned char* base = nullptr;
+  SG_TRY(scratch_base(&base));
+  cudaStream_t s = (cudaStream_t)stream;
+  const uint32_t w0 = div_up(n, 32), w1 = div_up(w0, 32);
+  bfs::Params P;
+  P.n = n;
+  P.w0 = w0;
+  P.w1 = w1;
+  P.m = m;
+  P.ro = dev_row_offsets;
+  P.col = dev_column_indices;
+  P.iro = dev_inv_row_offsets;
+  P.icol = dev_inv_column_indices;
+  P.source = source;
+  P.mode = direction;
+  P.pull_all = 0;
+  P.alpha = alpha;
+  P.beta = beta;
+  P.depth = dev_depth;
+  P.visited = reinterpret_cast<uint32_t*>(base + kOffVisited);
+  uint32_t* no_in = reinterpret_cast<uint32_t*>(base + kOffNoIn);
+  P.no_in_edges = no_in;
+  P.fb = reinterpret_cast<uint32_t*>(base + kOffFb);
+  P.sm = reinterpret_cast<uint32_t*>(base + kOffSm);
+  P.heavy_cap = (uint32_t)std::min<uint64_t>(n, m / bfs::kHeavy + 1);
+  P.heavy_v = reinterpret_cast<uint32_t*>(base + kOffHeavyV);
+  P.heavy_s = reinterpret_cast<uint32_t*>(base + kOffHeavyS);
+  P.cnt = reinterpret_cast<bfs::LevelCounters*>(base + kOffCnt);
+  P.bar = reinterpret_cast<sygraph::detail::GridBarrier*>(base + kOffBar);
+  P.log = reinterpret_cast<sg_level_record*>(base + kOffLog);
+  P.result = reinterpret_cast<unsigned long long*>(base + kOffResult);
+  P.schedule = nullptr;
+  P.schedule_len = 0;
+  // The previous call's contents stay in the array: the barrier must start at
+  // zero (the kernel initialises every other region it reads).
+  SG_CUDA(cudaMemsetAsync(P.bar, 0, sizeof(sygraph::detail::GridBarrier), s));
+  bfs::no_in_edges_kernel<<<grid_for((uint64_t)w0 * 32, 256), 256, 0, s>>>(dev_inv_row_offsets, n, w0, no_in);
+  SG_CHECK_LAUNCH();
+  SG_TRY(eng::launch_persistent(bfs::bfs_kernel, P, 2, s));
+  unsigned long long it = 0;
+  uint32_t err = 0;
+  SG_CUDA(cudaMemcpyAsync(&it, P.result, sizeof(it), cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaMemcpyAsync(&err, &P.bar->error, sizeof(err), cudaMemcpyDeviceToHost, s));
+  SG_CUDA(cudaStreamSynchronize(s));
+  if (err) return fail(SG_ERR_TIMEOUT, "sg_bfs_noalloc: a grid barrier wait ran out");
+  if (host_iterations) *host_iterations = it;
+  return SG_OK;
 }
 
 }  // extern "C"
