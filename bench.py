@@ -222,6 +222,12 @@ def profile_case(kind: str) -> None:
             det = a.run(2, ALPHA, BETA)
         print(json.dumps({"profile": "bfs", "source": src, "iterations": det.iterations,
                           "levels": a.level_records()}))
+    elif kind == "msbfs":
+        srcs = sg.io.sample_sources(g, N_SOURCES, seed=SOURCE_SEED)
+        a = sg.algorithms.MultiBFS(G, N_SOURCES)
+        for _ in range(2):
+            det = a.run(srcs, 2, ALPHA, BETA)
+        print(json.dumps({"profile": "msbfs", "sources": N_SOURCES, **det}))
     else:
         a = sg.algorithms.SSSP(G)
         for _ in range(2):
@@ -238,7 +244,7 @@ def main():
     ap.add_argument("--impl", default="sygraph_b200", choices=["sygraph_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sssp-sources", type=int, default=8)
-    ap.add_argument("--profile", choices=["bfs", "sssp"], default=None,
+    ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs"], default=None,
                     help="profiling case: build the graph, run 2 traversals of one kind and exit (few launches)")
     args = ap.parse_args()
     world, rank, local = dist_init()
@@ -353,6 +359,25 @@ def main():
     sg._lib.call("sg_free_host_pinned", hp_dst)
     sg._lib.call("sg_free_device", dsrc)
 
+    # the same 64 sources as one bit-parallel batch (one launch); identical depths
+    mbfs = sg.algorithms.MultiBFS(G, len(srcs))
+    for _ in range(2):
+        mbfs.run_async(srcs, 2, ALPHA, BETA)
+    torch.cuda.synchronize()
+    mb_ms = []
+    for _ in range(max(3, args.steps // 2)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        mbfs.run_async(srcs, 2, ALPHA, BETA)
+        b.record()
+        b.synchronize()
+        mb_ms.append(a.elapsed_time(b))
+    mb_det = mbfs.run(srcs, 2, ALPHA, BETA)
+    batched_ms = float(np.median(mb_ms))
+    batched_gteps = mb_det["reached_edges"] / (batched_ms * 1e-3) / 1e9
+    ms_bytes = 4 * (n + 1) + 4 * m + 4 * n * len(srcs)
+    del mbfs
+
     # SSSP on a subset of the same sources (reported beside the BFS line)
     sssp = sg.algorithms.SSSP(G)
     ss_edges, ss_ms = 0, 0.0
@@ -395,6 +420,13 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": base,
+            "batched": {"value": batched_gteps, "unit": "GTEPS", "sources_per_launch": len(srcs),
+                        "launch_ms": batched_ms, "speedup_vs_single_source": batched_gteps / value,
+                        "reached_edges": mb_det["reached_edges"], "reached_edges_single": step_edges,
+                        "roofline": {"bound": "hbm", "achieved": ms_bytes / (batched_ms * 1e-3) / 1e9,
+                                     "peak": peak, "unit": "GB/s",
+                                     "frac": ms_bytes / (batched_ms * 1e-3) / 1e9 / peak,
+                                     "bytes_per_launch": ms_bytes, "traffic": ncu_traffic("msbfs_kernel")}},
             "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
                      "roofline": {"bound": "hbm", "achieved": sssp_achieved, "peak": peak, "unit": "GB/s",
                                   "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,

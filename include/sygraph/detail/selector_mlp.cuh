@@ -1,0 +1,81 @@
+// Parameter layout of the strategy-selector MLP and its device-side forward
+// pass for one feature vector (one warp), used inside the traversal engines.
+//
+// 12 features -> 32 (ReLU) -> 32 (ReLU) -> 6 predicted log-times, one per
+// strategy: 0 push/warp, 1 push/CTA, 2 pull/warp, 3 pull/CTA, 4 pull_all/warp,
+// 5 pull_all/CTA.  Inputs are standardised with the training set's mean and
+// 1/std; lo/hi bound the training range (a feature outside it means the
+// network is not trusted and the caller falls back to the heuristic).
+#pragma once
+
+#include <cstdint>
+
+namespace sygraph {
+namespace detail {
+
+constexpr int kMlpIn = 12;
+constexpr int kMlpHidden = 32;
+constexpr int kMlpOut = 6;
+
+struct MlpParams {
+  // trainable block first (gradients and optimiser state cover only these)
+  float w1[kMlpHidden][kMlpIn];
+  float b1[kMlpHidden];
+  float w2[kMlpHidden][kMlpHidden];
+  float b2[kMlpHidden];
+  float w3[kMlpOut][kMlpHidden];
+  float b3[kMlpOut];
+  // input standardisation and trusted range
+  float mean[kMlpIn];
+  float inv_std[kMlpIn];
+  float lo[kMlpIn];
+  float hi[kMlpIn];
+};
+
+constexpr int kMlpTrainableCount =
+    kMlpHidden * kMlpIn + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
+constexpr int kMlpParamCount = (int)(sizeof(MlpParams) / sizeof(float));
+static_assert(kMlpParamCount == kMlpTrainableCount + 4 * kMlpIn, "MlpParams must be packed floats");
+
+#ifdef __CUDACC__
+// Forward pass by one full warp: lane j computes hidden unit j.  Returns, in
+// every lane, the strategy with the smallest predicted time among the set bits
+// of `allowed`, or -1 when a feature lies outside the trusted range.
+__device__ __forceinline__ int mlp_choose(const MlpParams* __restrict__ P, const float* f, uint32_t allowed) {
+  const uint32_t lane = threadIdx.x & 31;
+  bool out_of_range = false;
+  float x[kMlpIn];
+#pragma unroll
+  for (int i = 0; i < kMlpIn; i++) {
+    out_of_range |= f[i] < P->lo[i] || f[i] > P->hi[i];
+    x[i] = (f[i] - P->mean[i]) * P->inv_std[i];
+  }
+  if (out_of_range) return -1;
+  float h1 = P->b1[lane];
+#pragma unroll
+  for (int i = 0; i < kMlpIn; i++) h1 += P->w1[lane][i] * x[i];
+  h1 = h1 > 0.f ? h1 : 0.f;
+  float h2 = P->b2[lane];
+#pragma unroll 8
+  for (int i = 0; i < kMlpHidden; i++) h2 += P->w2[lane][i] * __shfl_sync(0xffffffffu, h1, i);
+  h2 = h2 > 0.f ? h2 : 0.f;
+  float best = 3.4e38f;
+  int arg = -1;
+#pragma unroll
+  for (int j = 0; j < kMlpOut; j++) {
+    float y = P->w3[j][lane] * h2;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) y += __shfl_xor_sync(0xffffffffu, y, d);
+    y += P->b3[j];
+    if (((allowed >> j) & 1u) && y < best) {
+      best = y;
+      arg = j;
+    }
+  }
+  // butterfly sums may round differently per lane: lane 0 decides for all
+  return __shfl_sync(0xffffffffu, arg, 0);
+}
+#endif
+
+}  // namespace detail
+}  // namespace sygraph

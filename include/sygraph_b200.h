@@ -78,6 +78,17 @@ const char* sg_version(void);
 #define SG_BFS_PUSH 0
 #define SG_BFS_PULL 1
 #define SG_BFS_HYBRID 2
+/* Not in the reference: the learned selector (sg_bfs_set_selector) picks each
+ * level's strategy, with the hybrid heuristic as its fallback. */
+#define SG_BFS_LEARNED 3
+
+/* Per-level strategies of the fused BFS engine (direction x mapping). */
+#define SG_STRATEGY_PUSH_WARP 0
+#define SG_STRATEGY_PUSH_CTA 1
+#define SG_STRATEGY_PULL_WARP 2
+#define SG_STRATEGY_PULL_CTA 3
+#define SG_STRATEGY_PULL_ALL_WARP 4
+#define SG_STRATEGY_PULL_ALL_CTA 5
 
 #define SG_WEIGHT_NONE 0
 #define SG_WEIGHT_F32 1
@@ -342,6 +353,44 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
                              float beta);
 sg_status sg_msbfs_get_depths(sg_msbfs h, uint32_t* host_depth);
 sg_status sg_msbfs_depths_device(sg_msbfs h, const uint32_t** dev_depth);
+
+/* Learned strategy selector (no counterpart in the reference, whose
+ * direction choice is the degree-threshold heuristic of bfs.hpp:325-350): a
+ * 12 -> 32 -> 32 -> 6 FP32 MLP predicting the log-time of a traversal level
+ * under each strategy (push / pull / pull_all x warp- / CTA-mapped).  The
+ * parameter block is sg_mlp_param_count() floats: w1[32][12], b1[32],
+ * w2[32][32], b2[32], w3[6][32], b3[6], then input mean[12], 1/std[12] and the
+ * trusted range lo[12], hi[12].  Training runs on the device with this
+ * library's own forward / backward / Adam kernels. */
+typedef struct sg_mlp_s* sg_mlp;
+uint32_t sg_mlp_param_count(void);
+sg_status sg_mlp_create(const float* host_params /* NULL: seeded initialisation */, sg_mlp* out);
+sg_status sg_mlp_destroy(sg_mlp h);
+sg_status sg_mlp_get_params(sg_mlp h, float* host_params);
+sg_status sg_mlp_set_params(sg_mlp h, const float* host_params);
+/* dev_y[n][6] = MLP(dev_x[n][12]) */
+sg_status sg_mlp_forward(sg_mlp h, const float* dev_x, uint32_t n, float* dev_y);
+/* Gradient of the masked mean squared error 0.5*mask*(y-t)^2 over n samples
+ * (trainable parameters; the normalisation entries get 0). */
+sg_status sg_mlp_gradient(sg_mlp h, const float* dev_x, const float* dev_t, const float* dev_mask, uint32_t n,
+                          float* host_grad, float* host_loss);
+/* `steps` full-batch Adam steps on that loss. */
+sg_status sg_mlp_train(sg_mlp h, const float* dev_x, const float* dev_t, const float* dev_mask, uint32_t n,
+                       uint32_t steps, float lr, float weight_decay, float* host_final_loss);
+
+/* Scheduling controls of the fused BFS engine (no counterpart in the
+ * reference; none changes any depth):
+ *   sg_bfs_set_schedule  forces the strategy of level i (SG_STRATEGY_*, or -1
+ *                        to let the mode decide) for i < len; len 0 clears it
+ *   sg_bfs_set_selector  the MLP used by SG_BFS_LEARNED and the strategies it
+ *                        may choose (bit mask over SG_STRATEGY_*)
+ *   sg_bfs_log_features  records the twelve selector features of each level
+ *                        decision; sg_bfs_level_features reads them (12 floats
+ *                        per level, level 0 first). */
+sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len);
+sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed);
+sg_status sg_bfs_log_features(sg_bfs b, int enable);
+sg_status sg_bfs_level_features(sg_bfs b, float* host_features, uint32_t cap_levels, uint32_t* count);
 
 /* SSSP(G) + init + run + getDistance (algorithms/sssp.hpp:109-217): frontier
  * Bellman-Ford with atomicMin, fused.  Distances have the graph's weight type

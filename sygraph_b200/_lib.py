@@ -135,6 +135,18 @@ SIGNATURES = {
     "sg_bfs_distances_device": (st, [vp, C.POINTER(u32p)]),
     "sg_bfs_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
     "sg_run_bfs": (st, [vp, C.c_uint32, C.c_int, C.c_float, C.c_float, u32p, C.POINTER(BfsDetails)]),
+    "sg_bfs_set_schedule": (st, [vp, C.POINTER(C.c_int), C.c_uint32]),
+    "sg_bfs_set_selector": (st, [vp, vp, C.c_uint32]),
+    "sg_bfs_log_features": (st, [vp, C.c_int]),
+    "sg_bfs_level_features": (st, [vp, f32p, C.c_uint32, u32p]),
+    "sg_mlp_param_count": (C.c_uint32, []),
+    "sg_mlp_create": (st, [f32p, C.POINTER(vp)]),
+    "sg_mlp_destroy": (st, [vp]),
+    "sg_mlp_get_params": (st, [vp, f32p]),
+    "sg_mlp_set_params": (st, [vp, f32p]),
+    "sg_mlp_forward": (st, [vp, vp, C.c_uint32, vp]),
+    "sg_mlp_gradient": (st, [vp, vp, vp, vp, C.c_uint32, f32p, f32p]),
+    "sg_mlp_train": (st, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, f32p]),
     "sg_msbfs_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
     "sg_msbfs_destroy": (st, [vp]),
     "sg_msbfs_run": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float, C.POINTER(MsbfsDetails)]),

@@ -18,6 +18,7 @@ class bfs_direction:  # noqa: N801 - algorithms::bfs_direction (bfs.hpp:29)
     push = 0
     pull = 1
     hybrid = 2
+    learned = 3  # not in the reference: the learned selector picks every level's strategy
 
 
 @dataclass
@@ -71,6 +72,29 @@ class BFS:
 
     def getDistance(self, v: int) -> int:
         return int(self.getDistances()[v])
+
+    def set_schedule(self, strategies) -> None:
+        """Force the strategy of level i (0..5, -1 = the mode decides)."""
+        s = np.ascontiguousarray(strategies if strategies is not None else [], np.int32)
+        call("sg_bfs_set_schedule", self.handle, s.ctypes.data_as(C.POINTER(C.c_int)), s.size)
+
+    def set_selector(self, mlp, allowed: int = 0x3F) -> None:
+        """The MLP of bfs_direction.learned (None detaches it)."""
+        self._mlp = mlp  # keep the device parameters alive
+        call("sg_bfs_set_selector", self.handle, mlp.handle if mlp is not None else None, allowed)
+
+    def log_features(self, enable: bool = True) -> None:
+        call("sg_bfs_log_features", self.handle, int(enable))
+
+    def level_features(self) -> np.ndarray:
+        out = np.zeros((_lib.SG_MAX_LOGGED_LEVELS, 12), np.float32)
+        cnt = C.c_uint32()
+        call("sg_bfs_level_features", self.handle, out.ctypes.data_as(C.POINTER(C.c_float)),
+             _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
+        return out[:cnt.value]
+
+    def level_times_us(self) -> np.ndarray:
+        return np.array([(r["t_end_ns"] - r["t_start_ns"]) / 1000.0 for r in self.level_records()])
 
     def level_records(self) -> list[dict]:
         recs = (_lib.LevelRecord * _lib.SG_MAX_LOGGED_LEVELS)()

@@ -5,141 +5,36 @@
 // Frontier F_L lives in bitmap fb[L%3] with a summary sm[L%3] (bit j of
 // summary word k set iff fb word 32k+j is non-zero); vertices of degree >=
 // kHeavy are also listed, with their first chunk index, in heavy[L&1] as they
-// are discovered.  Per level:
-//   push: warps take summary words (skipping empty regions) and expand the
-//         light vertices found there 32 at a time, edge-parallel by a shuffle
-//         scan; heavy vertices are expanded kChunk edges per warp.  Each
-//         unvisited neighbour is claimed with one atomicOr on the visited
-//         bitmap; the winner writes depth L+1 and sets its fb / summary bits.
-//   pull: one warp per 32 unvisited vertices; each lane scans its in-edges,
-//         four at a time, for a neighbour in F_L and stops at the first (the
-//         warp takes over long lists); the warp stores the visited and
-//         next-frontier words.
+// are discovered.  Per level, one of six strategies (bfs_strategies.cuh):
+//   push (warp- or CTA-mapped): each unvisited neighbour of F_L is claimed
+//         with one atomicOr on the visited bitmap; the winner writes depth L+1
+//         and sets its fb / summary bits; heavy vertices go in chunks.
+//   pull / pull_all (warp- or CTA-mapped): every unvisited vertex scans its
+//         in-edges for a neighbour in F_L (pull stops at the first); the
+//         owner stores the visited and next-frontier words.
 //   then: fb / summary of F_{L-1} are cleared, per-CTA totals are added,
-//         one grid barrier, and every CTA takes the same direction decision
-//         from the same counters.
+//         one grid barrier, and every CTA takes the same decision for the
+//         next level from the same counters: the reference heuristic, a
+//         forced schedule, or the learned selector (bfs_engine.cuh).
 // One grid barrier per level; no host round trip until the traversal ends.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <vector>
 
-#include "engine_common.cuh"
+#include "bfs_strategies.cuh"
 
 namespace sgb {
 namespace bfs {
 
 using namespace eng;
 
-constexpr uint32_t kHeavy = 256;      // degree from which a vertex is expanded in kChunk-edge chunks
-constexpr uint32_t kHeavyBuf = 1024;  // per-CTA staging of newly discovered heavy vertices
-
-struct LevelCounters {
-  unsigned long long heavy_packed;  // (entries << 32) | chunks of the heavy list being built
-  unsigned long long new_count;
-  unsigned long long new_deg;
-  unsigned long long pad;
-};
-
-struct Params {
-  uint32_t n, w0, w1;
-  uint64_t m;
-  const uint32_t* ro;  // forward CSR
-  const uint32_t* col;
-  const uint32_t* iro;  // inverse CSR (aliases forward when undirected)
-  const uint32_t* icol;
-  uint32_t source;
-  int mode;      // SG_BFS_PUSH / PULL / HYBRID
-  int pull_all;  // pull without short-circuit
-  float alpha, beta;
-  uint32_t* depth;
-  uint32_t* visited;
-  const uint32_t* no_in_edges;  // bitmap of vertices no edge reaches: never candidates
-  uint32_t* fb;                 // 3 * w0
-  uint32_t* sm;                 // 3 * w1
-  uint32_t* heavy_v;            // 2 * heavy_cap
-  uint32_t* heavy_s;            // 2 * heavy_cap
-  uint32_t heavy_cap;
-  LevelCounters* cnt;  // 3
-  GridBarrier* bar;
-  sg_level_record* log;
-  unsigned long long* result;  // [iterations, push, pull, visited_vertices, visited_edges]
-  const int* schedule;         // optional forced direction per level (0 push, 1 pull), -1 = heuristic
-  uint32_t schedule_len;
-};
-
-struct Shared {
-  uint32_t scan[32];
-  unsigned long long red[32];
-  uint32_t hv[kHeavyBuf];
-  uint32_t hd[kHeavyBuf];
-  uint32_t hn;
-  uint32_t base_e, base_c;
-};
-
-// Per-thread state of one level's expansion.
-struct Level {
-  const Params* P;
-  Shared* S;
-  LevelCounters* C;
-  uint32_t* fb_next;
-  uint32_t* sm_next;
-  uint32_t* hv_next;
-  uint32_t* hs_next;
-  uint32_t next_depth;
-  uint32_t n_new = 0;
-  unsigned long long deg_new = 0;
-
-  __device__ __forceinline__ void add_heavy(uint32_t u, uint32_t du) {
-    const uint32_t i = atomicAdd(&S->hn, 1u);
-    if (i < kHeavyBuf) {
-      S->hv[i] = u;
-      S->hd[i] = du;
-    } else {
-      const unsigned long long old = atomicAdd(&C->heavy_packed, (1ull << 32) | chunks_of(du));
-      hv_next[old >> 32] = u;
-      hs_next[old >> 32] = (uint32_t)old;
-    }
-  }
-  // u was discovered at this level (forward degree du); fb bit set by the caller.
-  __device__ __forceinline__ void discovered(uint32_t u, uint32_t du) {
-    st_cg(P->depth + u, next_depth);
-    n_new++;
-    deg_new += du;
-    if (du >= kHeavy) add_heavy(u, du);
-  }
-  // push: claim u through the visited bitmap
-  __device__ __forceinline__ void visit_push(uint32_t u) {
-    if (!sygraph::detail::bit_set_once(P->visited, u)) return;
-    const uint32_t du = P->ro[u + 1] - P->ro[u];
-    const uint32_t b = 1u << (u & 31);
-    if (atomicOr(fb_next + (u >> 5), b) == 0) atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31));
-    discovered(u, du);
-  }
-};
-
-// Expands 32 (vertex, beg, deg) triples of a warp edge-parallel.
-__device__ __forceinline__ void expand_group(Level& L, uint32_t beg, uint32_t deg) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t incl = warp_inclusive_scan(deg);
-  const uint32_t total = __shfl_sync(kFullMask, incl, 31);
-  const uint32_t excl = incl - deg;
-  for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-    const uint32_t r = r0 + lane;
-    const bool act = r < total;
-    const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
-    const uint32_t ob = __shfl_sync(kFullMask, beg, o);
-    const uint32_t oe = __shfl_sync(kFullMask, excl, o);
-    if (act) L.visit_push(L.P->col[ob + (r - oe)]);
-  }
-}
-
 __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
   __shared__ Shared S;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
-  const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
+  const uint32_t lane = threadIdx.x & 31;
   const uint32_t n = P.n, w0 = P.w0, w1 = P.w1, src = P.source, inf = n + 1;
   const uint32_t deg_src = P.ro[src + 1] - P.ro[src];
 
@@ -161,7 +56,7 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
   if (gtid < 3) {
     LevelCounters z = {};
     if (gtid == 2 && deg_src >= kHeavy) {
-      z.heavy_packed = (1ull << 32) | chunks_of(deg_src);
+      z.heavy_packed = (1ull << 32) | bfs_chunks(deg_src);
       P.heavy_v[0] = src;
       P.heavy_s[0] = 0;
     }
@@ -171,21 +66,25 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
   if (!grid_sync(P.bar)) return;
 
   unsigned long long unexplored = P.m - deg_src;
-  unsigned long long frontier_size = 1, frontier_deg = deg_src;
+  unsigned long long frontier_size = 1, frontier_deg = deg_src, prev_size = 1;
   unsigned long long visited_vertices = 1;
   unsigned long long n_push = 0, n_pull = 0;
-  int pull = P.mode == SG_BFS_PULL;
+  // level 0: the mode's first choice (the reference starts in push unless pull-only)
+  int strategy = P.mode == SG_BFS_PULL ? 2 : 0;
+  {
+    FeatureInputs x{1.0, (double)deg_src, (double)unexplored, 1.0, 1.0, 1.0, 1.0, 0};
+    const int d = decide(P, S, 0, x, 0, 0.f, 1.f, 1);
+    if (P.mode == kLearned) strategy = d;
+  }
 
   uint32_t level = 0;
   for (;; level++) {
-    if (P.schedule && level < P.schedule_len && P.schedule[level] >= 0) pull = P.schedule[level];
+    if (P.schedule && level < P.schedule_len && P.schedule[level] >= 0) strategy = P.schedule[level];
     LevelCounters* C = P.cnt + (level % 3);
     const LevelCounters* Cprev = P.cnt + ((level + 2) % 3);
-    uint32_t* fb_cur = P.fb + (size_t)(level % 3) * w0;
-    uint32_t* fb_next = P.fb + (size_t)((level + 1) % 3) * w0;
+    const uint32_t* fb_cur = P.fb + (size_t)(level % 3) * w0;
     uint32_t* fb_zero = P.fb + (size_t)((level + 2) % 3) * w0;
-    uint32_t* sm_cur = P.sm + (size_t)(level % 3) * w1;
-    uint32_t* sm_next = P.sm + (size_t)((level + 1) % 3) * w1;
+    const uint32_t* sm_cur = P.sm + (size_t)(level % 3) * w1;
     uint32_t* sm_zero = P.sm + (size_t)((level + 2) % 3) * w1;
     const uint32_t par = level & 1;
     if (gtid == 0) {
@@ -194,107 +93,25 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
     }
     const uint64_t t0 = gtid == 0 ? sygraph::detail::global_timer_ns() : 0;
 
-    Level L{&P, &S, C, fb_next, sm_next, P.heavy_v + (size_t)(par ^ 1) * P.heavy_cap,
-            P.heavy_s + (size_t)(par ^ 1) * P.heavy_cap, level + 1};
-    if (!pull) {
+    Level L{&P, &S, C, P.fb + (size_t)((level + 1) % 3) * w0, P.sm + (size_t)((level + 1) % 3) * w1,
+            P.heavy_v + (size_t)(par ^ 1) * P.heavy_cap, P.heavy_s + (size_t)(par ^ 1) * P.heavy_cap, level + 1};
+    if (strategy < 2) {
       n_push++;
       const unsigned long long hp = ld_cg(&Cprev->heavy_packed);
       const uint32_t n_heavy = (uint32_t)(hp >> 32), n_chunks = (uint32_t)hp;
-      const uint32_t* hv_cur = P.heavy_v + (size_t)par * P.heavy_cap;
-      const uint32_t* hs_cur = P.heavy_s + (size_t)par * P.heavy_cap;
-      const uint32_t units = w1 + n_chunks;
-      for (uint32_t unit = gwarp; unit < units; unit += nwarps) {
-        if (unit < w1) {
-          const uint32_t s = ld_cg(sm_cur + unit);
-          if (!s) continue;
-          const uint32_t bits = ((s >> lane) & 1u) ? ld_cg(fb_cur + unit * 32 + lane) : 0u;
-          const uint32_t c = __popc(bits);
-          const uint32_t incl = warp_inclusive_scan(c);
-          const uint32_t total = __shfl_sync(kFullMask, incl, 31);
-          const uint32_t excl = incl - c;
-          for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-            const uint32_t r = r0 + lane;
-            const bool act = r < total;
-            const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
-            const uint32_t ob = __shfl_sync(kFullMask, bits, o);
-            const uint32_t oe = __shfl_sync(kFullMask, excl, o);
-            uint32_t beg = 0, deg = 0;
-            if (act) {
-              const uint32_t v = (unit * 32 + o) * 32 + select_bit(ob, r - oe);
-              beg = P.ro[v];
-              deg = P.ro[v + 1] - beg;
-              if (deg >= kHeavy) deg = 0;  // expanded through the heavy list
-            }
-            expand_group(L, beg, deg);
-          }
-        } else {
-          const uint32_t c = unit - w1;
-          const uint32_t ent = find_chunk_owner(hs_cur, n_heavy, c);
-          const uint32_t v = ld_cg(hv_cur + ent);
-          const uint32_t first = ld_cg(hs_cur + ent);
-          const uint32_t cb = P.ro[v] + (c - first) * kChunk;
-          const uint32_t ce = min(P.ro[v + 1], cb + kChunk);
-          for (uint32_t eb = cb; eb < ce; eb += 32) {
-            const uint32_t e = eb + lane;
-            if (e < ce) L.visit_push(P.col[e]);
-          }
-        }
-      }
+      const uint32_t* hv = P.heavy_v + (size_t)par * P.heavy_cap;
+      const uint32_t* hs = P.heavy_s + (size_t)par * P.heavy_cap;
+      if (strategy == 0)
+        push_warp(L, fb_cur, sm_cur, hv, hs, n_heavy, n_chunks);
+      else
+        push_cta(L, fb_cur, sm_cur, hv, hs, n_heavy, n_chunks);
     } else {
       n_pull++;
-      const bool same = P.iro == P.ro;
-      for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
-        const uint32_t vw = ld_cg(P.visited + wi);
-        const uint32_t cand = ~vw & valid_bits(wi, w0, n);
-        if (!cand) continue;
-        const uint32_t v = wi * 32 + lane;
-        const bool mine = (cand >> lane) & 1u;
-        const uint32_t beg = mine ? P.iro[v] : 0u;
-        const uint32_t end = mine ? P.iro[v + 1] : 0u;
-        bool found = false;
-        uint32_t e = beg;
-        const uint32_t lim = P.pull_all ? end : min(end, beg + kPullSerial);
-        // four independent column loads and bitmap probes per step
-        while (e < lim && (P.pull_all || !found)) {
-          const uint32_t c0 = P.icol[e];
-          const uint32_t c1 = e + 1 < lim ? P.icol[e + 1] : c0;
-          const uint32_t c2 = e + 2 < lim ? P.icol[e + 2] : c0;
-          const uint32_t c3 = e + 3 < lim ? P.icol[e + 3] : c0;
-          const bool h = bit_test(fb_cur, c0) | bit_test(fb_cur, c1) | bit_test(fb_cur, c2) | bit_test(fb_cur, c3);
-          found |= h;
-          e += 4;
-        }
-        if (e > lim) e = lim;
-        if (!P.pull_all) {
-          // long lists that are still unresolved: the whole warp scans them
-          uint32_t left = __ballot_sync(kFullMask, mine && !found && e < end);
-          while (left) {
-            const uint32_t j = __ffs(left) - 1;
-            left &= left - 1;
-            const uint32_t jb = __shfl_sync(kFullMask, e, j);
-            const uint32_t je = __shfl_sync(kFullMask, end, j);
-            bool hit = false;
-            for (uint32_t eb = jb; eb < je; eb += 32) {
-              const uint32_t ee = eb + lane;
-              const bool h = ee < je && bit_test(fb_cur, P.icol[ee]);
-              if (__any_sync(kFullMask, h)) {
-                hit = true;
-                break;
-              }
-            }
-            if (lane == j) found = hit;
-          }
-        }
-        const uint32_t fmask = __ballot_sync(kFullMask, found);
-        if (fmask) {
-          if (found) L.discovered(v, same ? (end - beg) : (P.ro[v + 1] - P.ro[v]));
-          if (lane == 0) {
-            st_cg(P.visited + wi, vw | fmask);
-            st_cg(fb_next + wi, fmask);
-            atomicOr(sm_next + (wi >> 5), 1u << (wi & 31));
-          }
-        }
-      }
+      const bool sc = strategy < 4;
+      if (strategy & 1)
+        pull_cta(L, fb_cur, sc);
+      else
+        pull_warp(L, fb_cur, sc);
     }
     // clear F_{L-1}: only the words its summary flags
     for (uint32_t j = gwarp; j < w1; j += nwarps) {
@@ -309,8 +126,8 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
       const uint32_t nb = min(S.hn, kHeavyBuf);
       const uint32_t k0 = 2 * threadIdx.x;
       uint32_t my = 0;
-      if (k0 < nb) my += chunks_of(S.hd[k0]);
-      if (k0 + 1 < nb) my += chunks_of(S.hd[k0 + 1]);
+      if (k0 < nb) my += bfs_chunks(S.hd[k0]);
+      if (k0 + 1 < nb) my += bfs_chunks(S.hd[k0 + 1]);
       uint32_t total;
       const uint32_t ex = sygraph::detail::block_excl_scan(my, &total, S.scan);
       if (threadIdx.x == 0 && nb) {
@@ -324,17 +141,19 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
         for (uint32_t k = k0; k < k0 + 2 && k < nb; k++) {
           L.hv_next[S.base_e + k] = S.hv[k];
           L.hs_next[S.base_e + k] = pc;
-          pc += chunks_of(S.hd[k]);
+          pc += bfs_chunks(S.hd[k]);
         }
       }
       if (threadIdx.x == 0) S.hn = 0;
     }
     {
-      const unsigned long long c = block_sum<unsigned long long>(L.n_new, S.red);
-      const unsigned long long d = block_sum<unsigned long long>(L.deg_new, S.red);
+      unsigned long long v4[4] = {L.n_new, L.deg_new, L.wnz, L.snz};
+      block_sum4(v4, S);
       if (threadIdx.x == 0) {
-        if (c) atomicAdd(&C->new_count, c);
-        if (d) atomicAdd(&C->new_deg, d);
+        if (v4[0]) atomicAdd(&C->new_count, v4[0]);
+        if (v4[1]) atomicAdd(&C->new_deg, v4[1]);
+        if (v4[2]) atomicAdd(&C->words_nz, v4[2]);
+        if (v4[3]) atomicAdd(&C->sum_nz, v4[3]);
       }
     }
     if (!grid_sync(P.bar)) return;
@@ -346,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
     if (gtid == 0 && level < kMaxLog) {
       sg_level_record r;
       r.level = level;
-      r.strategy = pull ? (P.pull_all ? 4u : 2u) : 0u;
+      r.strategy = (uint32_t)strategy;
       r.frontier_size = (uint32_t)frontier_size;
       r.next_size = (uint32_t)next_size;
       r.frontier_degree = frontier_deg;
@@ -356,17 +175,15 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
       r.t_end_ns = sygraph::detail::global_timer_ns();
       P.log[level] = r;
     }
-    // BFS::evaluateHeuristic (bfs.hpp:325-350), same float arithmetic.
-    if (P.mode == SG_BFS_HYBRID) {
-      if (!pull) {
-        if ((float)(uint32_t)next_deg > (float)(uint32_t)unexplored / P.alpha) pull = 1;
-      } else {
-        if ((float)next_size < (float)n / P.beta) pull = 0;
-      }
-    }
+    prev_size = frontier_size;
     frontier_size = next_size;
     frontier_deg = next_deg;
     if (next_size == 0) break;
+    FeatureInputs x{(double)next_size, (double)next_deg, (double)unexplored, (double)visited_vertices,
+                    (double)ld_cg(&C->words_nz), (double)ld_cg(&C->sum_nz), (double)prev_size, strategy >= 2};
+    // (float)(uint32) casts: the reference's uint32 degree sums (bfs.hpp:327-330)
+    strategy = decide(P, S, strategy, x, level + 1, (float)(uint32_t)next_deg, (float)(uint32_t)unexplored,
+                      next_size);
   }
   if (gtid == 0) {
     P.result[0] = level + 1;
@@ -419,6 +236,9 @@ struct sg_bfs_s {
   unsigned long long* result = nullptr;
   int* schedule = nullptr;
   uint32_t schedule_len = 0;
+  const sygraph::detail::MlpParams* mlp = nullptr;  // not owned
+  uint32_t allowed = 0x3f;
+  float* features = nullptr;
   uint32_t last_iterations = 0;
   bool fresh = false;  // initialised but not run: depths not written yet
 };
@@ -445,10 +265,11 @@ static void bfs_release(sg_bfs b) {
   dev_free(b->log);
   dev_free(b->result);
   dev_free(b->schedule);
+  dev_free(b->features);
   delete b;
 }
 
-static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta, int pull_all) {
+static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   sg_graph g = b->g;
   bfs::Params P;
   P.n = g->n;
@@ -461,9 +282,11 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta, in
   P.icol = g->inv.col;
   P.source = b->source;
   P.mode = direction;
-  P.pull_all = pull_all;
   P.alpha = alpha;
   P.beta = beta;
+  P.mlp = b->mlp;
+  P.allowed = b->allowed;
+  P.features = b->features;
   P.depth = b->depth;
   P.visited = b->visited;
   P.no_in_edges = b->no_in;
@@ -501,7 +324,7 @@ static sg_status bfs_collect(sg_bfs b, sg_bfs_details* details) {
     std::vector<sg_level_record> recs(nlog ? nlog : 1);
     if (nlog) {
       SG_CUDA(cudaMemcpy(recs.data(), b->log, sizeof(sg_level_record) * nlog, cudaMemcpyDeviceToHost));
-      for (uint32_t i = 0; i < nlog; i++) details->step_is_pull[i] = recs[i].strategy != 0;
+      for (uint32_t i = 0; i < nlog; i++) details->step_is_pull[i] = recs[i].strategy >= 2;
     }
   }
   return SG_OK;
@@ -572,9 +395,58 @@ sg_status sg_bfs_run_async(sg_bfs b, int direction, float alpha, float beta) {
   clear_error();
   SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
   SG_REQUIRE(b->initialised, SG_ERR_NOT_INITIALIZED, "BFS instance not initialized");
-  SG_REQUIRE(direction >= SG_BFS_PUSH && direction <= SG_BFS_HYBRID, SG_ERR_INVALID, "unknown BFS direction");
+  SG_REQUIRE(direction >= SG_BFS_PUSH && direction <= SG_BFS_LEARNED, SG_ERR_INVALID, "unknown BFS direction");
+  SG_REQUIRE(direction != SG_BFS_LEARNED || b->mlp, SG_ERR_NOT_INITIALIZED,
+             "learned mode needs a selector (sg_bfs_set_selector)");
   b->fresh = false;
-  return bfs_launch(b, direction, alpha, beta, 0);
+  return bfs_launch(b, direction, alpha, beta);
+}
+
+sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_REQUIRE(len == 0 || host_strategies, SG_ERR_INVALID, "strategies is NULL");
+  for (uint32_t i = 0; i < len; i++)
+    SG_REQUIRE(host_strategies[i] >= -1 && host_strategies[i] <= 5, SG_ERR_INVALID, "strategy codes are -1..5");
+  dev_free(b->schedule);
+  b->schedule_len = 0;
+  if (len) {
+    SG_TRY(dev_alloc(&b->schedule, len));
+    SG_CUDA(cudaMemcpy(b->schedule, host_strategies, sizeof(int) * len, cudaMemcpyHostToDevice));
+    b->schedule_len = len;
+  }
+  return SG_OK;
+}
+
+sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_REQUIRE(!mlp || (allowed & 0x3fu), SG_ERR_INVALID, "no strategy allowed");
+  b->mlp = mlp ? static_cast<const sygraph::detail::MlpParams*>(mlp_device_params(mlp)) : nullptr;
+  b->allowed = allowed & 0x3fu;
+  return SG_OK;
+}
+
+sg_status sg_bfs_log_features(sg_bfs b, int enable) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  if (enable && !b->features) SG_TRY(dev_alloc(&b->features, 12ull * SG_MAX_LOGGED_LEVELS));
+  if (!enable) dev_free(b->features);
+  return SG_OK;
+}
+
+sg_status sg_bfs_level_features(sg_bfs b, float* host_features, uint32_t cap_levels, uint32_t* count) {
+  SG_REQUIRE(b && count, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(b->features, SG_ERR_NOT_INITIALIZED, "feature logging is off (sg_bfs_log_features)");
+  SG_CUDA(cudaStreamSynchronize(b->g->stream));
+  unsigned long long it = 0;
+  SG_CUDA(cudaMemcpy(&it, b->result, sizeof(it), cudaMemcpyDeviceToHost));
+  uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
+  if (k > cap_levels) k = cap_levels;
+  if (host_features && k)
+    SG_CUDA(cudaMemcpy(host_features, b->features, sizeof(float) * 12 * k, cudaMemcpyDeviceToHost));
+  *count = k;
+  return SG_OK;
 }
 
 sg_status sg_bfs_run(sg_bfs b, int direction, float alpha, float beta, sg_bfs_details* details) {
@@ -725,7 +597,9 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.icol = dev_inv_column_indices;
   P.source = source;
   P.mode = direction;
-  P.pull_all = 0;
+  P.mlp = nullptr;
+  P.allowed = 0x3f;
+  P.features = nullptr;
   P.alpha = alpha;
   P.beta = beta;
   P.depth = dev_depth;

@@ -1,0 +1,209 @@
+// State of the fused BFS engine (bfs.cu): parameters, per-level counters,
+// shared memory, the per-thread level context, the twelve selector features
+// and the per-level strategy decision.
+//
+// Strategies (one per level): 0 push/warp, 1 push/CTA, 2 pull/warp,
+// 3 pull/CTA, 4 pull_all/warp, 5 pull_all/CTA.  Every strategy yields the
+// same frontier sets (BFS levels are unique); only the schedule changes.
+#pragma once
+
+#include "engine_common.cuh"
+#include "sygraph/detail/selector_mlp.cuh"
+
+namespace sgb {
+namespace bfs {
+
+using namespace eng;
+
+constexpr uint32_t kHeavy = 256;      // degree from which a vertex is expanded in chunks by many warps
+constexpr uint32_t kHeavyBuf = 1024;  // per-CTA staging of newly discovered heavy vertices
+constexpr uint32_t kBfsChunk = 64;    // edges per heavy-vertex chunk (one warp, two steps)
+constexpr int kLearned = 3;           // mode: the MLP picks each level's strategy
+
+__device__ __forceinline__ uint32_t bfs_chunks(uint32_t deg) { return (deg + kBfsChunk - 1) / kBfsChunk; }
+
+struct LevelCounters {
+  unsigned long long heavy_packed;  // (entries << 32) | chunks of the heavy list being built
+  unsigned long long new_count;     // vertices that joined the next frontier
+  unsigned long long new_deg;       // their forward degrees
+  unsigned long long words_nz;      // non-zero words of the next frontier bitmap
+  unsigned long long sum_nz;        // non-zero words of its summary
+  unsigned long long pad[3];
+};
+
+struct Params {
+  uint32_t n, w0, w1;
+  uint64_t m;
+  const uint32_t* ro;  // forward CSR
+  const uint32_t* col;
+  const uint32_t* iro;  // inverse CSR (aliases forward when undirected)
+  const uint32_t* icol;
+  uint32_t source;
+  int mode;  // SG_BFS_PUSH / PULL / HYBRID / kLearned
+  float alpha, beta;
+  uint32_t* depth;
+  uint32_t* visited;
+  const uint32_t* no_in_edges;  // bitmap of vertices no edge reaches: never candidates
+  uint32_t* fb;                 // 3 * w0
+  uint32_t* sm;                 // 3 * w1
+  uint32_t* heavy_v;            // 2 * heavy_cap
+  uint32_t* heavy_s;            // 2 * heavy_cap
+  uint32_t heavy_cap;
+  LevelCounters* cnt;  // 3
+  GridBarrier* bar;
+  sg_level_record* log;
+  unsigned long long* result;  // [iterations, push, pull, visited_vertices, visited_edges]
+  const int* schedule;         // optional strategy per level (0..5), -1 = the mode decides
+  uint32_t schedule_len;
+  const sygraph::detail::MlpParams* mlp;  // learned mode
+  uint32_t allowed;                       // strategies the MLP may pick (bit mask)
+  float* features;                        // optional log: 12 floats per level decision
+};
+
+struct Shared {
+  uint32_t scan[32];
+  unsigned long long red[32][4];
+  uint32_t hv[kHeavyBuf];
+  uint32_t hd[kHeavyBuf];
+  uint32_t hn;
+  uint32_t base_e, base_c;
+  uint32_t beg[kThreads];
+  uint32_t incl[kThreads];
+  uint32_t flag[kThreads];
+  int choice;
+};
+
+// Per-thread context of one level's expansion.
+struct Level {
+  const Params* P;
+  Shared* S;
+  LevelCounters* C;
+  uint32_t* fb_next;
+  uint32_t* sm_next;
+  uint32_t* hv_next;
+  uint32_t* hs_next;
+  uint32_t next_depth;
+  uint32_t n_new = 0, wnz = 0, snz = 0;
+  unsigned long long deg_new = 0;
+
+  __device__ __forceinline__ void add_heavy(uint32_t u, uint32_t du) {
+    const uint32_t i = atomicAdd(&S->hn, 1u);
+    if (i < kHeavyBuf) {
+      S->hv[i] = u;
+      S->hd[i] = du;
+    } else {
+      const unsigned long long old = atomicAdd(&C->heavy_packed, (1ull << 32) | bfs_chunks(du));
+      hv_next[old >> 32] = u;
+      hs_next[old >> 32] = (uint32_t)old;
+    }
+  }
+  // u was discovered at this level (forward degree du); its frontier bit is set by the caller.
+  __device__ __forceinline__ void discovered(uint32_t u, uint32_t du) {
+    st_cg(P->depth + u, next_depth);
+    n_new++;
+    deg_new += du;
+    if (du >= kHeavy) add_heavy(u, du);
+  }
+  // push: claim u through the visited bitmap
+  __device__ __forceinline__ void visit_push(uint32_t u) {
+    if (!sygraph::detail::bit_set_once(P->visited, u)) return;
+    const uint32_t du = P->ro[u + 1] - P->ro[u];
+    if (atomicOr(fb_next + (u >> 5), 1u << (u & 31)) == 0) {
+      wnz++;
+      if (atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31)) == 0) snz++;
+    }
+    discovered(u, du);
+  }
+  // pull: a warp publishes the vertices of word wi it found (lane 0 calls)
+  __device__ __forceinline__ void publish_word(uint32_t wi, uint32_t vw, uint32_t fmask) {
+    st_cg(P->visited + wi, vw | fmask);
+    st_cg(fb_next + wi, fmask);
+    wnz++;
+    if (atomicOr(sm_next + (wi >> 5), 1u << (wi & 31)) == 0) snz++;
+  }
+};
+
+// Sums four per-thread values over the block; the totals are valid in thread 0.
+__device__ __forceinline__ void block_sum4(unsigned long long v[4], Shared& S) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    v[k] = sygraph::detail::warp_sum(v[k]);
+    if (lane == 0) S.red[warp][k] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      unsigned long long t = lane < nw ? S.red[lane][k] : 0ull;
+      v[k] = sygraph::detail::warp_sum(t);
+    }
+  }
+  __syncthreads();
+}
+
+// The twelve selector features of the frontier about to be expanded.
+struct FeatureInputs {
+  double ns;     // frontier size
+  double nd;     // frontier degree sum
+  double ud;     // unexplored degree (unvisited vertices)
+  double vis;    // visited vertices
+  double wnz;    // non-zero frontier bitmap words
+  double snz;    // non-zero summary words
+  double prev;   // previous frontier size
+  int cur_pull;  // direction of the level that produced this frontier
+};
+
+__device__ __forceinline__ void compute_features(const Params& P, const FeatureInputs& x, float f[12]) {
+  const float n = (float)P.n, m = (float)(P.m ? P.m : 1);
+  f[0] = log2f(1.f + (float)x.ns) / log2f(1.f + n);
+  f[1] = (float)x.ns / n;
+  f[2] = log2f(1.f + (float)x.nd) / log2f(1.f + m);
+  f[3] = (float)x.nd / m;
+  f[4] = (float)x.ud / m;
+  f[5] = (n - (float)x.vis) / n;
+  f[6] = (float)x.wnz / (float)P.w0;
+  f[7] = (float)x.snz / (float)P.w1;
+  f[8] = log2f(1.f + (float)x.nd / fmaxf(1.f, (float)x.ns)) / 16.f;
+  f[9] = log2f(1.f + m / n) / 8.f;
+  f[10] = x.cur_pull ? 1.f : 0.f;
+  f[11] = fminf(16.f, fmaxf(-16.f, log2f((1.f + (float)x.ns) / (1.f + (float)x.prev)))) / 16.f;
+}
+
+// Strategy of the next level, identical in every CTA (same inputs, same
+// arithmetic).  Heuristic: BFS::evaluateHeuristic (bfs.hpp:325-350), with the
+// reference's float arithmetic; the learned mode asks the MLP (warp 0) and
+// falls back to the heuristic outside the trusted feature range.
+__device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const FeatureInputs& x, uint32_t level,
+                                      float next_deg_f, float unexplored_f, unsigned long long next_size) {
+  const bool cur_pull = cur >= 2;
+  bool pull = cur_pull;
+  if (P.mode == SG_BFS_HYBRID || P.mode == kLearned) {
+    if (!cur_pull) {
+      if (next_deg_f > unexplored_f / P.alpha) pull = true;
+    } else {
+      if ((float)next_size < (float)P.n / P.beta) pull = false;
+    }
+  }
+  int h = P.mode == SG_BFS_PUSH ? 0 : P.mode == SG_BFS_PULL ? 2 : (pull ? 2 : 0);
+  const bool log = P.features && blockIdx.x == 0 && level < kMaxLog;
+  if (P.mode == kLearned && P.mlp || log) {
+    if (threadIdx.x < 32) {
+      float f[12];
+      compute_features(P, x, f);
+      if (log && threadIdx.x == 0)
+        for (int i = 0; i < 12; i++) P.features[(size_t)level * 12 + i] = f[i];
+      if (P.mode == kLearned && P.mlp) {
+        const int c = sygraph::detail::mlp_choose(P.mlp, f, P.allowed);
+        if (threadIdx.x == 0) S.choice = c;
+      }
+    }
+    __syncthreads();
+    if (P.mode == kLearned && P.mlp && S.choice >= 0) h = S.choice;
+    __syncthreads();
+  }
+  return h;
+}
+
+}  // namespace bfs
+}  // namespace sgb

@@ -1,0 +1,233 @@
+// The expansion strategies of the BFS engine (bfs.cu), one call per level.
+//   push/warp : warps take summary words, expand the frontier's light vertices
+//               32 at a time, edge-parallel by a shuffle scan
+//   push/CTA  : a CTA takes 16 frontier words (512 candidates), scans their
+//               degrees across the block and walks the combined edge range
+//               (shared-memory binary search from edge rank to source)
+//   pull/warp : one warp per 32 unvisited vertices, each lane scans its own
+//               in-edges with the next column index prefetched; the warp
+//               helps with long lists
+//   pull/CTA  : a CTA takes 512 unvisited candidates and walks all their
+//               in-edges edge-parallel, with a per-candidate done flag
+// Heavy vertices (degree >= kHeavy) of a push level are expanded from the
+// heavy list in kBfsChunk-edge chunks by both push strategies.
+#pragma once
+
+#include "bfs_engine.cuh"
+
+namespace sgb {
+namespace bfs {
+
+__device__ __forceinline__ uint32_t smem_upper_bound(const uint32_t* a, uint32_t n, uint32_t r) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] <= r)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Expands 32 (beg, deg) ranges of a warp edge-parallel.
+__device__ __forceinline__ void expand_group(Level& L, uint32_t beg, uint32_t deg) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t incl = warp_inclusive_scan(deg);
+  const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+  const uint32_t excl = incl - deg;
+  for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+    const uint32_t r = r0 + lane;
+    const bool act = r < total;
+    const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+    const uint32_t ob = __shfl_sync(kFullMask, beg, o);
+    const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+    if (act) L.visit_push(L.P->col[ob + (r - oe)]);
+  }
+}
+
+// Heavy-vertex chunks, warp-strided from `first_warp`.
+__device__ __forceinline__ void push_heavy(Level& L, const uint32_t* hv, const uint32_t* hs, uint32_t n_heavy,
+                                           uint32_t n_chunks, uint32_t first_unit, uint32_t units_end) {
+  const Params& P = *L.P;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t unit = gwarp; unit < units_end; unit += nwarps) {
+    if (unit < first_unit) continue;
+    const uint32_t c = unit - first_unit;
+    const uint32_t ent = find_chunk_owner(hs, n_heavy, c);
+    const uint32_t v = ld_cg(hv + ent);
+    const uint32_t first = ld_cg(hs + ent);
+    const uint32_t cb = P.ro[v] + (c - first) * kBfsChunk;
+    const uint32_t ce = min(P.ro[v + 1], cb + kBfsChunk);
+    for (uint32_t eb = cb; eb < ce; eb += 32) {
+      const uint32_t e = eb + lane;
+      if (e < ce) L.visit_push(P.col[e]);
+    }
+  }
+  (void)n_chunks;
+}
+
+__device__ __forceinline__ void push_warp(Level& L, const uint32_t* fb_cur, const uint32_t* sm_cur,
+                                          const uint32_t* hv, const uint32_t* hs, uint32_t n_heavy,
+                                          uint32_t n_chunks) {
+  const Params& P = *L.P;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t w1 = P.w1;
+  for (uint32_t unit = gwarp; unit < w1; unit += nwarps) {
+    const uint32_t s = ld_cg(sm_cur + unit);
+    if (!s) continue;
+    const uint32_t bits = ((s >> lane) & 1u) ? ld_cg(fb_cur + unit * 32 + lane) : 0u;
+    const uint32_t c = __popc(bits);
+    const uint32_t incl = warp_inclusive_scan(c);
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    const uint32_t excl = incl - c;
+    for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      const bool act = r < total;
+      const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+      const uint32_t ob = __shfl_sync(kFullMask, bits, o);
+      const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+      uint32_t beg = 0, deg = 0;
+      if (act) {
+        const uint32_t v = (unit * 32 + o) * 32 + select_bit(ob, r - oe);
+        beg = P.ro[v];
+        deg = P.ro[v + 1] - beg;
+        if (deg >= kHeavy) deg = 0;  // expanded through the heavy list
+      }
+      expand_group(L, beg, deg);
+    }
+  }
+  // heavy chunks continue the warp numbering after the summary words
+  push_heavy(L, hv, hs, n_heavy, n_chunks, w1, w1 + n_chunks);
+}
+
+__device__ __forceinline__ void push_cta(Level& L, const uint32_t* fb_cur, const uint32_t* sm_cur, const uint32_t* hv,
+                                         const uint32_t* hs, uint32_t n_heavy, uint32_t n_chunks) {
+  const Params& P = *L.P;
+  Shared& S = *L.S;
+  const uint32_t t = threadIdx.x, lane = t & 31, wl = t >> 5;
+  const uint32_t ngroups = (P.w0 + 15) / 16;
+  for (uint32_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    const uint32_t s16 = (ld_cg(sm_cur + (g >> 1)) >> ((g & 1) * 16)) & 0xffffu;
+    if (!s16) continue;  // the same for every thread of the CTA
+    const uint32_t w = g * 16 + wl;
+    const uint32_t word = (((s16 >> wl) & 1u) && w < P.w0) ? ld_cg(fb_cur + w) : 0u;
+    const bool act = (word >> lane) & 1u;
+    const uint32_t v = w * 32 + lane;
+    const uint32_t beg = act ? P.ro[v] : 0u;
+    uint32_t deg = act ? P.ro[v + 1] - beg : 0u;
+    if (deg >= kHeavy) deg = 0;
+    uint32_t total;
+    const uint32_t excl = sygraph::detail::block_excl_scan(deg, &total, S.scan);
+    S.beg[t] = beg;
+    S.incl[t] = excl + deg;
+    __syncthreads();
+    for (uint32_t r = t; r < total; r += blockDim.x) {
+      const uint32_t slot = smem_upper_bound(S.incl, blockDim.x, r);
+      const uint32_t before = slot ? S.incl[slot - 1] : 0u;
+      L.visit_push(P.col[S.beg[slot] + (r - before)]);
+    }
+    __syncthreads();
+  }
+  push_heavy(L, hv, hs, n_heavy, n_chunks, 0, n_chunks);
+}
+
+__device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool short_circuit) {
+  const Params& P = *L.P;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool same = P.iro == P.ro;
+  for (uint32_t wi = gwarp; wi < P.w0; wi += nwarps) {
+    const uint32_t vw = ld_cg(P.visited + wi);
+    const uint32_t cand = ~vw & valid_bits(wi, P.w0, P.n);
+    if (!cand) continue;
+    const uint32_t v = wi * 32 + lane;
+    const bool mine = (cand >> lane) & 1u;
+    const uint32_t beg = mine ? P.iro[v] : 0u;
+    const uint32_t end = mine ? P.iro[v + 1] : 0u;
+    bool found = false;
+    uint32_t e = beg;
+    const uint32_t lim = short_circuit ? min(end, beg + kPullSerial) : end;
+    // the next column index is loaded while the current frontier bit is tested
+    uint32_t c = e < lim ? P.icol[e] : 0u;
+    while (e < lim) {
+      const uint32_t cn = e + 1 < lim ? P.icol[e + 1] : 0u;
+      if (bit_test(fb_cur, c)) {
+        found = true;
+        if (short_circuit) break;
+      }
+      c = cn;
+      e++;
+    }
+    if (short_circuit) {
+      // long lists that are still unresolved: the whole warp scans them
+      uint32_t left = __ballot_sync(kFullMask, mine && !found && e < end);
+      while (left) {
+        const uint32_t j = __ffs(left) - 1;
+        left &= left - 1;
+        const uint32_t jb = __shfl_sync(kFullMask, e, j);
+        const uint32_t je = __shfl_sync(kFullMask, end, j);
+        bool hit = false;
+        for (uint32_t eb = jb; eb < je; eb += 32) {
+          const uint32_t ee = eb + lane;
+          const bool h = ee < je && bit_test(fb_cur, P.icol[ee]);
+          if (__any_sync(kFullMask, h)) {
+            hit = true;
+            break;
+          }
+        }
+        if (lane == j) found = hit;
+      }
+    }
+    const uint32_t fmask = __ballot_sync(kFullMask, found);
+    if (fmask) {
+      if (found) L.discovered(v, same ? (end - beg) : (P.ro[v + 1] - P.ro[v]));
+      if (lane == 0) L.publish_word(wi, vw, fmask);
+    }
+  }
+}
+
+__device__ __forceinline__ void pull_cta(Level& L, const uint32_t* fb_cur, bool short_circuit) {
+  const Params& P = *L.P;
+  Shared& S = *L.S;
+  const uint32_t t = threadIdx.x, lane = t & 31, wl = t >> 5;
+  const uint32_t ngroups = (P.w0 + 15) / 16;
+  const bool same = P.iro == P.ro;
+  volatile uint32_t* flag = S.flag;
+  for (uint32_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    const uint32_t w = g * 16 + wl;
+    const uint32_t vw = w < P.w0 ? ld_cg(P.visited + w) : 0xffffffffu;
+    const uint32_t cand = w < P.w0 ? (~vw & valid_bits(w, P.w0, P.n)) : 0u;
+    if (!__syncthreads_or(cand != 0)) continue;
+    const bool mine = (cand >> lane) & 1u;
+    const uint32_t v = w * 32 + lane;
+    const uint32_t beg = mine ? P.iro[v] : 0u;
+    const uint32_t deg = mine ? P.iro[v + 1] - beg : 0u;
+    uint32_t total;
+    const uint32_t excl = sygraph::detail::block_excl_scan(deg, &total, S.scan);
+    S.beg[t] = beg;
+    S.incl[t] = excl + deg;
+    flag[t] = 0u;
+    __syncthreads();
+    for (uint32_t r = t; r < total; r += blockDim.x) {
+      const uint32_t slot = smem_upper_bound(S.incl, blockDim.x, r);
+      if (short_circuit && flag[slot]) continue;
+      const uint32_t before = slot ? S.incl[slot - 1] : 0u;
+      if (bit_test(fb_cur, P.icol[S.beg[slot] + (r - before)])) flag[slot] = 1u;
+    }
+    __syncthreads();
+    const bool found = mine && flag[t];
+    const uint32_t fmask = __ballot_sync(kFullMask, found);
+    if (found) L.discovered(v, same ? deg : (P.ro[v + 1] - P.ro[v]));
+    if (lane == 0 && fmask) L.publish_word(w, vw, fmask);
+    __syncthreads();
+  }
+}
+
+}  // namespace bfs
+}  // namespace sgb

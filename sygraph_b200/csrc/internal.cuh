@@ -89,6 +89,9 @@ inline unsigned grid_for(uint64_t work_items, unsigned block, unsigned per_sm = 
   return (unsigned)(need < cap ? need : cap);
 }
 
+// Device address of an sg_mlp's parameter block (selector.cu).
+const void* mlp_device_params(sg_mlp h);
+
 // ------------------------------------------------------------------ handles --
 struct GraphDir {
   uint32_t* ro = nullptr;

@@ -1,0 +1,240 @@
+"""Training pipeline of the learned BFS strategy selector.
+
+BFS levels are unique, so level L visits the same frontier whichever
+strategies ran before it: timing every level under each of the six forced
+strategies (one traversal per strategy, repeated, median per level) gives the
+full per-level cost table of a (graph, source) pair.  One training sample per
+level and strategy run: the twelve features the engine logged for that level
+(the same device code computes them at inference) and the six measured
+log-times; the loss is masked MSE on log-time and the MLP trains on the GPU
+(sg_mlp_train).  Evaluation reports, per traversal, the summed level time of
+the heuristic's choices, of the MLP's choices and of the per-level best.
+
+    python -m sygraph_b200.train_selector collect --out data.npz
+    python -m sygraph_b200.train_selector train --data data.npz --model selector_b200.npz
+    python -m sygraph_b200.train_selector evaluate --data held_out.npz --model selector_b200.npz
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import algorithms, build, io
+from .selector import IN, OUT, STRATEGIES, MODEL_PATH, Mlp
+
+HYBRID_ALPHA, HYBRID_BETA = 15.0, 24.0
+MAX_LEVELS = 4096
+
+# (name, generator, kwargs): RMAT skews and scales, grids with and without
+# long-range pairs, uniform random graphs.  The held-out set uses other seeds
+# and larger scales than any training graph.
+TRAIN_GRAPHS = [
+    ("rmat16", "rmat", dict(scale=16, seed=11)),
+    ("rmat18", "rmat", dict(scale=18, seed=12)),
+    ("rmat20", "rmat", dict(scale=20, seed=13)),
+    ("rmat20_ef8", "rmat", dict(scale=20, edge_factor=8, seed=14)),
+    ("rmat21_flat", "rmat", dict(scale=21, a=0.45, b=0.22, c=0.22, seed=15)),
+    ("rmat21_skew", "rmat", dict(scale=21, a=0.65, b=0.15, c=0.15, seed=16)),
+    ("rmat22", "rmat", dict(scale=22, seed=17)),
+    ("uniform20", "rmat", dict(scale=20, a=0.25, b=0.25, c=0.25, seed=18)),
+    ("grid512", "grid", dict(side=512, long_range_frac=0.0, seed=19)),
+    ("grid1024_lr", "grid", dict(side=1024, long_range_frac=0.02, seed=20)),
+    ("grid2048_lr", "grid", dict(side=2048, long_range_frac=0.005, seed=21)),
+]
+EVAL_GRAPHS = [
+    ("rmat22_heldout", "rmat", dict(scale=22, seed=101)),
+    ("rmat23", "rmat", dict(scale=23, seed=102)),
+    ("grid4096_lr", "grid", dict(side=4096, long_range_frac=0.01, seed=103)),
+    ("uniform21", "rmat", dict(scale=21, a=0.25, b=0.25, c=0.25, seed=104)),
+]
+
+
+def make_graph(kind: str, kw: dict):
+    return io.rmat(**kw) if kind == "rmat" else io.grid(**kw)
+
+
+def _forced_levels(bfs, source: int, strategy: int, reps: int):
+    """Median level times (us) and the logged features of one forced run."""
+    bfs.set_schedule([strategy] * MAX_LEVELS)
+    times, feats = [], None
+    for _ in range(reps):
+        bfs.init(source)
+        bfs.run(algorithms.bfs_direction.hybrid, HYBRID_ALPHA, HYBRID_BETA)
+        times.append(bfs.level_times_us())
+        if feats is None:
+            feats = bfs.level_features()
+    bfs.set_schedule(None)
+    return np.median(np.stack(times), 0), feats
+
+
+def profile_traversal(bfs, source: int, reps: int = 5) -> dict:
+    """Per-level cost table t[L, s] and features for one (graph, source)."""
+    t, F = [], []
+    for s in range(OUT):
+        ts, fs = _forced_levels(bfs, source, s, reps)
+        t.append(ts)
+        F.append(fs)
+    levels = min(len(x) for x in t)
+    T = np.stack([x[:levels] for x in t], 1)  # levels x 6
+    Fe = np.stack([f[:levels] for f in F], 0)  # 6 x levels x 12
+    # the heuristic's own schedule (reference hybrid) on the same source
+    bfs.init(source)
+    bfs.run(algorithms.bfs_direction.hybrid, HYBRID_ALPHA, HYBRID_BETA)
+    h = np.array([r["strategy"] for r in bfs.level_records()][:levels], np.int32)
+    return {"T": T, "F": Fe, "heuristic": h}
+
+
+def collect(graphs, sources_per_graph: int = 6, reps: int = 5, log=print) -> dict:
+    """Training samples (X, Y, M, group) plus, per traversal, its cost table,
+    the heuristic's schedule and the push/warp run's features, concatenated
+    over levels with `offsets` marking each traversal."""
+    X, Y, M, group, H, TT, F0 = [], [], [], [], [], [], []
+    names = []
+    gid = 0
+    for name, kind, kw in graphs:
+        t0 = time.time()
+        csr = make_graph(kind, kw)
+        G = build.fromCSR(csr)
+        bfs = algorithms.BFS(G)
+        bfs.log_features(True)
+        srcs = [int(np.argmax(csr.degrees()))] + [int(s) for s in io.sample_sources(csr, sources_per_graph - 1,
+                                                                                     seed=gid + 7)]
+        for src in srcs:
+            p = profile_traversal(bfs, src, reps)
+            logT = np.log(np.maximum(p["T"], 0.05))
+            for s in range(OUT):
+                for L in range(p["T"].shape[0]):
+                    X.append(p["F"][s, L])
+                    Y.append(logT[L])
+                    M.append(np.ones(OUT, np.float32))
+                    group.append(gid)
+            H.append(p["heuristic"])
+            TT.append(p["T"])
+            F0.append(p["F"][0])
+            names.append(f"{name}:{src}")
+            gid += 1
+        log(f"{name}: n={csr.n} m={csr.m} sources={len(srcs)} {time.time() - t0:.1f}s")
+        del bfs, G
+    lens = [len(t) for t in TT]
+    return {
+        "X": np.asarray(X, np.float32), "Y": np.asarray(Y, np.float32), "M": np.asarray(M, np.float32),
+        "group": np.asarray(group, np.int32), "names": np.asarray(names),
+        "T": np.concatenate(TT).astype(np.float32), "H": np.concatenate(H).astype(np.int32),
+        "F0": np.concatenate(F0).astype(np.float32), "offsets": np.concatenate([[0], np.cumsum(lens)]).astype(np.int64),
+    }
+
+
+def traversals(data: dict):
+    """(name, T[levels,6], heuristic[levels], features[levels,12]) per traversal."""
+    o = data["offsets"]
+    for i in range(len(o) - 1):
+        a, b = int(o[i]), int(o[i + 1])
+        yield str(data["names"][i]), data["T"][a:b], data["H"][a:b], data["F0"][a:b]
+
+
+def simulate_choices(mlp: Mlp, F: np.ndarray, heuristic: np.ndarray, allowed: int = 0x3F) -> np.ndarray:
+    """The learned mode's schedule on a traversal: the MLP's argmin per level
+    with the current-direction feature following its own previous choice, the
+    heuristic where a feature leaves the trusted range (as the engine does)."""
+    p = mlp.params
+    t0 = p.size - 4 * IN
+    lo, hi = p[t0 + 2 * IN:t0 + 3 * IN], p[t0 + 3 * IN:t0 + 4 * IN]
+    out = np.empty(len(F), np.int32)
+    prev = 0
+    for L in range(len(F)):
+        f = F[L].copy()
+        if L > 0:
+            f[10] = 1.0 if prev >= 2 else 0.0
+        if np.any(f < lo) or np.any(f > hi):
+            out[L] = heuristic[L]
+        else:
+            out[L] = int(mlp.choose(f[None, :], allowed)[0])
+        prev = out[L]
+    return out
+
+
+def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F) -> dict:
+    """Summed level time (us) per traversal under the heuristic's schedule,
+    the MLP's schedule and the per-level best; totals and regret."""
+    rows = []
+    for name, T, H, F in traversals(data):
+        c = simulate_choices(mlp, F, H, allowed)
+        idx = np.arange(len(T))
+        rows.append({"traversal": name, "levels": len(T), "heuristic_us": float(T[idx, H].sum()),
+                     "learned_us": float(T[idx, c].sum()), "best_us": float(T.min(1).sum()),
+                     "learned_schedule": "".join(map(str, c)), "heuristic_schedule": "".join(map(str, H))})
+    tot = {k: sum(r[k] for r in rows) for k in ("heuristic_us", "learned_us", "best_us")}
+    tot["speedup_vs_heuristic"] = tot["heuristic_us"] / max(tot["learned_us"], 1e-9)
+    tot["regret_learned"] = tot["learned_us"] / max(tot["best_us"], 1e-9) - 1.0
+    tot["regret_heuristic"] = tot["heuristic_us"] / max(tot["best_us"], 1e-9) - 1.0
+    return {"total": tot, "traversals": rows}
+
+
+def train(data: dict, steps: int = 6000, lr: float = 3e-3, seed: int = 0, holdout_groups: int = 0) -> Mlp:
+    """Fit the MLP on the GPU; normalisation and trusted range from X."""
+    X, Y, M = data["X"], data["Y"], data["M"]
+    rng = np.random.default_rng(seed)
+    I, H, O = IN, 32, OUT
+    p = np.zeros(H * I + H + H * H + H + O * H + O + 4 * I, np.float32)
+    # He-uniform initialisation of the trainable block
+    k = 0
+    for rows, cols in ((H, I), (H, H), (O, H)):
+        lim = np.sqrt(6.0 / cols)
+        p[k:k + rows * cols] = rng.uniform(-lim, lim, rows * cols)
+        k += rows * cols + rows
+    p[k - O:k] = float(Y.mean())  # output bias starts at the mean log-time
+    mlp = Mlp(p)
+    mlp.set_normalisation(X)
+    mlp.train(X, Y, M, steps=steps, lr=lr)
+    return mlp
+
+
+def _save(data: dict, path: str) -> None:
+    np.savez_compressed(path, **data)
+
+
+def _load(path: str) -> dict:
+    with np.load(path) as d:
+        return {k: d[k] for k in d.files}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    c = sub.add_parser("collect")
+    c.add_argument("--out", required=True)
+    c.add_argument("--set", choices=["train", "eval"], default="train")
+    c.add_argument("--sources", type=int, default=6)
+    c.add_argument("--reps", type=int, default=5)
+    t = sub.add_parser("train")
+    t.add_argument("--data", required=True)
+    t.add_argument("--model", default=str(MODEL_PATH))
+    t.add_argument("--steps", type=int, default=6000)
+    t.add_argument("--lr", type=float, default=3e-3)
+    e = sub.add_parser("evaluate")
+    e.add_argument("--data", required=True)
+    e.add_argument("--model", default=str(MODEL_PATH))
+    e.add_argument("--json", default=None)
+    a = ap.parse_args(argv)
+    if a.cmd == "collect":
+        _save(collect(TRAIN_GRAPHS if a.set == "train" else EVAL_GRAPHS, a.sources, a.reps), a.out)
+    elif a.cmd == "train":
+        data = _load(a.data)
+        mlp = train(data, a.steps, a.lr)
+        rep = evaluate(mlp, data)
+        mlp.save(a.model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
+        print(json.dumps(rep["total"]))
+    else:
+        rep = evaluate(Mlp.load(a.model), _load(a.data))
+        print(json.dumps(rep["total"]))
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(rep, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
