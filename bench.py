@@ -191,6 +191,16 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def _launch_ms(torch, fn) -> float:
+    """Device time of what `fn` enqueues, by CUDA events on the current stream."""
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    fn()
+    b.record()
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
 def cpu_baseline(g, srcs, sg):
     import oracle
     cores = os.cpu_count() or 1
@@ -359,6 +369,39 @@ def main():
     sg._lib.call("sg_free_host_pinned", hp_dst)
     sg._lib.call("sg_free_device", dsrc)
 
+    # learned selector (committed model) on the same sources, and on a held-out
+    # 4096 x 4096 grid with 2% long-range pairs, against the reference heuristic
+    from sygraph_b200 import selector
+    mlp = selector.Mlp.load()
+    learned = {"model": "sygraph_b200/models/selector_b200.npz"}
+    bfs.set_selector(mlp)
+    learned_ms = float(np.mean([_launch_ms(torch, lambda s=s: (bfs.init(int(s)), bfs.run_async(3, ALPHA, BETA)))
+                                for s in srcs]))
+    learned.update({"rmat_launch_ms": learned_ms, "rmat_heuristic_launch_ms": kern_ms,
+                    "rmat_speedup_vs_heuristic": kern_ms / learned_ms})
+    gg = sg.io.grid(4096, long_range_frac=0.02, seed=103)
+    Gg = sg.graph.build.fromCSR(gg)
+    bg = sg.algorithms.BFS(Gg)
+    bg.set_selector(mlp)
+    gsrc = sg.io.sample_sources(gg, 4, seed=SOURCE_SEED)
+    same = True
+    t_h, t_l = [], []
+    for s in gsrc:
+        bg.init(int(s))
+        bg.run(2, ALPHA, BETA)
+        d_h = bg.getDistances()
+        bg.init(int(s))
+        bg.run(3, ALPHA, BETA)
+        same &= bool(np.array_equal(d_h, bg.getDistances()))
+        for _ in range(3):
+            t_h.append(_launch_ms(torch, lambda s=s: (bg.init(int(s)), bg.run_async(2, ALPHA, BETA))))
+            t_l.append(_launch_ms(torch, lambda s=s: (bg.init(int(s)), bg.run_async(3, ALPHA, BETA))))
+    learned.update({"grid4096_heuristic_ms": float(np.median(t_h)), "grid4096_learned_ms": float(np.median(t_l)),
+                    "grid4096_speedup_vs_heuristic": float(np.median(t_h) / np.median(t_l)),
+                    "identical_depths": same})
+    bfs.set_selector(None)
+    del bg, Gg, gg
+
     # the same 64 sources as one bit-parallel batch (one launch); identical depths
     mbfs = sg.algorithms.MultiBFS(G, len(srcs))
     for _ in range(2):
@@ -427,6 +470,7 @@ def main():
                                      "peak": peak, "unit": "GB/s",
                                      "frac": ms_bytes / (batched_ms * 1e-3) / 1e9 / peak,
                                      "bytes_per_launch": ms_bytes, "traffic": ncu_traffic("msbfs_kernel")}},
+            "learned": learned,
             "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
                      "roofline": {"bound": "hbm", "achieved": sssp_achieved, "peak": peak, "unit": "GB/s",
                                   "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,

@@ -126,6 +126,9 @@ __device__ __forceinline__ T block_sum(T v, T* s_red) {
 __device__ __forceinline__ bool bit_test(const uint32_t* bm, uint32_t i) {
   return (ld_cg(bm + (i >> 5)) >> (i & 31)) & 1u;
 }
+// L1-cached test, for a bitmap nobody writes until the next grid barrier (a
+// frontier being expanded): the barrier's acquire fence orders these weak
+// loads after every write of the previous level.
 __device__ __forceinline__ bool bit_test_ro(const uint32_t* bm, uint32_t i) {
   return (bm[i >> 5] >> (i & 31)) & 1u;
 }

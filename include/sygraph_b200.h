@@ -353,6 +353,9 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
                              float beta);
 sg_status sg_msbfs_get_depths(sg_msbfs h, uint32_t* host_depth);
 sg_status sg_msbfs_depths_device(sg_msbfs h, const uint32_t** dev_depth);
+/* Per-level log of the last batch (strategy 0 push / 2 pull, sizes and
+ * degrees of the frontier union, device timestamps), as sg_bfs_level_records. */
+sg_status sg_msbfs_level_records(sg_msbfs h, sg_level_record* host_records, uint32_t cap, uint32_t* count);
 
 /* Learned strategy selector (no counterpart in the reference, whose
  * direction choice is the degree-threshold heuristic of bfs.hpp:325-350): a

@@ -148,6 +148,7 @@ SIGNATURES = {
     "sg_mlp_gradient": (st, [vp, vp, vp, vp, C.c_uint32, f32p, f32p]),
     "sg_mlp_train": (st, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, f32p]),
     "sg_msbfs_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
+    "sg_msbfs_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
     "sg_msbfs_destroy": (st, [vp]),
     "sg_msbfs_run": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float, C.POINTER(MsbfsDetails)]),
     "sg_msbfs_run_async": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float]),

@@ -135,6 +135,12 @@ class MultiBFS:
         call("sg_msbfs_run_async", self.handle, _ptr(src), src.size, direction, alpha, beta)
         self.k = src.size
 
+    def level_records(self) -> list[dict]:
+        recs = (_lib.LevelRecord * _lib.SG_MAX_LOGGED_LEVELS)()
+        cnt = C.c_uint32()
+        call("sg_msbfs_level_records", self.handle, recs, _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
+        return [{k: getattr(recs[i], k) for k, _ in _lib.LevelRecord._fields_} for i in range(cnt.value)]
+
     def getDistances(self) -> np.ndarray:
         """k x n depths (row s: depths from sources[s])."""
         out = np.empty((self.k, self.G.getVertexCount()), np.uint32)

@@ -157,7 +157,7 @@ __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool
     uint32_t c = e < lim ? P.icol[e] : 0u;
     while (e < lim) {
       const uint32_t cn = e + 1 < lim ? P.icol[e + 1] : 0u;
-      if (bit_test(fb_cur, c)) {
+      if (bit_test_ro(fb_cur, c)) {
         found = true;
         if (short_circuit) break;
       }
@@ -175,7 +175,7 @@ __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool
         bool hit = false;
         for (uint32_t eb = jb; eb < je; eb += 32) {
           const uint32_t ee = eb + lane;
-          const bool h = ee < je && bit_test(fb_cur, P.icol[ee]);
+          const bool h = ee < je && bit_test_ro(fb_cur, P.icol[ee]);
           if (__any_sync(kFullMask, h)) {
             hit = true;
             break;
@@ -218,7 +218,7 @@ __device__ __forceinline__ void pull_cta(Level& L, const uint32_t* fb_cur, bool 
       const uint32_t slot = smem_upper_bound(S.incl, blockDim.x, r);
       if (short_circuit && flag[slot]) continue;
       const uint32_t before = slot ? S.incl[slot - 1] : 0u;
-      if (bit_test(fb_cur, P.icol[S.beg[slot] + (r - before)])) flag[slot] = 1u;
+      if (bit_test_ro(fb_cur, P.icol[S.beg[slot] + (r - before)])) flag[slot] = 1u;
     }
     __syncthreads();
     const bool found = mine && flag[t];

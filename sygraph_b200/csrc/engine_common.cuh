@@ -14,6 +14,7 @@ namespace sgb {
 namespace eng {
 
 using sygraph::detail::bit_test;
+using sygraph::detail::bit_test_ro;
 using sygraph::detail::GridBarrier;
 using sygraph::detail::grid_sync;
 using sygraph::detail::kFullMask;

@@ -11,9 +11,14 @@
 //         atomicOr on seen[u] claims the bits, atomicOr on F'[u] publishes them
 //   pull: for every u not done: OR the frontier masks of its in-neighbours,
 //         stopping once every missing source is covered; u owns seen[u]
-// Depths land in a source-major k x n array: pull writes for one source are
-// coalesced across the warp's 32 consecutive vertices.  Entries never
-// reached are filled with n+1 at the end.  One grid barrier per level.
+// No depth is stored during the traversal.  When F_{L-1} is cleared, each
+// active vertex folds its mask into the depth bit-planes: plane b holds, per
+// source bit, bit b of the vertex's depth, so v's planes get F_{L-1}[v] OR-ed
+// into every plane b with bit b of L-1 set (one writer per vertex and level).
+// After the last level one pass turns planes + seen into the source-major
+// k x n depth array with full coalesced row stores (n+1 where a source never
+// reached the vertex).  Plane b is zeroed at level 2^b, one level before its
+// first fold.  One grid barrier per level.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -60,7 +65,9 @@ struct Params {
   uint32_t heavy_cap;
   LevelCounters* cnt;
   GridBarrier* bar;
-  uint32_t* depth;   // k * n, source-major
+  u64* planes;       // n_planes * n: bit b of each (source, vertex) depth
+  uint32_t n_planes;
+  uint32_t* depth;   // k * n, source-major, written after the last level
   sg_level_record* log;
   u64* result;       // [iterations, push, pull, reached_edges]
 };
@@ -112,7 +119,6 @@ struct Level {
       done_deg += du;
       atomicOr(P->done + (u >> 5), 1u << (u & 31));
     }
-    for (u64 x = nw; x; x &= x - 1) st_cg(P->depth + (size_t)(__ffsll(x) - 1) * P->n + u, next_depth);
     if (atomicOr(F_next + u, nw) == 0) {
       const uint32_t b = 1u << (u & 31);
       if (atomicOr(fa_next + (u >> 5), b) == 0) atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31));
@@ -142,6 +148,37 @@ __device__ __forceinline__ void expand_group(Level& L, uint32_t beg, uint32_t de
     const uint32_t oe = __shfl_sync(kFullMask, excl, o);
     const u64 of = shfl64(fv, o);
     if (act) L.visit_push(L.P->col[ob + (r - oe)], of);
+  }
+}
+
+// Source-major depths of a warp's 32 consecutive vertices: bit b of depth(s, u)
+// is bit s of plane b (planes below pb; F_last carries depth `last`); n+1
+// where source s never reached u.  Every row store is a full 128-byte line.
+template <int PB>
+__device__ __forceinline__ void materialise(const Params& P, const u64* F_last, uint32_t last, uint32_t pb) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n = P.n;
+  for (uint32_t wi = gwarp; wi < P.w0; wi += nwarps) {
+    const uint32_t u = wi * 32 + lane;
+    const bool in = u < n;
+    const u64 sn = in ? ld_cg(P.seen + u) : 0ull;
+    const u64 fl = in ? ld_cg(F_last + u) : 0ull;
+    u64 pl[PB];
+#pragma unroll
+    for (int b = 0; b < PB; b++) {
+      u64 x = (in && (uint32_t)b < pb) ? ld_cg(P.planes + (size_t)b * n + u) : 0ull;
+      if ((last >> b) & 1u) x |= fl;
+      pl[b] = x;
+    }
+    if (!in) continue;
+    for (uint32_t s = 0; s < P.k; s++) {
+      uint32_t d = 0;
+#pragma unroll
+      for (int b = 0; b < PB; b++) d |= (uint32_t)((pl[b] >> s) & 1ull) << b;
+      __stcs(P.depth + (size_t)s * n + u, ((sn >> s) & 1ull) ? d : n + 1);
+    }
   }
 }
 
@@ -183,7 +220,6 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
       const u64 before = P.F[s];
       P.seen[s] |= bit;
       P.F[s] = before | bit;
-      P.depth[(size_t)i * n + s] = 0;
       if (before == 0) {
         const uint32_t d = P.ro[s + 1] - P.ro[s];
         cnt++;
@@ -263,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
               const uint32_t v = (unit * 32 + o) * 32 + select_bit(ob, r - oe);
               beg = P.ro[v];
               deg = P.ro[v + 1] - beg;
-              fv = ld_cg(F_cur + v);
+              fv = F_cur[v];  // read-only until the next barrier: L1-cached
               if (deg >= kHeavy) deg = 0;
             }
             expand_group(L, beg, deg, fv);
@@ -275,7 +311,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
           const uint32_t first = ld_cg(hs_cur + ent);
           const uint32_t cb = P.ro[v] + (c - first) * kChunk;
           const uint32_t ce = min(P.ro[v + 1], cb + kChunk);
-          const u64 fv = ld_cg(F_cur + v);
+          const u64 fv = F_cur[v];  // read-only until the next barrier: L1-cached
           for (uint32_t eb = cb; eb < ce; eb += 32) {
             const uint32_t e = eb + lane;
             if (e < ce) L.visit_push(P.col[e], fv);
@@ -300,7 +336,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
         while (e < lim && (acc | su) != P.all) {
           const uint32_t c0 = P.icol[e];
           const uint32_t c1 = e + 1 < lim ? P.icol[e + 1] : c0;
-          acc |= ld_cg(F_cur + c0) | ld_cg(F_cur + c1);
+          acc |= F_cur[c0] | F_cur[c1];
           e += 2;
         }
         if (e > lim) e = lim;
@@ -314,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
           u64 part = 0;
           for (uint32_t eb = jb; eb < je; eb += 32) {
             const uint32_t ee = eb + lane;
-            if (ee < je) part |= ld_cg(F_cur + P.icol[ee]);
+            if (ee < je) part |= F_cur[P.icol[ee]];
             // warp OR-reduce, stop once everything missing is covered
             u64 r = part;
 #pragma unroll
@@ -337,15 +373,6 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
           if ((su | nw) == P.all) L.done_deg += du;
           if (du >= kHeavy) L.add_heavy(u, du);
         }
-        // depth of each newly reached (source, vertex): one coalesced row per source
-        u64 any = got ? nw : 0ull;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) any |= ((u64)__shfl_xor_sync(kFullMask, (uint32_t)(any >> 32), d) << 32) |
-                                                __shfl_xor_sync(kFullMask, (uint32_t)any, d);
-        for (u64 x = any; x; x &= x - 1) {
-          const uint32_t s = __ffsll(x) - 1;
-          if (got && ((nw >> s) & 1ull)) st_cg(P.depth + (size_t)s * n + u, level + 1);
-        }
         const uint32_t gmask = __ballot_sync(kFullMask, got);
         const uint32_t dmask = __ballot_sync(kFullMask, mine && (su | nw) == P.all);
         if (lane == 0) {
@@ -357,16 +384,36 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
         }
       }
     }
-    // clear F_{L-1}
-    for (uint32_t j = gwarp; j < w1; j += nwarps) {
-      const uint32_t s = ld_cg(sm_zero + j);
-      if (!s) continue;
-      const uint32_t w = j * 32 + lane;
-      const uint32_t bits = ((s >> lane) & 1u) ? ld_cg(fa_zero + w) : 0u;
-      for (uint32_t b = bits; b; b &= b - 1) st_cg(F_zero + w * 32 + (__ffs(b) - 1), 0ull);
-      if ((s >> lane) & 1u) st_cg(fa_zero + w, 0u);
-      __syncwarp();
-      if (lane == 0) st_cg(sm_zero + j, 0u);
+    // plane b is first folded at level 2^b + 1: zero it now
+    if (level && !(level & (level - 1))) {
+      u64* pz = P.planes + (size_t)(__ffs(level) - 1) * n;
+      for (uint32_t i = gtid; i < n; i += nthreads) st_cg(pz + i, 0ull);
+    }
+    // fold F_{L-1} (depth L-1) into the planes and clear it, one fa word per warp step
+    if (level) {
+      const uint32_t dprev = level - 1;
+      for (uint32_t j = gwarp; j < w1; j += nwarps) {
+        const uint32_t s = ld_cg(sm_zero + j);
+        if (!s) continue;
+        for (uint32_t x = s; x; x &= x - 1) {
+          const uint32_t w = j * 32 + (__ffs(x) - 1);
+          const uint32_t word = ld_cg(fa_zero + w);
+          if ((word >> lane) & 1u) {
+            const uint32_t v = w * 32 + lane;
+            const u64 f = ld_cg(F_zero + v);
+            uint32_t b = 0;
+            for (uint32_t d = dprev; d; d >>= 1, b++)
+              if (d & 1u) {
+                u64* p = P.planes + (size_t)b * n + v;
+                st_cg(p, ld_cg(p) | f);
+              }
+            st_cg(F_zero + v, 0ull);
+          }
+        }
+        __syncwarp();
+        if ((s >> lane) & 1u) st_cg(fa_zero + j * 32 + lane, 0u);
+        if (lane == 0) st_cg(sm_zero + j, 0u);
+      }
     }
     __syncthreads();
     {
@@ -434,19 +481,18 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
     frontier_deg = next_deg;
     if (next_size == 0) break;
   }
-  // entries never reached: n+1 (one coalesced row store per source and warp)
-  for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
-    const uint32_t u = wi * 32 + lane;
-    const bool in = u < n;
-    const u64 miss = in ? (P.all & ~ld_cg(P.seen + u)) : 0ull;
-    u64 any = miss;
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) any |= ((u64)__shfl_xor_sync(kFullMask, (uint32_t)(any >> 32), d) << 32) |
-                                            __shfl_xor_sync(kFullMask, (uint32_t)any, d);
-    for (u64 x = any; x; x &= x - 1) {
-      const uint32_t s = __ffsll(x) - 1;
-      if ((miss >> s) & 1ull) st_cg(P.depth + (size_t)s * n + u, n + 1);
-    }
+  // depths from the planes; F of the last level (depth `level`) is folded in registers
+  {
+    const uint32_t pb = level ? 32 - __clz(level) : 0;
+    const u64* F_last = P.F + (size_t)(level % 3) * n;
+    if (pb <= 4)
+      materialise<4>(P, F_last, level, pb);
+    else if (pb <= 8)
+      materialise<8>(P, F_last, level, pb);
+    else if (pb <= 16)
+      materialise<16>(P, F_last, level, pb);
+    else
+      materialise<32>(P, F_last, level, pb);
   }
   if (gtid == 0) {
     P.result[0] = level + 1;
@@ -480,6 +526,8 @@ struct sg_msbfs_s {
   uint32_t *fa = nullptr, *sm = nullptr, *done = nullptr, *no_in = nullptr;
   uint32_t *heavy_v = nullptr, *heavy_s = nullptr;
   uint32_t* sources = nullptr;
+  unsigned long long* planes = nullptr;
+  uint32_t n_planes = 0;
   uint32_t* depth = nullptr;
   ms::LevelCounters* cnt = nullptr;
   sygraph::detail::GridBarrier* bar = nullptr;
@@ -499,6 +547,7 @@ static void msbfs_release(sg_msbfs h) {
   dev_free(h->heavy_v);
   dev_free(h->heavy_s);
   dev_free(h->sources);
+  dev_free(h->planes);
   dev_free(h->depth);
   dev_free(h->cnt);
   dev_free(h->bar);
@@ -522,8 +571,11 @@ sg_status sg_msbfs_create(sg_graph g, uint32_t max_sources, sg_msbfs* out) {
   h->w1 = div_up(h->w0, 32);
   h->heavy_cap = (uint32_t)std::min<uint64_t>(g->n, g->m / ms::kHeavy + 1);
   const uint64_t n = g->n;
+  // depths are below n: planes for the bits of n - 1 (at least one)
+  h->n_planes = 1;
+  while (h->n_planes < 32 && (n - 1) >> h->n_planes) h->n_planes++;
   sg_status s;
-  if ((s = dev_alloc(&h->seen, n)) || (s = dev_alloc(&h->F, 3 * n)) || (s = dev_alloc(&h->fa, 3ull * h->w0)) ||
+  if ((s = dev_alloc(&h->planes, (uint64_t)h->n_planes * n)) || (s = dev_alloc(&h->seen, n)) || (s = dev_alloc(&h->F, 3 * n)) || (s = dev_alloc(&h->fa, 3ull * h->w0)) ||
       (s = dev_alloc(&h->sm, 3ull * h->w1)) || (s = dev_alloc(&h->done, h->w0)) || (s = dev_alloc(&h->no_in, h->w0)) ||
       (s = dev_alloc(&h->heavy_v, 2ull * h->heavy_cap)) || (s = dev_alloc(&h->heavy_s, 2ull * h->heavy_cap)) ||
       (s = dev_alloc(&h->sources, 64)) || (s = dev_alloc(&h->depth, (uint64_t)max_sources * n)) ||
@@ -586,6 +638,8 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
   P.heavy_cap = h->heavy_cap;
   P.cnt = h->cnt;
   P.bar = h->bar;
+  P.planes = h->planes;
+  P.n_planes = h->n_planes;
   P.depth = h->depth;
   P.log = h->log;
   P.result = h->result;
@@ -617,6 +671,18 @@ sg_status sg_msbfs_get_depths(sg_msbfs h, uint32_t* host_depth) {
   SG_CUDA(cudaMemcpyAsync(host_depth, h->depth, sizeof(uint32_t) * (uint64_t)h->last_k * h->g->n,
                           cudaMemcpyDeviceToHost, h->g->stream));
   SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  return SG_OK;
+}
+
+sg_status sg_msbfs_level_records(sg_msbfs h, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
+  SG_REQUIRE(h && count, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  unsigned long long it = 0;
+  if (h->last_k) SG_CUDA(cudaMemcpy(&it, h->result, sizeof(it), cudaMemcpyDeviceToHost));
+  uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
+  if (k > cap) k = cap;
+  if (host_records && k) SG_CUDA(cudaMemcpy(host_records, h->log, sizeof(sg_level_record) * k, cudaMemcpyDeviceToHost));
+  *count = k;
   return SG_OK;
 }
 

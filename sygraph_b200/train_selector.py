@@ -47,7 +47,7 @@ TRAIN_GRAPHS = [
 EVAL_GRAPHS = [
     ("rmat22_heldout", "rmat", dict(scale=22, seed=101)),
     ("rmat23", "rmat", dict(scale=23, seed=102)),
-    ("grid4096_lr", "grid", dict(side=4096, long_range_frac=0.01, seed=103)),
+    ("grid4096_lr", "grid", dict(side=4096, long_range_frac=0.02, seed=103)),
     ("uniform21", "rmat", dict(scale=21, a=0.25, b=0.25, c=0.25, seed=104)),
 ]
 
@@ -135,23 +135,27 @@ def traversals(data: dict):
         yield str(data["names"][i]), data["T"][a:b], data["H"][a:b], data["F0"][a:b]
 
 
-def simulate_choices(mlp: Mlp, F: np.ndarray, heuristic: np.ndarray, allowed: int = 0x3F) -> np.ndarray:
+def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.ndarray,
+                     allowed: int = 0x3F) -> np.ndarray:
     """The learned mode's schedule on a traversal: the MLP's argmin per level
-    with the current-direction feature following its own previous choice, the
-    heuristic where a feature leaves the trusted range (as the engine does)."""
-    p = mlp.params
-    t0 = p.size - 4 * IN
-    lo, hi = p[t0 + 2 * IN:t0 + 3 * IN], p[t0 + 3 * IN:t0 + 4 * IN]
+    (`forward` maps a feature batch to predicted log-times) with the
+    current-direction feature following its own previous choice, and the
+    heuristic where a feature leaves the trusted range, as the engine does."""
+    t0 = params.size - 4 * IN
+    lo, hi = params[t0 + 2 * IN:t0 + 3 * IN], params[t0 + 3 * IN:t0 + 4 * IN]
+    banned = [j for j in range(OUT) if not (allowed >> j) & 1]
     out = np.empty(len(F), np.int32)
     prev = 0
     for L in range(len(F)):
-        f = F[L].copy()
+        f = np.array(F[L], np.float32)
         if L > 0:
             f[10] = 1.0 if prev >= 2 else 0.0
         if np.any(f < lo) or np.any(f > hi):
             out[L] = heuristic[L]
         else:
-            out[L] = int(mlp.choose(f[None, :], allowed)[0])
+            y = np.array(forward(f[None, :]), np.float64)[0]
+            y[banned] = np.inf
+            out[L] = int(np.argmin(y))
         prev = out[L]
     return out
 
@@ -160,8 +164,9 @@ def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F) -> dict:
     """Summed level time (us) per traversal under the heuristic's schedule,
     the MLP's schedule and the per-level best; totals and regret."""
     rows = []
+    params = mlp.params
     for name, T, H, F in traversals(data):
-        c = simulate_choices(mlp, F, H, allowed)
+        c = simulate_choices(params, mlp.forward, F, H, allowed)
         idx = np.arange(len(T))
         rows.append({"traversal": name, "levels": len(T), "heuristic_us": float(T[idx, H].sum()),
                      "learned_us": float(T[idx, c].sum()), "best_us": float(T.min(1).sum()),

@@ -51,3 +51,20 @@ def test_msbfs_directed_and_star(sg, oracle):
     mb = sg.algorithms.MultiBFS(Gs, 8)
     mb.run(s2)
     assert np.array_equal(mb.getDistances(), oracle.bfs_multi(star, s2))
+
+
+@pytest.mark.parametrize("n", [3000, 70_000])
+def test_msbfs_long_diameter_depth_planes(sg, oracle, n):
+    """Depths above 2^12 and 2^16 (wider depth bit-plane sets), and a second
+    batch on the same instance after a deeper one left its planes dirty."""
+    path = sg.io.fromCOO(n, np.arange(n - 1), np.arange(1, n), symmetrize=True)
+    G = sg.graph.build.fromCSR(path)
+    mb = sg.algorithms.MultiBFS(G, 64)
+    srcs = np.array([0, n - 1, n // 2, 17], np.uint32)
+    for direction in (0, 2):
+        det = mb.run(srcs, direction, 15.0, 24.0)
+        assert np.array_equal(mb.getDistances(), oracle.bfs_multi(path, srcs))
+        assert det["iterations"] == n
+    shallow = np.array([n // 2, n // 2 + 1], np.uint32)
+    mb.run(shallow)
+    assert np.array_equal(mb.getDistances(), oracle.bfs_multi(path, shallow))

@@ -1,0 +1,79 @@
+"""What the trained selector gains over the reference heuristic, on per-level
+cost tables measured on a B200 for held-out graphs (RMAT-22 with another
+seed, RMAT-23, a 4096x4096 grid with long-range pairs, a uniform random
+graph).  The fixture was made by
+`python -m sygraph_b200.train_selector collect --set eval --out tests/golden/selector_eval_b200.npz`
+and the model by `... train`; the schedules here come from the FP64 oracle
+forward pass of the committed parameters, replaying the engine's rule
+(MLP argmin inside the trusted range, heuristic outside it)."""
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+EVAL = ROOT / "tests" / "golden" / "selector_eval_b200.npz"
+MODEL = ROOT / "sygraph_b200" / "models" / "selector_b200.npz"
+
+
+@pytest.fixture(scope="module")
+def tables():
+    from sygraph_b200 import train_selector as ts
+    with np.load(EVAL) as d:
+        data = {k: d[k] for k in d.files}
+    with np.load(MODEL) as m:
+        params = m["params"].astype(np.float32)
+    return ts, data, params
+
+
+def _schedules(ts, data, params):
+    from oracle import mlp as omlp
+    fwd = lambda X: omlp.forward(params.astype(np.float64), X)[0]  # noqa: E731
+    out = []
+    for name, T, H, F in ts.traversals(data):
+        c = ts.simulate_choices(params, fwd, F, H)
+        idx = np.arange(len(T))
+        out.append((name, T[idx, H].sum(), T[idx, c].sum(), T.min(1).sum(), c, H))
+    return out
+
+
+def test_model_file_layout(tables):
+    ts, _, params = tables
+    from oracle import mlp as omlp
+    assert params.size == sum(int(np.prod(s)) for _, s in omlp.SHAPES)
+    t = params.size - 48
+    lo, hi = params[t + 24:t + 36], params[t + 36:t + 48]
+    assert np.all(lo < hi) and np.all(np.isfinite(params))
+
+
+def test_learned_schedule_beats_heuristic_on_held_out_graphs(tables):
+    ts, data, params = tables
+    rows = _schedules(ts, data, params)
+    heur = sum(r[1] for r in rows)
+    learned = sum(r[2] for r in rows)
+    best = sum(r[3] for r in rows)
+    # the whole held-out set: at least 25% less time than the heuristic,
+    # within 10% of the per-level best
+    assert learned <= 0.8 * heur, (learned, heur)
+    assert learned <= 1.10 * best, (learned, best)
+    # and no traversal more than 10% slower than under the heuristic
+    for name, h, l, _, _, _ in rows:
+        assert l <= 1.10 * h, (name, l, h)
+
+
+def test_learned_schedule_on_rmat_is_no_worse_than_heuristic(tables):
+    ts, data, params = tables
+    rows = [r for r in _schedules(ts, data, params) if r[0].startswith("rmat")]
+    assert rows
+    heur = sum(r[1] for r in rows)
+    learned = sum(r[2] for r in rows)
+    assert learned <= 1.03 * heur
+
+
+def test_regret_bookkeeping_matches_tables(tables):
+    """Heuristic schedules in the fixture are the reference's push/pull
+    choices (strategy 0 or 2 only) and cover every level."""
+    ts, data, _ = tables
+    for name, T, H, F in ts.traversals(data):
+        assert T.shape[1] == 6 and len(H) == len(T) == len(F)
+        assert set(np.unique(H)) <= {0, 2}
+        assert np.all(T > 0)

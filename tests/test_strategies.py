@@ -91,7 +91,7 @@ def test_schedule_argument_checks(sg, graphs):
     bfs.init(0)
     with pytest.raises(sg._lib.SygraphError) as ei:
         bfs.run(sg.algorithms.bfs_direction.learned)  # no selector attached
-    assert ei.value.status == sg._lib.SG_ERR_INVALID
+    assert ei.value.status == sg._lib.SG_ERR_NOT_INITIALIZED
 
 
 def _trusting_mlp(selector, seed):
