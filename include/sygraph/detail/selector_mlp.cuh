@@ -38,10 +38,48 @@ constexpr int kMlpParamCount = (int)(sizeof(MlpParams) / sizeof(float));
 static_assert(kMlpParamCount == kMlpTrainableCount + 4 * kMlpIn, "MlpParams must be packed floats");
 
 #ifdef __CUDACC__
-// Forward pass by one full warp: lane j computes hidden unit j.  Returns, in
-// every lane, the strategy with the smallest predicted time among the set bits
-// of `allowed`, or -1 when a feature lies outside the trusted range.
-__device__ __forceinline__ int mlp_choose(const MlpParams* __restrict__ P, const float* f, uint32_t allowed) {
+// Shared-memory copy of the parameters for inference inside the traversal
+// engines: the two hidden-layer matrices transposed, so that lane j reads
+// element j of a row (no bank conflicts), and no global load on the path.
+struct MlpStaged {
+  float w1t[kMlpIn][kMlpHidden];
+  float b1[kMlpHidden];
+  float w2t[kMlpHidden][kMlpHidden];
+  float b2[kMlpHidden];
+  float w3[kMlpOut][kMlpHidden];
+  float b3[kMlpOut];
+  float mean[kMlpIn];
+  float inv_std[kMlpIn];
+  float lo[kMlpIn];
+  float hi[kMlpIn];
+};
+
+// Block-cooperative copy; the caller synchronises the block afterwards.
+__device__ __forceinline__ void mlp_stage(const MlpParams* __restrict__ g, MlpStaged* s) {
+  for (int t = threadIdx.x; t < kMlpIn * kMlpHidden; t += blockDim.x)
+    s->w1t[t / kMlpHidden][t % kMlpHidden] = g->w1[t % kMlpHidden][t / kMlpHidden];
+  for (int t = threadIdx.x; t < kMlpHidden * kMlpHidden; t += blockDim.x)
+    s->w2t[t / kMlpHidden][t % kMlpHidden] = g->w2[t % kMlpHidden][t / kMlpHidden];
+  for (int t = threadIdx.x; t < kMlpOut * kMlpHidden; t += blockDim.x) s->w3[t / kMlpHidden][t % kMlpHidden] =
+      g->w3[t / kMlpHidden][t % kMlpHidden];
+  for (int t = threadIdx.x; t < kMlpHidden; t += blockDim.x) {
+    s->b1[t] = g->b1[t];
+    s->b2[t] = g->b2[t];
+  }
+  for (int t = threadIdx.x; t < kMlpIn; t += blockDim.x) {
+    s->mean[t] = g->mean[t];
+    s->inv_std[t] = g->inv_std[t];
+    s->lo[t] = g->lo[t];
+    s->hi[t] = g->hi[t];
+  }
+  for (int t = threadIdx.x; t < kMlpOut; t += blockDim.x) s->b3[t] = g->b3[t];
+}
+
+// Forward pass by one full warp: lane j computes hidden unit j, summing in
+// the same order as the training kernels.  Returns, in every lane, the
+// strategy with the smallest predicted time among the set bits of
+// `allowed`, or -1 when a feature lies outside the trusted range.
+__device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const float* f, uint32_t allowed) {
   const uint32_t lane = threadIdx.x & 31;
   bool out_of_range = false;
   float x[kMlpIn];
@@ -53,11 +91,11 @@ __device__ __forceinline__ int mlp_choose(const MlpParams* __restrict__ P, const
   if (out_of_range) return -1;
   float h1 = P->b1[lane];
 #pragma unroll
-  for (int i = 0; i < kMlpIn; i++) h1 += P->w1[lane][i] * x[i];
+  for (int i = 0; i < kMlpIn; i++) h1 += P->w1t[i][lane] * x[i];
   h1 = h1 > 0.f ? h1 : 0.f;
   float h2 = P->b2[lane];
 #pragma unroll 8
-  for (int i = 0; i < kMlpHidden; i++) h2 += P->w2[lane][i] * __shfl_sync(0xffffffffu, h1, i);
+  for (int i = 0; i < kMlpHidden; i++) h2 += P->w2t[i][lane] * __shfl_sync(0xffffffffu, h1, i);
   h2 = h2 > 0.f ? h2 : 0.f;
   float best = 3.4e38f;
   int arg = -1;

@@ -417,6 +417,32 @@ sg_status sg_cc(sg_graph g, uint32_t* host_labels, uint64_t* iterations);
  * delta_s(v), v != s, float32. */
 sg_status sg_bc(sg_graph g, const uint32_t* host_sources, uint32_t k, float* host_bc);
 
+/* Batched BC (no counterpart in the reference, which runs one source per
+ * BC::run): up to 64 sources per launch as bit-parallel frontiers, the same
+ * sum as sg_bc over those sources (float32; every sum in a fixed order, so
+ * repeated runs give identical bits).  The per-level frontier history sizes
+ * the device memory: history_levels = 0 picks it from the graph size, and a
+ * deeper traversal enlarges it and runs again (SG_ERR_NOMEM when it cannot). */
+typedef struct sg_bc_batch_s* sg_bc_batch;
+typedef struct {
+  uint64_t iterations;      /* forward levels */
+  uint64_t reached_edges;   /* sum over (source, reached vertex) of its out-degree */
+  uint64_t history_levels;  /* history capacity used */
+  uint64_t history_retries; /* runs repeated after enlarging the history */
+} sg_bc_batch_details;
+sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* out);
+sg_status sg_bc_batch_destroy(sg_bc_batch h);
+/* accumulate != 0 adds this batch into the device bc array instead of
+ * overwriting it. */
+sg_status sg_bc_batch_run_async(sg_bc_batch h, const uint32_t* host_sources, uint32_t k, int accumulate);
+sg_status sg_bc_batch_run(sg_bc_batch h, const uint32_t* host_sources, uint32_t k, int accumulate,
+                          sg_bc_batch_details* details);
+sg_status sg_bc_batch_get(sg_bc_batch h, float* host_bc);
+sg_status sg_bc_batch_bc_device(sg_bc_batch h, const float** dev_bc);
+sg_status sg_bc_batch_level_records(sg_bc_batch h, sg_level_record* host_records, uint32_t cap, uint32_t* count);
+/* One-shot: any number of sources, in batches of 64. */
+sg_status sg_bc_batched(sg_graph g, const uint32_t* host_sources, uint32_t k, float* host_bc);
+
 /* TC(G) + init + run + getNumTriangles (algorithms/tc.hpp:58-138), exact:
  * degree-ordered DAG and sorted-list segmented intersection, uint64.  When
  * host_per_vertex is non-NULL it receives getNumTriangles(v): for every edge

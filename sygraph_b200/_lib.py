@@ -60,6 +60,11 @@ class MsbfsDetails(C.Structure):
                 ("reached_edges", C.c_uint64)]
 
 
+class BcBatchDetails(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("reached_edges", C.c_uint64), ("history_levels", C.c_uint64),
+                ("history_retries", C.c_uint64)]
+
+
 class HostCSR(C.Structure):
     _fields_ = [("n", C.c_uint32), ("m", C.c_uint64), ("row_offsets", u32p), ("column_indices", u32p),
                 ("values", vp), ("value_type", C.c_int), ("flags", C.c_uint32)]
@@ -148,6 +153,14 @@ SIGNATURES = {
     "sg_mlp_gradient": (st, [vp, vp, vp, vp, C.c_uint32, f32p, f32p]),
     "sg_mlp_train": (st, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, f32p]),
     "sg_msbfs_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
+    "sg_bc_batch_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
+    "sg_bc_batch_destroy": (st, [vp]),
+    "sg_bc_batch_run_async": (st, [vp, u32p, C.c_uint32, C.c_int]),
+    "sg_bc_batch_run": (st, [vp, u32p, C.c_uint32, C.c_int, C.POINTER(BcBatchDetails)]),
+    "sg_bc_batch_get": (st, [vp, f32p]),
+    "sg_bc_batch_bc_device": (st, [vp, C.POINTER(vp)]),
+    "sg_bc_batch_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
+    "sg_bc_batched": (st, [vp, u32p, C.c_uint32, f32p]),
     "sg_msbfs_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
     "sg_msbfs_destroy": (st, [vp]),
     "sg_msbfs_run": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float, C.POINTER(MsbfsDetails)]),

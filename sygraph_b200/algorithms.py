@@ -233,6 +233,56 @@ class BC:
         return self.values
 
 
+class BatchedBC:
+    """Brandes BC with up to 64 sources per launch (bit-parallel frontiers);
+    getBC() equals BC(G) over the same sources within float32 rounding, and
+    repeated runs give identical bits."""
+
+    def __init__(self, G: Graph, history_levels: int = 0):
+        self.G = G
+        h = C.c_void_p()
+        call("sg_bc_batch_create", G.handle, history_levels, C.byref(h))
+        self.handle = h
+        self.details = None
+
+    def run(self, sources, accumulate: bool = False) -> dict:
+        """Sources in batches of 64; the first batch overwrites unless `accumulate`."""
+        src = np.ascontiguousarray(np.atleast_1d(sources), np.uint32)
+        tot = {"iterations": 0, "reached_edges": 0, "history_levels": 0, "history_retries": 0}
+        for i in range(0, src.size, 64):
+            part = np.ascontiguousarray(src[i:i + 64])
+            d = _lib.BcBatchDetails()
+            call("sg_bc_batch_run", self.handle, _ptr(part), part.size, int(accumulate or i > 0), C.byref(d))
+            tot["iterations"] = max(tot["iterations"], int(d.iterations))
+            tot["reached_edges"] += int(d.reached_edges)
+            tot["history_levels"] = int(d.history_levels)
+            tot["history_retries"] += int(d.history_retries)
+        self.details = tot
+        return tot
+
+    def run_async(self, sources, accumulate: bool = False) -> None:
+        src = np.ascontiguousarray(np.atleast_1d(sources), np.uint32)
+        assert src.size <= 64
+        call("sg_bc_batch_run_async", self.handle, _ptr(src), src.size, int(accumulate))
+
+    def getBC(self) -> np.ndarray:
+        out = np.empty(self.G.getVertexCount(), np.float32)
+        call("sg_bc_batch_get", self.handle, out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def level_records(self) -> list[dict]:
+        recs = (_lib.LevelRecord * _lib.SG_MAX_LOGGED_LEVELS)()
+        cnt = C.c_uint32()
+        call("sg_bc_batch_level_records", self.handle, recs, _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
+        return [{k: getattr(recs[i], k) for k, _ in _lib.LevelRecord._fields_} for i in range(cnt.value)]
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib.sg_bc_batch_destroy(h)
+            self.handle = None
+
+
 class TC:
     """algorithms::TC (tc.hpp:473-565), exact."""
 

@@ -1,0 +1,663 @@
+// Batched Brandes betweenness centrality: up to 64 sources per launch as
+// bit-parallel frontiers (bit s of a vertex's uint64 mask = source s), one
+// persistent cooperative kernel for the forward and backward sweeps.
+// Per source the arithmetic is BC::run (algorithms/bc.hpp:118-200): sigma by
+// forward levels, delta_s(v) = sum over successors u of
+// sigma_s(v)/sigma_s(u) * (1 + delta_s(u)), bc[v] += delta_s(v) for v != s.
+//
+// Layout: hist[L][v] = sources for which v has depth L (one uint64 array per
+// level, kept for the backward sweep), seen[v] = OR of hist[0..L][v], and
+// sigma / delta as vertex-major rows of 64 floats (row v is 256 bytes: lane
+// l of a warp holds sources 2l and 2l+1, so a row is one coalesced load).
+//
+// Forward level L (one fused pull pass, no atomics): every vertex u that some
+// source has not reached scans its in-neighbours w in adjacency order;
+// m = hist[L][w] & ~seen[u] are the sources reaching u through w at depth
+// L+1; u's new mask is the OR of the m's and sigma_s(u) the sum of
+// sigma_s(w) over the w with bit s in m, added in adjacency order.  Light
+// vertices take a warp each (lanes over 32 edges, then over sources);
+// vertices of degree >= kCtaDeg take a whole CTA, whose warps split the list
+// and add their partial sums in warp order.  So every sum has a fixed order:
+// results do not depend on scheduling.
+//
+// Backward level L (from the deepest down to 1): every v with hist[L][v] != 0
+// gathers over its out-neighbours u with m = hist[L+1][u] & hist[L][v]:
+// acc_s += (1 + delta_s(u)) / sigma_s(u); delta_s(v) = sigma_s(v) * acc_s and
+// bc[v] += the warp's fixed-order sum of delta_s(v) over s in hist[L][v].
+//
+// One grid barrier per level in each sweep.  When the depth exceeds the
+// history capacity the kernel stops with a flag and the host enlarges the
+// history (or falls back to the per-source engine) and runs again.
+#include <algorithm>
+#include <vector>
+
+#include "engine_common.cuh"
+
+namespace sgb {
+namespace bcb {
+
+using namespace eng;
+using u64 = unsigned long long;
+
+constexpr uint32_t kCtaDeg = 2048;  // degree from which a vertex takes a whole CTA
+constexpr uint32_t kRow = 64;       // floats per sigma / delta row
+
+struct Counters {
+  u64 new_count;     // vertices that gained a source this level
+  u64 reached;       // sum over (source, newly reached vertex) of its out-degree
+  u64 big;           // CTA-sized vertices deferred to the CTA phase
+  u64 pad[5];
+};
+
+struct Params {
+  uint32_t n, w0, k;
+  uint64_t m;
+  const uint32_t* ro;   // out-edges (backward sweep, reached-edge counts)
+  const uint32_t* col;
+  const uint32_t* iro;  // in-edges (forward sweep); alias ro / col when undirected
+  const uint32_t* icol;
+  const uint32_t* sources;
+  u64 all;
+  u64* seen;
+  u64* hist;            // cap_levels * n
+  uint32_t cap_levels;
+  uint32_t* act;        // cap_levels * w0: hist[L] != 0
+  uint32_t* done;       // w0: every source reached (or no in-edge)
+  const uint32_t* no_in_edges;
+  uint32_t* big_list;   // n: CTA-sized vertices of the current level
+  float* sigma;         // n * 64
+  float* delta;         // n * 64
+  float* bc;            // n
+  int accumulate;       // add into bc instead of overwriting
+  Counters* cnt;        // 2 slots, alternating by level
+  GridBarrier* bar;
+  sg_level_record* log;
+  u64* result;          // [levels, overflow, reached_edges, backward_levels]
+};
+
+struct Shared {
+  float part[16][kRow];  // per-warp partial sums of a CTA-sized vertex
+  u64 mask[16];
+  uint32_t scan[32];
+  u64 red[32];
+  uint32_t nbig;
+};
+
+__device__ __forceinline__ u64 shfl64(u64 x, uint32_t src) {
+  const uint32_t lo = __shfl_sync(kFullMask, (uint32_t)x, src);
+  const uint32_t hi = __shfl_sync(kFullMask, (uint32_t)(x >> 32), src);
+  return ((u64)hi << 32) | lo;
+}
+
+__device__ __forceinline__ u64 warp_or64(u64 x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x |= shfl64(x, (threadIdx.x & 31) ^ d);
+  return x;
+}
+
+// The two floats of row w that lane `lane` owns (sources 2*lane, 2*lane+1).
+// Rows are written in earlier levels by other SMs: loaded through L2.
+__device__ __forceinline__ float2 row2(const float* rows, uint32_t w, uint32_t lane) {
+  return __ldcg(reinterpret_cast<const float2*>(rows + (size_t)w * kRow) + lane);
+}
+
+// Forward gather over in-edges [beg, end) of u for level L: ORs the masks
+// m = hist_L[w] & ~su and adds sigma rows.  Returns the OR (in every lane).
+__device__ __forceinline__ u64 forward_gather(const Params& P, const u64* hist_L, uint32_t beg, uint32_t end, u64 su,
+                                              float& a0, float& a1) {
+  const uint32_t lane = threadIdx.x & 31;
+  u64 acc_mask = 0;
+  for (uint32_t eb = beg; eb < end; eb += 32) {
+    const uint32_t e = eb + lane;
+    uint32_t w = 0;
+    u64 mw = 0;
+    if (e < end) {
+      w = P.icol[e];
+      mw = __ldcg(hist_L + w) & ~su;
+    }
+    acc_mask |= mw;
+    uint32_t ball = __ballot_sync(kFullMask, mw != 0);
+    while (ball) {
+      const uint32_t j = __ffs(ball) - 1;
+      ball &= ball - 1;
+      const uint32_t wj = __shfl_sync(kFullMask, w, j);
+      const u64 mj = shfl64(mw, j);
+      const uint32_t b = (uint32_t)(mj >> (2 * lane)) & 3u;
+      if (b) {
+        const float2 r = row2(P.sigma, wj, lane);
+        if (b & 1u) a0 += r.x;
+        if (b & 2u) a1 += r.y;
+      }
+    }
+  }
+  return warp_or64(acc_mask);
+}
+
+// Backward gather over out-edges [beg, end) of v: acc_s += (1+delta_s(u))/sigma_s(u)
+// for the u with bit s in hist_next[u] & fv.
+__device__ __forceinline__ void backward_gather(const Params& P, const u64* hist_next, uint32_t beg, uint32_t end,
+                                                u64 fv, float& a0, float& a1) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t eb = beg; eb < end; eb += 32) {
+    const uint32_t e = eb + lane;
+    uint32_t u = 0;
+    u64 mu = 0;
+    if (e < end) {
+      u = P.col[e];
+      mu = __ldcg(hist_next + u) & fv;
+    }
+    uint32_t ball = __ballot_sync(kFullMask, mu != 0);
+    while (ball) {
+      const uint32_t j = __ffs(ball) - 1;
+      ball &= ball - 1;
+      const uint32_t uj = __shfl_sync(kFullMask, u, j);
+      const u64 mj = shfl64(mu, j);
+      const uint32_t b = (uint32_t)(mj >> (2 * lane)) & 3u;
+      if (b) {
+        const float2 s = row2(P.sigma, uj, lane);
+        const float2 d = row2(P.delta, uj, lane);
+        if (b & 1u) a0 += (1.0f + d.x) / s.x;
+        if (b & 2u) a1 += (1.0f + d.y) / s.y;
+      }
+    }
+  }
+}
+
+constexpr uint32_t kBigList = 256;  // CTA-sized vertices a CTA defers per level (more: done by the warp)
+
+struct Local {
+  u64 new_count = 0, reached = 0;
+};
+
+// Forward result of vertex u: seen, hist[L+1], sigma entries of its new
+// sources, the act / done bits.  Every lane calls; nm is warp-uniform.
+__device__ __forceinline__ void forward_finish(const Params& P, u64* hist_N, uint32_t* act_N, uint32_t u, u64 su,
+                                               u64 nm, float a0, float a1, Local& loc) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (!nm) return;
+  const uint32_t b = (uint32_t)(nm >> (2 * lane)) & 3u;
+  float* row = P.sigma + (size_t)u * kRow + 2 * lane;
+  if (b == 3u) {
+    __stcg(reinterpret_cast<float2*>(row), make_float2(a0, a1));
+  } else if (b == 1u) {
+    __stcg(row, a0);
+  } else if (b == 2u) {
+    __stcg(row + 1, a1);
+  }
+  if (lane == 0) {
+    st_cg(P.seen + u, su | nm);
+    st_cg(hist_N + u, nm);
+    atomicOr(act_N + (u >> 5), 1u << (u & 31));
+    if ((su | nm) == P.all) atomicOr(P.done + (u >> 5), 1u << (u & 31));
+    loc.new_count++;
+    loc.reached += (u64)__popcll(nm) * (P.ro[u + 1] - P.ro[u]);
+  }
+}
+
+// Backward result of vertex v: delta entries for its sources at this level
+// and bc[v] += their fixed-order sum.
+__device__ __forceinline__ void backward_finish(const Params& P, uint32_t v, u64 fv, float a0, float a1) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t b = (uint32_t)(fv >> (2 * lane)) & 3u;
+  float d0 = 0.f, d1 = 0.f;
+  if (b) {
+    const float2 s = row2(P.sigma, v, lane);
+    float* row = P.delta + (size_t)v * kRow + 2 * lane;
+    if (b & 1u) {
+      d0 = s.x * a0;
+      __stcg(row, d0);
+    }
+    if (b & 2u) {
+      d1 = s.y * a1;
+      __stcg(row + 1, d1);
+    }
+  }
+  float t = d0 + d1;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) t += __shfl_xor_sync(kFullMask, t, d);
+  if (lane == 0) st_cg(P.bc + v, ld_cg(P.bc + v) + t);
+}
+
+// A CTA-sized vertex: 16 warps gather contiguous slices of its list, partial
+// sums are added in warp order.  Called by every thread of the block.
+template <bool kForward>
+__device__ __forceinline__ void cta_vertex(const Params& P, Shared& S, const u64* hist_src, u64* hist_N,
+                                           uint32_t* act_N, uint32_t x, Local& loc) {
+  const uint32_t lane = threadIdx.x & 31, wl = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t beg = kForward ? P.iro[x] : P.ro[x];
+  const uint32_t end = kForward ? P.iro[x + 1] : P.ro[x + 1];
+  const uint32_t deg = end - beg;
+  const uint32_t slice = ((deg + nw - 1) / nw + 31) & ~31u;
+  const uint32_t sb = min(end, beg + wl * slice), se = min(end, sb + slice);
+  const u64 sx = kForward ? ld_cg(P.seen + x) : ld_cg(hist_src + x);
+  float a0 = 0.f, a1 = 0.f;
+  u64 mk = 0;
+  if (kForward)
+    mk = forward_gather(P, hist_src, sb, se, sx, a0, a1);
+  else if (hist_N)
+    backward_gather(P, hist_N, sb, se, sx, a0, a1);
+  S.part[wl][2 * lane] = a0;
+  S.part[wl][2 * lane + 1] = a1;
+  if (lane == 0) S.mask[wl] = mk;
+  __syncthreads();
+  if (wl == 0) {
+    float t0 = 0.f, t1 = 0.f;
+    u64 all = 0;
+    for (uint32_t w = 0; w < nw; w++) {
+      t0 += S.part[w][2 * lane];
+      t1 += S.part[w][2 * lane + 1];
+      all |= S.mask[w];
+    }
+    if (kForward)
+      forward_finish(P, hist_N, act_N, x, sx, all, t0, t1, loc);
+    else
+      backward_finish(P, x, sx, t0, t1);
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void block_add(Local& loc, Shared& S, Counters* C) {
+  const u64 a = block_sum<u64>(loc.new_count, S.red);
+  const u64 b = block_sum<u64>(loc.reached, S.red);
+  if (threadIdx.x == 0) {
+    if (a) atomicAdd(&C->new_count, a);
+    if (b) atomicAdd(&C->reached, b);
+  }
+}
+
+struct BigList {
+  uint32_t v[kBigList];
+  uint32_t count;
+};
+
+__global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
+  __shared__ Shared S;
+  __shared__ BigList B;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
+  const uint32_t n = P.n, w0 = P.w0;
+
+  // ---- clear: seen, hist[0..1], act[0..1], done = no in-edges, bc
+  for (uint32_t i = gtid; i < n; i += nthreads) {
+    st_cg(P.seen + i, 0ull);
+    st_cg(P.hist + i, 0ull);
+    st_cg(P.hist + (size_t)n + i, 0ull);
+    if (!P.accumulate) st_cg(P.bc + i, 0.f);
+  }
+  for (uint32_t i = gtid; i < w0; i += nthreads) {
+    st_cg(P.act + i, 0u);
+    st_cg(P.act + w0 + i, 0u);
+    st_cg(P.done + i, P.no_in_edges[i]);
+  }
+  if (gtid < 3) {
+    Counters z = {};
+    P.cnt[gtid] = z;
+  }
+  if (threadIdx.x == 0) B.count = 0;
+  if (!grid_sync(P.bar)) return;
+  // ---- sources: depth 0, sigma 1
+  u64 reached_total = 0;
+  for (uint32_t i = 0; i < P.k; i++) reached_total += P.ro[P.sources[i] + 1] - P.ro[P.sources[i]];
+  if (gtid == 0) {
+    for (uint32_t i = 0; i < P.k; i++) {
+      const uint32_t s = P.sources[i];
+      const u64 now = P.seen[s] | (1ull << i);
+      P.seen[s] = now;
+      P.hist[s] = now;
+      P.act[s >> 5] |= 1u << (s & 31);
+      if (now == P.all) P.done[s >> 5] |= 1u << (s & 31);
+      P.sigma[(size_t)s * kRow + i] = 1.0f;
+    }
+    __threadfence();
+  }
+  if (!grid_sync(P.bar)) return;
+
+  // ---- forward sweep
+  uint32_t L = 0;
+  bool overflow = false;
+  for (;; L++) {
+    if (L + 1 >= P.cap_levels) {
+      overflow = true;
+      break;
+    }
+    Counters* C = P.cnt + (L % 3);
+    if (gtid == 0) {
+      Counters z = {};
+      P.cnt[(L + 1) % 3] = z;
+    }
+    const uint64_t t0 = gtid == 0 ? sygraph::detail::global_timer_ns() : 0;
+    const u64* hist_L = P.hist + (size_t)L * n;
+    u64* hist_N = P.hist + (size_t)(L + 1) * n;
+    uint32_t* act_N = P.act + (size_t)(L + 1) * w0;
+    if (L + 2 < P.cap_levels) {  // hist / act of level L+2 start empty
+      u64* h2 = P.hist + (size_t)(L + 2) * n;
+      for (uint32_t i = gtid; i < n; i += nthreads) st_cg(h2 + i, 0ull);
+      uint32_t* a2 = P.act + (size_t)(L + 2) * w0;
+      for (uint32_t i = gtid; i < w0; i += nthreads) st_cg(a2 + i, 0u);
+    }
+    Local loc;
+    for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+      uint32_t cand = ~ld_cg(P.done + wi) & valid_bits(wi, w0, n);
+      while (cand) {
+        const uint32_t u = wi * 32 + (__ffs(cand) - 1);
+        cand &= cand - 1;
+        const uint32_t beg = P.iro[u], end = P.iro[u + 1];
+        if (end - beg >= kCtaDeg) {
+          uint32_t slot = kBigList;
+          if (lane == 0) slot = atomicAdd(&B.count, 1u);
+          slot = __shfl_sync(kFullMask, slot, 0);
+          if (slot < kBigList) {
+            if (lane == 0) B.v[slot] = u;
+            continue;
+          }
+        }
+        const u64 su = ld_cg(P.seen + u);
+        float a0 = 0.f, a1 = 0.f;
+        const u64 nm = forward_gather(P, hist_L, beg, end, su, a0, a1);
+        forward_finish(P, hist_N, act_N, u, su, nm, a0, a1, loc);
+      }
+    }
+    __syncthreads();
+    const uint32_t nbig = min(B.count, kBigList);
+    for (uint32_t i = 0; i < nbig; i++) cta_vertex<true>(P, S, hist_L, hist_N, act_N, B.v[i], loc);
+    __syncthreads();
+    if (threadIdx.x == 0) B.count = 0;
+    block_add(loc, S, C);
+    if (!grid_sync(P.bar)) return;
+    const u64 next = ld_cg(&C->new_count);
+    reached_total += ld_cg(&C->reached);
+    if (gtid == 0 && L < kMaxLog) {
+      sg_level_record r = {};
+      r.level = L;
+      r.strategy = 2;
+      r.next_size = (uint32_t)next;
+      r.t_start_ns = t0;
+      r.t_end_ns = sygraph::detail::global_timer_ns();
+      P.log[L] = r;
+    }
+    if (next == 0) break;
+  }
+  if (overflow) {
+    if (gtid == 0) {
+      P.result[0] = L + 1;
+      P.result[1] = 1;
+    }
+    return;
+  }
+  // ---- backward sweep: levels L .. 1 (L is the deepest non-empty level)
+  const uint32_t Lmax = L;
+  for (uint32_t Lb = Lmax; Lb >= 1; Lb--) {
+    const u64* hist_B = P.hist + (size_t)Lb * n;
+    const u64* hist_next = Lb < Lmax ? P.hist + (size_t)(Lb + 1) * n : nullptr;
+    const uint32_t* act_B = P.act + (size_t)Lb * w0;
+    Local unused;
+    for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+      uint32_t word = ld_cg(act_B + wi);
+      while (word) {
+        const uint32_t v = wi * 32 + (__ffs(word) - 1);
+        word &= word - 1;
+        const uint32_t beg = P.ro[v], end = P.ro[v + 1];
+        if (end - beg >= kCtaDeg && hist_next) {
+          uint32_t slot = kBigList;
+          if (lane == 0) slot = atomicAdd(&B.count, 1u);
+          slot = __shfl_sync(kFullMask, slot, 0);
+          if (slot < kBigList) {
+            if (lane == 0) B.v[slot] = v;
+            continue;
+          }
+        }
+        const u64 fv = ld_cg(hist_B + v);
+        float a0 = 0.f, a1 = 0.f;
+        if (hist_next) backward_gather(P, hist_next, beg, end, fv, a0, a1);
+        backward_finish(P, v, fv, a0, a1);
+      }
+    }
+    __syncthreads();
+    const uint32_t nbig = min(B.count, kBigList);
+    for (uint32_t i = 0; i < nbig; i++)
+      cta_vertex<false>(P, S, hist_B, const_cast<u64*>(hist_next), nullptr, B.v[i], unused);
+    __syncthreads();
+    if (threadIdx.x == 0) B.count = 0;
+    if (!grid_sync(P.bar)) return;
+  }
+  if (gtid == 0) {
+    P.result[0] = Lmax + 1;
+    P.result[1] = 0;
+    P.result[2] = reached_total;
+    P.result[3] = Lmax;
+  }
+}
+
+__global__ void no_in_edges_kernel(const uint32_t* __restrict__ iro, uint32_t n, uint32_t w0, uint32_t* out) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < (uint64_t)w0 * 32;
+       base += gridDim.x * blockDim.x) {
+    const uint32_t v = base + lane;
+    const bool z = v < n && iro[v + 1] == iro[v];
+    const uint32_t msk = __ballot_sync(kFullMask, z);
+    if (lane == 0) out[base >> 5] = msk;
+  }
+}
+
+}  // namespace bcb
+}  // namespace sgb
+
+using namespace sgb;
+
+struct sg_bc_batch_s {
+  sg_graph g = nullptr;
+  uint32_t w0 = 0, cap_levels = 0, last_k = 0;
+  unsigned long long* seen = nullptr;
+  unsigned long long* hist = nullptr;
+  uint32_t *act = nullptr, *done = nullptr, *no_in = nullptr, *sources = nullptr;
+  float *sigma = nullptr, *delta = nullptr, *bc = nullptr;
+  bcb::Counters* cnt = nullptr;
+  sygraph::detail::GridBarrier* bar = nullptr;
+  sg_level_record* log = nullptr;
+  unsigned long long* result = nullptr;
+};
+
+namespace {
+
+void bcb_release(sg_bc_batch h) {
+  if (!h) return;
+  dev_free(h->seen);
+  dev_free(h->hist);
+  dev_free(h->act);
+  dev_free(h->done);
+  dev_free(h->no_in);
+  dev_free(h->sources);
+  dev_free(h->sigma);
+  dev_free(h->delta);
+  dev_free(h->bc);
+  dev_free(h->cnt);
+  dev_free(h->bar);
+  dev_free(h->log);
+  dev_free(h->result);
+  delete h;
+}
+
+uint64_t level_bytes(sg_bc_batch h) { return 8ull * h->g->n + 4ull * h->w0; }
+
+// History of `levels` levels (frontier masks + activity words).
+sg_status bcb_history(sg_bc_batch h, uint32_t levels) {
+  dev_free(h->hist);
+  dev_free(h->act);
+  h->cap_levels = 0;
+  SG_TRY(dev_alloc(&h->hist, (uint64_t)levels * h->g->n));
+  SG_TRY(dev_alloc(&h->act, (uint64_t)levels * h->w0));
+  h->cap_levels = levels;
+  return SG_OK;
+}
+
+// Levels that fit in a quarter of the free device memory.
+uint32_t bcb_max_levels(sg_bc_batch h) {
+  size_t f = 0, t = 0;
+  if (cudaMemGetInfo(&f, &t) != cudaSuccess) return h->cap_levels;
+  const uint64_t have = (uint64_t)h->cap_levels * level_bytes(h);
+  const uint64_t lv = (f / 4 + have) / level_bytes(h);
+  return (uint32_t)std::min<uint64_t>(lv, 1u << 20);
+}
+
+sg_status bcb_launch(sg_bc_batch h, uint32_t k, int accumulate) {
+  sg_graph g = h->g;
+  SG_CUDA(cudaMemsetAsync(h->bar, 0, sizeof(*h->bar), g->stream));
+  SG_CUDA(cudaMemsetAsync(h->result, 0, 4 * sizeof(unsigned long long), g->stream));
+  bcb::Params P;
+  P.n = g->n;
+  P.w0 = h->w0;
+  P.k = k;
+  P.m = g->m;
+  P.ro = g->fwd.ro;
+  P.col = g->fwd.col;
+  P.iro = g->inv.ro;
+  P.icol = g->inv.col;
+  P.sources = h->sources;
+  P.all = k == 64 ? ~0ull : ((1ull << k) - 1ull);
+  P.seen = h->seen;
+  P.hist = h->hist;
+  P.cap_levels = h->cap_levels;
+  P.act = h->act;
+  P.done = h->done;
+  P.no_in_edges = h->no_in;
+  P.big_list = nullptr;
+  P.sigma = h->sigma;
+  P.delta = h->delta;
+  P.bc = h->bc;
+  P.accumulate = accumulate;
+  P.cnt = h->cnt;
+  P.bar = h->bar;
+  P.log = h->log;
+  P.result = h->result;
+  return eng::launch_persistent(bcb::bc_batch_kernel, P, 2, g->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* out) {
+  clear_error();
+  SG_REQUIRE(g && out, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(g->n > 0, SG_ERR_INVALID, "graph has no vertices");
+  *out = nullptr;
+  sg_bc_batch h = new sg_bc_batch_s();
+  h->g = g;
+  h->w0 = div_up(g->n, 32);
+  const uint64_t n = g->n;
+  uint32_t levels = history_levels;
+  if (!levels) levels = (uint32_t)std::max<uint64_t>(16, std::min<uint64_t>(256, (2ull << 30) / level_bytes(h)));
+  levels = std::max<uint32_t>(levels, 2);
+  sg_status s;
+  if ((s = dev_alloc(&h->seen, n)) || (s = dev_alloc(&h->done, h->w0)) || (s = dev_alloc(&h->no_in, h->w0)) ||
+      (s = dev_alloc(&h->sources, 64)) || (s = dev_alloc(&h->sigma, n * bcb::kRow)) ||
+      (s = dev_alloc(&h->delta, n * bcb::kRow)) || (s = dev_alloc(&h->bc, n)) || (s = dev_alloc(&h->cnt, 3)) ||
+      (s = dev_alloc(&h->bar, 1)) || (s = dev_alloc(&h->log, SG_MAX_LOGGED_LEVELS)) ||
+      (s = dev_alloc(&h->result, 4)) || (s = bcb_history(h, levels))) {
+    bcb_release(h);
+    return s;
+  }
+  bcb::no_in_edges_kernel<<<grid_for((uint64_t)h->w0 * 32, 256), 256, 0, g->stream>>>(g->inv.ro, g->n, h->w0, h->no_in);
+  if (cudaGetLastError() != cudaSuccess) {
+    bcb_release(h);
+    return fail(SG_ERR_CUDA, "batched BC set-up kernel failed to launch");
+  }
+  count_launch();
+  if (cudaMemsetAsync(h->bc, 0, sizeof(float) * n, g->stream) != cudaSuccess) {
+    bcb_release(h);
+    return fail(SG_ERR_CUDA, "batched BC set-up failed");
+  }
+  *out = h;
+  return SG_OK;
+}
+
+sg_status sg_bc_batch_destroy(sg_bc_batch h) {
+  if (h) {
+    cudaStreamSynchronize(h->g->stream);
+    bcb_release(h);
+  }
+  return SG_OK;
+}
+
+sg_status sg_bc_batch_run_async(sg_bc_batch h, const uint32_t* host_sources, uint32_t k, int accumulate) {
+  clear_error();
+  SG_REQUIRE(h && host_sources, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(k >= 1 && k <= 64, SG_ERR_INVALID, "a batch holds 1 to 64 sources");
+  for (uint32_t i = 0; i < k; i++) SG_REQUIRE(host_sources[i] < h->g->n, SG_ERR_INVALID, "source out of range");
+  SG_CUDA(cudaMemcpyAsync(h->sources, host_sources, sizeof(uint32_t) * k, cudaMemcpyHostToDevice, h->g->stream));
+  h->last_k = k;
+  return bcb_launch(h, k, accumulate);
+}
+
+sg_status sg_bc_batch_run(sg_bc_batch h, const uint32_t* host_sources, uint32_t k, int accumulate,
+                          sg_bc_batch_details* details) {
+  SG_TRY(sg_bc_batch_run_async(h, host_sources, k, accumulate));
+  uint32_t retries = 0;
+  for (;;) {
+    unsigned long long r[4];
+    sygraph::detail::GridBarrier b;
+    SG_CUDA(cudaMemcpyAsync(r, h->result, sizeof(r), cudaMemcpyDeviceToHost, h->g->stream));
+    SG_CUDA(cudaMemcpyAsync(&b, h->bar, sizeof(b), cudaMemcpyDeviceToHost, h->g->stream));
+    SG_CUDA(cudaStreamSynchronize(h->g->stream));
+    if (b.error) return fail(SG_ERR_TIMEOUT, "batched BC: a grid barrier wait ran out");
+    if (r[1]) {
+      // deeper than the history: enlarge it (bc is untouched before the backward sweep) and run again
+      const uint32_t want = std::min<uint32_t>(bcb_max_levels(h), h->cap_levels * 4);
+      SG_REQUIRE(want > h->cap_levels, SG_ERR_NOMEM, "batched BC: the traversal is deeper than the history that fits");
+      SG_TRY(bcb_history(h, want));
+      SG_TRY(bcb_launch(h, k, accumulate));
+      retries++;
+      continue;
+    }
+    if (details) {
+      details->iterations = r[0];
+      details->reached_edges = r[2];
+      details->history_levels = h->cap_levels;
+      details->history_retries = retries;
+    }
+    return SG_OK;
+  }
+}
+
+sg_status sg_bc_batch_get(sg_bc_batch h, float* host_bc) {
+  SG_REQUIRE(h && host_bc, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaMemcpyAsync(host_bc, h->bc, sizeof(float) * h->g->n, cudaMemcpyDeviceToHost, h->g->stream));
+  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  return SG_OK;
+}
+
+sg_status sg_bc_batch_bc_device(sg_bc_batch h, const float** dev_bc) {
+  SG_REQUIRE(h && dev_bc, SG_ERR_INVALID, "NULL argument");
+  *dev_bc = h->bc;
+  return SG_OK;
+}
+
+sg_status sg_bc_batch_level_records(sg_bc_batch h, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
+  SG_REQUIRE(h && count, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  unsigned long long it = 0;
+  if (h->last_k) SG_CUDA(cudaMemcpy(&it, h->result, sizeof(it), cudaMemcpyDeviceToHost));
+  uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
+  if (k > cap) k = cap;
+  if (host_records && k) SG_CUDA(cudaMemcpy(host_records, h->log, sizeof(sg_level_record) * k, cudaMemcpyDeviceToHost));
+  *count = k;
+  return SG_OK;
+}
+
+sg_status sg_bc_batched(sg_graph g, const uint32_t* host_sources, uint32_t k, float* host_bc) {
+  clear_error();
+  SG_REQUIRE(g && host_bc, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(k == 0 || host_sources, SG_ERR_INVALID, "sources is NULL");
+  sg_bc_batch h = nullptr;
+  SG_TRY(sg_bc_batch_create(g, 0, &h));
+  sg_status s = SG_OK;
+  for (uint32_t i = 0; i < k && s == SG_OK; i += 64)
+    s = sg_bc_batch_run(h, host_sources + i, std::min<uint32_t>(64, k - i), i > 0, nullptr);
+  if (s == SG_OK) s = sg_bc_batch_get(h, host_bc);
+  sg_bc_batch_destroy(h);
+  return s;
+}
+
+}  // extern "C"

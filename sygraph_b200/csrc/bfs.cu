@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
     P.cnt[gtid] = z;
   }
   if (threadIdx.x == 0) S.hn = 0;
+  if (P.mode == kLearned && P.mlp) sygraph::detail::mlp_stage(P.mlp, &S.mlp);
   if (!grid_sync(P.bar)) return;
 
   unsigned long long unexplored = P.m - deg_src;

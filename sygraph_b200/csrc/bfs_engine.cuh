@@ -71,6 +71,7 @@ struct Shared {
   uint32_t incl[kThreads];
   uint32_t flag[kThreads];
   int choice;
+  sygraph::detail::MlpStaged mlp;  // learned mode: parameters staged once per launch
 };
 
 // Per-thread context of one level's expansion.
@@ -194,7 +195,7 @@ __device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const
       if (log && threadIdx.x == 0)
         for (int i = 0; i < 12; i++) P.features[(size_t)level * 12 + i] = f[i];
       if (P.mode == kLearned && P.mlp) {
-        const int c = sygraph::detail::mlp_choose(P.mlp, f, P.allowed);
+        const int c = sygraph::detail::mlp_choose(&S.mlp, f, P.allowed);
         if (threadIdx.x == 0) S.choice = c;
       }
     }

@@ -43,6 +43,10 @@ TRAIN_GRAPHS = [
     ("grid512", "grid", dict(side=512, long_range_frac=0.0, seed=19)),
     ("grid1024_lr", "grid", dict(side=1024, long_range_frac=0.02, seed=20)),
     ("grid2048_lr", "grid", dict(side=2048, long_range_frac=0.005, seed=21)),
+    ("grid2048_lr2", "grid", dict(side=2048, long_range_frac=0.02, seed=22)),
+    ("grid3072_lr1", "grid", dict(side=3072, long_range_frac=0.01, seed=23)),
+    ("grid1536_lr3", "grid", dict(side=1536, long_range_frac=0.03, seed=24)),
+    ("rmat22_b", "rmat", dict(scale=22, seed=25)),
 ]
 EVAL_GRAPHS = [
     ("rmat22_heldout", "rmat", dict(scale=22, seed=101)),
