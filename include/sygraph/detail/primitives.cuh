@@ -123,6 +123,12 @@ __device__ __forceinline__ T block_sum(T v, T* s_red) {
   return t;
 }
 
+__device__ __forceinline__ uint32_t warp_min(uint32_t v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, d));
+  return v;
+}
+
 __device__ __forceinline__ bool bit_test(const uint32_t* bm, uint32_t i) {
   return (ld_cg(bm + (i >> 5)) >> (i & 31)) & 1u;
 }

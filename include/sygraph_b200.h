@@ -110,6 +110,9 @@ sg_status sg_free_host_pinned(void* host_ptr);
 /* kind: 0 host->device, 1 device->host, 2 device->device, 3 default (unified addressing) */
 sg_status sg_memcpy(void* dst, const void* src, uint64_t bytes, int kind, void* stream);
 sg_status sg_memset(void* dev_ptr, int value, uint64_t bytes, void* stream);
+/* A non-blocking stream (does not synchronise with the legacy default stream). */
+sg_status sg_stream_create(void** stream);
+sg_status sg_stream_destroy(void* stream);
 sg_status sg_stream_synchronize(void* stream);
 sg_status sg_device_synchronize(void);
 /* Number of kernels this library has launched in this process (all entry
@@ -352,6 +355,8 @@ sg_status sg_msbfs_run(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int
 sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int direction, float alpha,
                              float beta);
 sg_status sg_msbfs_get_depths(sg_msbfs h, uint32_t* host_depth);
+/* As sg_sssp_set_launch. */
+sg_status sg_msbfs_set_launch(sg_msbfs h, void* stream, uint32_t max_ctas);
 sg_status sg_msbfs_depths_device(sg_msbfs h, const uint32_t** dev_depth);
 /* Per-level log of the last batch (strategy 0 push / 2 pull, sizes and
  * degrees of the frontier union, device timestamps), as sg_bfs_level_records. */
@@ -390,6 +395,8 @@ sg_status sg_mlp_train(sg_mlp h, const float* dev_x, const float* dev_t, const f
  *   sg_bfs_log_features  records the twelve selector features of each level
  *                        decision; sg_bfs_level_features reads them (12 floats
  *                        per level, level 0 first). */
+/* As sg_sssp_set_launch. */
+sg_status sg_bfs_set_launch(sg_bfs b, void* stream, uint32_t max_ctas);
 sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len);
 sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed);
 sg_status sg_bfs_log_features(sg_bfs b, int enable);
@@ -403,6 +410,16 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out);
 sg_status sg_sssp_destroy(sg_sssp s);
 sg_status sg_sssp_init(sg_sssp s, uint32_t source);
 sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations);
+/* Near-far bucketing (not in the reference): relaxations to a distance
+ * below a threshold stay in the frontier, the others wait until the frontier
+ * empties and the threshold moves up by delta.  Distances are unchanged (the
+ * same fixed point); the iteration count and the work are not.  0 (the
+ * default) is the reference's frontier Bellman-Ford. */
+sg_status sg_sssp_set_delta(sg_sssp s, double delta);
+/* Stream of this instance's launches and copies (NULL: the graph's stream)
+ * and a cap on its persistent grid (0: every SM), so that several instances
+ * can share the GPU.  Waits for work queued on the previous stream. */
+sg_status sg_sssp_set_launch(sg_sssp s, void* stream, uint32_t max_ctas);
 sg_status sg_sssp_run_async(sg_sssp s);
 sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist);
 sg_status sg_sssp_distances_device(sg_sssp s, const void** dev_dist);

@@ -91,6 +91,8 @@ SIGNATURES = {
     "sg_free_host_pinned": (st, [vp]),
     "sg_memcpy": (st, [vp, vp, C.c_uint64, C.c_int, vp]),
     "sg_memset": (st, [vp, C.c_int, C.c_uint64, vp]),
+    "sg_stream_create": (st, [C.POINTER(vp)]),
+    "sg_stream_destroy": (st, [vp]),
     "sg_stream_synchronize": (st, [vp]),
     "sg_device_synchronize": (st, []),
     # graph
@@ -153,6 +155,10 @@ SIGNATURES = {
     "sg_mlp_gradient": (st, [vp, vp, vp, vp, C.c_uint32, f32p, f32p]),
     "sg_mlp_train": (st, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, f32p]),
     "sg_msbfs_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
+    "sg_sssp_set_delta": (st, [vp, C.c_double]),
+    "sg_sssp_set_launch": (st, [vp, vp, C.c_uint32]),
+    "sg_bfs_set_launch": (st, [vp, vp, C.c_uint32]),
+    "sg_msbfs_set_launch": (st, [vp, vp, C.c_uint32]),
     "sg_bc_batch_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
     "sg_bc_batch_destroy": (st, [vp]),
     "sg_bc_batch_run_async": (st, [vp, u32p, C.c_uint32, C.c_int]),

@@ -176,6 +176,10 @@ class SSSP:
     def run_async(self) -> None:
         call("sg_sssp_run_async", self.handle)
 
+    def set_delta(self, delta: float) -> None:
+        """Near-far threshold step (0: the reference's frontier Bellman-Ford)."""
+        call("sg_sssp_set_delta", self.handle, float(delta))
+
     def getDistances(self) -> np.ndarray:
         dt = np.float32 if self.G.value_type == WEIGHT_F32 else np.uint32
         out = np.empty(self.G.getVertexCount(), dt)

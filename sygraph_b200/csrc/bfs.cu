@@ -219,6 +219,8 @@ using namespace sgb;
 
 struct sg_bfs_s {
   sg_graph g = nullptr;
+  cudaStream_t stream = nullptr;  // launches and copies (the graph's stream unless set)
+  uint32_t max_ctas = 0;          // 0: the whole GPU
   uint32_t source = 0;
   bool initialised = false;
   uint32_t w0 = 0;
@@ -246,7 +248,7 @@ struct sg_bfs_s {
 
 static sg_status bfs_materialise(sg_bfs b) {
   if (!b->fresh) return SG_OK;
-  bfs::fill_depth_kernel<<<grid_for(b->g->n, 256), 256, 0, b->g->stream>>>(b->depth, b->g->n, b->source);
+  bfs::fill_depth_kernel<<<grid_for(b->g->n, 256), 256, 0, b->stream>>>(b->depth, b->g->n, b->source);
   SG_CHECK_LAUNCH();
   b->fresh = false;
   return SG_OK;
@@ -302,16 +304,16 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.result = b->result;
   P.schedule = b->schedule_len ? b->schedule : nullptr;
   P.schedule_len = b->schedule_len;
-  SG_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(*b->bar), g->stream));
-  return eng::launch_persistent(bfs::bfs_kernel, P, 2, g->stream);
+  SG_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(*b->bar), b->stream));
+  return eng::launch_persistent(bfs::bfs_kernel, P, 2, b->stream, b->max_ctas);
 }
 
 static sg_status bfs_collect(sg_bfs b, sg_bfs_details* details) {
   unsigned long long res[5];
   sygraph::detail::GridBarrier bar;
-  SG_CUDA(cudaMemcpyAsync(res, b->result, sizeof(res), cudaMemcpyDeviceToHost, b->g->stream));
-  SG_CUDA(cudaMemcpyAsync(&bar, b->bar, sizeof(bar), cudaMemcpyDeviceToHost, b->g->stream));
-  SG_CUDA(cudaStreamSynchronize(b->g->stream));
+  SG_CUDA(cudaMemcpyAsync(res, b->result, sizeof(res), cudaMemcpyDeviceToHost, b->stream));
+  SG_CUDA(cudaMemcpyAsync(&bar, b->bar, sizeof(bar), cudaMemcpyDeviceToHost, b->stream));
+  SG_CUDA(cudaStreamSynchronize(b->stream));
   if (bar.error) return fail(SG_ERR_TIMEOUT, "BFS engine: a grid barrier wait ran out");
   b->last_iterations = (uint32_t)res[0];
   if (details) {
@@ -340,6 +342,7 @@ sg_status sg_bfs_create(sg_graph g, sg_bfs* out) {
   SG_REQUIRE(g->n > 0, SG_ERR_INVALID, "graph has no vertices");
   sg_bfs b = new sg_bfs_s();
   b->g = g;
+  b->stream = g->stream;
   b->w0 = div_up(g->n, 32);
   b->w1 = div_up(b->w0, 32);
   const uint64_t n = g->n;
@@ -367,7 +370,7 @@ sg_status sg_bfs_create(sg_graph g, sg_bfs* out) {
 
 sg_status sg_bfs_destroy(sg_bfs b) {
   if (b) {
-    cudaStreamSynchronize(b->g->stream);
+    cudaStreamSynchronize(b->stream);
     bfs_release(b);
   }
   return SG_OK;
@@ -401,6 +404,15 @@ sg_status sg_bfs_run_async(sg_bfs b, int direction, float alpha, float beta) {
              "learned mode needs a selector (sg_bfs_set_selector)");
   b->fresh = false;
   return bfs_launch(b, direction, alpha, beta);
+}
+
+sg_status sg_bfs_set_launch(sg_bfs b, void* stream, uint32_t max_ctas) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_CUDA(cudaStreamSynchronize(b->stream));  // set-up work queued on the old stream
+  b->stream = stream ? (cudaStream_t)stream : b->g->stream;
+  b->max_ctas = max_ctas;
+  return SG_OK;
 }
 
 sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len) {
@@ -439,7 +451,7 @@ sg_status sg_bfs_log_features(sg_bfs b, int enable) {
 sg_status sg_bfs_level_features(sg_bfs b, float* host_features, uint32_t cap_levels, uint32_t* count) {
   SG_REQUIRE(b && count, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(b->features, SG_ERR_NOT_INITIALIZED, "feature logging is off (sg_bfs_log_features)");
-  SG_CUDA(cudaStreamSynchronize(b->g->stream));
+  SG_CUDA(cudaStreamSynchronize(b->stream));
   unsigned long long it = 0;
   SG_CUDA(cudaMemcpy(&it, b->result, sizeof(it), cudaMemcpyDeviceToHost));
   uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
@@ -459,8 +471,8 @@ sg_status sg_bfs_get_distances(sg_bfs b, uint32_t* host_depth) {
   SG_REQUIRE(b && host_depth, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(b->initialised, SG_ERR_NOT_INITIALIZED, "BFS instance not initialized");
   SG_TRY(bfs_materialise(b));
-  SG_CUDA(cudaMemcpyAsync(host_depth, b->depth, sizeof(uint32_t) * b->g->n, cudaMemcpyDeviceToHost, b->g->stream));
-  SG_CUDA(cudaStreamSynchronize(b->g->stream));
+  SG_CUDA(cudaMemcpyAsync(host_depth, b->depth, sizeof(uint32_t) * b->g->n, cudaMemcpyDeviceToHost, b->stream));
+  SG_CUDA(cudaStreamSynchronize(b->stream));
   return SG_OK;
 }
 
@@ -473,7 +485,7 @@ sg_status sg_bfs_distances_device(sg_bfs b, const uint32_t** dev_depth) {
 
 sg_status sg_bfs_level_records(sg_bfs b, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
   SG_REQUIRE(b && count, SG_ERR_INVALID, "NULL argument");
-  SG_CUDA(cudaStreamSynchronize(b->g->stream));
+  SG_CUDA(cudaStreamSynchronize(b->stream));
   unsigned long long it = 0;
   SG_CUDA(cudaMemcpy(&it, b->result, sizeof(it), cudaMemcpyDeviceToHost));
   uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);

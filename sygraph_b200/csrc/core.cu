@@ -145,6 +145,20 @@ sg_status sg_memset(void* dev_ptr, int value, uint64_t bytes, void* stream) {
   return SG_OK;
 }
 
+sg_status sg_stream_create(void** stream) {
+  clear_error();
+  SG_REQUIRE(stream, SG_ERR_INVALID, "NULL argument");
+  cudaStream_t st = nullptr;
+  SG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  *stream = st;
+  return SG_OK;
+}
+
+sg_status sg_stream_destroy(void* stream) {
+  if (stream) SG_CUDA(cudaStreamDestroy((cudaStream_t)stream));
+  return SG_OK;
+}
+
 sg_status sg_stream_synchronize(void* stream) {
   SG_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
   return SG_OK;

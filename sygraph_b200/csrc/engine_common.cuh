@@ -201,10 +201,12 @@ __device__ __forceinline__ uint32_t valid_bits(uint32_t wi, uint32_t w0, uint32_
   return (wi == w0 - 1 && rem) ? ((1u << rem) - 1u) : 0xffffffffu;
 }
 
-// Cooperative launch with a grid that fills every SM `blocks_per_sm` times.
+// Cooperative launch with a grid that fills every SM `blocks_per_sm` times,
+// or at most `max_grid` CTAs (a share of the GPU, so that launches on other
+// streams can be resident at the same time).
 template <typename Params>
 inline sg_status launch_persistent(void (*kernel)(Params), const Params& p, int blocks_per_sm, cudaStream_t stream,
-                                   unsigned* grid_out = nullptr) {
+                                   unsigned max_grid = 0, unsigned* grid_out = nullptr) {
   int dev = 0, coop = 0;
   SG_CUDA(cudaGetDevice(&dev));
   SG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
@@ -213,7 +215,8 @@ inline sg_status launch_persistent(void (*kernel)(Params), const Params& p, int 
   SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, 0));
   SG_REQUIRE(occ > 0, SG_ERR_CUDA, "engine kernel does not fit on an SM");
   const int per_sm = occ < blocks_per_sm ? occ : blocks_per_sm;
-  const unsigned grid = (unsigned)(per_sm * device_props().sm_count);
+  unsigned grid = (unsigned)(per_sm * device_props().sm_count);
+  if (max_grid && max_grid < grid) grid = max_grid;
   void* args[] = {(void*)&p};
   SG_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(kThreads), args, 0, stream));
   count_launch();

@@ -520,6 +520,8 @@ using namespace sgb;
 
 struct sg_msbfs_s {
   sg_graph g = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t max_ctas = 0;
   uint32_t k = 0, w0 = 0, w1 = 0, heavy_cap = 0;
   unsigned long long* seen = nullptr;
   unsigned long long* F = nullptr;
@@ -566,6 +568,7 @@ sg_status sg_msbfs_create(sg_graph g, uint32_t max_sources, sg_msbfs* out) {
   *out = nullptr;
   sg_msbfs h = new sg_msbfs_s();
   h->g = g;
+  h->stream = g->stream;
   h->k = max_sources;
   h->w0 = div_up(g->n, 32);
   h->w1 = div_up(h->w0, 32);
@@ -596,7 +599,7 @@ sg_status sg_msbfs_create(sg_graph g, uint32_t max_sources, sg_msbfs* out) {
 
 sg_status sg_msbfs_destroy(sg_msbfs h) {
   if (h) {
-    cudaStreamSynchronize(h->g->stream);
+    cudaStreamSynchronize(h->stream);
     msbfs_release(h);
   }
   return SG_OK;
@@ -610,8 +613,8 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
   SG_REQUIRE(direction >= SG_BFS_PUSH && direction <= SG_BFS_HYBRID, SG_ERR_INVALID, "unknown BFS direction");
   for (uint32_t i = 0; i < k; i++) SG_REQUIRE(host_sources[i] < h->g->n, SG_ERR_INVALID, "source out of range");
   sg_graph g = h->g;
-  SG_CUDA(cudaMemcpyAsync(h->sources, host_sources, sizeof(uint32_t) * k, cudaMemcpyHostToDevice, g->stream));
-  SG_CUDA(cudaMemsetAsync(h->bar, 0, sizeof(*h->bar), g->stream));
+  SG_CUDA(cudaMemcpyAsync(h->sources, host_sources, sizeof(uint32_t) * k, cudaMemcpyHostToDevice, h->stream));
+  SG_CUDA(cudaMemsetAsync(h->bar, 0, sizeof(*h->bar), h->stream));
   ms::Params P;
   P.n = g->n;
   P.w0 = h->w0;
@@ -644,7 +647,7 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
   P.log = h->log;
   P.result = h->result;
   h->last_k = k;
-  return eng::launch_persistent(ms::msbfs_kernel, P, 2, g->stream);
+  return eng::launch_persistent(ms::msbfs_kernel, P, 2, h->stream, h->max_ctas);
 }
 
 sg_status sg_msbfs_run(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int direction, float alpha, float beta,
@@ -652,9 +655,9 @@ sg_status sg_msbfs_run(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int
   SG_TRY(sg_msbfs_run_async(h, host_sources, k, direction, alpha, beta));
   unsigned long long r[4];
   sygraph::detail::GridBarrier b;
-  SG_CUDA(cudaMemcpyAsync(r, h->result, sizeof(r), cudaMemcpyDeviceToHost, h->g->stream));
-  SG_CUDA(cudaMemcpyAsync(&b, h->bar, sizeof(b), cudaMemcpyDeviceToHost, h->g->stream));
-  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  SG_CUDA(cudaMemcpyAsync(r, h->result, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+  SG_CUDA(cudaMemcpyAsync(&b, h->bar, sizeof(b), cudaMemcpyDeviceToHost, h->stream));
+  SG_CUDA(cudaStreamSynchronize(h->stream));
   if (b.error) return fail(SG_ERR_TIMEOUT, "multi-source BFS: a grid barrier wait ran out");
   if (details) {
     details->iterations = r[0];
@@ -665,18 +668,27 @@ sg_status sg_msbfs_run(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int
   return SG_OK;
 }
 
+sg_status sg_msbfs_set_launch(sg_msbfs h, void* stream, uint32_t max_ctas) {
+  clear_error();
+  SG_REQUIRE(h, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t)stream : h->g->stream;
+  h->max_ctas = max_ctas;
+  return SG_OK;
+}
+
 sg_status sg_msbfs_get_depths(sg_msbfs h, uint32_t* host_depth) {
   SG_REQUIRE(h && host_depth, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(h->last_k, SG_ERR_NOT_INITIALIZED, "no batch has run");
   SG_CUDA(cudaMemcpyAsync(host_depth, h->depth, sizeof(uint32_t) * (uint64_t)h->last_k * h->g->n,
-                          cudaMemcpyDeviceToHost, h->g->stream));
-  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+                          cudaMemcpyDeviceToHost, h->stream));
+  SG_CUDA(cudaStreamSynchronize(h->stream));
   return SG_OK;
 }
 
 sg_status sg_msbfs_level_records(sg_msbfs h, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
   SG_REQUIRE(h && count, SG_ERR_INVALID, "NULL argument");
-  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  SG_CUDA(cudaStreamSynchronize(h->stream));
   unsigned long long it = 0;
   if (h->last_k) SG_CUDA(cudaMemcpy(&it, h->result, sizeof(it), cudaMemcpyDeviceToHost));
   uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);

@@ -19,6 +19,13 @@ namespace {
 
 using namespace eng;
 
+// Near-far bookkeeping of one refill pass (three rotating slots).
+struct Refill {
+  unsigned long long moved, remaining;
+  uint32_t far_min;  // bit pattern of the smallest distance left in the far set
+  uint32_t pad[3];
+};
+
 template <typename W>
 struct SsspParams {
   PushLoop L;
@@ -26,18 +33,45 @@ struct SsspParams {
   W* dist;
   const W* w;
   unsigned long long* result;
+  uint32_t* far;  // w0 words: improved vertices at or beyond the threshold
+  Refill* refill;
+  W delta;        // 0: plain frontier Bellman-Ford (every improved vertex is near)
 };
+
+// Non-negative floats and unsigned integers both order like their bits.
+template <typename W>
+__device__ __forceinline__ uint32_t order_bits(W x) {
+  if constexpr (sizeof(W) == 4 && W(0.5) != W(0))
+    return __float_as_uint(x);
+  else
+    return (uint32_t)x;
+}
+template <typename W>
+__device__ __forceinline__ W from_order_bits(uint32_t b) {
+  if constexpr (sizeof(W) == 4 && W(0.5) != W(0))
+    return __uint_as_float(b);
+  else
+    return (W)b;
+}
 
 template <typename W>
 struct SsspVisitor : NextFrontier {
   using src_t = W;
   W* dist;
   const W* w;
+  uint32_t* far;
+  W threshold;
+  bool bucketed;
   __device__ __forceinline__ W src(uint32_t v) const { return ld_cg(dist + v); }
   __device__ __forceinline__ bool visit(uint32_t u, uint32_t e, W dv, uint32_t) {
     const W nd = dv + w[e];
     if (!(nd < ld_cg(dist + u))) return false;
-    return nd < sygraph::detail::atomic_min_nonneg(dist + u, nd);
+    if (!(nd < sygraph::detail::atomic_min_nonneg(dist + u, nd))) return false;
+    if (bucketed && !(nd < threshold)) {
+      atomicOr(far + (u >> 5), 1u << (u & 31));
+      return false;
+    }
+    return true;
   }
 };
 
@@ -58,18 +92,98 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
     Counters z = {};
     P.L.cnt[gtid] = z;
   }
+  const bool bucketed = P.delta > W(0);
+  if (bucketed) {
+    for (uint32_t i = gtid; i < w0; i += nthreads) st_cg(P.far + i, 0u);
+    if (gtid < 3) {
+      Refill z = {};
+      z.far_min = 0xffffffffu;
+      P.refill[gtid] = z;
+    }
+  }
   if (!grid_sync(P.L.bar)) return;
-  const uint32_t levels = push_levels(
-      P.L,
-      [&](uint32_t, uint32_t* fb_next) {
-        SsspVisitor<W> v;
-        v.fb_next = fb_next;
-        v.dist = P.dist;
-        v.w = P.w;
-        return v;
-      },
-      s_scan, s_red);
-  if (gtid == 0) P.result[0] = levels;
+  // Near-far: vertices improved to a distance below the threshold stay in the
+  // frontier, the others wait in the far set; when the near frontier is empty
+  // the threshold moves up by delta (or to the far set's minimum) and the far
+  // vertices below it become the next frontier.  Every improved vertex is
+  // relaxed again before the end, so the fixed point is Bellman-Ford's.
+  W threshold = P.delta;
+  unsigned long long total = 0;
+  uint32_t pass = 0;
+  for (;;) {
+    const uint32_t levels = push_levels(
+        P.L,
+        [&](uint32_t, uint32_t* fb_next) {
+          SsspVisitor<W> v;
+          v.fb_next = fb_next;
+          v.dist = P.dist;
+          v.w = P.w;
+          v.far = P.far;
+          v.threshold = threshold;
+          v.bucketed = bucketed;
+          return v;
+        },
+        s_scan, s_red);
+    if (!levels) return;
+    total += levels;
+    if (!bucketed) break;
+    bool refilled = false;
+    for (;;) {
+      // far vertices below the new threshold become fb[0]; fb[1], fb[2] cleared
+      Refill* R = P.refill + (pass % 3);
+      if (gtid == 0) {
+        Refill z = {};
+        z.far_min = 0xffffffffu;
+        P.refill[(pass + 1) % 3] = z;
+      }
+      if (gtid < 3) {
+        Counters z = {};
+        P.L.cnt[gtid] = z;
+      }
+      const W next_t = threshold + P.delta;
+      unsigned long long moved = 0, remaining = 0;
+      uint32_t fmin = 0xffffffffu;
+      for (uint32_t i = gtid; i < w0; i += nthreads) {
+        const uint32_t f = ld_cg(P.far + i);
+        uint32_t near = 0;
+        for (uint32_t b = f; b; b &= b - 1) {
+          const uint32_t bit = __ffs(b) - 1;
+          const W d = ld_cg(P.dist + i * 32 + bit);
+          if (d < next_t)
+            near |= 1u << bit;
+          else
+            fmin = min(fmin, order_bits<W>(d));
+        }
+        st_cg(P.L.fb + i, near);
+        st_cg(P.L.fb + w0 + i, 0u);
+        st_cg(P.L.fb + 2 * w0 + i, 0u);
+        if (f) st_cg(P.far + i, f & ~near);
+        moved += __popc(near);
+        remaining += __popc(f & ~near);
+      }
+      const unsigned long long mv = block_sum<unsigned long long>(moved, s_red);
+      const unsigned long long rm = block_sum<unsigned long long>(remaining, s_red);
+      fmin = sygraph::detail::warp_min(fmin);
+      if ((threadIdx.x & 31) == 0 && fmin != 0xffffffffu) atomicMin(&R->far_min, fmin);
+      if (threadIdx.x == 0) {
+        if (mv) atomicAdd(&R->moved, mv);
+        if (rm) atomicAdd(&R->remaining, rm);
+      }
+      if (!grid_sync(P.L.bar)) return;
+      pass++;
+      threshold = next_t;
+      if (ld_cg(&R->moved)) {
+        refilled = true;
+        break;
+      }
+      if (!ld_cg(&R->remaining)) break;
+      // nothing below the new threshold: jump to the far set's minimum
+      const W m = from_order_bits<W>(ld_cg(&R->far_min));
+      if (threshold < m) threshold = m;
+    }
+    if (!refilled) break;
+  }
+  if (gtid == 0) P.result[0] = total;
 }
 
 struct CcParams {
@@ -176,10 +290,15 @@ using namespace sgb;
 
 struct sg_sssp_s {
   sg_graph g = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t max_ctas = 0;
   uint32_t source = 0;
   bool initialised = false;
   bool fresh = false;  // initialised but not run: distances not written yet
   void* dist = nullptr;
+  uint32_t* far = nullptr;
+  Refill* refill = nullptr;
+  double delta = 0.0;  // near-far threshold step; 0 = the reference's frontier Bellman-Ford
   PushWorkspace ws;
 };
 
@@ -195,9 +314,9 @@ static sg_status sssp_materialise(sg_sssp s) {
   if (!s->fresh) return SG_OK;
   sg_graph g = s->g;
   if (g->value_type == SG_WEIGHT_F32)
-    fill_dist_kernel<float><<<grid_for(g->n, 256), 256, 0, g->stream>>>((float*)s->dist, g->n, s->source);
+    fill_dist_kernel<float><<<grid_for(g->n, 256), 256, 0, s->stream>>>((float*)s->dist, g->n, s->source);
   else
-    fill_dist_kernel<uint32_t><<<grid_for(g->n, 256), 256, 0, g->stream>>>((uint32_t*)s->dist, g->n, s->source);
+    fill_dist_kernel<uint32_t><<<grid_for(g->n, 256), 256, 0, s->stream>>>((uint32_t*)s->dist, g->n, s->source);
   SG_CHECK_LAUNCH();
   s->fresh = false;
   return SG_OK;
@@ -205,13 +324,16 @@ static sg_status sssp_materialise(sg_sssp s) {
 
 static sg_status sssp_launch(sg_sssp s) {
   sg_graph g = s->g;
-  SG_CUDA(cudaMemsetAsync(s->ws.bar, 0, sizeof(GridBarrier), g->stream));
+  SG_CUDA(cudaMemsetAsync(s->ws.bar, 0, sizeof(GridBarrier), s->stream));
   if (g->value_type == SG_WEIGHT_F32) {
-    SsspParams<float> P{s->ws.loop(g), s->source, (float*)s->dist, (const float*)g->fwd.val, s->ws.result};
-    return launch_persistent(sssp_kernel<float>, P, 2, g->stream);
+    SsspParams<float> P{s->ws.loop(g), s->source, (float*)s->dist, (const float*)g->fwd.val, s->ws.result,
+                        s->far, s->refill, (float)s->delta};
+    return launch_persistent(sssp_kernel<float>, P, 2, s->stream, s->max_ctas);
   }
-  SsspParams<uint32_t> P{s->ws.loop(g), s->source, (uint32_t*)s->dist, (const uint32_t*)g->fwd.val, s->ws.result};
-  return launch_persistent(sssp_kernel<uint32_t>, P, 2, g->stream);
+  const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
+  SsspParams<uint32_t> P{s->ws.loop(g), s->source, (uint32_t*)s->dist, (const uint32_t*)g->fwd.val, s->ws.result,
+                         s->far, s->refill, d};
+  return launch_persistent(sssp_kernel<uint32_t>, P, 2, s->stream, s->max_ctas);
 }
 
 extern "C" {
@@ -223,13 +345,18 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out) {
   *out = nullptr;
   sg_sssp s = new sg_sssp_s();
   s->g = g;
+  s->stream = g->stream;
   uint32_t* d = nullptr;
   sg_status st = dev_alloc(&d, g->n);
   s->dist = d;
   if (st == SG_OK) st = s->ws.alloc(g->n);
+  if (st == SG_OK) st = dev_alloc(&s->far, div_up(g->n, 32));
+  if (st == SG_OK) st = dev_alloc(&s->refill, 3);
   if (st != SG_OK) {
     s->ws.release();
     cudaFree(s->dist);
+    dev_free(s->far);
+    dev_free(s->refill);
     delete s;
     return st;
   }
@@ -239,11 +366,30 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out) {
 
 sg_status sg_sssp_destroy(sg_sssp s) {
   if (s) {
-    cudaStreamSynchronize(s->g->stream);
+    cudaStreamSynchronize(s->stream);
     s->ws.release();
     cudaFree(s->dist);
+    dev_free(s->far);
+    dev_free(s->refill);
     delete s;
   }
+  return SG_OK;
+}
+
+sg_status sg_sssp_set_launch(sg_sssp s, void* stream, uint32_t max_ctas) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  SG_CUDA(cudaStreamSynchronize(s->stream));
+  s->stream = stream ? (cudaStream_t)stream : s->g->stream;
+  s->max_ctas = max_ctas;
+  return SG_OK;
+}
+
+sg_status sg_sssp_set_delta(sg_sssp s, double delta) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  SG_REQUIRE(delta >= 0.0 && delta < 1e30, SG_ERR_INVALID, "delta must be finite and non-negative");
+  s->delta = delta;
   return SG_OK;
 }
 
@@ -267,15 +413,15 @@ sg_status sg_sssp_run_async(sg_sssp s) {
 
 sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations) {
   SG_TRY(sg_sssp_run_async(s));
-  return s->ws.finish(s->g->stream, iterations);
+  return s->ws.finish(s->stream, iterations);
 }
 
 sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist) {
   SG_REQUIRE(s && host_dist, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(s->initialised, SG_ERR_NOT_INITIALIZED, "SSSP instance not initialized");
   SG_TRY(sssp_materialise(s));
-  SG_CUDA(cudaMemcpyAsync(host_dist, s->dist, sizeof(uint32_t) * s->g->n, cudaMemcpyDeviceToHost, s->g->stream));
-  SG_CUDA(cudaStreamSynchronize(s->g->stream));
+  SG_CUDA(cudaMemcpyAsync(host_dist, s->dist, sizeof(uint32_t) * s->g->n, cudaMemcpyDeviceToHost, s->stream));
+  SG_CUDA(cudaStreamSynchronize(s->stream));
   return SG_OK;
 }
 

@@ -1,0 +1,84 @@
+"""Near-far SSSP (sg_sssp_set_delta): every threshold step gives the
+oracle's distances bit for bit, since bucketing only reorders relaxations
+towards the same least fixed point."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("delta", [0.01, 0.1, 0.5, 3.0, 1e6])
+def test_nearfar_rmat_f32(sg, oracle, rmat, delta):
+    g = rmat(14, perm_seed=3)
+    G = sg.graph.build.fromCSR(g)
+    s = sg.algorithms.SSSP(G)
+    s.set_delta(delta)
+    for src in [int(np.argmax(g.degrees()))] + [int(x) for x in sg.io.sample_sources(g, 2, seed=4)]:
+        s.init(src)
+        s.run()
+        ref = oracle.sssp_dijkstra(g, src)
+        assert np.array_equal(s.getDistances().view(np.uint32), ref.view(np.uint32)), (delta, src)
+
+
+@pytest.mark.parametrize("delta", [1, 7, 64, 1000])
+def test_nearfar_u32_grid_and_unreachable(sg, oracle, delta):
+    g = sg.io.grid(80, 0.02, seed=1, weight_seed=2, value_type=sg.WEIGHT_U32)
+    G = sg.graph.build.fromCSR(g)
+    s = sg.algorithms.SSSP(G)
+    s.set_delta(delta)
+    for src in (0, 3200):
+        s.init(src)
+        s.run()
+        assert np.array_equal(s.getDistances(), oracle.sssp_dijkstra(g, src))
+    rng = np.random.default_rng(3)
+    n = 2000
+    w = (rng.integers(1, 1 << 24, 6000) / float(1 << 24)).astype(np.float32)
+    gd = sg.io.fromCOO(n, rng.integers(0, n, 6000), rng.integers(0, n, 6000), w, dedupe=True,
+                       drop_self_loops=True)
+    s2 = sg.algorithms.SSSP(sg.graph.build.fromCSR(gd, sg.Properties(directed=True, weighted=True)))
+    s2.set_delta(0.05)
+    s2.init(7)
+    s2.run()
+    assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gd, 7))
+
+
+def test_nearfar_argument_checks_and_reset(sg, oracle, rmat):
+    g = rmat(10)
+    s = sg.algorithms.SSSP(sg.graph.build.fromCSR(g))
+    with pytest.raises(sg._lib.SygraphError):
+        s.set_delta(-1.0)
+    s.set_delta(0.2)
+    s.init(3)
+    s.run()
+    a = s.getDistances()
+    s.set_delta(0.0)  # back to the reference schedule
+    s.init(3)
+    s.run()
+    assert np.array_equal(a.view(np.uint32), s.getDistances().view(np.uint32))
+
+
+def test_instances_on_own_streams_with_grid_caps(sg, oracle, rmat):
+    """Two instances on separate streams with a share of the SMs each, run
+    back to back without a host wait, give the single-instance results."""
+    import ctypes as C
+    g = rmat(13, perm_seed=2)
+    G = sg.graph.build.fromCSR(g)
+    streams = []
+    for _ in range(2):
+        h = C.c_void_p()
+        sg._lib.call("sg_stream_create", C.byref(h))
+        streams.append(h)
+    b = sg.algorithms.BFS(G)
+    s = sg.algorithms.SSSP(G)
+    sg._lib.call("sg_bfs_set_launch", b.handle, streams[0], 74)
+    sg._lib.call("sg_sssp_set_launch", s.handle, streams[1], 74)
+    s.set_delta(0.3)
+    src = int(np.argmax(g.degrees()))
+    b.init(src)
+    s.init(src)
+    b.run_async(2, 15.0, 24.0)
+    s.run_async()
+    assert np.array_equal(b.getDistances(), oracle.bfs_levels(g, src))
+    assert np.array_equal(s.getDistances().view(np.uint32), oracle.sssp_dijkstra(g, src).view(np.uint32))
+    for h in streams:
+        sg._lib.call("sg_stream_destroy", h)
