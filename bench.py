@@ -41,6 +41,10 @@ SCALE, EDGE_FACTOR, A, B, C = 22, 16, 0.57, 0.19, 0.19
 GRAPH_SEED, WEIGHT_SEED, SOURCE_SEED = 1, 2, 3
 N_SOURCES = 64
 ALPHA, BETA = 15.0, 24.0
+# batched BFS: pull once the frontier's out-degree exceeds the in-degree of the
+# vertices some source has not reached (alpha 1); push again below n/beta
+MS_ALPHA, MS_BETA = 1.0, 24.0
+BC_SCALE, BC_SOURCES = 20, 64
 METRIC = "BFS/SSSP GTEPS & %HBM roofline on RMAT-22; learned+batched vs plain speedup"
 
 
@@ -405,21 +409,41 @@ def main():
     # the same 64 sources as one bit-parallel batch (one launch); identical depths
     mbfs = sg.algorithms.MultiBFS(G, len(srcs))
     for _ in range(2):
-        mbfs.run_async(srcs, 2, ALPHA, BETA)
+        mbfs.run_async(srcs, 2, MS_ALPHA, MS_BETA)
     torch.cuda.synchronize()
     mb_ms = []
     for _ in range(max(3, args.steps // 2)):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        mbfs.run_async(srcs, 2, ALPHA, BETA)
+        mbfs.run_async(srcs, 2, MS_ALPHA, MS_BETA)
         b.record()
         b.synchronize()
         mb_ms.append(a.elapsed_time(b))
-    mb_det = mbfs.run(srcs, 2, ALPHA, BETA)
+    mb_det = mbfs.run(srcs, 2, MS_ALPHA, MS_BETA)
     batched_ms = float(np.median(mb_ms))
     batched_gteps = mb_det["reached_edges"] / (batched_ms * 1e-3) / 1e9
     ms_bytes = 4 * (n + 1) + 4 * m + 4 * n * len(srcs)
     del mbfs
+
+    # batched Brandes BC: 64 sources per launch on RMAT-20 against the
+    # per-source engine on the same sources (float32, both checked equal within 1e-4)
+    gbc = sg.io.rmat(BC_SCALE, EDGE_FACTOR, A, B, C, seed=1)
+    Gbc = sg.graph.build.fromCSR(gbc)
+    sbc = sg.io.sample_sources(gbc, BC_SOURCES, seed=SOURCE_SEED)
+    bcb = sg.algorithms.BatchedBC(Gbc)
+    bc_det = bcb.run(sbc)
+    bc_ms = float(np.median([_launch_ms(torch, lambda: bcb.run_async(sbc)) for _ in range(3)]))
+    x_bc = bcb.getBC()
+    bc1 = sg.algorithms.BC(Gbc)
+    bc1.init(sbc)
+    bc1_ms = _launch_ms(torch, bc1.run)
+    y_bc = bc1.getBC().astype(np.float64)
+    bc_rel = float(np.max(np.abs(x_bc - y_bc) / np.maximum(1.0, np.abs(y_bc))))
+    bc_line = {"value": bc_det["reached_edges"] / (bc_ms * 1e-3) / 1e9, "unit": "GTEPS",
+               "workload": f"Brandes BC, {BC_SOURCES} sources, RMAT-{BC_SCALE} ef{EDGE_FACTOR}",
+               "launch_ms": bc_ms, "per_source_ms": bc1_ms, "speedup_vs_per_source": bc1_ms / bc_ms,
+               "max_rel_diff_vs_per_source": bc_rel, "forward_levels": bc_det["iterations"]}
+    del bcb, bc1, Gbc, gbc
 
     # SSSP on a subset of the same sources (reported beside the BFS line)
     sssp = sg.algorithms.SSSP(G)
@@ -471,6 +495,7 @@ def main():
                                      "frac": ms_bytes / (batched_ms * 1e-3) / 1e9 / peak,
                                      "bytes_per_launch": ms_bytes, "traffic": ncu_traffic("msbfs_kernel")}},
             "learned": learned,
+            "bc_batched": bc_line,
             "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
                      "roofline": {"bound": "hbm", "achieved": sssp_achieved, "peak": peak, "unit": "GB/s",
                                   "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,

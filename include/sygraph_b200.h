@@ -456,6 +456,8 @@ sg_status sg_bc_batch_run(sg_bc_batch h, const uint32_t* host_sources, uint32_t 
                           sg_bc_batch_details* details);
 sg_status sg_bc_batch_get(sg_bc_batch h, float* host_bc);
 sg_status sg_bc_batch_bc_device(sg_bc_batch h, const float** dev_bc);
+/* Log of the last batch: forward levels first (strategy 0: marked sparse
+ * level, 2: pull over every vertex not done), then backward levels (7). */
 sg_status sg_bc_batch_level_records(sg_bc_batch h, sg_level_record* host_records, uint32_t cap, uint32_t* count);
 /* One-shot: any number of sources, in batches of 64. */
 sg_status sg_bc_batched(sg_graph g, const uint32_t* host_sources, uint32_t k, float* host_bc);

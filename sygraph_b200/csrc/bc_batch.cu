@@ -7,27 +7,31 @@
 //
 // Layout: hist[L][v] = sources for which v has depth L (one uint64 array per
 // level, kept for the backward sweep), seen[v] = OR of hist[0..L][v], and
-// sigma / delta as vertex-major rows of 64 floats (row v is 256 bytes: lane
-// l of a warp holds sources 2l and 2l+1, so a row is one coalesced load).
+// sigma / q as vertex-major rows of 64 floats (row v is 256 bytes: lane l of
+// a warp holds sources 2l and 2l+1, so a row is one coalesced load), with
+// q_s(v) = (1 + delta_s(v)) / sigma_s(v), the one row a successor contributes.
 //
-// Forward level L (one fused pull pass, no atomics): every vertex u that some
-// source has not reached scans its in-neighbours w in adjacency order;
-// m = hist[L][w] & ~seen[u] are the sources reaching u through w at depth
-// L+1; u's new mask is the OR of the m's and sigma_s(u) the sum of
-// sigma_s(w) over the w with bit s in m, added in adjacency order.  Light
-// vertices take a warp each (lanes over 32 edges, then over sources);
-// vertices of degree >= kCtaDeg take a whole CTA, whose warps split the list
-// and add their partial sums in warp order.  So every sum has a fixed order:
-// results do not depend on scheduling.
+// Forward level L, one fused pull pass without atomics: every candidate u
+// (a vertex some source has not reached) scans its in-neighbours w in
+// adjacency order; m = hist[L][w] & ~seen[u] are the sources reaching u
+// through w at depth L+1; u's new mask is the OR of the m's and sigma_s(u)
+// the sum of sigma_s(w) over the w with bit s in m, added in adjacency order.
+// When the frontier's out-degree is small against the in-degree of the
+// vertices not yet done, a mark pass first flags the out-neighbours of the
+// frontier and only those are candidates (one more barrier, far less work).
+// Light vertices take a warp each (lanes over 32 edges, then over sources,
+// with up to kUnroll row loads in flight); vertices of degree >= kCtaDeg take
+// a whole CTA whose warps split the list and add their partial sums in warp
+// order.  So every sum has a fixed order: results do not depend on scheduling.
 //
 // Backward level L (from the deepest down to 1): every v with hist[L][v] != 0
 // gathers over its out-neighbours u with m = hist[L+1][u] & hist[L][v]:
-// acc_s += (1 + delta_s(u)) / sigma_s(u); delta_s(v) = sigma_s(v) * acc_s and
+// acc_s += q_s(u); delta_s(v) = sigma_s(v) * acc_s, q_s(v) is stored and
 // bc[v] += the warp's fixed-order sum of delta_s(v) over s in hist[L][v].
 //
-// One grid barrier per level in each sweep.  When the depth exceeds the
-// history capacity the kernel stops with a flag and the host enlarges the
-// history (or falls back to the per-source engine) and runs again.
+// One grid barrier per level in each sweep (two on marked forward levels).
+// When the depth exceeds the history capacity the kernel stops with a flag
+// and the host enlarges the history and runs again.
 #include <algorithm>
 #include <vector>
 
@@ -39,22 +43,27 @@ namespace bcb {
 using namespace eng;
 using u64 = unsigned long long;
 
-constexpr uint32_t kCtaDeg = 2048;  // degree from which a vertex takes a whole CTA
-constexpr uint32_t kRow = 64;       // floats per sigma / delta row
+constexpr uint32_t kCtaDeg = 2048;    // degree from which a vertex takes a whole CTA
+constexpr uint32_t kRow = 64;         // floats per sigma / q row
+constexpr uint32_t kUnroll = 8;       // row loads a warp keeps in flight
+constexpr uint32_t kBigList = 256;    // CTA-sized vertices a CTA defers per level (more: done by the warp)
+constexpr uint32_t kSparseRatio = 4;  // mark pass when frontier out-degree * ratio < undone in-degree
+constexpr uint32_t kBackwardLog = 7;  // strategy code of backward levels in the level log
 
 struct Counters {
-  u64 new_count;     // vertices that gained a source this level
-  u64 reached;       // sum over (source, newly reached vertex) of its out-degree
-  u64 big;           // CTA-sized vertices deferred to the CTA phase
-  u64 pad[5];
+  u64 new_count;  // vertices that gained a source this level
+  u64 reached;    // sum over (source, newly reached vertex) of its out-degree
+  u64 new_deg;    // out-degree sum of the vertices that gained a source
+  u64 done_in;    // in-degree sum of the vertices every source has now reached
+  u64 pad[4];
 };
 
 struct Params {
   uint32_t n, w0, k;
   uint64_t m;
-  const uint32_t* ro;   // out-edges (backward sweep, reached-edge counts)
+  const uint32_t* ro;   // out-edges (mark pass, backward sweep, reached-edge counts)
   const uint32_t* col;
-  const uint32_t* iro;  // in-edges (forward sweep); alias ro / col when undirected
+  const uint32_t* iro;  // in-edges (forward pull); alias ro / col when undirected
   const uint32_t* icol;
   const uint32_t* sources;
   u64 all;
@@ -63,16 +72,16 @@ struct Params {
   uint32_t cap_levels;
   uint32_t* act;        // cap_levels * w0: hist[L] != 0
   uint32_t* done;       // w0: every source reached (or no in-edge)
+  uint32_t* cand;       // w0: marked candidates of a sparse level (zero between levels)
   const uint32_t* no_in_edges;
-  uint32_t* big_list;   // n: CTA-sized vertices of the current level
   float* sigma;         // n * 64
-  float* delta;         // n * 64
+  float* q;             // n * 64
   float* bc;            // n
   int accumulate;       // add into bc instead of overwriting
-  Counters* cnt;        // 2 slots, alternating by level
+  Counters* cnt;        // 3 rotating slots
   GridBarrier* bar;
   sg_level_record* log;
-  u64* result;          // [levels, overflow, reached_edges, backward_levels]
+  u64* result;          // [forward levels, overflow, reached_edges, log entries]
 };
 
 struct Shared {
@@ -80,7 +89,15 @@ struct Shared {
   u64 mask[16];
   uint32_t scan[32];
   u64 red[32];
-  uint32_t nbig;
+};
+
+struct BigList {
+  uint32_t v[kBigList];
+  uint32_t count;
+};
+
+struct Local {
+  u64 new_count = 0, reached = 0, new_deg = 0, done_in = 0;
 };
 
 __device__ __forceinline__ u64 shfl64(u64 x, uint32_t src) {
@@ -101,6 +118,35 @@ __device__ __forceinline__ float2 row2(const float* rows, uint32_t w, uint32_t l
   return __ldcg(reinterpret_cast<const float2*>(rows + (size_t)w * kRow) + lane);
 }
 
+// Adds, in lane order, the rows of the lanes set in `ball` (warp-uniform):
+// lane j of the ballot contributes row x_j to the sources of its mask m_j.
+// Up to kUnroll independent row loads are issued before their additions.
+__device__ __forceinline__ void add_rows(const float* rows, uint32_t ball, uint32_t x, u64 m, float& a0, float& a1) {
+  const uint32_t lane = threadIdx.x & 31;
+  while (ball) {
+    float2 r[kUnroll];
+    uint32_t bs[kUnroll];
+#pragma unroll
+    for (uint32_t t = 0; t < kUnroll; t++) {
+      bs[t] = 0u;
+      r[t] = make_float2(0.f, 0.f);
+      if (ball) {
+        const uint32_t j = __ffs(ball) - 1;
+        ball &= ball - 1;
+        const uint32_t xj = __shfl_sync(kFullMask, x, j);
+        const u64 mj = shfl64(m, j);
+        bs[t] = (uint32_t)(mj >> (2 * lane)) & 3u;
+        if (bs[t]) r[t] = row2(rows, xj, lane);
+      }
+    }
+#pragma unroll
+    for (uint32_t t = 0; t < kUnroll; t++) {
+      if (bs[t] & 1u) a0 += r[t].x;
+      if (bs[t] & 2u) a1 += r[t].y;
+    }
+  }
+}
+
 // Forward gather over in-edges [beg, end) of u for level L: ORs the masks
 // m = hist_L[w] & ~su and adds sigma rows.  Returns the OR (in every lane).
 __device__ __forceinline__ u64 forward_gather(const Params& P, const u64* hist_L, uint32_t beg, uint32_t end, u64 su,
@@ -116,25 +162,13 @@ __device__ __forceinline__ u64 forward_gather(const Params& P, const u64* hist_L
       mw = __ldcg(hist_L + w) & ~su;
     }
     acc_mask |= mw;
-    uint32_t ball = __ballot_sync(kFullMask, mw != 0);
-    while (ball) {
-      const uint32_t j = __ffs(ball) - 1;
-      ball &= ball - 1;
-      const uint32_t wj = __shfl_sync(kFullMask, w, j);
-      const u64 mj = shfl64(mw, j);
-      const uint32_t b = (uint32_t)(mj >> (2 * lane)) & 3u;
-      if (b) {
-        const float2 r = row2(P.sigma, wj, lane);
-        if (b & 1u) a0 += r.x;
-        if (b & 2u) a1 += r.y;
-      }
-    }
+    add_rows(P.sigma, __ballot_sync(kFullMask, mw != 0), w, mw, a0, a1);
   }
   return warp_or64(acc_mask);
 }
 
-// Backward gather over out-edges [beg, end) of v: acc_s += (1+delta_s(u))/sigma_s(u)
-// for the u with bit s in hist_next[u] & fv.
+// Backward gather over out-edges [beg, end) of v: acc_s += q_s(u) for the u
+// with bit s in hist_next[u] & fv.
 __device__ __forceinline__ void backward_gather(const Params& P, const u64* hist_next, uint32_t beg, uint32_t end,
                                                 u64 fv, float& a0, float& a1) {
   const uint32_t lane = threadIdx.x & 31;
@@ -146,28 +180,9 @@ __device__ __forceinline__ void backward_gather(const Params& P, const u64* hist
       u = P.col[e];
       mu = __ldcg(hist_next + u) & fv;
     }
-    uint32_t ball = __ballot_sync(kFullMask, mu != 0);
-    while (ball) {
-      const uint32_t j = __ffs(ball) - 1;
-      ball &= ball - 1;
-      const uint32_t uj = __shfl_sync(kFullMask, u, j);
-      const u64 mj = shfl64(mu, j);
-      const uint32_t b = (uint32_t)(mj >> (2 * lane)) & 3u;
-      if (b) {
-        const float2 s = row2(P.sigma, uj, lane);
-        const float2 d = row2(P.delta, uj, lane);
-        if (b & 1u) a0 += (1.0f + d.x) / s.x;
-        if (b & 2u) a1 += (1.0f + d.y) / s.y;
-      }
-    }
+    add_rows(P.q, __ballot_sync(kFullMask, mu != 0), u, mu, a0, a1);
   }
 }
-
-constexpr uint32_t kBigList = 256;  // CTA-sized vertices a CTA defers per level (more: done by the warp)
-
-struct Local {
-  u64 new_count = 0, reached = 0;
-};
 
 // Forward result of vertex u: seen, hist[L+1], sigma entries of its new
 // sources, the act / done bits.  Every lane calls; nm is warp-uniform.
@@ -185,31 +200,37 @@ __device__ __forceinline__ void forward_finish(const Params& P, u64* hist_N, uin
     __stcg(row + 1, a1);
   }
   if (lane == 0) {
+    const uint32_t dout = P.ro[u + 1] - P.ro[u];
     st_cg(P.seen + u, su | nm);
     st_cg(hist_N + u, nm);
     atomicOr(act_N + (u >> 5), 1u << (u & 31));
-    if ((su | nm) == P.all) atomicOr(P.done + (u >> 5), 1u << (u & 31));
+    if ((su | nm) == P.all) {
+      atomicOr(P.done + (u >> 5), 1u << (u & 31));
+      loc.done_in += P.iro[u + 1] - P.iro[u];
+    }
     loc.new_count++;
-    loc.reached += (u64)__popcll(nm) * (P.ro[u + 1] - P.ro[u]);
+    loc.new_deg += dout;
+    loc.reached += (u64)__popcll(nm) * dout;
   }
 }
 
-// Backward result of vertex v: delta entries for its sources at this level
-// and bc[v] += their fixed-order sum.
+// Backward result of vertex v: delta_s(v) = sigma_s(v) * acc_s for its
+// sources at this level, q_s(v) = (1 + delta_s(v)) / sigma_s(v) stored for
+// its predecessors, and bc[v] += the fixed-order sum of the deltas.
 __device__ __forceinline__ void backward_finish(const Params& P, uint32_t v, u64 fv, float a0, float a1) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t b = (uint32_t)(fv >> (2 * lane)) & 3u;
   float d0 = 0.f, d1 = 0.f;
   if (b) {
     const float2 s = row2(P.sigma, v, lane);
-    float* row = P.delta + (size_t)v * kRow + 2 * lane;
+    float* row = P.q + (size_t)v * kRow + 2 * lane;
     if (b & 1u) {
       d0 = s.x * a0;
-      __stcg(row, d0);
+      __stcg(row, (1.0f + d0) / s.x);
     }
     if (b & 2u) {
       d1 = s.y * a1;
-      __stcg(row + 1, d1);
+      __stcg(row + 1, (1.0f + d1) / s.y);
     }
   }
   float t = d0 + d1;
@@ -218,8 +239,8 @@ __device__ __forceinline__ void backward_finish(const Params& P, uint32_t v, u64
   if (lane == 0) st_cg(P.bc + v, ld_cg(P.bc + v) + t);
 }
 
-// A CTA-sized vertex: 16 warps gather contiguous slices of its list, partial
-// sums are added in warp order.  Called by every thread of the block.
+// A CTA-sized vertex: the warps gather contiguous slices of its list and the
+// partial sums are added in warp order.  Called by every thread of the block.
 template <bool kForward>
 __device__ __forceinline__ void cta_vertex(const Params& P, Shared& S, const u64* hist_src, u64* hist_N,
                                            uint32_t* act_N, uint32_t x, Local& loc) {
@@ -259,27 +280,59 @@ __device__ __forceinline__ void cta_vertex(const Params& P, Shared& S, const u64
 __device__ __forceinline__ void block_add(Local& loc, Shared& S, Counters* C) {
   const u64 a = block_sum<u64>(loc.new_count, S.red);
   const u64 b = block_sum<u64>(loc.reached, S.red);
+  const u64 c = block_sum<u64>(loc.new_deg, S.red);
+  const u64 d = block_sum<u64>(loc.done_in, S.red);
   if (threadIdx.x == 0) {
     if (a) atomicAdd(&C->new_count, a);
     if (b) atomicAdd(&C->reached, b);
+    if (c) atomicAdd(&C->new_deg, c);
+    if (d) atomicAdd(&C->done_in, d);
   }
 }
 
-struct BigList {
-  uint32_t v[kBigList];
-  uint32_t count;
-};
+// Defers vertex x to the CTA phase when it is CTA-sized and the list has room;
+// returns true when deferred.  Warp-uniform.
+__device__ __forceinline__ bool defer_big(BigList& B, uint32_t x, uint32_t deg) {
+  if (deg < kCtaDeg) return false;
+  uint32_t slot = kBigList;
+  if ((threadIdx.x & 31) == 0) slot = atomicAdd(&B.count, 1u);
+  slot = __shfl_sync(kFullMask, slot, 0);
+  if (slot >= kBigList) return false;
+  if ((threadIdx.x & 31) == 0) B.v[slot] = x;
+  return true;
+}
+
+// Mark pass of a sparse level: out-neighbours of the frontier that some
+// source has not reached become candidates (idempotent bit sets).
+__device__ __forceinline__ void mark_candidates(const Params& P, const uint32_t* act_L) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t wi = gwarp; wi < P.w0; wi += nwarps) {
+    uint32_t word = ld_cg(act_L + wi);
+    while (word) {
+      const uint32_t v = wi * 32 + (__ffs(word) - 1);
+      word &= word - 1;
+      const uint32_t beg = P.ro[v], end = P.ro[v + 1];
+      for (uint32_t e = beg + lane; e < end; e += 32) {
+        const uint32_t u = P.col[e];
+        const uint32_t b = 1u << (u & 31);
+        if ((ld_cg(P.done + (u >> 5)) & b) || (ld_cg(P.cand + (u >> 5)) & b)) continue;
+        atomicOr(P.cand + (u >> 5), b);
+      }
+    }
+  }
+}
 
 __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
   __shared__ Shared S;
   __shared__ BigList B;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
-  const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
   const uint32_t n = P.n, w0 = P.w0;
 
-  // ---- clear: seen, hist[0..1], act[0..1], done = no in-edges, bc
+  // ---- clear: seen, hist[0..1], act[0..1], cand, done = no in-edges, bc
   for (uint32_t i = gtid; i < n; i += nthreads) {
     st_cg(P.seen + i, 0ull);
     st_cg(P.hist + i, 0ull);
@@ -289,6 +342,7 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
   for (uint32_t i = gtid; i < w0; i += nthreads) {
     st_cg(P.act + i, 0u);
     st_cg(P.act + w0 + i, 0u);
+    st_cg(P.cand + i, 0u);
     st_cg(P.done + i, P.no_in_edges[i]);
   }
   if (gtid < 3) {
@@ -314,6 +368,16 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
   }
   if (!grid_sync(P.bar)) return;
 
+  // frontier out-degree (distinct sources) and in-degree of the vertices not done
+  u64 frontier_deg = 0;
+  for (uint32_t i = 0; i < P.k; i++) {
+    bool first = true;
+    for (uint32_t j = 0; j < i; j++) first &= P.sources[j] != P.sources[i];
+    if (first) frontier_deg += P.ro[P.sources[i] + 1] - P.ro[P.sources[i]];
+  }
+  u64 undone_in = P.m;
+  uint32_t n_log = 0;
+
   // ---- forward sweep
   uint32_t L = 0;
   bool overflow = false;
@@ -337,22 +401,24 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
       uint32_t* a2 = P.act + (size_t)(L + 2) * w0;
       for (uint32_t i = gtid; i < w0; i += nthreads) st_cg(a2 + i, 0u);
     }
+    const bool sparse = frontier_deg * kSparseRatio < undone_in;
+    if (sparse) {
+      mark_candidates(P, P.act + (size_t)L * w0);
+      if (!grid_sync(P.bar)) return;
+    }
     Local loc;
     for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
       uint32_t cand = ~ld_cg(P.done + wi) & valid_bits(wi, w0, n);
+      if (sparse) {
+        const uint32_t c = ld_cg(P.cand + wi);
+        if (c) st_cg(P.cand + wi, 0u);  // the mark bitmap is zero again for the next level
+        cand &= c;
+      }
       while (cand) {
         const uint32_t u = wi * 32 + (__ffs(cand) - 1);
         cand &= cand - 1;
         const uint32_t beg = P.iro[u], end = P.iro[u + 1];
-        if (end - beg >= kCtaDeg) {
-          uint32_t slot = kBigList;
-          if (lane == 0) slot = atomicAdd(&B.count, 1u);
-          slot = __shfl_sync(kFullMask, slot, 0);
-          if (slot < kBigList) {
-            if (lane == 0) B.v[slot] = u;
-            continue;
-          }
-        }
+        if (defer_big(B, u, end - beg)) continue;
         const u64 su = ld_cg(P.seen + u);
         float a0 = 0.f, a1 = 0.f;
         const u64 nm = forward_gather(P, hist_L, beg, end, su, a0, a1);
@@ -368,27 +434,34 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
     if (!grid_sync(P.bar)) return;
     const u64 next = ld_cg(&C->new_count);
     reached_total += ld_cg(&C->reached);
-    if (gtid == 0 && L < kMaxLog) {
+    frontier_deg = ld_cg(&C->new_deg);
+    undone_in -= ld_cg(&C->done_in);
+    if (gtid == 0 && n_log < kMaxLog) {
       sg_level_record r = {};
       r.level = L;
-      r.strategy = 2;
+      r.strategy = sparse ? 0u : 2u;
       r.next_size = (uint32_t)next;
+      r.next_degree = frontier_deg;
+      r.unexplored_degree = undone_in;
       r.t_start_ns = t0;
       r.t_end_ns = sygraph::detail::global_timer_ns();
-      P.log[L] = r;
+      P.log[n_log] = r;
     }
+    n_log++;
     if (next == 0) break;
   }
   if (overflow) {
     if (gtid == 0) {
       P.result[0] = L + 1;
       P.result[1] = 1;
+      P.result[3] = min(n_log, kMaxLog);
     }
     return;
   }
-  // ---- backward sweep: levels L .. 1 (L is the deepest non-empty level)
+  // ---- backward sweep: levels Lmax .. 1 (Lmax is the deepest non-empty level)
   const uint32_t Lmax = L;
   for (uint32_t Lb = Lmax; Lb >= 1; Lb--) {
+    const uint64_t t0 = gtid == 0 ? sygraph::detail::global_timer_ns() : 0;
     const u64* hist_B = P.hist + (size_t)Lb * n;
     const u64* hist_next = Lb < Lmax ? P.hist + (size_t)(Lb + 1) * n : nullptr;
     const uint32_t* act_B = P.act + (size_t)Lb * w0;
@@ -399,15 +472,7 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
         const uint32_t v = wi * 32 + (__ffs(word) - 1);
         word &= word - 1;
         const uint32_t beg = P.ro[v], end = P.ro[v + 1];
-        if (end - beg >= kCtaDeg && hist_next) {
-          uint32_t slot = kBigList;
-          if (lane == 0) slot = atomicAdd(&B.count, 1u);
-          slot = __shfl_sync(kFullMask, slot, 0);
-          if (slot < kBigList) {
-            if (lane == 0) B.v[slot] = v;
-            continue;
-          }
-        }
+        if (hist_next && defer_big(B, v, end - beg)) continue;
         const u64 fv = ld_cg(hist_B + v);
         float a0 = 0.f, a1 = 0.f;
         if (hist_next) backward_gather(P, hist_next, beg, end, fv, a0, a1);
@@ -421,12 +486,21 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
     __syncthreads();
     if (threadIdx.x == 0) B.count = 0;
     if (!grid_sync(P.bar)) return;
+    if (gtid == 0 && n_log < kMaxLog) {
+      sg_level_record r = {};
+      r.level = Lb;
+      r.strategy = kBackwardLog;
+      r.t_start_ns = t0;
+      r.t_end_ns = sygraph::detail::global_timer_ns();
+      P.log[n_log] = r;
+    }
+    n_log++;
   }
   if (gtid == 0) {
     P.result[0] = Lmax + 1;
     P.result[1] = 0;
     P.result[2] = reached_total;
-    P.result[3] = Lmax;
+    P.result[3] = min(n_log, kMaxLog);
   }
 }
 
@@ -452,7 +526,8 @@ struct sg_bc_batch_s {
   unsigned long long* seen = nullptr;
   unsigned long long* hist = nullptr;
   uint32_t *act = nullptr, *done = nullptr, *no_in = nullptr, *sources = nullptr;
-  float *sigma = nullptr, *delta = nullptr, *bc = nullptr;
+  uint32_t* cand = nullptr;
+  float *sigma = nullptr, *q = nullptr, *bc = nullptr;
   bcb::Counters* cnt = nullptr;
   sygraph::detail::GridBarrier* bar = nullptr;
   sg_level_record* log = nullptr;
@@ -470,7 +545,8 @@ void bcb_release(sg_bc_batch h) {
   dev_free(h->no_in);
   dev_free(h->sources);
   dev_free(h->sigma);
-  dev_free(h->delta);
+  dev_free(h->q);
+  dev_free(h->cand);
   dev_free(h->bc);
   dev_free(h->cnt);
   dev_free(h->bar);
@@ -522,9 +598,9 @@ sg_status bcb_launch(sg_bc_batch h, uint32_t k, int accumulate) {
   P.act = h->act;
   P.done = h->done;
   P.no_in_edges = h->no_in;
-  P.big_list = nullptr;
   P.sigma = h->sigma;
-  P.delta = h->delta;
+  P.q = h->q;
+  P.cand = h->cand;
   P.bc = h->bc;
   P.accumulate = accumulate;
   P.cnt = h->cnt;
@@ -553,7 +629,7 @@ sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* o
   sg_status s;
   if ((s = dev_alloc(&h->seen, n)) || (s = dev_alloc(&h->done, h->w0)) || (s = dev_alloc(&h->no_in, h->w0)) ||
       (s = dev_alloc(&h->sources, 64)) || (s = dev_alloc(&h->sigma, n * bcb::kRow)) ||
-      (s = dev_alloc(&h->delta, n * bcb::kRow)) || (s = dev_alloc(&h->bc, n)) || (s = dev_alloc(&h->cnt, 3)) ||
+      (s = dev_alloc(&h->q, n * bcb::kRow)) || (s = dev_alloc(&h->cand, h->w0)) || (s = dev_alloc(&h->bc, n)) || (s = dev_alloc(&h->cnt, 3)) ||
       (s = dev_alloc(&h->bar, 1)) || (s = dev_alloc(&h->log, SG_MAX_LOGGED_LEVELS)) ||
       (s = dev_alloc(&h->result, 4)) || (s = bcb_history(h, levels))) {
     bcb_release(h);
@@ -638,7 +714,7 @@ sg_status sg_bc_batch_level_records(sg_bc_batch h, sg_level_record* host_records
   SG_REQUIRE(h && count, SG_ERR_INVALID, "NULL argument");
   SG_CUDA(cudaStreamSynchronize(h->g->stream));
   unsigned long long it = 0;
-  if (h->last_k) SG_CUDA(cudaMemcpy(&it, h->result, sizeof(it), cudaMemcpyDeviceToHost));
+  if (h->last_k) SG_CUDA(cudaMemcpy(&it, h->result + 3, sizeof(it), cudaMemcpyDeviceToHost));
   uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
   if (k > cap) k = cap;
   if (host_records && k) SG_CUDA(cudaMemcpy(host_records, h->log, sizeof(sg_level_record) * k, cudaMemcpyDeviceToHost));

@@ -182,9 +182,19 @@ def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F) -> dict:
     return {"total": tot, "traversals": rows}
 
 
-def train(data: dict, steps: int = 6000, lr: float = 3e-3, seed: int = 0, holdout_groups: int = 0) -> Mlp:
+def level_weights(Y: np.ndarray, lo: float = 0.25, hi: float = 8.0) -> np.ndarray:
+    """Per-sample loss weights: the square root of the level's best time
+    against the median level, clipped to [lo, hi], so that the levels that
+    dominate a traversal's time dominate the fit."""
+    best = np.exp(Y.min(1))
+    return np.clip(np.sqrt(best / np.median(best)), lo, hi).astype(np.float32)
+
+
+def train(data: dict, steps: int = 6000, lr: float = 3e-3, seed: int = 0, weighted: bool = True) -> Mlp:
     """Fit the MLP on the GPU; normalisation and trusted range from X."""
     X, Y, M = data["X"], data["Y"], data["M"]
+    if weighted:
+        M = (M * level_weights(Y)[:, None]).astype(np.float32)
     rng = np.random.default_rng(seed)
     I, H, O = IN, 32, OUT
     p = np.zeros(H * I + H + H * H + H + O * H + O + 4 * I, np.float32)
