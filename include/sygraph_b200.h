@@ -468,6 +468,52 @@ sg_status sg_bc_batched(sg_graph g, const uint32_t* host_sources, uint32_t k, fl
  * (u,v) with u < v, |N(u) n N(v)| added to u. */
 sg_status sg_tc(sg_graph g, uint64_t* total, uint64_t* host_per_vertex);
 
+/* -------------------------------------------------------------- serving -- */
+/* Query serving with continuous batching (no counterpart in the reference,
+ * which runs one algorithm call at a time).  Graphs stay resident; queries are
+ * submitted from any host thread and a dispatcher thread runs them on `slots`
+ * CUDA streams, each launch capped to ctas_per_slot CTAs so that launches of
+ * different slots overlap on the GPU.  A query is admitted when a slot is free
+ * and its workspace (per slot and graph) fits in memory_budget, after idle
+ * workspaces are evicted least recently used first; otherwise it waits.  When
+ * a slot frees, the pending BFS queries of the oldest query's graph (up to
+ * max_batch, at least min_batch) run as one batched launch; SSSP queries run
+ * singly, near-far with sssp_delta when it is > 0.  Each result equals the
+ * single-query entry point's, bit for bit.  host_out receives n depths
+ * (uint32) or distances (the graph's weight type); pinned memory keeps the
+ * copy asynchronous, NULL skips it. */
+typedef struct sg_server_s* sg_server;
+typedef struct {
+  uint32_t slots;          /* concurrent launches (0: 4) */
+  uint32_t max_batch;      /* BFS queries per batched launch, <= 64 (0: 64) */
+  uint32_t min_batch;      /* fewer pending BFS queries of a graph run singly (0: 4) */
+  uint32_t ctas_per_slot;  /* persistent grid per launch (0: 2 * SMs / slots) */
+  uint64_t memory_budget;  /* workspace bytes (0: half the free device memory) */
+  double sssp_delta;       /* near-far step of SSSP queries (0: the reference schedule) */
+} sg_server_config;
+#define SG_QUERY_BFS 0
+#define SG_QUERY_SSSP 1
+typedef struct {
+  sg_status status;
+  uint32_t graph, source, batch_size;
+  int kind;
+  uint64_t submit_ns, start_ns, end_ns; /* host steady clock */
+} sg_query_result;
+typedef struct {
+  uint64_t submitted, completed, failed, launches, batched_queries;
+  uint64_t evictions, deferred_admissions;
+  uint64_t workspace_bytes, peak_workspace_bytes, memory_budget;
+} sg_server_stats;
+sg_status sg_server_create(const sg_server_config* cfg, sg_server* out);
+sg_status sg_server_destroy(sg_server s);
+sg_status sg_server_add_graph(sg_server s, sg_graph g, uint32_t* graph_id);
+sg_status sg_server_submit(sg_server s, uint32_t graph_id, int kind, uint32_t source, void* host_out,
+                           uint64_t* ticket);
+/* Blocks until the query completes (SG_ERR_TIMEOUT after timeout_s; <= 0 waits without limit). */
+sg_status sg_server_wait(sg_server s, uint64_t ticket, double timeout_s, sg_query_result* result);
+sg_status sg_server_drain(sg_server s, double timeout_s);
+sg_status sg_server_get_stats(sg_server s, sg_server_stats* stats);
+
 /* ------------------------------------------------------- host graph I/O -- */
 /* Host CSR owned by the library (malloc'd); free with sg_host_csr_free. */
 typedef struct {

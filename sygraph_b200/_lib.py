@@ -65,6 +65,22 @@ class BcBatchDetails(C.Structure):
                 ("history_retries", C.c_uint64)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("max_batch", C.c_uint32), ("min_batch", C.c_uint32),
+                ("ctas_per_slot", C.c_uint32), ("memory_budget", C.c_uint64), ("sssp_delta", C.c_double)]
+
+
+class QueryResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("graph", C.c_uint32), ("source", C.c_uint32), ("batch_size", C.c_uint32),
+                ("kind", C.c_int), ("submit_ns", C.c_uint64), ("start_ns", C.c_uint64), ("end_ns", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "failed", "launches", "batched_queries",
+                                          "evictions", "deferred_admissions", "workspace_bytes",
+                                          "peak_workspace_bytes", "memory_budget")]
+
+
 class HostCSR(C.Structure):
     _fields_ = [("n", C.c_uint32), ("m", C.c_uint64), ("row_offsets", u32p), ("column_indices", u32p),
                 ("values", vp), ("value_type", C.c_int), ("flags", C.c_uint32)]
@@ -155,6 +171,13 @@ SIGNATURES = {
     "sg_mlp_gradient": (st, [vp, vp, vp, vp, C.c_uint32, f32p, f32p]),
     "sg_mlp_train": (st, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, f32p]),
     "sg_msbfs_create": (st, [vp, C.c_uint32, C.POINTER(vp)]),
+    "sg_server_create": (st, [C.POINTER(ServerConfig), C.POINTER(vp)]),
+    "sg_server_destroy": (st, [vp]),
+    "sg_server_add_graph": (st, [vp, vp, u32p]),
+    "sg_server_submit": (st, [vp, C.c_uint32, C.c_int, C.c_uint32, vp, u64p]),
+    "sg_server_wait": (st, [vp, C.c_uint64, C.c_double, C.POINTER(QueryResult)]),
+    "sg_server_drain": (st, [vp, C.c_double]),
+    "sg_server_get_stats": (st, [vp, C.POINTER(ServerStats)]),
     "sg_sssp_set_delta": (st, [vp, C.c_double]),
     "sg_sssp_set_launch": (st, [vp, vp, C.c_uint32]),
     "sg_bfs_set_launch": (st, [vp, vp, C.c_uint32]),
