@@ -38,6 +38,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 SCALE, EDGE_FACTOR, A, B, C = 22, 16, 0.57, 0.19, 0.19
+RMAT_ABC = (A, B, C)  # main() binds the name C to ctypes
 GRAPH_SEED, WEIGHT_SEED, SOURCE_SEED = 1, 2, 3
 N_SOURCES = 64
 ALPHA, BETA = 15.0, 24.0
@@ -250,6 +251,44 @@ def profile_case(kind: str) -> None:
         print(json.dumps({"profile": "sssp", "source": src, "iterations": it}))
 
 
+SERVE_SCALES = (14, 16, 18, 20, 21, 22, 22, 23)
+SERVE_QPS = (1000.0, 3000.0)
+SERVE_SECONDS = 2.0
+SERVE_SLOTS = 4
+SSSP_DELTA = 0.3
+
+
+def serving_bench(sg, torch) -> dict:
+    """Eight resident RMAT graphs (edge factor 16, float32 weights), Poisson
+    BFS/SSSP queries (70/30, uniform graph and source) through the serving
+    engine; the same query stream one at a time through the single-query
+    entry points.  Results stay on the device (no host copy per query)."""
+    from sygraph_b200 import serving
+    graphs, Gs = [], []
+    for i, sc in enumerate(SERVE_SCALES):
+        g = sg.io.rmat(sc, EDGE_FACTOR, *RMAT_ABC, seed=31 + i, weight_seed=41 + i, value_type=sg.WEIGHT_F32)
+        graphs.append(g)
+        Gs.append(sg.graph.build.fromCSR(g))
+    sizes = [g.n for g in graphs]
+    srv = serving.Server(slots=SERVE_SLOTS, sssp_delta=SSSP_DELTA)
+    gids = [srv.add_graph(G) for G in Gs]
+    warm = serving.make_workload(sizes, 200.0, 1.0, 0.7, seed=5)
+    serving.run_open_loop(srv, gids, warm)
+    out = {"graphs": [f"RMAT-{s}" for s in SERVE_SCALES], "slots": SERVE_SLOTS, "sssp_delta": SSSP_DELTA,
+           "mix": "70% BFS / 30% SSSP", "runs": []}
+    for qps in SERVE_QPS:
+        wl = serving.make_workload(sizes, qps, SERVE_SECONDS, 0.7, seed=int(qps))
+        r = serving.run_open_loop(srv, gids, wl)
+        out["runs"].append({"qps_offered": qps, **r})
+    out["stats"] = srv.stats()
+    srv.close()
+    wl = serving.make_workload(sizes, 1000.0, 0.3, 0.7, seed=9)
+    out["one_at_a_time"] = serving.run_one_at_a_time(Gs, wl, sssp_delta=SSSP_DELTA)
+    best = max(r["qps_served"] for r in out["runs"])
+    out["served_qps_vs_one_at_a_time"] = best / out["one_at_a_time"]["qps_served"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -257,6 +296,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sygraph_b200", choices=["sygraph_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving sub-benchmark")
     ap.add_argument("--sssp-sources", type=int, default=8)
     ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs"], default=None,
                     help="profiling case: build the graph, run 2 traversals of one kind and exit (few launches)")
@@ -427,7 +467,7 @@ def main():
 
     # batched Brandes BC: 64 sources per launch on RMAT-20 against the
     # per-source engine on the same sources (float32, both checked equal within 1e-4)
-    gbc = sg.io.rmat(BC_SCALE, EDGE_FACTOR, A, B, C, seed=1)
+    gbc = sg.io.rmat(BC_SCALE, EDGE_FACTOR, *RMAT_ABC, seed=1)
     Gbc = sg.graph.build.fromCSR(gbc)
     sbc = sg.io.sample_sources(gbc, BC_SOURCES, seed=SOURCE_SEED)
     bcb = sg.algorithms.BatchedBC(Gbc)
@@ -466,6 +506,23 @@ def main():
     sssp_gteps = ss_edges / (ss_ms * 1e-3) / 1e9
     sssp_kern = ss_ms / k_ss
     sssp_achieved = sssp_bytes / (sssp_kern * 1e-3) / 1e9
+    # near-far bucketing on the same sources: the same distances (checked), less work
+    sssp.set_delta(SSSP_DELTA)
+    nf_ms, nf_same = 0.0, True
+    for s in srcs[:k_ss]:
+        sssp.init(int(s))
+        sssp.run_async()
+        d_nf = sssp.getDistances()
+        sssp.set_delta(0.0)
+        sssp.init(int(s))
+        sssp.run()
+        nf_same &= bool(np.array_equal(d_nf.view(np.uint32), sssp.getDistances().view(np.uint32)))
+        sssp.set_delta(SSSP_DELTA)
+        sssp.init(int(s))
+        nf_ms += _launch_ms(torch, sssp.run_async)
+    nf_kern = nf_ms / k_ss
+
+    serve = None if (args.no_serving or world > 1) else serving_bench(sg, torch)
 
     if rank == 0:
         base = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(g, srcs[:8], sg)
@@ -496,7 +553,12 @@ def main():
                                      "bytes_per_launch": ms_bytes, "traffic": ncu_traffic("msbfs_kernel")}},
             "learned": learned,
             "bc_batched": bc_line,
+            "serving": serve,
             "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
+                     "schedule": "frontier Bellman-Ford (the reference's)",
+                     "near_far": {"delta": SSSP_DELTA, "launch_ms": nf_kern,
+                                  "value": ss_edges / (nf_ms * 1e-3) / 1e9, "unit": "GTEPS",
+                                  "speedup": sssp_kern / nf_kern, "identical_distances": nf_same},
                      "roofline": {"bound": "hbm", "achieved": sssp_achieved, "peak": peak, "unit": "GB/s",
                                   "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,
                                   "traffic": ncu_traffic("sssp_kernel")}},

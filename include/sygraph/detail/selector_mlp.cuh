@@ -77,9 +77,12 @@ __device__ __forceinline__ void mlp_stage(const MlpParams* __restrict__ g, MlpSt
 
 // Forward pass by one full warp: lane j computes hidden unit j, summing in
 // the same order as the training kernels.  Returns, in every lane, the
-// strategy with the smallest predicted time among the set bits of
-// `allowed`, or -1 when a feature lies outside the trusted range.
-__device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const float* f, uint32_t allowed) {
+// strategy with the smallest predicted time among the set bits of `allowed`
+// -- unless `fallback` (the heuristic's choice, when allowed) is predicted
+// within `margin` of it in log-time, which keeps the fallback -- or -1 when a
+// feature lies outside the trusted range.
+__device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const float* f, uint32_t allowed,
+                                          int fallback = -1, float margin = 0.f) {
   const uint32_t lane = threadIdx.x & 31;
   bool out_of_range = false;
   float x[kMlpIn];
@@ -97,7 +100,7 @@ __device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const
 #pragma unroll 8
   for (int i = 0; i < kMlpHidden; i++) h2 += P->w2t[i][lane] * __shfl_sync(0xffffffffu, h1, i);
   h2 = h2 > 0.f ? h2 : 0.f;
-  float best = 3.4e38f;
+  float best = 3.4e38f, y_fallback = 3.4e38f;
   int arg = -1;
 #pragma unroll
   for (int j = 0; j < kMlpOut; j++) {
@@ -105,11 +108,13 @@ __device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) y += __shfl_xor_sync(0xffffffffu, y, d);
     y += P->b3[j];
+    if (j == fallback) y_fallback = y;
     if (((allowed >> j) & 1u) && y < best) {
       best = y;
       arg = j;
     }
   }
+  if (fallback >= 0 && ((allowed >> fallback) & 1u) && y_fallback - best <= margin) arg = fallback;
   // butterfly sums may round differently per lane: lane 0 decides for all
   return __shfl_sync(0xffffffffu, arg, 0);
 }

@@ -392,6 +392,8 @@ sg_status sg_mlp_train(sg_mlp h, const float* dev_x, const float* dev_t, const f
  *                        to let the mode decide) for i < len; len 0 clears it
  *   sg_bfs_set_selector  the MLP used by SG_BFS_LEARNED and the strategies it
  *                        may choose (bit mask over SG_STRATEGY_*)
+ *   sg_bfs_set_selector_margin  the predicted log-time gain the MLP needs to
+ *                        overrule the hybrid heuristic's choice (default 0.05)
  *   sg_bfs_log_features  records the twelve selector features of each level
  *                        decision; sg_bfs_level_features reads them (12 floats
  *                        per level, level 0 first). */
@@ -399,6 +401,7 @@ sg_status sg_mlp_train(sg_mlp h, const float* dev_x, const float* dev_t, const f
 sg_status sg_bfs_set_launch(sg_bfs b, void* stream, uint32_t max_ctas);
 sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len);
 sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed);
+sg_status sg_bfs_set_selector_margin(sg_bfs b, float margin);
 sg_status sg_bfs_log_features(sg_bfs b, int enable);
 sg_status sg_bfs_level_features(sg_bfs b, float* host_features, uint32_t cap_levels, uint32_t* count);
 
@@ -418,7 +421,8 @@ sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations);
 sg_status sg_sssp_set_delta(sg_sssp s, double delta);
 /* Stream of this instance's launches and copies (NULL: the graph's stream)
  * and a cap on its persistent grid (0: every SM), so that several instances
- * can share the GPU.  Waits for work queued on the previous stream. */
+ * can share the GPU.  Waits for work queued on the previous stream.  The
+ * stream must stay valid until the instance is destroyed or given another. */
 sg_status sg_sssp_set_launch(sg_sssp s, void* stream, uint32_t max_ctas);
 sg_status sg_sssp_run_async(sg_sssp s);
 sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist);

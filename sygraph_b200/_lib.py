@@ -160,6 +160,7 @@ SIGNATURES = {
     "sg_run_bfs": (st, [vp, C.c_uint32, C.c_int, C.c_float, C.c_float, u32p, C.POINTER(BfsDetails)]),
     "sg_bfs_set_schedule": (st, [vp, C.POINTER(C.c_int), C.c_uint32]),
     "sg_bfs_set_selector": (st, [vp, vp, C.c_uint32]),
+    "sg_bfs_set_selector_margin": (st, [vp, C.c_float]),
     "sg_bfs_log_features": (st, [vp, C.c_int]),
     "sg_bfs_level_features": (st, [vp, f32p, C.c_uint32, u32p]),
     "sg_mlp_param_count": (C.c_uint32, []),

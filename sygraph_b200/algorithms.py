@@ -78,10 +78,13 @@ class BFS:
         s = np.ascontiguousarray(strategies if strategies is not None else [], np.int32)
         call("sg_bfs_set_schedule", self.handle, s.ctypes.data_as(C.POINTER(C.c_int)), s.size)
 
-    def set_selector(self, mlp, allowed: int = 0x3F) -> None:
-        """The MLP of bfs_direction.learned (None detaches it)."""
+    def set_selector(self, mlp, allowed: int = 0x3F, margin: float | None = None) -> None:
+        """The MLP of bfs_direction.learned (None detaches it); `margin` is the
+        predicted log-time gain it needs to overrule the heuristic."""
         self._mlp = mlp  # keep the device parameters alive
         call("sg_bfs_set_selector", self.handle, mlp.handle if mlp is not None else None, allowed)
+        if margin is not None:
+            call("sg_bfs_set_selector_margin", self.handle, float(margin))
 
     def log_features(self, enable: bool = True) -> None:
         call("sg_bfs_log_features", self.handle, int(enable))

@@ -43,10 +43,10 @@ namespace bcb {
 using namespace eng;
 using u64 = unsigned long long;
 
-constexpr uint32_t kCtaDeg = 2048;    // degree from which a vertex takes a whole CTA
+constexpr uint32_t kCtaDeg = 1024;    // degree from which a vertex takes a whole CTA
+constexpr uint32_t kMarkDeg = 256;    // frontier out-degree from which the whole grid marks its edges
 constexpr uint32_t kRow = 64;         // floats per sigma / q row
 constexpr uint32_t kUnroll = 8;       // row loads a warp keeps in flight
-constexpr uint32_t kBigList = 256;    // CTA-sized vertices a CTA defers per level (more: done by the warp)
 constexpr uint32_t kSparseRatio = 4;  // mark pass when frontier out-degree * ratio < undone in-degree
 constexpr uint32_t kBackwardLog = 7;  // strategy code of backward levels in the level log
 
@@ -55,7 +55,9 @@ struct Counters {
   u64 reached;    // sum over (source, newly reached vertex) of its out-degree
   u64 new_deg;    // out-degree sum of the vertices that gained a source
   u64 done_in;    // in-degree sum of the vertices every source has now reached
-  u64 pad[4];
+  uint32_t big;   // CTA-sized vertices of this phase (global list)
+  uint32_t mark;  // high-degree vertices of the next frontier (mark list)
+  u64 pad[3];
 };
 
 struct Params {
@@ -73,6 +75,9 @@ struct Params {
   uint32_t* act;        // cap_levels * w0: hist[L] != 0
   uint32_t* done;       // w0: every source reached (or no in-edge)
   uint32_t* cand;       // w0: marked candidates of a sparse level (zero between levels)
+  uint32_t* big;        // big_cap: CTA-sized vertices of the current phase
+  uint32_t* mark;       // 2 * big_cap: frontier vertices of out-degree >= kMarkDeg, by level parity
+  uint32_t big_cap;     // > (number of edges) / kMarkDeg
   const uint32_t* no_in_edges;
   float* sigma;         // n * 64
   float* q;             // n * 64
@@ -89,11 +94,6 @@ struct Shared {
   u64 mask[16];
   uint32_t scan[32];
   u64 red[32];
-};
-
-struct BigList {
-  uint32_t v[kBigList];
-  uint32_t count;
 };
 
 struct Local {
@@ -186,8 +186,9 @@ __device__ __forceinline__ void backward_gather(const Params& P, const u64* hist
 
 // Forward result of vertex u: seen, hist[L+1], sigma entries of its new
 // sources, the act / done bits.  Every lane calls; nm is warp-uniform.
-__device__ __forceinline__ void forward_finish(const Params& P, u64* hist_N, uint32_t* act_N, uint32_t u, u64 su,
-                                               u64 nm, float a0, float a1, Local& loc) {
+__device__ __forceinline__ void forward_finish(const Params& P, u64* hist_N, uint32_t* act_N, uint32_t* mark_N,
+                                               Counters* C, uint32_t u, u64 su, u64 nm, float a0, float a1,
+                                               Local& loc) {
   const uint32_t lane = threadIdx.x & 31;
   if (!nm) return;
   const uint32_t b = (uint32_t)(nm >> (2 * lane)) & 3u;
@@ -210,6 +211,7 @@ __device__ __forceinline__ void forward_finish(const Params& P, u64* hist_N, uin
     }
     loc.new_count++;
     loc.new_deg += dout;
+    if (dout >= kMarkDeg) mark_N[atomicAdd(&C->mark, 1u)] = u;
     loc.reached += (u64)__popcll(nm) * dout;
   }
 }
@@ -243,7 +245,7 @@ __device__ __forceinline__ void backward_finish(const Params& P, uint32_t v, u64
 // partial sums are added in warp order.  Called by every thread of the block.
 template <bool kForward>
 __device__ __forceinline__ void cta_vertex(const Params& P, Shared& S, const u64* hist_src, u64* hist_N,
-                                           uint32_t* act_N, uint32_t x, Local& loc) {
+                                           uint32_t* act_N, uint32_t* mark_N, Counters* C, uint32_t x, Local& loc) {
   const uint32_t lane = threadIdx.x & 31, wl = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t beg = kForward ? P.iro[x] : P.ro[x];
   const uint32_t end = kForward ? P.iro[x + 1] : P.ro[x + 1];
@@ -270,7 +272,7 @@ __device__ __forceinline__ void cta_vertex(const Params& P, Shared& S, const u64
       all |= S.mask[w];
     }
     if (kForward)
-      forward_finish(P, hist_N, act_N, x, sx, all, t0, t1, loc);
+      forward_finish(P, hist_N, act_N, mark_N, C, x, sx, all, t0, t1, loc);
     else
       backward_finish(P, x, sx, t0, t1);
   }
@@ -290,21 +292,27 @@ __device__ __forceinline__ void block_add(Local& loc, Shared& S, Counters* C) {
   }
 }
 
-// Defers vertex x to the CTA phase when it is CTA-sized and the list has room;
-// returns true when deferred.  Warp-uniform.
-__device__ __forceinline__ bool defer_big(BigList& B, uint32_t x, uint32_t deg) {
+// Appends CTA-sized vertex x to the phase's global list (processed after the
+// phase's light pass, CTAs taking entries round-robin); true when deferred.
+// Warp-uniform.
+__device__ __forceinline__ bool defer_big(const Params& P, Counters* C, uint32_t x, uint32_t deg) {
   if (deg < kCtaDeg) return false;
-  uint32_t slot = kBigList;
-  if ((threadIdx.x & 31) == 0) slot = atomicAdd(&B.count, 1u);
-  slot = __shfl_sync(kFullMask, slot, 0);
-  if (slot >= kBigList) return false;
-  if ((threadIdx.x & 31) == 0) B.v[slot] = x;
+  if ((threadIdx.x & 31) == 0) P.big[atomicAdd(&C->big, 1u)] = x;
   return true;
 }
 
+__device__ __forceinline__ void mark_one(const Params& P, uint32_t u) {
+  const uint32_t b = 1u << (u & 31);
+  if ((ld_cg(P.done + (u >> 5)) & b) || (ld_cg(P.cand + (u >> 5)) & b)) return;
+  atomicOr(P.cand + (u >> 5), b);
+}
+
 // Mark pass of a sparse level: out-neighbours of the frontier that some
-// source has not reached become candidates (idempotent bit sets).
-__device__ __forceinline__ void mark_candidates(const Params& P, const uint32_t* act_L) {
+// source has not reached become candidates (idempotent bit sets).  Frontier
+// vertices of out-degree < kMarkDeg take a warp each; the others, listed when
+// they joined the frontier, take a CTA each, round-robin over the grid.
+__device__ __forceinline__ void mark_candidates(const Params& P, const uint32_t* act_L, const uint32_t* mark_L,
+                                                uint32_t n_mark) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -314,19 +322,19 @@ __device__ __forceinline__ void mark_candidates(const Params& P, const uint32_t*
       const uint32_t v = wi * 32 + (__ffs(word) - 1);
       word &= word - 1;
       const uint32_t beg = P.ro[v], end = P.ro[v + 1];
-      for (uint32_t e = beg + lane; e < end; e += 32) {
-        const uint32_t u = P.col[e];
-        const uint32_t b = 1u << (u & 31);
-        if ((ld_cg(P.done + (u >> 5)) & b) || (ld_cg(P.cand + (u >> 5)) & b)) continue;
-        atomicOr(P.cand + (u >> 5), b);
-      }
+      if (end - beg >= kMarkDeg) continue;
+      for (uint32_t e = beg + lane; e < end; e += 32) mark_one(P, P.col[e]);
     }
+  }
+  for (uint32_t i = blockIdx.x; i < n_mark; i += gridDim.x) {
+    const uint32_t v = ld_cg(mark_L + i);
+    const uint32_t beg = P.ro[v], end = P.ro[v + 1];
+    for (uint32_t e = beg + threadIdx.x; e < end; e += blockDim.x) mark_one(P, P.col[e]);
   }
 }
 
 __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
   __shared__ Shared S;
-  __shared__ BigList B;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
   const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
@@ -349,52 +357,56 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
     Counters z = {};
     P.cnt[gtid] = z;
   }
-  if (threadIdx.x == 0) B.count = 0;
   if (!grid_sync(P.bar)) return;
-  // ---- sources: depth 0, sigma 1
-  u64 reached_total = 0;
-  for (uint32_t i = 0; i < P.k; i++) reached_total += P.ro[P.sources[i] + 1] - P.ro[P.sources[i]];
+  // ---- sources: depth 0, sigma 1; high-degree sources go on the level-0 mark list
+  u64 reached_total = 0, frontier_deg = 0;
+  for (uint32_t i = 0; i < P.k; i++) {
+    const uint32_t d = P.ro[P.sources[i] + 1] - P.ro[P.sources[i]];
+    reached_total += d;
+    bool first = true;
+    for (uint32_t j = 0; j < i; j++) first &= P.sources[j] != P.sources[i];
+    if (first) frontier_deg += d;
+  }
   if (gtid == 0) {
+    uint32_t nm = 0;
     for (uint32_t i = 0; i < P.k; i++) {
       const uint32_t s = P.sources[i];
-      const u64 now = P.seen[s] | (1ull << i);
+      const u64 before = P.seen[s];
+      const u64 now = before | (1ull << i);
       P.seen[s] = now;
       P.hist[s] = now;
       P.act[s >> 5] |= 1u << (s & 31);
       if (now == P.all) P.done[s >> 5] |= 1u << (s & 31);
       P.sigma[(size_t)s * kRow + i] = 1.0f;
+      if (!before && P.ro[s + 1] - P.ro[s] >= kMarkDeg) P.mark[nm++] = s;
     }
+    P.cnt[2].mark = nm;
     __threadfence();
   }
   if (!grid_sync(P.bar)) return;
 
-  // frontier out-degree (distinct sources) and in-degree of the vertices not done
-  u64 frontier_deg = 0;
-  for (uint32_t i = 0; i < P.k; i++) {
-    bool first = true;
-    for (uint32_t j = 0; j < i; j++) first &= P.sources[j] != P.sources[i];
-    if (first) frontier_deg += P.ro[P.sources[i] + 1] - P.ro[P.sources[i]];
-  }
-  u64 undone_in = P.m;
-  uint32_t n_log = 0;
+  u64 undone_in = P.m;  // in-degree of the vertices some source has not reached
+  uint32_t n_log = 0, phase = 0;
 
   // ---- forward sweep
   uint32_t L = 0;
   bool overflow = false;
-  for (;; L++) {
+  for (;; L++, phase++) {
     if (L + 1 >= P.cap_levels) {
       overflow = true;
       break;
     }
-    Counters* C = P.cnt + (L % 3);
+    Counters* C = P.cnt + (phase % 3);
+    const Counters* Cprev = P.cnt + ((phase + 2) % 3);
     if (gtid == 0) {
       Counters z = {};
-      P.cnt[(L + 1) % 3] = z;
+      P.cnt[(phase + 1) % 3] = z;
     }
     const uint64_t t0 = gtid == 0 ? sygraph::detail::global_timer_ns() : 0;
     const u64* hist_L = P.hist + (size_t)L * n;
     u64* hist_N = P.hist + (size_t)(L + 1) * n;
     uint32_t* act_N = P.act + (size_t)(L + 1) * w0;
+    uint32_t* mark_N = P.mark + (size_t)((L + 1) & 1) * P.big_cap;
     if (L + 2 < P.cap_levels) {  // hist / act of level L+2 start empty
       u64* h2 = P.hist + (size_t)(L + 2) * n;
       for (uint32_t i = gtid; i < n; i += nthreads) st_cg(h2 + i, 0ull);
@@ -403,7 +415,7 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
     }
     const bool sparse = frontier_deg * kSparseRatio < undone_in;
     if (sparse) {
-      mark_candidates(P, P.act + (size_t)L * w0);
+      mark_candidates(P, P.act + (size_t)L * w0, P.mark + (size_t)(L & 1) * P.big_cap, ld_cg(&Cprev->mark));
       if (!grid_sync(P.bar)) return;
     }
     Local loc;
@@ -418,18 +430,17 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
         const uint32_t u = wi * 32 + (__ffs(cand) - 1);
         cand &= cand - 1;
         const uint32_t beg = P.iro[u], end = P.iro[u + 1];
-        if (defer_big(B, u, end - beg)) continue;
+        if (defer_big(P, C, u, end - beg)) continue;
         const u64 su = ld_cg(P.seen + u);
         float a0 = 0.f, a1 = 0.f;
         const u64 nm = forward_gather(P, hist_L, beg, end, su, a0, a1);
-        forward_finish(P, hist_N, act_N, u, su, nm, a0, a1, loc);
+        forward_finish(P, hist_N, act_N, mark_N, C, u, su, nm, a0, a1, loc);
       }
     }
-    __syncthreads();
-    const uint32_t nbig = min(B.count, kBigList);
-    for (uint32_t i = 0; i < nbig; i++) cta_vertex<true>(P, S, hist_L, hist_N, act_N, B.v[i], loc);
-    __syncthreads();
-    if (threadIdx.x == 0) B.count = 0;
+    if (!grid_sync(P.bar)) return;
+    const uint32_t nbig = ld_cg(&C->big);
+    for (uint32_t i = blockIdx.x; i < nbig; i += gridDim.x)
+      cta_vertex<true>(P, S, hist_L, hist_N, act_N, mark_N, C, ld_cg(P.big + i), loc);
     block_add(loc, S, C);
     if (!grid_sync(P.bar)) return;
     const u64 next = ld_cg(&C->new_count);
@@ -458,9 +469,15 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
     }
     return;
   }
+  phase++;
   // ---- backward sweep: levels Lmax .. 1 (Lmax is the deepest non-empty level)
   const uint32_t Lmax = L;
-  for (uint32_t Lb = Lmax; Lb >= 1; Lb--) {
+  for (uint32_t Lb = Lmax; Lb >= 1; Lb--, phase++) {
+    Counters* C = P.cnt + (phase % 3);
+    if (gtid == 0) {
+      Counters z = {};
+      P.cnt[(phase + 1) % 3] = z;
+    }
     const uint64_t t0 = gtid == 0 ? sygraph::detail::global_timer_ns() : 0;
     const u64* hist_B = P.hist + (size_t)Lb * n;
     const u64* hist_next = Lb < Lmax ? P.hist + (size_t)(Lb + 1) * n : nullptr;
@@ -472,19 +489,17 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
         const uint32_t v = wi * 32 + (__ffs(word) - 1);
         word &= word - 1;
         const uint32_t beg = P.ro[v], end = P.ro[v + 1];
-        if (hist_next && defer_big(B, v, end - beg)) continue;
+        if (hist_next && defer_big(P, C, v, end - beg)) continue;
         const u64 fv = ld_cg(hist_B + v);
         float a0 = 0.f, a1 = 0.f;
         if (hist_next) backward_gather(P, hist_next, beg, end, fv, a0, a1);
         backward_finish(P, v, fv, a0, a1);
       }
     }
-    __syncthreads();
-    const uint32_t nbig = min(B.count, kBigList);
-    for (uint32_t i = 0; i < nbig; i++)
-      cta_vertex<false>(P, S, hist_B, const_cast<u64*>(hist_next), nullptr, B.v[i], unused);
-    __syncthreads();
-    if (threadIdx.x == 0) B.count = 0;
+    if (!grid_sync(P.bar)) return;
+    const uint32_t nbig = ld_cg(&C->big);
+    for (uint32_t i = blockIdx.x; i < nbig; i += gridDim.x)
+      cta_vertex<false>(P, S, hist_B, const_cast<u64*>(hist_next), nullptr, nullptr, C, ld_cg(P.big + i), unused);
     if (!grid_sync(P.bar)) return;
     if (gtid == 0 && n_log < kMaxLog) {
       sg_level_record r = {};
@@ -527,6 +542,7 @@ struct sg_bc_batch_s {
   unsigned long long* hist = nullptr;
   uint32_t *act = nullptr, *done = nullptr, *no_in = nullptr, *sources = nullptr;
   uint32_t* cand = nullptr;
+  uint32_t *big = nullptr, *mark = nullptr, big_cap = 0;
   float *sigma = nullptr, *q = nullptr, *bc = nullptr;
   bcb::Counters* cnt = nullptr;
   sygraph::detail::GridBarrier* bar = nullptr;
@@ -547,6 +563,8 @@ void bcb_release(sg_bc_batch h) {
   dev_free(h->sigma);
   dev_free(h->q);
   dev_free(h->cand);
+  dev_free(h->big);
+  dev_free(h->mark);
   dev_free(h->bc);
   dev_free(h->cnt);
   dev_free(h->bar);
@@ -601,6 +619,9 @@ sg_status bcb_launch(sg_bc_batch h, uint32_t k, int accumulate) {
   P.sigma = h->sigma;
   P.q = h->q;
   P.cand = h->cand;
+  P.big = h->big;
+  P.mark = h->mark;
+  P.big_cap = h->big_cap;
   P.bc = h->bc;
   P.accumulate = accumulate;
   P.cnt = h->cnt;
@@ -622,6 +643,8 @@ sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* o
   sg_bc_batch h = new sg_bc_batch_s();
   h->g = g;
   h->w0 = div_up(g->n, 32);
+  // at most m / kMarkDeg vertices have a degree >= kMarkDeg (>= kCtaDeg too)
+  h->big_cap = (uint32_t)std::min<uint64_t>(g->n, g->m / bcb::kMarkDeg + 2);
   const uint64_t n = g->n;
   uint32_t levels = history_levels;
   if (!levels) levels = (uint32_t)std::max<uint64_t>(16, std::min<uint64_t>(256, (2ull << 30) / level_bytes(h)));
@@ -629,7 +652,8 @@ sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* o
   sg_status s;
   if ((s = dev_alloc(&h->seen, n)) || (s = dev_alloc(&h->done, h->w0)) || (s = dev_alloc(&h->no_in, h->w0)) ||
       (s = dev_alloc(&h->sources, 64)) || (s = dev_alloc(&h->sigma, n * bcb::kRow)) ||
-      (s = dev_alloc(&h->q, n * bcb::kRow)) || (s = dev_alloc(&h->cand, h->w0)) || (s = dev_alloc(&h->bc, n)) || (s = dev_alloc(&h->cnt, 3)) ||
+      (s = dev_alloc(&h->q, n * bcb::kRow)) || (s = dev_alloc(&h->cand, h->w0)) ||
+      (s = dev_alloc(&h->big, h->big_cap)) || (s = dev_alloc(&h->mark, 2ull * h->big_cap)) || (s = dev_alloc(&h->bc, n)) || (s = dev_alloc(&h->cnt, 3)) ||
       (s = dev_alloc(&h->bar, 1)) || (s = dev_alloc(&h->log, SG_MAX_LOGGED_LEVELS)) ||
       (s = dev_alloc(&h->result, 4)) || (s = bcb_history(h, levels))) {
     bcb_release(h);

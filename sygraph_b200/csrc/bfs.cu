@@ -241,6 +241,7 @@ struct sg_bfs_s {
   uint32_t schedule_len = 0;
   const sygraph::detail::MlpParams* mlp = nullptr;  // not owned
   uint32_t allowed = 0x3f;
+  float margin = 0.05f;
   float* features = nullptr;
   uint32_t last_iterations = 0;
   bool fresh = false;  // initialised but not run: depths not written yet
@@ -289,6 +290,7 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.beta = beta;
   P.mlp = b->mlp;
   P.allowed = b->allowed;
+  P.margin = b->margin;
   P.features = b->features;
   P.depth = b->depth;
   P.visited = b->visited;
@@ -428,6 +430,14 @@ sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len
     SG_CUDA(cudaMemcpy(b->schedule, host_strategies, sizeof(int) * len, cudaMemcpyHostToDevice));
     b->schedule_len = len;
   }
+  return SG_OK;
+}
+
+sg_status sg_bfs_set_selector_margin(sg_bfs b, float margin) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_REQUIRE(margin >= 0.f && margin < 100.f, SG_ERR_INVALID, "margin must be in [0, 100)");
+  b->margin = margin;
   return SG_OK;
 }
 
@@ -612,6 +622,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.mode = direction;
   P.mlp = nullptr;
   P.allowed = 0x3f;
+  P.margin = 0.f;
   P.features = nullptr;
   P.alpha = alpha;
   P.beta = beta;

@@ -57,6 +57,7 @@ struct Params {
   uint32_t schedule_len;
   const sygraph::detail::MlpParams* mlp;  // learned mode
   uint32_t allowed;                       // strategies the MLP may pick (bit mask)
+  float margin;                           // log-time gain the MLP must predict to overrule the heuristic
   float* features;                        // optional log: 12 floats per level decision
 };
 
@@ -195,7 +196,7 @@ __device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const
       if (log && threadIdx.x == 0)
         for (int i = 0; i < 12; i++) P.features[(size_t)level * 12 + i] = f[i];
       if (P.mode == kLearned && P.mlp) {
-        const int c = sygraph::detail::mlp_choose(&S.mlp, f, P.allowed);
+        const int c = sygraph::detail::mlp_choose(&S.mlp, f, P.allowed, h, P.margin);
         if (threadIdx.x == 0) S.choice = c;
       }
     }

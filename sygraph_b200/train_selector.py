@@ -26,6 +26,10 @@ from . import algorithms, build, io
 from .selector import IN, OUT, STRATEGIES, MODEL_PATH, Mlp
 
 HYBRID_ALPHA, HYBRID_BETA = 15.0, 24.0
+# the engine keeps the heuristic's choice unless the MLP predicts it at least
+# this much slower in log-time (chosen on the training tables: most of the
+# gain, no training traversal more than about 1% slower than the heuristic)
+MARGIN = 0.05
 MAX_LEVELS = 4096
 
 # (name, generator, kwargs): RMAT skews and scales, grids with and without
@@ -140,7 +144,7 @@ def traversals(data: dict):
 
 
 def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.ndarray,
-                     allowed: int = 0x3F) -> np.ndarray:
+                     allowed: int = 0x3F, margin: float = MARGIN) -> np.ndarray:
     """The learned mode's schedule on a traversal: the MLP's argmin per level
     (`forward` maps a feature batch to predicted log-times) with the
     current-direction feature following its own previous choice, and the
@@ -159,7 +163,8 @@ def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.n
         else:
             y = np.array(forward(f[None, :]), np.float64)[0]
             y[banned] = np.inf
-            out[L] = int(np.argmin(y))
+            best, h = int(np.argmin(y)), int(heuristic[L])
+            out[L] = h if np.isfinite(y[h]) and y[h] - y[best] <= margin else best
         prev = out[L]
     return out
 

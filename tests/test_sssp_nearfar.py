@@ -80,5 +80,9 @@ def test_instances_on_own_streams_with_grid_caps(sg, oracle, rmat):
     s.run_async()
     assert np.array_equal(b.getDistances(), oracle.bfs_levels(g, src))
     assert np.array_equal(s.getDistances().view(np.uint32), oracle.sssp_dijkstra(g, src).view(np.uint32))
+    # an instance uses its stream until it is destroyed: destroy the instances first
+    del b, s
+    import gc
+    gc.collect()
     for h in streams:
         sg._lib.call("sg_stream_destroy", h)

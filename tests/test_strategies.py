@@ -118,7 +118,7 @@ def test_learned_mode_parity_and_mask(sg, oracle, graphs):
         bfs = sg.algorithms.BFS(G)
         for seed, allowed in ((1, 0x3F), (2, 0x03), (3, 0x0C), (4, 0x30), (5, 0x21)):
             m = _trusting_mlp(selector, seed)
-            bfs.set_selector(m, allowed)
+            bfs.set_selector(m, allowed, margin=0.0)  # plain argmin, checked below
             bfs.log_features(True)
             for s in _sources(sg, g)[:2]:
                 bfs.init(s)
@@ -175,3 +175,20 @@ def test_feature_log_matches_level_records(sg, rmat):
         assert F[i, 1] == pytest.approx(r["frontier_size"] / n, rel=1e-5)
         if i > 0:
             assert F[i, 10] == (1.0 if recs[i - 1]["strategy"] >= 2 else 0.0)
+
+
+def test_learned_mode_margin_keeps_the_heuristic(sg, oracle, rmat):
+    """A margin no prediction can clear leaves every level to the heuristic."""
+    from sygraph_b200 import selector
+    g = rmat(14, perm_seed=7)
+    G = sg.graph.build.fromCSR(g)
+    bfs = sg.algorithms.BFS(G)
+    bfs.set_selector(_trusting_mlp(selector, 9), margin=99.0)
+    s = int(np.argmax(g.degrees()))
+    bfs.init(s)
+    det = bfs.run(sg.algorithms.bfs_direction.learned, 15.0, 24.0)
+    ref, it, steps = oracle.bfs_frontier(g, s, 2, 15.0, 24.0)
+    assert np.array_equal(bfs.getDistances(), ref) and det.iterations == it
+    assert [r["strategy"] for r in bfs.level_records()] == [2 * x for x in steps]
+    with pytest.raises(sg._lib.SygraphError):
+        bfs.set_selector(None, margin=-1.0)
