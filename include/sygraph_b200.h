@@ -401,6 +401,11 @@ sg_status sg_mlp_train(sg_mlp h, const float* dev_x, const float* dev_t, const f
 sg_status sg_bfs_set_launch(sg_bfs b, void* stream, uint32_t max_ctas);
 sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len);
 sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed);
+/* Probe order of short-circuit pull levels: bit L of reverse_levels (L < 64)
+ * makes level L probe each vertex's in-neighbours from the back of its sorted
+ * list (the parents of late-level vertices tend to have high ids).  Any
+ * parent gives the same depth; only the work changes. */
+sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels);
 sg_status sg_bfs_set_selector_margin(sg_bfs b, float margin);
 sg_status sg_bfs_log_features(sg_bfs b, int enable);
 sg_status sg_bfs_level_features(sg_bfs b, float* host_features, uint32_t cap_levels, uint32_t* count);
@@ -419,6 +424,9 @@ sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations);
  * same fixed point); the iteration count and the work are not.  0 (the
  * default) is the reference's frontier Bellman-Ford. */
 sg_status sg_sssp_set_delta(sg_sssp s, double delta);
+/* Per-iteration log of the last run (frontier size and out-degree, vertices
+ * improved, device timestamps), as sg_bfs_level_records. */
+sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count);
 /* Stream of this instance's launches and copies (NULL: the graph's stream)
  * and a cap on its persistent grid (0: every SM), so that several instances
  * can share the GPU.  Waits for work queued on the previous stream.  The

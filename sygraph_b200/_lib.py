@@ -161,6 +161,7 @@ SIGNATURES = {
     "sg_bfs_set_schedule": (st, [vp, C.POINTER(C.c_int), C.c_uint32]),
     "sg_bfs_set_selector": (st, [vp, vp, C.c_uint32]),
     "sg_bfs_set_selector_margin": (st, [vp, C.c_float]),
+    "sg_bfs_set_pull_order": (st, [vp, C.c_uint64]),
     "sg_bfs_log_features": (st, [vp, C.c_int]),
     "sg_bfs_level_features": (st, [vp, f32p, C.c_uint32, u32p]),
     "sg_mlp_param_count": (C.c_uint32, []),
@@ -180,6 +181,7 @@ SIGNATURES = {
     "sg_server_drain": (st, [vp, C.c_double]),
     "sg_server_get_stats": (st, [vp, C.POINTER(ServerStats)]),
     "sg_sssp_set_delta": (st, [vp, C.c_double]),
+    "sg_sssp_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
     "sg_sssp_set_launch": (st, [vp, vp, C.c_uint32]),
     "sg_bfs_set_launch": (st, [vp, vp, C.c_uint32]),
     "sg_msbfs_set_launch": (st, [vp, vp, C.c_uint32]),

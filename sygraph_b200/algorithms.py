@@ -86,6 +86,10 @@ class BFS:
         if margin is not None:
             call("sg_bfs_set_selector_margin", self.handle, float(margin))
 
+    def set_pull_order(self, reverse_levels: int) -> None:
+        """Bit L: level L's pull probes in-neighbours from the back."""
+        call("sg_bfs_set_pull_order", self.handle, int(reverse_levels))
+
     def log_features(self, enable: bool = True) -> None:
         call("sg_bfs_log_features", self.handle, int(enable))
 
@@ -178,6 +182,12 @@ class SSSP:
 
     def run_async(self) -> None:
         call("sg_sssp_run_async", self.handle)
+
+    def level_records(self) -> list[dict]:
+        recs = (_lib.LevelRecord * _lib.SG_MAX_LOGGED_LEVELS)()
+        cnt = C.c_uint32()
+        call("sg_sssp_level_records", self.handle, recs, _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
+        return [{k: getattr(recs[i], k) for k, _ in _lib.LevelRecord._fields_} for i in range(cnt.value)]
 
     def set_delta(self, delta: float) -> None:
         """Near-far threshold step (0: the reference's frontier Bellman-Ford)."""

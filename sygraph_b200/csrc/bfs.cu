@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
       if (strategy & 1)
         pull_cta(L, fb_cur, sc);
       else
-        pull_warp(L, fb_cur, sc);
+        pull_warp(L, fb_cur, sc, level < 64 && ((P.pull_reverse >> level) & 1ull));
     }
     // clear F_{L-1}: only the words its summary flags
     for (uint32_t j = gwarp; j < w1; j += nwarps) {
@@ -242,6 +242,7 @@ struct sg_bfs_s {
   const sygraph::detail::MlpParams* mlp = nullptr;  // not owned
   uint32_t allowed = 0x3f;
   float margin = 0.05f;
+  unsigned long long pull_reverse = 0;  // levels whose pull probes in-neighbours from the back
   float* features = nullptr;
   uint32_t last_iterations = 0;
   bool fresh = false;  // initialised but not run: depths not written yet
@@ -291,6 +292,7 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.mlp = b->mlp;
   P.allowed = b->allowed;
   P.margin = b->margin;
+  P.pull_reverse = b->pull_reverse;
   P.features = b->features;
   P.depth = b->depth;
   P.visited = b->visited;
@@ -430,6 +432,13 @@ sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len
     SG_CUDA(cudaMemcpy(b->schedule, host_strategies, sizeof(int) * len, cudaMemcpyHostToDevice));
     b->schedule_len = len;
   }
+  return SG_OK;
+}
+
+sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  b->pull_reverse = reverse_levels;
   return SG_OK;
 }
 
@@ -623,6 +632,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.mlp = nullptr;
   P.allowed = 0x3f;
   P.margin = 0.f;
+  P.pull_reverse = 0;
   P.features = nullptr;
   P.alpha = alpha;
   P.beta = beta;

@@ -58,6 +58,7 @@ struct Params {
   const sygraph::detail::MlpParams* mlp;  // learned mode
   uint32_t allowed;                       // strategies the MLP may pick (bit mask)
   float margin;                           // log-time gain the MLP must predict to overrule the heuristic
+  unsigned long long pull_reverse;        // bit L: level L's pull probes in-neighbours from the back
   float* features;                        // optional log: 12 floats per level decision
 };
 

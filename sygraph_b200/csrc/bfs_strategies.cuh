@@ -136,12 +136,89 @@ __device__ __forceinline__ void push_cta(Level& L, const uint32_t* fb_cur, const
   push_heavy(L, hv, hs, n_heavy, n_chunks, 0, n_chunks);
 }
 
-__device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool short_circuit) {
+// Position of the k-th in-neighbour probed (from the front, or from the back
+// of the sorted list when `reverse`).
+__device__ __forceinline__ uint32_t probe_pos(uint32_t beg, uint32_t end, uint32_t k, bool reverse) {
+  return reverse ? end - 1 - k : beg + k;
+}
+
+// Rest of a short-circuit pull of word wi after its first probe: unresolved
+// lanes probe the next in-neighbours serially (next column index loaded while
+// the current bit is tested) up to kPullSerial, the warp scans longer lists
+// together; then the word's new vertices are published.
+__device__ __forceinline__ void pull_word_finish(Level& L, const uint32_t* fb_cur, uint32_t wi, uint32_t vw, bool mine,
+                                                 uint32_t v, uint32_t beg, uint32_t end, bool found, bool reverse) {
+  const Params& P = *L.P;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t deg = end - beg;
+  const uint32_t lim = min(deg, kPullSerial);
+  if (mine && !found && lim > 1) {
+    uint32_t k = 1;
+    uint32_t c = P.icol[probe_pos(beg, end, k, reverse)];
+    for (;;) {
+      const uint32_t cn = k + 1 < lim ? P.icol[probe_pos(beg, end, k + 1, reverse)] : 0u;
+      if (bit_test_ro(fb_cur, c)) {
+        found = true;
+        break;
+      }
+      if (++k >= lim) break;
+      c = cn;
+    }
+  }
+  uint32_t left = __ballot_sync(kFullMask, mine && !found && lim < deg);
+  while (left) {
+    const uint32_t j = __ffs(left) - 1;
+    left &= left - 1;
+    const uint32_t jb = __shfl_sync(kFullMask, beg, j);
+    const uint32_t je = __shfl_sync(kFullMask, end, j);
+    bool hit = false;
+    for (uint32_t kb = kPullSerial; kb < je - jb; kb += 32) {
+      const uint32_t kk = kb + lane;
+      const bool h = kk < je - jb && bit_test_ro(fb_cur, P.icol[probe_pos(jb, je, kk, reverse)]);
+      if (__any_sync(kFullMask, h)) {
+        hit = true;
+        break;
+      }
+    }
+    if (lane == j) found = hit;
+  }
+  const uint32_t fmask = __ballot_sync(kFullMask, found);
+  if (fmask) {
+    if (found) L.discovered(v, P.iro == P.ro ? deg : (P.ro[v + 1] - P.ro[v]));
+    if (lane == 0) L.publish_word(wi, vw, fmask);
+  }
+}
+
+__device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool short_circuit, bool reverse) {
   const Params& P = *L.P;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const bool same = P.iro == P.ro;
+  if (short_circuit) {
+    // two words per step: both words' first probes are in flight together
+    for (uint32_t wa = gwarp; wa < P.w0; wa += 2 * nwarps) {
+      const uint32_t wb = wa + nwarps;
+      const bool has_b = wb < P.w0;
+      const uint32_t vwa = ld_cg(P.visited + wa);
+      const uint32_t vwb = has_b ? ld_cg(P.visited + wb) : 0xffffffffu;
+      const uint32_t ca = ~vwa & valid_bits(wa, P.w0, P.n);
+      const uint32_t cb = has_b ? (~vwb & valid_bits(wb, P.w0, P.n)) : 0u;
+      if (!(ca | cb)) continue;
+      const uint32_t va = wa * 32 + lane, vb = wb * 32 + lane;
+      const bool ma = (ca >> lane) & 1u, mb = (cb >> lane) & 1u;
+      const uint32_t ba = ma ? P.iro[va] : 0u, ea = ma ? P.iro[va + 1] : 0u;
+      const uint32_t bb = mb ? P.iro[vb] : 0u, eb = mb ? P.iro[vb + 1] : 0u;
+      const uint32_t xa = ea > ba ? P.icol[probe_pos(ba, ea, 0, reverse)] : 0u;
+      const uint32_t xb = eb > bb ? P.icol[probe_pos(bb, eb, 0, reverse)] : 0u;
+      const bool fa = ea > ba && bit_test_ro(fb_cur, xa);
+      const bool fbb = eb > bb && bit_test_ro(fb_cur, xb);
+      if (ca) pull_word_finish(L, fb_cur, wa, vwa, ma, va, ba, ea, fa, reverse);
+      if (cb) pull_word_finish(L, fb_cur, wb, vwb, mb, vb, bb, eb, fbb, reverse);
+    }
+    return;
+  }
+  // pull_all: every in-neighbour of every unvisited vertex is scanned
   for (uint32_t wi = gwarp; wi < P.w0; wi += nwarps) {
     const uint32_t vw = ld_cg(P.visited + wi);
     const uint32_t cand = ~vw & valid_bits(wi, P.w0, P.n);
@@ -152,37 +229,12 @@ __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool
     const uint32_t end = mine ? P.iro[v + 1] : 0u;
     bool found = false;
     uint32_t e = beg;
-    const uint32_t lim = short_circuit ? min(end, beg + kPullSerial) : end;
-    // the next column index is loaded while the current frontier bit is tested
-    uint32_t c = e < lim ? P.icol[e] : 0u;
-    while (e < lim) {
-      const uint32_t cn = e + 1 < lim ? P.icol[e + 1] : 0u;
-      if (bit_test_ro(fb_cur, c)) {
-        found = true;
-        if (short_circuit) break;
-      }
+    uint32_t c = e < end ? P.icol[e] : 0u;
+    while (e < end) {
+      const uint32_t cn = e + 1 < end ? P.icol[e + 1] : 0u;
+      found |= bit_test_ro(fb_cur, c);
       c = cn;
       e++;
-    }
-    if (short_circuit) {
-      // long lists that are still unresolved: the whole warp scans them
-      uint32_t left = __ballot_sync(kFullMask, mine && !found && e < end);
-      while (left) {
-        const uint32_t j = __ffs(left) - 1;
-        left &= left - 1;
-        const uint32_t jb = __shfl_sync(kFullMask, e, j);
-        const uint32_t je = __shfl_sync(kFullMask, end, j);
-        bool hit = false;
-        for (uint32_t eb = jb; eb < je; eb += 32) {
-          const uint32_t ee = eb + lane;
-          const bool h = ee < je && bit_test_ro(fb_cur, P.icol[ee]);
-          if (__any_sync(kFullMask, h)) {
-            hit = true;
-            break;
-          }
-        }
-        if (lane == j) found = hit;
-      }
     }
     const uint32_t fmask = __ballot_sync(kFullMask, found);
     if (fmask) {

@@ -37,6 +37,7 @@ struct Counters {
   unsigned long long big_packed;  // (entries << 32) | chunks: one atomic keeps both in order
   unsigned long long new_count;   // vertices that joined the next frontier
   unsigned long long new_deg;     // sum of their (forward) degrees
+  unsigned long long frontier_deg;  // push loop: out-degree sum of the frontier being expanded
 };
 
 // Frontier as queues, rebuilt from the bitmap when a push step needs them.
@@ -65,9 +66,11 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
     const uint32_t wi = base + threadIdx.x;
     const uint32_t bits = wi < wend ? ld_cg(fb + wi) : 0u;
     uint32_t n_small = 0, n_big = 0, n_chunk = 0;
+    unsigned long long fdeg = 0;
     for (uint32_t b = bits; b; b &= b - 1) {
       const uint32_t v = wi * 32 + __ffs(b) - 1;
       const uint32_t d = ro[v + 1] - ro[v];
+      fdeg += d;
       if (d < kSmallDeg) {
         n_small++;
       } else {
@@ -78,6 +81,8 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
     uint32_t t_pack, t_chunk;
     const uint32_t e_pack = block_excl_scan(n_small | (n_big << 16), &t_pack, s_scan);
     const uint32_t e_chunk = block_excl_scan(n_chunk, &t_chunk, s_scan);
+    fdeg = sygraph::detail::warp_sum(fdeg);
+    if ((threadIdx.x & 31) == 0 && fdeg) atomicAdd(&C->frontier_deg, fdeg);
     if (threadIdx.x == 0) {
       const uint32_t ts = t_pack & 0xffffu, tb = t_pack >> 16;
       s_base_small = ts ? atomicAdd(&C->small_tail, ts) : 0u;

@@ -17,6 +17,8 @@ struct PushLoop {
   Queues q;
   Counters* cnt;  // 3, zeroed before entry
   GridBarrier* bar;
+  sg_level_record* log = nullptr;  // optional per-level log, entry log_base + level
+  uint32_t log_base = 0;
 };
 
 // Marks u in the next frontier bitmap; counts it when this call set the bit.
@@ -45,6 +47,7 @@ __device__ __forceinline__ uint32_t push_levels(const PushLoop& S, MakeVisitor m
       Counters z = {};
       S.cnt[(level + 1) % 3] = z;
     }
+    const uint64_t t0 = (S.log && gtid == 0) ? sygraph::detail::global_timer_ns() : 0;
     compact_frontier(fb_cur, S.w0, S.ro, C, S.q, s_scan);
     if (!grid_sync(S.bar)) return 0;
     const uint32_t ns = ld_cg(&C->small_tail);
@@ -55,6 +58,16 @@ __device__ __forceinline__ uint32_t push_levels(const PushLoop& S, MakeVisitor m
     const unsigned long long c = block_sum<unsigned long long>(vis.n_new, s_red);
     if (threadIdx.x == 0 && c) atomicAdd(&C->new_count, c);
     if (!grid_sync(S.bar)) return 0;
+    if (S.log && gtid == 0 && S.log_base + level < kMaxLog) {
+      sg_level_record r = {};
+      r.level = S.log_base + level;
+      r.frontier_size = ns + (uint32_t)(bp >> 32);
+      r.frontier_degree = ld_cg(&C->frontier_deg);
+      r.next_size = (uint32_t)ld_cg(&C->new_count);
+      r.t_start_ns = t0;
+      r.t_end_ns = sygraph::detail::global_timer_ns();
+      S.log[S.log_base + level] = r;
+    }
     if (ld_cg(&C->new_count) == 0) return level + 1;
   }
 }

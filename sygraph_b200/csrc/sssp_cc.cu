@@ -110,9 +110,11 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   W threshold = P.delta;
   unsigned long long total = 0;
   uint32_t pass = 0;
+  PushLoop loop = P.L;
   for (;;) {
+    loop.log_base = (uint32_t)min(total, (unsigned long long)kMaxLog);
     const uint32_t levels = push_levels(
-        P.L,
+        loop,
         [&](uint32_t, uint32_t* fb_next) {
           SsspVisitor<W> v;
           v.fb_next = fb_next;
@@ -183,7 +185,10 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
     }
     if (!refilled) break;
   }
-  if (gtid == 0) P.result[0] = total;
+  if (gtid == 0) {
+    P.result[0] = total;
+    P.result[1] = pass;
+  }
 }
 
 struct CcParams {
@@ -296,6 +301,7 @@ struct sg_sssp_s {
   bool initialised = false;
   bool fresh = false;  // initialised but not run: distances not written yet
   void* dist = nullptr;
+  sg_level_record* log = nullptr;
   uint32_t* far = nullptr;
   Refill* refill = nullptr;
   double delta = 0.0;  // near-far threshold step; 0 = the reference's frontier Bellman-Ford
@@ -325,13 +331,15 @@ static sg_status sssp_materialise(sg_sssp s) {
 static sg_status sssp_launch(sg_sssp s) {
   sg_graph g = s->g;
   SG_CUDA(cudaMemsetAsync(s->ws.bar, 0, sizeof(GridBarrier), s->stream));
+  PushLoop L = s->ws.loop(g);
+  L.log = s->log;
   if (g->value_type == SG_WEIGHT_F32) {
-    SsspParams<float> P{s->ws.loop(g), s->source, (float*)s->dist, (const float*)g->fwd.val, s->ws.result,
+    SsspParams<float> P{L, s->source, (float*)s->dist, (const float*)g->fwd.val, s->ws.result,
                         s->far, s->refill, (float)s->delta};
     return launch_persistent(sssp_kernel<float>, P, 2, s->stream, s->max_ctas);
   }
   const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
-  SsspParams<uint32_t> P{s->ws.loop(g), s->source, (uint32_t*)s->dist, (const uint32_t*)g->fwd.val, s->ws.result,
+  SsspParams<uint32_t> P{L, s->source, (uint32_t*)s->dist, (const uint32_t*)g->fwd.val, s->ws.result,
                          s->far, s->refill, d};
   return launch_persistent(sssp_kernel<uint32_t>, P, 2, s->stream, s->max_ctas);
 }
@@ -352,11 +360,13 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out) {
   if (st == SG_OK) st = s->ws.alloc(g->n);
   if (st == SG_OK) st = dev_alloc(&s->far, div_up(g->n, 32));
   if (st == SG_OK) st = dev_alloc(&s->refill, 3);
+  if (st == SG_OK) st = dev_alloc(&s->log, SG_MAX_LOGGED_LEVELS);
   if (st != SG_OK) {
     s->ws.release();
     cudaFree(s->dist);
     dev_free(s->far);
     dev_free(s->refill);
+    dev_free(s->log);
     delete s;
     return st;
   }
@@ -371,8 +381,21 @@ sg_status sg_sssp_destroy(sg_sssp s) {
     cudaFree(s->dist);
     dev_free(s->far);
     dev_free(s->refill);
+    dev_free(s->log);
     delete s;
   }
+  return SG_OK;
+}
+
+sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
+  SG_REQUIRE(s && count, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaStreamSynchronize(s->stream));
+  unsigned long long it = 0;
+  SG_CUDA(cudaMemcpy(&it, s->ws.result, sizeof(it), cudaMemcpyDeviceToHost));
+  uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
+  if (k > cap) k = cap;
+  if (host_records && k) SG_CUDA(cudaMemcpy(host_records, s->log, sizeof(sg_level_record) * k, cudaMemcpyDeviceToHost));
+  *count = k;
   return SG_OK;
 }
 
