@@ -282,7 +282,7 @@ def serving_bench(sg, torch) -> dict:
         out["runs"].append({"qps_offered": qps, **r})
     out["stats"] = srv.stats()
     srv.close()
-    wl = serving.make_workload(sizes, 1000.0, 0.3, 0.7, seed=9)
+    wl = serving.make_workload(sizes, 1000.0, 1.0, 0.7, seed=9)
     out["one_at_a_time"] = serving.run_one_at_a_time(Gs, wl, sssp_delta=SSSP_DELTA)
     best = max(r["qps_served"] for r in out["runs"])
     out["served_qps_vs_one_at_a_time"] = best / out["one_at_a_time"]["qps_served"]

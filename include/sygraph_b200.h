@@ -424,6 +424,12 @@ sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations);
  * same fixed point); the iteration count and the work are not.  0 (the
  * default) is the reference's frontier Bellman-Ford. */
 sg_status sg_sssp_set_delta(sg_sssp s, double delta);
+/* Pull iterations (not in the reference): an iteration whose frontier
+ * out-degree times `ratio` exceeds the edge count runs as one pull sweep
+ * (every vertex takes the minimum over its in-neighbours in the frontier, no
+ * atomics) instead of a push.  Distances are unchanged; 0 (the default) is
+ * push only, as the reference. */
+sg_status sg_sssp_set_pull(sg_sssp s, uint32_t ratio);
 /* Per-iteration log of the last run (frontier size and out-degree, vertices
  * improved, device timestamps), as sg_bfs_level_records. */
 sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count);
@@ -498,7 +504,7 @@ typedef struct sg_server_s* sg_server;
 typedef struct {
   uint32_t slots;          /* concurrent launches (0: 4) */
   uint32_t max_batch;      /* BFS queries per batched launch, <= 64 (0: 64) */
-  uint32_t min_batch;      /* fewer pending BFS queries of a graph run singly (0: 4) */
+  uint32_t min_batch;      /* fewer pending BFS queries of a graph run singly (0: 16) */
   uint32_t ctas_per_slot;  /* persistent grid per launch (0: 2 * SMs / slots) */
   uint64_t memory_budget;  /* workspace bytes (0: half the free device memory) */
   double sssp_delta;       /* near-far step of SSSP queries (0: the reference schedule) */

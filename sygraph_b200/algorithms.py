@@ -189,6 +189,10 @@ class SSSP:
         call("sg_sssp_level_records", self.handle, recs, _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
         return [{k: getattr(recs[i], k) for k, _ in _lib.LevelRecord._fields_} for i in range(cnt.value)]
 
+    def set_pull(self, ratio: int) -> None:
+        """Pull iterations when frontier out-degree * ratio > m (0: push only)."""
+        call("sg_sssp_set_pull", self.handle, int(ratio))
+
     def set_delta(self, delta: float) -> None:
         """Near-far threshold step (0: the reference's frontier Bellman-Ford)."""
         call("sg_sssp_set_delta", self.handle, float(delta))

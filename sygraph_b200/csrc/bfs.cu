@@ -435,6 +435,17 @@ sg_status sg_bfs_set_schedule(sg_bfs b, const int* host_strategies, uint32_t len
   return SG_OK;
 }
 
+}  // extern "C"
+
+sg_status sgb::bfs_launch_status(sg_bfs b) {
+  uint32_t err = 0;
+  SG_CUDA(cudaMemcpyAsync(&err, &b->bar->error, sizeof(err), cudaMemcpyDeviceToHost, b->stream));
+  SG_CUDA(cudaStreamSynchronize(b->stream));
+  return err ? fail(SG_ERR_TIMEOUT, "BFS engine: a grid barrier wait ran out") : SG_OK;
+}
+
+extern "C" {
+
 sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels) {
   clear_error();
   SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");

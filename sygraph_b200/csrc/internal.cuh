@@ -91,6 +91,11 @@ inline unsigned grid_for(uint64_t work_items, unsigned block, unsigned per_sm = 
 
 // Device address of an sg_mlp's parameter block (selector.cu).
 const void* mlp_device_params(sg_mlp h);
+// SG_ERR_TIMEOUT when the last launch of the instance left its grid barrier's
+// error flag set (read after its stream completed; used by the server).
+sg_status bfs_launch_status(sg_bfs b);
+sg_status msbfs_launch_status(sg_msbfs h);
+sg_status sssp_launch_status(sg_sssp s);
 
 // ------------------------------------------------------------------ handles --
 struct GraphDir {

@@ -668,6 +668,17 @@ sg_status sg_msbfs_run(sg_msbfs h, const uint32_t* host_sources, uint32_t k, int
   return SG_OK;
 }
 
+}  // extern "C"
+
+sg_status sgb::msbfs_launch_status(sg_msbfs h) {
+  uint32_t err = 0;
+  SG_CUDA(cudaMemcpyAsync(&err, &h->bar->error, sizeof(err), cudaMemcpyDeviceToHost, h->stream));
+  SG_CUDA(cudaStreamSynchronize(h->stream));
+  return err ? fail(SG_ERR_TIMEOUT, "batched BFS: a grid barrier wait ran out") : SG_OK;
+}
+
+extern "C" {
+
 sg_status sg_msbfs_set_launch(sg_msbfs h, void* stream, uint32_t max_ctas) {
   clear_error();
   SG_REQUIRE(h, SG_ERR_INVALID, "NULL argument");

@@ -346,8 +346,17 @@ void dispatcher(sg_server_s* s) {
       const cudaError_t e = cudaEventQuery(sl.ev);
       if (e == cudaErrorNotReady) continue;
       sl.busy = false;
-      finish(s, sl.batch, e == cudaSuccess ? SG_OK : SG_ERR_CUDA);
+      sg_status st = e == cudaSuccess ? SG_OK : SG_ERR_CUDA;
       if (e != cudaSuccess) cudaGetLastError();
+      if (st == SG_OK) {  // a launch whose grid barrier timed out did not finish its work
+        auto it = sl.ws.find(ws_key(sl.graph, sl.ws_kind));
+        if (it != sl.ws.end()) {
+          if (sl.ws_kind == kWsBfs) st = sgb::bfs_launch_status((sg_bfs)it->second.handle);
+          if (sl.ws_kind == kWsBatch) st = sgb::msbfs_launch_status((sg_msbfs)it->second.handle);
+          if (sl.ws_kind == kWsSssp) st = sgb::sssp_launch_status((sg_sssp)it->second.handle);
+        }
+      }
+      finish(s, sl.batch, st);
       sl.batch.clear();
       completed = true;
     }
@@ -379,7 +388,7 @@ sg_status sg_server_create(const sg_server_config* cfg, sg_server* out) {
   if (cfg) c = *cfg;
   if (!c.slots) c.slots = 4;
   if (!c.max_batch) c.max_batch = 64;
-  if (!c.min_batch) c.min_batch = 4;
+  if (!c.min_batch) c.min_batch = 16;
   SG_REQUIRE(c.slots <= 64, SG_ERR_INVALID, "at most 64 slots");
   SG_REQUIRE(c.max_batch <= 64, SG_ERR_INVALID, "a batch holds at most 64 queries");
   SG_REQUIRE(c.sssp_delta >= 0.0, SG_ERR_INVALID, "sssp_delta must be non-negative");

@@ -12,7 +12,10 @@
 //   with atomicMax; a vertex whose label grew joins the next frontier
 //   (cc.hpp:135-168).  The fixed point is the maximum id over the vertices
 //   that reach v.
+#include <vector>
+
 #include "push_engine.cuh"
+#include "sssp_pull.cuh"
 
 namespace sgb {
 namespace {
@@ -22,8 +25,9 @@ using namespace eng;
 // Near-far bookkeeping of one refill pass (three rotating slots).
 struct Refill {
   unsigned long long moved, remaining;
-  uint32_t far_min;  // bit pattern of the smallest distance left in the far set
-  uint32_t pad[3];
+  unsigned long long moved_deg;  // out-degree sum of the vertices moved to the frontier
+  uint32_t far_min;              // bit pattern of the smallest distance left in the far set
+  uint32_t pad;
 };
 
 template <typename W>
@@ -36,6 +40,9 @@ struct SsspParams {
   uint32_t* far;  // w0 words: improved vertices at or beyond the threshold
   Refill* refill;
   W delta;        // 0: plain frontier Bellman-Ford (every improved vertex is near)
+  PullArgs<W> pull;
+  uint32_t pull_ratio;  // pull when the frontier's out-degree * pull_ratio > m (0: push only)
+  unsigned long long m;
 };
 
 // Non-negative floats and unsigned integers both order like their bits.
@@ -60,8 +67,17 @@ struct SsspVisitor : NextFrontier {
   W* dist;
   const W* w;
   uint32_t* far;
+  const uint32_t* ro;
   W threshold;
   bool bucketed;
+  unsigned long long deg_new = 0;
+  __device__ __forceinline__ void mark(uint32_t u) {
+    const uint32_t b = 1u << (u & 31);
+    if (!(atomicOr(fb_next + (u >> 5), b) & b)) {
+      n_new++;
+      deg_new += ro[u + 1] - ro[u];
+    }
+  }
   __device__ __forceinline__ W src(uint32_t v) const { return ld_cg(dist + v); }
   __device__ __forceinline__ bool visit(uint32_t u, uint32_t e, W dv, uint32_t) {
     const W nd = dv + w[e];
@@ -74,6 +90,73 @@ struct SsspVisitor : NextFrontier {
     return true;
   }
 };
+
+// The SSSP level loop: per iteration, push (compact the frontier, expand it
+// with atomicMin relaxations) or, when the frontier's out-degree is a large
+// part of the edges, one pull sweep.  Returns the number of iterations, or 0
+// when a barrier timed out.  `fdeg0` is the out-degree of the first frontier.
+template <typename W>
+__device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const PushLoop& S, W threshold, bool bucketed,
+                                                unsigned long long fdeg0, uint32_t* s_scan, unsigned long long* s_red) {
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  for (uint32_t level = 0;; level++) {
+    Counters* C = S.cnt + (level % 3);
+    const Counters* Cprev = S.cnt + ((level + 2) % 3);
+    uint32_t* fb_cur = S.fb + (size_t)(level % 3) * S.w0;
+    uint32_t* fb_next = S.fb + (size_t)((level + 1) % 3) * S.w0;
+    uint32_t* fb_zero = S.fb + (size_t)((level + 2) % 3) * S.w0;
+    const unsigned long long fdeg = level ? ld_cg(&Cprev->new_deg) : fdeg0;
+    if (gtid == 0) {
+      Counters z = {};
+      S.cnt[(level + 1) % 3] = z;
+    }
+    const uint64_t t0 = (S.log && gtid == 0) ? sygraph::detail::global_timer_ns() : 0;
+    const bool pull = P.pull_ratio && fdeg * P.pull_ratio > P.m;
+    unsigned long long n_new = 0, deg_new = 0;
+    uint32_t ns = 0;
+    unsigned long long bp = 0;
+    if (!pull) {
+      compact_frontier(fb_cur, S.w0, S.ro, C, S.q, s_scan);
+      if (!grid_sync(S.bar)) return 0;
+      ns = ld_cg(&C->small_tail);
+      bp = ld_cg(&C->big_packed);
+      SsspVisitor<W> v;
+      v.fb_next = fb_next;
+      v.dist = P.dist;
+      v.w = P.w;
+      v.far = P.far;
+      v.ro = S.ro;
+      v.threshold = threshold;
+      v.bucketed = bucketed;
+      push_expand(S.ro, S.col, S.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
+      n_new = v.n_new;
+      deg_new = v.deg_new;
+    } else {
+      sssp_pull_sweep(P.pull, fb_cur, fb_next, threshold, bucketed, n_new, deg_new);
+    }
+    for (uint32_t i = gtid; i < S.w0; i += nthreads) st_cg(fb_zero + i, 0u);
+    const unsigned long long c = block_sum<unsigned long long>(n_new, s_red);
+    const unsigned long long d = block_sum<unsigned long long>(deg_new, s_red);
+    if (threadIdx.x == 0) {
+      if (c) atomicAdd(&C->new_count, c);
+      if (d) atomicAdd(&C->new_deg, d);
+    }
+    if (!grid_sync(S.bar)) return 0;
+    if (S.log && gtid == 0 && S.log_base + level < kMaxLog) {
+      sg_level_record r = {};
+      r.level = S.log_base + level;
+      r.strategy = pull ? 2u : 0u;
+      r.frontier_size = pull ? 0u : ns + (uint32_t)(bp >> 32);
+      r.frontier_degree = fdeg;
+      r.next_size = (uint32_t)ld_cg(&C->new_count);
+      r.t_start_ns = t0;
+      r.t_end_ns = sygraph::detail::global_timer_ns();
+      S.log[S.log_base + level] = r;
+    }
+    if (ld_cg(&C->new_count) == 0) return level + 1;
+  }
+}
 
 template <typename W>
 __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
@@ -111,21 +194,10 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   unsigned long long total = 0;
   uint32_t pass = 0;
   PushLoop loop = P.L;
+  unsigned long long fdeg0 = P.L.ro[src + 1] - P.L.ro[src];
   for (;;) {
     loop.log_base = (uint32_t)min(total, (unsigned long long)kMaxLog);
-    const uint32_t levels = push_levels(
-        loop,
-        [&](uint32_t, uint32_t* fb_next) {
-          SsspVisitor<W> v;
-          v.fb_next = fb_next;
-          v.dist = P.dist;
-          v.w = P.w;
-          v.far = P.far;
-          v.threshold = threshold;
-          v.bucketed = bucketed;
-          return v;
-        },
-        s_scan, s_red);
+    const uint32_t levels = sssp_levels(P, loop, threshold, bucketed, fdeg0, s_scan, s_red);
     if (!levels) return;
     total += levels;
     if (!bucketed) break;
@@ -143,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
         P.L.cnt[gtid] = z;
       }
       const W next_t = threshold + P.delta;
-      unsigned long long moved = 0, remaining = 0;
+      unsigned long long moved = 0, remaining = 0, mdeg = 0;
       uint32_t fmin = 0xffffffffu;
       for (uint32_t i = gtid; i < w0; i += nthreads) {
         const uint32_t f = ld_cg(P.far + i);
@@ -151,9 +223,11 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
         for (uint32_t b = f; b; b &= b - 1) {
           const uint32_t bit = __ffs(b) - 1;
           const W d = ld_cg(P.dist + i * 32 + bit);
-          if (d < next_t)
+          if (d < next_t) {
             near |= 1u << bit;
-          else
+            const uint32_t v = i * 32 + bit;
+            mdeg += P.L.ro[v + 1] - P.L.ro[v];
+          } else
             fmin = min(fmin, order_bits<W>(d));
         }
         st_cg(P.L.fb + i, near);
@@ -165,16 +239,19 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       }
       const unsigned long long mv = block_sum<unsigned long long>(moved, s_red);
       const unsigned long long rm = block_sum<unsigned long long>(remaining, s_red);
+      const unsigned long long md = block_sum<unsigned long long>(mdeg, s_red);
       fmin = sygraph::detail::warp_min(fmin);
       if ((threadIdx.x & 31) == 0 && fmin != 0xffffffffu) atomicMin(&R->far_min, fmin);
       if (threadIdx.x == 0) {
         if (mv) atomicAdd(&R->moved, mv);
         if (rm) atomicAdd(&R->remaining, rm);
+        if (md) atomicAdd(&R->moved_deg, md);
       }
       if (!grid_sync(P.L.bar)) return;
       pass++;
       threshold = next_t;
       if (ld_cg(&R->moved)) {
+        fdeg0 = ld_cg(&R->moved_deg);
         refilled = true;
         break;
       }
@@ -305,6 +382,10 @@ struct sg_sssp_s {
   uint32_t* far = nullptr;
   Refill* refill = nullptr;
   double delta = 0.0;  // near-far threshold step; 0 = the reference's frontier Bellman-Ford
+  uint32_t pull_ratio = 0;  // pull iterations when frontier out-degree * ratio > m; 0 = push only
+  uint32_t* heavy_v = nullptr;      // vertices of in-degree >= kPullHeavy
+  uint32_t* heavy_first = nullptr;  // their first chunk index
+  uint32_t n_heavy = 0, n_chunks = 0;
   PushWorkspace ws;
 };
 
@@ -336,11 +417,19 @@ static sg_status sssp_launch(sg_sssp s) {
   if (g->value_type == SG_WEIGHT_F32) {
     SsspParams<float> P{L, s->source, (float*)s->dist, (const float*)g->fwd.val, s->ws.result,
                         s->far, s->refill, (float)s->delta};
+    P.pull = PullArgs<float>{g->n, L.w0, g->fwd.ro, g->inv.ro, g->inv.col, (const float*)g->inv.val,
+                             (float*)s->dist, s->far, s->heavy_v, s->heavy_first, s->n_heavy, s->n_chunks};
+    P.pull_ratio = s->pull_ratio;
+    P.m = g->m;
     return launch_persistent(sssp_kernel<float>, P, 2, s->stream, s->max_ctas);
   }
   const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
   SsspParams<uint32_t> P{L, s->source, (uint32_t*)s->dist, (const uint32_t*)g->fwd.val, s->ws.result,
                          s->far, s->refill, d};
+  P.pull = PullArgs<uint32_t>{g->n, L.w0, g->fwd.ro, g->inv.ro, g->inv.col, (const uint32_t*)g->inv.val,
+                              (uint32_t*)s->dist, s->far, s->heavy_v, s->heavy_first, s->n_heavy, s->n_chunks};
+  P.pull_ratio = s->pull_ratio;
+  P.m = g->m;
   return launch_persistent(sssp_kernel<uint32_t>, P, 2, s->stream, s->max_ctas);
 }
 
@@ -361,12 +450,42 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out) {
   if (st == SG_OK) st = dev_alloc(&s->far, div_up(g->n, 32));
   if (st == SG_OK) st = dev_alloc(&s->refill, 3);
   if (st == SG_OK) st = dev_alloc(&s->log, SG_MAX_LOGGED_LEVELS);
+  if (st == SG_OK) {
+    // static chunk list of the vertices pulled in chunks (in-degree >= kPullHeavy)
+    std::vector<uint32_t> iro((size_t)g->n + 1), hv, hf;
+    if (cudaMemcpy(iro.data(), g->inv.ro, sizeof(uint32_t) * iro.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cudaGetLastError();
+      st = fail(SG_ERR_CUDA, "SSSP set-up: reading the in-edge offsets failed");
+    }
+    uint32_t chunks = 0;
+    for (uint32_t v = 0; st == SG_OK && v < g->n; v++) {
+      const uint32_t d = iro[v + 1] - iro[v];
+      if (d >= eng::kPullHeavy) {
+        hv.push_back(v);
+        hf.push_back(chunks);
+        chunks += (d + eng::kPullChunk - 1) / eng::kPullChunk;
+      }
+    }
+    if (st == SG_OK && !hv.empty()) {
+      st = dev_alloc(&s->heavy_v, hv.size());
+      if (st == SG_OK) st = dev_alloc(&s->heavy_first, hf.size());
+      if (st == SG_OK && (cudaMemcpy(s->heavy_v, hv.data(), 4 * hv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+                          cudaMemcpy(s->heavy_first, hf.data(), 4 * hf.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
+        cudaGetLastError();
+        st = fail(SG_ERR_CUDA, "SSSP set-up: uploading the chunk list failed");
+      }
+      s->n_heavy = (uint32_t)hv.size();
+      s->n_chunks = chunks;
+    }
+  }
   if (st != SG_OK) {
     s->ws.release();
     cudaFree(s->dist);
     dev_free(s->far);
     dev_free(s->refill);
     dev_free(s->log);
+    dev_free(s->heavy_v);
+    dev_free(s->heavy_first);
     delete s;
     return st;
   }
@@ -382,10 +501,30 @@ sg_status sg_sssp_destroy(sg_sssp s) {
     dev_free(s->far);
     dev_free(s->refill);
     dev_free(s->log);
+    dev_free(s->heavy_v);
+    dev_free(s->heavy_first);
     delete s;
   }
   return SG_OK;
 }
+
+sg_status sg_sssp_set_pull(sg_sssp s, uint32_t ratio) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  s->pull_ratio = ratio;
+  return SG_OK;
+}
+
+}  // extern "C"
+
+sg_status sgb::sssp_launch_status(sg_sssp s) {
+  uint32_t err = 0;
+  SG_CUDA(cudaMemcpyAsync(&err, &s->ws.bar->error, sizeof(err), cudaMemcpyDeviceToHost, s->stream));
+  SG_CUDA(cudaStreamSynchronize(s->stream));
+  return err ? fail(SG_ERR_TIMEOUT, "SSSP engine: a grid barrier wait ran out") : SG_OK;
+}
+
+extern "C" {
 
 sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
   SG_REQUIRE(s && count, SG_ERR_INVALID, "NULL argument");

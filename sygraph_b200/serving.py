@@ -44,7 +44,7 @@ class PinnedBuffer:
 
 
 class Server:
-    def __init__(self, slots: int = 4, max_batch: int = 64, min_batch: int = 4, ctas_per_slot: int = 0,
+    def __init__(self, slots: int = 4, max_batch: int = 64, min_batch: int = 16, ctas_per_slot: int = 0,
                  memory_budget: int = 0, sssp_delta: float = 0.0):
         cfg = _lib.ServerConfig(slots, max_batch, min_batch, ctas_per_slot, memory_budget, sssp_delta)
         h = C.c_void_p()

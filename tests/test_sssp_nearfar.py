@@ -86,3 +86,44 @@ def test_instances_on_own_streams_with_grid_caps(sg, oracle, rmat):
     gc.collect()
     for h in streams:
         sg._lib.call("sg_stream_destroy", h)
+
+
+@pytest.mark.parametrize("ratio", [1, 4, 1000])
+@pytest.mark.parametrize("delta", [0.0, 0.1])
+def test_pull_iterations_rmat_f32(sg, oracle, rmat, ratio, delta):
+    g = rmat(14, perm_seed=3)
+    s = sg.algorithms.SSSP(sg.graph.build.fromCSR(g))
+    s.set_pull(ratio)
+    s.set_delta(delta)
+    for src in [int(np.argmax(g.degrees()))] + [int(x) for x in sg.io.sample_sources(g, 2, seed=4)]:
+        s.init(src)
+        s.run()
+        ref = oracle.sssp_dijkstra(g, src)
+        assert np.array_equal(s.getDistances().view(np.uint32), ref.view(np.uint32)), (ratio, delta, src)
+    if ratio == 1000:
+        assert any(r["strategy"] == 2 for r in s.level_records())  # some iterations pulled
+
+
+def test_pull_iterations_directed_hubs_and_u32(sg, oracle):
+    rng = np.random.default_rng(8)
+    n = 6000
+    hubs = rng.integers(0, n, 5)
+    src = np.concatenate([rng.integers(0, n, 40000), rng.integers(0, n, 8000)])
+    dst = np.concatenate([rng.integers(0, n, 40000), np.repeat(hubs, 1600)])  # hubs: in-degree > 256
+    w = (rng.integers(1, 1 << 24, src.size) / float(1 << 24)).astype(np.float32)
+    gd = sg.io.fromCOO(n, src, dst, w, dedupe=True, drop_self_loops=True)
+    s = sg.algorithms.SSSP(sg.graph.build.fromCSR(gd, sg.Properties(directed=True, weighted=True)))
+    for ratio, delta in ((1000, 0.0), (1000, 0.05), (2, 0.0)):
+        s.set_pull(ratio)
+        s.set_delta(delta)
+        for v in (int(hubs[0]), 11):
+            s.init(v)
+            s.run()
+            assert np.array_equal(s.getDistances(), oracle.sssp_dijkstra(gd, v)), (ratio, delta, v)
+    gg = sg.io.grid(80, 0.02, seed=1, weight_seed=2, value_type=sg.WEIGHT_U32)
+    s2 = sg.algorithms.SSSP(sg.graph.build.fromCSR(gg))
+    s2.set_pull(1000)
+    s2.set_delta(64)
+    s2.init(0)
+    s2.run()
+    assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gg, 0))
