@@ -241,10 +241,20 @@ def profile_case(kind: str) -> None:
         srcs = sg.io.sample_sources(g, N_SOURCES, seed=SOURCE_SEED)
         a = sg.algorithms.MultiBFS(G, N_SOURCES)
         for _ in range(2):
-            det = a.run(srcs, 2, ALPHA, BETA)
+            det = a.run(srcs, 2, MS_ALPHA, MS_BETA)
         print(json.dumps({"profile": "msbfs", "sources": N_SOURCES, **det}))
+    elif kind == "bc":
+        gbc = sg.io.rmat(BC_SCALE, EDGE_FACTOR, *RMAT_ABC, seed=1)
+        Gbc = sg.graph.build.fromCSR(gbc)
+        sbc = sg.io.sample_sources(gbc, BC_SOURCES, seed=SOURCE_SEED)
+        a = sg.algorithms.BatchedBC(Gbc)
+        for _ in range(2):
+            det = a.run(sbc)
+        print(json.dumps({"profile": "bc", "sources": BC_SOURCES, **det}))
     else:
         a = sg.algorithms.SSSP(G)
+        a.set_pull(SSSP_PULL)
+        a.set_delta(SSSP_DELTA)
         for _ in range(2):
             a.init(src)
             it = a.run()
@@ -256,6 +266,7 @@ SERVE_QPS = (1000.0, 3000.0)
 SERVE_SECONDS = 2.0
 SERVE_SLOTS = 4
 SSSP_DELTA = 0.1
+SSSP_PULL = 4  # pull iterations when the frontier's out-degree exceeds m / 4
 
 
 def serving_bench(sg, torch) -> dict:
@@ -298,7 +309,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sub-benchmark")
     ap.add_argument("--sssp-sources", type=int, default=8)
-    ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs"], default=None,
+    ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs", "bc"], default=None,
                     help="profiling case: build the graph, run 2 traversals of one kind and exit (few launches)")
     args = ap.parse_args()
     world, rank, local = dist_init()

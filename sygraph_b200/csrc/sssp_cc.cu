@@ -45,22 +45,6 @@ struct SsspParams {
   unsigned long long m;
 };
 
-// Non-negative floats and unsigned integers both order like their bits.
-template <typename W>
-__device__ __forceinline__ uint32_t order_bits(W x) {
-  if constexpr (sizeof(W) == 4 && W(0.5) != W(0))
-    return __float_as_uint(x);
-  else
-    return (uint32_t)x;
-}
-template <typename W>
-__device__ __forceinline__ W from_order_bits(uint32_t b) {
-  if constexpr (sizeof(W) == 4 && W(0.5) != W(0))
-    return __uint_as_float(b);
-  else
-    return (W)b;
-}
-
 template <typename W>
 struct SsspVisitor : NextFrontier {
   using src_t = W;
@@ -97,7 +81,8 @@ struct SsspVisitor : NextFrontier {
 // when a barrier timed out.  `fdeg0` is the out-degree of the first frontier.
 template <typename W>
 __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const PushLoop& S, W threshold, bool bucketed,
-                                                unsigned long long fdeg0, uint32_t* s_scan, unsigned long long* s_red) {
+                                                unsigned long long fdeg0, uint32_t* s_scan, unsigned long long* s_red,
+                                                uint32_t* s_best) {
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
   for (uint32_t level = 0;; level++) {
@@ -133,7 +118,7 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
       n_new = v.n_new;
       deg_new = v.deg_new;
     } else {
-      sssp_pull_sweep(P.pull, fb_cur, fb_next, threshold, bucketed, n_new, deg_new);
+      sssp_pull_sweep(P.pull, fb_cur, fb_next, threshold, bucketed, n_new, deg_new, s_best);
     }
     for (uint32_t i = gtid; i < S.w0; i += nthreads) st_cg(fb_zero + i, 0u);
     const unsigned long long c = block_sum<unsigned long long>(n_new, s_red);
@@ -162,6 +147,7 @@ template <typename W>
 __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   __shared__ uint32_t s_scan[32];
   __shared__ unsigned long long s_red[32];
+  __shared__ uint32_t s_best[kThreads];
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
   const uint32_t n = P.L.n, w0 = P.L.w0, src = P.source;
   const W inf = (W)(n + 1);  // (weight_t)(size + 1), sssp.hpp:43
@@ -197,7 +183,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   unsigned long long fdeg0 = P.L.ro[src + 1] - P.L.ro[src];
   for (;;) {
     loop.log_base = (uint32_t)min(total, (unsigned long long)kMaxLog);
-    const uint32_t levels = sssp_levels(P, loop, threshold, bucketed, fdeg0, s_scan, s_red);
+    const uint32_t levels = sssp_levels(P, loop, threshold, bucketed, fdeg0, s_scan, s_red, s_best);
     if (!levels) return;
     total += levels;
     if (!bucketed) break;

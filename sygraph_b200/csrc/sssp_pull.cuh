@@ -4,10 +4,12 @@
 // atomicMin per improving edge.  The minimum is exact and order-independent,
 // so a pull iteration reaches the same fixed point as a push iteration.
 //
-//   light vertex (in-degree < kPullHeavy): a warp per bitmap word; lists of
-//       at most 32 in-neighbours are scanned by their lane (next column index
-//       loaded while the current frontier bit is tested), longer ones by the
-//       whole warp with a min-reduction; only the owner writes d[u].
+//   light vertex (in-degree < kPullHeavy): a warp per bitmap word; the
+//       in-lists of the word's 32 vertices are walked edge-parallel (a warp
+//       scan of their degrees maps lanes to consecutive edges, so column and
+//       weight loads are coalesced) and each candidate goes into the owner's
+//       shared-memory slot by atomicMin on order-preserving bits; only the
+//       owner writes d[u].
 //   heavy vertex: its in-list is cut into kPullChunk-edge chunks (a static
 //       list built when the instance is created); warps take chunks
 //       grid-stride and finish each with one atomicMin on d[u].
@@ -20,6 +22,22 @@ namespace eng {
 
 constexpr uint32_t kPullHeavy = 256;  // in-degree from which a vertex is pulled in chunks
 constexpr uint32_t kPullChunk = 256;  // in-edges per chunk
+
+// Non-negative floats and unsigned integers both order like their bits.
+template <typename W>
+__device__ __forceinline__ uint32_t order_bits(W x) {
+  if constexpr (sizeof(W) == 4 && W(0.5) != W(0))
+    return __float_as_uint(x);
+  else
+    return (uint32_t)x;
+}
+template <typename W>
+__device__ __forceinline__ W from_order_bits(uint32_t b) {
+  if constexpr (sizeof(W) == 4 && W(0.5) != W(0))
+    return __uint_as_float(b);
+  else
+    return (W)b;
+}
 
 template <typename W>
 __device__ __forceinline__ W warp_min_w(W x) {
@@ -62,54 +80,43 @@ __device__ __forceinline__ void pull_mark(const PullArgs<W>& A, uint32_t* fb_nex
   }
 }
 
+// s_best: one uint32 per thread of the block (the warp's 32 owner slots).
 template <typename W>
 __device__ __forceinline__ void sssp_pull_sweep(const PullArgs<W>& A, const uint32_t* fb_cur, uint32_t* fb_next,
                                                 W threshold, bool bucketed, unsigned long long& n_new,
-                                                unsigned long long& deg_new) {
+                                                unsigned long long& deg_new, uint32_t* s_best) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t* best_slot = s_best + (threadIdx.x & ~31u);
   for (uint32_t wi = gwarp; wi < A.w0; wi += nwarps) {
     const uint32_t v = wi * 32 + lane;
     const bool in = v < A.n;
     const uint32_t beg = in ? A.iro[v] : 0u, end = in ? A.iro[v + 1] : 0u;
-    const uint32_t deg = end - beg;
-    const bool light = in && deg < kPullHeavy;
+    const bool light = in && end - beg < kPullHeavy;
+    const uint32_t dg = light ? end - beg : 0u;
+    const uint32_t incl = warp_inclusive_scan(dg);
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    if (!total) continue;
+    const uint32_t excl = incl - dg;
     const W d0 = light ? ld_cg(A.dist + v) : W(0);
-    W best = d0;
-    if (light && deg <= 32) {
-      uint32_t e = beg;
-      uint32_t c = e < end ? A.icol[e] : 0u;
-      while (e < end) {
-        const uint32_t cn = e + 1 < end ? A.icol[e + 1] : 0u;
-        if (bit_test_ro(fb_cur, c)) {
-          const W cand = ld_cg(A.dist + c) + A.iw[e];
-          best = cand < best ? cand : best;
-        }
-        c = cn;
-        e++;
+    best_slot[lane] = light ? order_bits<W>(d0) : 0xffffffffu;
+    __syncwarp();
+    for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      const bool act = r < total;
+      const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+      const uint32_t ob = __shfl_sync(kFullMask, beg, o);
+      const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+      if (act) {
+        const uint32_t e = ob + (r - oe);
+        const uint32_t c = A.icol[e];
+        if (bit_test_ro(fb_cur, c)) atomicMin(best_slot + o, order_bits<W>(ld_cg(A.dist + c) + A.iw[e]));
       }
     }
-    // medium lists: the warp scans each with a min-reduction
-    uint32_t med = __ballot_sync(kFullMask, light && deg > 32);
-    while (med) {
-      const uint32_t j = __ffs(med) - 1;
-      med &= med - 1;
-      const uint32_t jb = __shfl_sync(kFullMask, beg, j), je = __shfl_sync(kFullMask, end, j);
-      W part = __shfl_sync(kFullMask, best, j);
-      for (uint32_t eb = jb; eb < je; eb += 32) {
-        const uint32_t e = eb + lane;
-        if (e < je) {
-          const uint32_t c = A.icol[e];
-          if (bit_test_ro(fb_cur, c)) {
-            const W cand = ld_cg(A.dist + c) + A.iw[e];
-            part = cand < part ? cand : part;
-          }
-        }
-      }
-      part = warp_min_w(part);
-      if (lane == j) best = part;
-    }
+    __syncwarp();
+    const W best = from_order_bits<W>(best_slot[lane]);
+    __syncwarp();
     if (light && best < d0) {
       st_cg(A.dist + v, best);
       pull_mark(A, fb_next, v, best, threshold, bucketed, n_new, deg_new);
