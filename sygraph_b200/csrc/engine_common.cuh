@@ -54,10 +54,11 @@ using sygraph::detail::block_sum;
 
 // Bitmap -> queues.  Each CTA owns a contiguous range of bitmap words, counts
 // the vertices there by class, reserves its slots with one atomic per list
-// and writes them in vertex order.
+// and writes them in vertex order.  When `accumulate` is given, each word is
+// also OR-ed into it (one thread per word).
 __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb, uint32_t w0,
                                                  const uint32_t* __restrict__ ro, Counters* C, Queues q,
-                                                 uint32_t* s_scan) {
+                                                 uint32_t* s_scan, uint32_t* accumulate = nullptr) {
   __shared__ uint32_t s_base_small, s_base_big, s_base_chunk;
   const uint32_t per_block = (w0 + gridDim.x - 1) / gridDim.x;
   const uint32_t wbeg = blockIdx.x * per_block;
@@ -65,6 +66,7 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
   for (uint32_t base = wbeg; base < wend; base += blockDim.x) {
     const uint32_t wi = base + threadIdx.x;
     const uint32_t bits = wi < wend ? ld_cg(fb + wi) : 0u;
+    if (accumulate && bits) st_cg(accumulate + wi, ld_cg(accumulate + wi) | bits);
     uint32_t n_small = 0, n_big = 0, n_chunk = 0;
     unsigned long long fdeg = 0;
     for (uint32_t b = bits; b; b &= b - 1) {

@@ -37,7 +37,8 @@ struct SsspParams {
   W* dist;
   const W* w;
   unsigned long long* result;
-  uint32_t* far;  // w0 words: improved vertices at or beyond the threshold
+  uint32_t* far;     // w0 words: improved vertices at or beyond the threshold
+  uint32_t* bucket;  // w0 words: vertices expanded in the current bucket (their heavy edges wait)
   Refill* refill;
   W delta;        // 0: plain frontier Bellman-Ford (every improved vertex is near)
   PullArgs<W> pull;
@@ -53,7 +54,9 @@ struct SsspVisitor : NextFrontier {
   uint32_t* far;
   const uint32_t* ro;
   W threshold;
+  W delta;
   bool bucketed;
+  int phase;  // 0: every edge (plain) or light edges (w < delta); 1: heavy edges only
   unsigned long long deg_new = 0;
   __device__ __forceinline__ void mark(uint32_t u) {
     const uint32_t b = 1u << (u & 31);
@@ -64,7 +67,9 @@ struct SsspVisitor : NextFrontier {
   }
   __device__ __forceinline__ W src(uint32_t v) const { return ld_cg(dist + v); }
   __device__ __forceinline__ bool visit(uint32_t u, uint32_t e, W dv, uint32_t) {
-    const W nd = dv + w[e];
+    const W we = w[e];
+    if (bucketed && ((phase == 0) != (we < delta))) return false;
+    const W nd = dv + we;
     if (!(nd < ld_cg(dist + u))) return false;
     if (!(nd < sygraph::detail::atomic_min_nonneg(dist + u, nd))) return false;
     if (bucketed && !(nd < threshold)) {
@@ -97,12 +102,13 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
       S.cnt[(level + 1) % 3] = z;
     }
     const uint64_t t0 = (S.log && gtid == 0) ? sygraph::detail::global_timer_ns() : 0;
-    const bool pull = P.pull_ratio && fdeg * P.pull_ratio > P.m;
+    // pull sweeps relax every edge: not with the light / heavy split
+    const bool pull = !bucketed && P.pull_ratio && fdeg * P.pull_ratio > P.m;
     unsigned long long n_new = 0, deg_new = 0;
     uint32_t ns = 0;
     unsigned long long bp = 0;
     if (!pull) {
-      compact_frontier(fb_cur, S.w0, S.ro, C, S.q, s_scan);
+      compact_frontier(fb_cur, S.w0, S.ro, C, S.q, s_scan, bucketed ? P.bucket : nullptr);
       if (!grid_sync(S.bar)) return 0;
       ns = ld_cg(&C->small_tail);
       bp = ld_cg(&C->big_packed);
@@ -113,7 +119,9 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
       v.far = P.far;
       v.ro = S.ro;
       v.threshold = threshold;
+      v.delta = P.delta;
       v.bucketed = bucketed;
+      v.phase = 0;
       push_expand(S.ro, S.col, S.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
       n_new = v.n_new;
       deg_new = v.deg_new;
@@ -163,7 +171,10 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   }
   const bool bucketed = P.delta > W(0);
   if (bucketed) {
-    for (uint32_t i = gtid; i < w0; i += nthreads) st_cg(P.far + i, 0u);
+    for (uint32_t i = gtid; i < w0; i += nthreads) {
+      st_cg(P.far + i, 0u);
+      st_cg(P.bucket + i, 0u);
+    }
     if (gtid < 3) {
       Refill z = {};
       z.far_min = 0xffffffffu;
@@ -187,6 +198,28 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
     if (!levels) return;
     total += levels;
     if (!bucketed) break;
+    {
+      // heavy edges (w >= delta) of the bucket's vertices, relaxed once with
+      // their final distances: they land at or beyond the threshold (far)
+      Counters* Ch = P.L.cnt + (levels % 3);  // zeroed by the last level, unused since
+      compact_frontier(P.bucket, w0, P.L.ro, Ch, P.L.q, s_scan);
+      if (!grid_sync(P.L.bar)) return;
+      const uint32_t ns = ld_cg(&Ch->small_tail);
+      const unsigned long long bp = ld_cg(&Ch->big_packed);
+      SsspVisitor<W> v;
+      v.fb_next = P.L.fb + (size_t)((levels + 1) % 3) * w0;
+      v.dist = P.dist;
+      v.w = P.w;
+      v.far = P.far;
+      v.ro = P.L.ro;
+      v.threshold = threshold;
+      v.delta = P.delta;
+      v.bucketed = true;
+      v.phase = 1;
+      push_expand(P.L.ro, P.L.col, P.L.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
+      for (uint32_t i = gtid; i < w0; i += nthreads) st_cg(P.bucket + i, 0u);
+      if (!grid_sync(P.L.bar)) return;
+    }
     bool refilled = false;
     for (;;) {
       // far vertices below the new threshold become fb[0]; fb[1], fb[2] cleared
@@ -366,6 +399,7 @@ struct sg_sssp_s {
   void* dist = nullptr;
   sg_level_record* log = nullptr;
   uint32_t* far = nullptr;
+  uint32_t* bucket = nullptr;
   Refill* refill = nullptr;
   double delta = 0.0;  // near-far threshold step; 0 = the reference's frontier Bellman-Ford
   uint32_t pull_ratio = 0;  // pull iterations when frontier out-degree * ratio > m; 0 = push only
@@ -402,7 +436,7 @@ static sg_status sssp_launch(sg_sssp s) {
   L.log = s->log;
   if (g->value_type == SG_WEIGHT_F32) {
     SsspParams<float> P{L, s->source, (float*)s->dist, (const float*)g->fwd.val, s->ws.result,
-                        s->far, s->refill, (float)s->delta};
+                        s->far, s->bucket, s->refill, (float)s->delta};
     P.pull = PullArgs<float>{g->n, L.w0, g->fwd.ro, g->inv.ro, g->inv.col, (const float*)g->inv.val,
                              (float*)s->dist, s->far, s->heavy_v, s->heavy_first, s->n_heavy, s->n_chunks};
     P.pull_ratio = s->pull_ratio;
@@ -411,7 +445,7 @@ static sg_status sssp_launch(sg_sssp s) {
   }
   const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
   SsspParams<uint32_t> P{L, s->source, (uint32_t*)s->dist, (const uint32_t*)g->fwd.val, s->ws.result,
-                         s->far, s->refill, d};
+                         s->far, s->bucket, s->refill, d};
   P.pull = PullArgs<uint32_t>{g->n, L.w0, g->fwd.ro, g->inv.ro, g->inv.col, (const uint32_t*)g->inv.val,
                               (uint32_t*)s->dist, s->far, s->heavy_v, s->heavy_first, s->n_heavy, s->n_chunks};
   P.pull_ratio = s->pull_ratio;
@@ -434,6 +468,7 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out) {
   s->dist = d;
   if (st == SG_OK) st = s->ws.alloc(g->n);
   if (st == SG_OK) st = dev_alloc(&s->far, div_up(g->n, 32));
+  if (st == SG_OK) st = dev_alloc(&s->bucket, div_up(g->n, 32));
   if (st == SG_OK) st = dev_alloc(&s->refill, 3);
   if (st == SG_OK) st = dev_alloc(&s->log, SG_MAX_LOGGED_LEVELS);
   if (st == SG_OK) {
@@ -468,6 +503,7 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out) {
     s->ws.release();
     cudaFree(s->dist);
     dev_free(s->far);
+    dev_free(s->bucket);
     dev_free(s->refill);
     dev_free(s->log);
     dev_free(s->heavy_v);
@@ -485,6 +521,7 @@ sg_status sg_sssp_destroy(sg_sssp s) {
     s->ws.release();
     cudaFree(s->dist);
     dev_free(s->far);
+    dev_free(s->bucket);
     dev_free(s->refill);
     dev_free(s->log);
     dev_free(s->heavy_v);
