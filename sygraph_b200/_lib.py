@@ -162,6 +162,7 @@ SIGNATURES = {
     "sg_bfs_set_selector": (st, [vp, vp, C.c_uint32]),
     "sg_bfs_set_selector_margin": (st, [vp, C.c_float]),
     "sg_bfs_set_pull_order": (st, [vp, C.c_uint64]),
+    "sg_bfs_set_pull_words": (st, [vp, C.c_uint32]),
     "sg_bfs_log_features": (st, [vp, C.c_int]),
     "sg_bfs_level_features": (st, [vp, f32p, C.c_uint32, u32p]),
     "sg_mlp_param_count": (C.c_uint32, []),

@@ -243,6 +243,7 @@ struct sg_bfs_s {
   uint32_t allowed = 0x3f;
   float margin = 0.05f;
   unsigned long long pull_reverse = 0;  // levels whose pull probes in-neighbours from the back
+  uint32_t pull_words = 2;              // bitmap words per warp step of a short-circuit pull
   float* features = nullptr;
   uint32_t last_iterations = 0;
   bool fresh = false;  // initialised but not run: depths not written yet
@@ -293,6 +294,7 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.allowed = b->allowed;
   P.margin = b->margin;
   P.pull_reverse = b->pull_reverse;
+  P.pull_words = b->pull_words;
   P.features = b->features;
   P.depth = b->depth;
   P.visited = b->visited;
@@ -450,6 +452,14 @@ sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels) {
   clear_error();
   SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
   b->pull_reverse = reverse_levels;
+  return SG_OK;
+}
+
+sg_status sg_bfs_set_pull_words(sg_bfs b, uint32_t words) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_REQUIRE(words == 2 || words == 4, SG_ERR_INVALID, "2 or 4 words per warp step");
+  b->pull_words = words;
   return SG_OK;
 }
 
@@ -644,6 +654,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.allowed = 0x3f;
   P.margin = 0.f;
   P.pull_reverse = 0;
+  P.pull_words = 2;
   P.features = nullptr;
   P.alpha = alpha;
   P.beta = beta;

@@ -59,6 +59,7 @@ struct Params {
   uint32_t allowed;                       // strategies the MLP may pick (bit mask)
   float margin;                           // log-time gain the MLP must predict to overrule the heuristic
   unsigned long long pull_reverse;        // bit L: level L's pull probes in-neighbours from the back
+  uint32_t pull_words;                    // bitmap words per warp step of a short-circuit pull (2 or 4)
   float* features;                        // optional log: 12 floats per level decision
 };
 

@@ -189,6 +189,48 @@ __device__ __forceinline__ void pull_word_finish(Level& L, const uint32_t* fb_cu
   }
 }
 
+// Short-circuit pull, U bitmap words per warp step: the candidates and first
+// probes of all U words are issued before any word is finished, so U x 32
+// first-neighbour loads are in flight per warp.
+template <int U>
+__device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, bool reverse) {
+  const Params& P = *L.P;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t wbase = gwarp; wbase < P.w0; wbase += U * nwarps) {
+    uint32_t vw[U], cd[U], b[U], e[U];
+    bool f[U];
+    uint32_t any = 0;
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const uint32_t w = wbase + k * nwarps;
+      vw[k] = w < P.w0 ? ld_cg(P.visited + w) : 0xffffffffu;
+      cd[k] = w < P.w0 ? (~vw[k] & valid_bits(w, P.w0, P.n)) : 0u;
+      any |= cd[k];
+    }
+    if (!any) continue;
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const uint32_t v = (wbase + k * nwarps) * 32 + lane;
+      const bool m = (cd[k] >> lane) & 1u;
+      b[k] = m ? P.iro[v] : 0u;
+      e[k] = m ? P.iro[v + 1] : 0u;
+    }
+    uint32_t x[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) x[k] = e[k] > b[k] ? P.icol[probe_pos(b[k], e[k], 0, reverse)] : 0u;
+#pragma unroll
+    for (int k = 0; k < U; k++) f[k] = e[k] > b[k] && bit_test_ro(fb_cur, x[k]);
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      if (!cd[k]) continue;
+      const uint32_t w = wbase + k * nwarps;
+      pull_word_finish(L, fb_cur, w, vw[k], (cd[k] >> lane) & 1u, w * 32 + lane, b[k], e[k], f[k], reverse);
+    }
+  }
+}
+
 __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool short_circuit, bool reverse) {
   const Params& P = *L.P;
   const uint32_t lane = threadIdx.x & 31;
@@ -196,26 +238,10 @@ __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const bool same = P.iro == P.ro;
   if (short_circuit) {
-    // two words per step: both words' first probes are in flight together
-    for (uint32_t wa = gwarp; wa < P.w0; wa += 2 * nwarps) {
-      const uint32_t wb = wa + nwarps;
-      const bool has_b = wb < P.w0;
-      const uint32_t vwa = ld_cg(P.visited + wa);
-      const uint32_t vwb = has_b ? ld_cg(P.visited + wb) : 0xffffffffu;
-      const uint32_t ca = ~vwa & valid_bits(wa, P.w0, P.n);
-      const uint32_t cb = has_b ? (~vwb & valid_bits(wb, P.w0, P.n)) : 0u;
-      if (!(ca | cb)) continue;
-      const uint32_t va = wa * 32 + lane, vb = wb * 32 + lane;
-      const bool ma = (ca >> lane) & 1u, mb = (cb >> lane) & 1u;
-      const uint32_t ba = ma ? P.iro[va] : 0u, ea = ma ? P.iro[va + 1] : 0u;
-      const uint32_t bb = mb ? P.iro[vb] : 0u, eb = mb ? P.iro[vb + 1] : 0u;
-      const uint32_t xa = ea > ba ? P.icol[probe_pos(ba, ea, 0, reverse)] : 0u;
-      const uint32_t xb = eb > bb ? P.icol[probe_pos(bb, eb, 0, reverse)] : 0u;
-      const bool fa = ea > ba && bit_test_ro(fb_cur, xa);
-      const bool fbb = eb > bb && bit_test_ro(fb_cur, xb);
-      if (ca) pull_word_finish(L, fb_cur, wa, vwa, ma, va, ba, ea, fa, reverse);
-      if (cb) pull_word_finish(L, fb_cur, wb, vwb, mb, vb, bb, eb, fbb, reverse);
-    }
+    if (P.pull_words == 4)
+      pull_words<4>(L, fb_cur, reverse);
+    else
+      pull_words<2>(L, fb_cur, reverse);
     return;
   }
   // pull_all: every in-neighbour of every unvisited vertex is scanned

@@ -1,6 +1,7 @@
 // Status plumbing, device helpers and the device CSR graph
 // (graph::build::fromCSR / GraphCSR, graph/build.hpp:31-41,
 // graph/impls/graph_csr.hpp:158-439).
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -54,6 +55,56 @@ const DeviceProps& device_props() {
 __global__ void k_indegree(const uint32_t* __restrict__ col, uint64_t m, uint32_t* __restrict__ cnt) {
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x)
     atomicAdd(cnt + col[e], 1u);
+}
+
+// Each row of the forward CSR sorted by (weight, column) on the host: weights
+// are float32 or uint32, non-negative, so their bit patterns order like them.
+sg_status graph_weight_sorted(sg_graph g) {
+  std::lock_guard<std::mutex> lk(g->wsort_mu);
+  if (g->wcol) return SG_OK;
+  SG_REQUIRE(g->fwd.val && g->value_type != SG_WEIGHT_NONE, SG_ERR_INVALID, "the graph has no weights");
+  const uint32_t n = g->n;
+  const uint64_t m = g->m;
+  std::vector<uint32_t> ro((size_t)n + 1), col(m ? m : 1), val(m ? m : 1);
+  SG_CUDA(cudaStreamSynchronize(g->stream));
+  SG_CUDA(cudaMemcpy(ro.data(), g->fwd.ro, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost));
+  SG_CUDA(cudaMemcpy(col.data(), g->fwd.col, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
+  SG_CUDA(cudaMemcpy(val.data(), g->fwd.val, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
+#pragma omp parallel
+  {
+    std::vector<uint64_t> key;
+#pragma omp for schedule(dynamic, 4096)
+    for (int64_t v = 0; v < (int64_t)n; v++) {
+      const uint32_t b = ro[v], e = ro[v + 1];
+      if (e - b < 2) continue;
+      key.resize(e - b);
+      for (uint32_t i = b; i < e; i++) key[i - b] = ((uint64_t)val[i] << 32) | col[i];
+      std::sort(key.begin(), key.end());
+      for (uint32_t i = b; i < e; i++) {
+        val[i] = (uint32_t)(key[i - b] >> 32);
+        col[i] = (uint32_t)key[i - b];
+      }
+    }
+  }
+  uint32_t* wc = nullptr;
+  uint32_t* wv = nullptr;
+  SG_TRY(dev_alloc(&wc, m));
+  sg_status s = dev_alloc(&wv, m);
+  if (s != SG_OK) {
+    dev_free(wc);
+    return s;
+  }
+  if (cudaMemcpy(wc, col.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(wv, val.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    dev_free(wc);
+    dev_free(wv);
+    return fail(SG_ERR_CUDA, "uploading the weight-sorted adjacency failed");
+  }
+  g->wcol = wc;
+  g->wval = wv;
+  g->bytes += 8ull * m;
+  return SG_OK;
 }
 
 }  // namespace sgb
@@ -213,6 +264,8 @@ static sg_status build_inverse(sg_graph g, const uint32_t* h_ro, const uint32_t*
 
 static void release_graph(sg_graph g) {
   if (!g) return;
+  dev_free(g->wcol);
+  if (g->wval) cudaFree(g->wval);
   if (g->owns_inverse) {
     dev_free(g->inv.ro);
     dev_free(g->inv.col);

@@ -52,13 +52,23 @@ __device__ __forceinline__ uint32_t chunks_of(uint32_t deg) { return (deg + kChu
 using sygraph::detail::block_excl_scan;
 using sygraph::detail::block_sum;
 
+// Edge range [lo[v], hi[v + shift]) of vertex v in a push step: the whole row
+// (lo = hi = row offsets, shift 1) or a prefix / suffix of it.
+struct RowRange {
+  const uint32_t* lo;
+  const uint32_t* hi;
+  uint32_t shift;
+  __device__ __forceinline__ uint32_t beg(uint32_t v) const { return lo[v]; }
+  __device__ __forceinline__ uint32_t end(uint32_t v) const { return hi[v + shift]; }
+};
+
 // Bitmap -> queues.  Each CTA owns a contiguous range of bitmap words, counts
 // the vertices there by class, reserves its slots with one atomic per list
 // and writes them in vertex order.  When `accumulate` is given, each word is
 // also OR-ed into it (one thread per word).
-__device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb, uint32_t w0,
-                                                 const uint32_t* __restrict__ ro, Counters* C, Queues q,
-                                                 uint32_t* s_scan, uint32_t* accumulate = nullptr) {
+__device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb, uint32_t w0, RowRange R,
+                                                 Counters* C, Queues q, uint32_t* s_scan,
+                                                 uint32_t* accumulate = nullptr) {
   __shared__ uint32_t s_base_small, s_base_big, s_base_chunk;
   const uint32_t per_block = (w0 + gridDim.x - 1) / gridDim.x;
   const uint32_t wbeg = blockIdx.x * per_block;
@@ -71,7 +81,7 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
     unsigned long long fdeg = 0;
     for (uint32_t b = bits; b; b &= b - 1) {
       const uint32_t v = wi * 32 + __ffs(b) - 1;
-      const uint32_t d = ro[v + 1] - ro[v];
+      const uint32_t d = R.end(v) - R.beg(v);
       fdeg += d;
       if (d < kSmallDeg) {
         n_small++;
@@ -100,7 +110,7 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
     uint32_t pc = s_base_chunk + e_chunk;
     for (uint32_t b = bits; b; b &= b - 1) {
       const uint32_t v = wi * 32 + __ffs(b) - 1;
-      const uint32_t d = ro[v + 1] - ro[v];
+      const uint32_t d = R.end(v) - R.beg(v);
       if (d < kSmallDeg) {
         q.small[ps++] = v;
       } else {
@@ -134,9 +144,8 @@ __device__ __forceinline__ uint32_t find_chunk_owner(const uint32_t* big_start, 
 // (u, e, src_state, v) relaxes one edge and returns true when u must join the
 // next frontier; Visitor::mark(u) is then called by that lane.
 template <class Visitor>
-__device__ __forceinline__ void push_expand(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
-                                            Queues q, uint32_t n_small, uint32_t n_big, uint32_t n_chunks,
-                                            Visitor& vis) {
+__device__ __forceinline__ void push_expand(RowRange R, const uint32_t* __restrict__ col, Queues q, uint32_t n_small,
+                                            uint32_t n_big, uint32_t n_chunks, Visitor& vis) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -148,8 +157,8 @@ __device__ __forceinline__ void push_expand(const uint32_t* __restrict__ ro, con
       const uint32_t idx = unit * 32 + lane;
       const bool valid = idx < n_small;
       const uint32_t v = valid ? ld_cg(q.small + idx) : 0u;
-      const uint32_t beg = valid ? ro[v] : 0u;
-      const uint32_t deg = valid ? ro[v + 1] - beg : 0u;
+      const uint32_t beg = valid ? R.beg(v) : 0u;
+      const uint32_t deg = valid ? R.end(v) - beg : 0u;
       const S sv = valid ? vis.src(v) : S();
       const uint32_t incl = warp_inclusive_scan(deg);
       const uint32_t total = __shfl_sync(kFullMask, incl, 31);
@@ -173,7 +182,7 @@ __device__ __forceinline__ void push_expand(const uint32_t* __restrict__ ro, con
       const uint32_t ent = find_chunk_owner(q.big_start, n_big, c);
       const uint32_t v = ld_cg(q.big + ent);
       const uint32_t first = ld_cg(q.big_start + ent);
-      const uint32_t vb = ro[v], ve = ro[v + 1];
+      const uint32_t vb = R.beg(v), ve = R.end(v);
       const uint32_t cb = vb + (c - first) * kChunk;
       const uint32_t ce = min(ve, cb + kChunk);
       const S sv = vis.src(v);
@@ -186,6 +195,19 @@ __device__ __forceinline__ void push_expand(const uint32_t* __restrict__ ro, con
       }
     }
   }
+}
+
+__device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb, uint32_t w0,
+                                                 const uint32_t* __restrict__ ro, Counters* C, Queues q,
+                                                 uint32_t* s_scan) {
+  compact_frontier(fb, w0, RowRange{ro, ro, 1}, C, q, s_scan);
+}
+
+template <class Visitor>
+__device__ __forceinline__ void push_expand(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
+                                            Queues q, uint32_t n_small, uint32_t n_big, uint32_t n_chunks,
+                                            Visitor& vis) {
+  push_expand(RowRange{ro, ro, 1}, col, q, n_small, n_big, n_chunks, vis);
 }
 
 // Position of the k-th (0-based) set bit of x.

@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <mutex>
 #include <cstdio>
 #include <string>
 
@@ -91,6 +92,8 @@ inline unsigned grid_for(uint64_t work_items, unsigned block, unsigned per_sm = 
 
 // Device address of an sg_mlp's parameter block (selector.cu).
 const void* mlp_device_params(sg_mlp h);
+// Builds g->wcol / g->wval once (weighted graphs only).
+sg_status graph_weight_sorted(sg_graph g);
 // SG_ERR_TIMEOUT when the last launch of the instance left its grid barrier's
 // error flag set (read after its stream completed; used by the server).
 sg_status bfs_launch_status(sg_bfs b);
@@ -107,6 +110,12 @@ struct GraphDir {
 }  // namespace sgb
 
 struct sg_graph_s {
+  // forward adjacency with each row sorted by (weight, column): the light /
+  // heavy edge split of delta-stepping reads a prefix / suffix of a row;
+  // built on first use (graph_weight_sorted), row offsets are fwd.ro
+  uint32_t* wcol = nullptr;
+  void* wval = nullptr;
+  std::mutex wsort_mu;
   uint32_t n = 0;
   uint64_t m = 0;
   uint32_t flags = 0;

@@ -44,6 +44,9 @@ struct SsspParams {
   PullArgs<W> pull;
   uint32_t pull_ratio;  // pull when the frontier's out-degree * pull_ratio > m (0: push only)
   unsigned long long m;
+  const uint32_t* split;  // delta-stepping: first edge of weight >= delta in each weight-sorted row
+  const uint32_t* wcol;   // weight-sorted rows (same row offsets)
+  const W* wval;
 };
 
 template <typename W>
@@ -54,9 +57,7 @@ struct SsspVisitor : NextFrontier {
   uint32_t* far;
   const uint32_t* ro;
   W threshold;
-  W delta;
   bool bucketed;
-  int phase;  // 0: every edge (plain) or light edges (w < delta); 1: heavy edges only
   unsigned long long deg_new = 0;
   __device__ __forceinline__ void mark(uint32_t u) {
     const uint32_t b = 1u << (u & 31);
@@ -67,9 +68,7 @@ struct SsspVisitor : NextFrontier {
   }
   __device__ __forceinline__ W src(uint32_t v) const { return ld_cg(dist + v); }
   __device__ __forceinline__ bool visit(uint32_t u, uint32_t e, W dv, uint32_t) {
-    const W we = w[e];
-    if (bucketed && ((phase == 0) != (we < delta))) return false;
-    const W nd = dv + we;
+    const W nd = dv + w[e];
     if (!(nd < ld_cg(dist + u))) return false;
     if (!(nd < sygraph::detail::atomic_min_nonneg(dist + u, nd))) return false;
     if (bucketed && !(nd < threshold)) {
@@ -108,21 +107,21 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
     uint32_t ns = 0;
     unsigned long long bp = 0;
     if (!pull) {
-      compact_frontier(fb_cur, S.w0, S.ro, C, S.q, s_scan, bucketed ? P.bucket : nullptr);
+      // bucketed: light edges only, the prefix of each weight-sorted row
+      const RowRange R = bucketed ? RowRange{S.ro, P.split, 0} : RowRange{S.ro, S.ro, 1};
+      compact_frontier(fb_cur, S.w0, R, C, S.q, s_scan, bucketed ? P.bucket : nullptr);
       if (!grid_sync(S.bar)) return 0;
       ns = ld_cg(&C->small_tail);
       bp = ld_cg(&C->big_packed);
       SsspVisitor<W> v;
       v.fb_next = fb_next;
       v.dist = P.dist;
-      v.w = P.w;
+      v.w = bucketed ? P.wval : P.w;
       v.far = P.far;
       v.ro = S.ro;
       v.threshold = threshold;
-      v.delta = P.delta;
       v.bucketed = bucketed;
-      v.phase = 0;
-      push_expand(S.ro, S.col, S.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
+      push_expand(R, bucketed ? P.wcol : S.col, S.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
       n_new = v.n_new;
       deg_new = v.deg_new;
     } else {
@@ -202,21 +201,20 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       // heavy edges (w >= delta) of the bucket's vertices, relaxed once with
       // their final distances: they land at or beyond the threshold (far)
       Counters* Ch = P.L.cnt + (levels % 3);  // zeroed by the last level, unused since
-      compact_frontier(P.bucket, w0, P.L.ro, Ch, P.L.q, s_scan);
+      const RowRange Rh{P.split, P.L.ro, 1};   // the suffix of each weight-sorted row
+      compact_frontier(P.bucket, w0, Rh, Ch, P.L.q, s_scan);
       if (!grid_sync(P.L.bar)) return;
       const uint32_t ns = ld_cg(&Ch->small_tail);
       const unsigned long long bp = ld_cg(&Ch->big_packed);
       SsspVisitor<W> v;
       v.fb_next = P.L.fb + (size_t)((levels + 1) % 3) * w0;
       v.dist = P.dist;
-      v.w = P.w;
+      v.w = P.wval;
       v.far = P.far;
       v.ro = P.L.ro;
       v.threshold = threshold;
-      v.delta = P.delta;
       v.bucketed = true;
-      v.phase = 1;
-      push_expand(P.L.ro, P.L.col, P.L.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
+      push_expand(Rh, P.wcol, P.L.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
       for (uint32_t i = gtid; i < w0; i += nthreads) st_cg(P.bucket + i, 0u);
       if (!grid_sync(P.L.bar)) return;
     }
@@ -400,6 +398,8 @@ struct sg_sssp_s {
   sg_level_record* log = nullptr;
   uint32_t* far = nullptr;
   uint32_t* bucket = nullptr;
+  uint32_t* split = nullptr;  // for split_delta
+  double split_delta = -1.0;
   Refill* refill = nullptr;
   double delta = 0.0;  // near-far threshold step; 0 = the reference's frontier Bellman-Ford
   uint32_t pull_ratio = 0;  // pull iterations when frontier out-degree * ratio > m; 0 = push only
@@ -408,6 +408,23 @@ struct sg_sssp_s {
   uint32_t n_heavy = 0, n_chunks = 0;
   PushWorkspace ws;
 };
+
+// First edge of weight >= delta in each weight-sorted row (binary search).
+template <typename W>
+__global__ void split_kernel(const uint32_t* __restrict__ ro, const W* __restrict__ wval, uint32_t n, W delta,
+                             uint32_t* __restrict__ split) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    uint32_t lo = ro[v], hi = ro[v + 1];
+    while (lo < hi) {
+      const uint32_t mid = lo + ((hi - lo) >> 1);
+      if (wval[mid] < delta)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    split[v] = lo;
+  }
+}
 
 template <typename W>
 __global__ void fill_dist_kernel(W* dist, uint32_t n, uint32_t src) {
@@ -431,6 +448,20 @@ static sg_status sssp_materialise(sg_sssp s) {
 
 static sg_status sssp_launch(sg_sssp s) {
   sg_graph g = s->g;
+  if (s->delta > 0.0 && s->split_delta != s->delta) {
+    // delta-stepping reads the weight-sorted rows: their light prefix / heavy suffix
+    SG_TRY(graph_weight_sorted(g));
+    if (!s->split) SG_TRY(dev_alloc(&s->split, g->n));
+    if (g->value_type == SG_WEIGHT_F32)
+      split_kernel<float><<<grid_for(g->n, 256), 256, 0, s->stream>>>(g->fwd.ro, (const float*)g->wval, g->n,
+                                                                       (float)s->delta, s->split);
+    else
+      split_kernel<uint32_t><<<grid_for(g->n, 256), 256, 0, s->stream>>>(
+          g->fwd.ro, (const uint32_t*)g->wval, g->n,
+          (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)), s->split);
+    SG_CHECK_LAUNCH();
+    s->split_delta = s->delta;
+  }
   SG_CUDA(cudaMemsetAsync(s->ws.bar, 0, sizeof(GridBarrier), s->stream));
   PushLoop L = s->ws.loop(g);
   L.log = s->log;
@@ -441,6 +472,9 @@ static sg_status sssp_launch(sg_sssp s) {
                              (float*)s->dist, s->far, s->heavy_v, s->heavy_first, s->n_heavy, s->n_chunks};
     P.pull_ratio = s->pull_ratio;
     P.m = g->m;
+    P.split = s->split;
+    P.wcol = g->wcol;
+    P.wval = (const float*)g->wval;
     return launch_persistent(sssp_kernel<float>, P, 2, s->stream, s->max_ctas);
   }
   const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
@@ -450,6 +484,9 @@ static sg_status sssp_launch(sg_sssp s) {
                               (uint32_t*)s->dist, s->far, s->heavy_v, s->heavy_first, s->n_heavy, s->n_chunks};
   P.pull_ratio = s->pull_ratio;
   P.m = g->m;
+  P.split = s->split;
+  P.wcol = g->wcol;
+  P.wval = (const uint32_t*)g->wval;
   return launch_persistent(sssp_kernel<uint32_t>, P, 2, s->stream, s->max_ctas);
 }
 
@@ -504,6 +541,7 @@ sg_status sg_sssp_create(sg_graph g, sg_sssp* out) {
     cudaFree(s->dist);
     dev_free(s->far);
     dev_free(s->bucket);
+    dev_free(s->split);
     dev_free(s->refill);
     dev_free(s->log);
     dev_free(s->heavy_v);
@@ -522,6 +560,7 @@ sg_status sg_sssp_destroy(sg_sssp s) {
     cudaFree(s->dist);
     dev_free(s->far);
     dev_free(s->bucket);
+    dev_free(s->split);
     dev_free(s->refill);
     dev_free(s->log);
     dev_free(s->heavy_v);
