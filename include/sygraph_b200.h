@@ -406,8 +406,8 @@ sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed);
  * list (the parents of late-level vertices tend to have high ids).  Any
  * parent gives the same depth; only the work changes. */
 sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels);
-/* Bitmap words a warp takes per step of a short-circuit pull (2, the default,
- * or 4): more first-neighbour probes in flight, more registers. */
+/* Bitmap words a warp takes per step of a short-circuit pull (2 or 4, the
+ * default): more words put more first-neighbour probes in flight. */
 sg_status sg_bfs_set_pull_words(sg_bfs b, uint32_t words);
 sg_status sg_bfs_set_selector_margin(sg_bfs b, float margin);
 sg_status sg_bfs_log_features(sg_bfs b, int enable);

@@ -243,7 +243,7 @@ struct sg_bfs_s {
   uint32_t allowed = 0x3f;
   float margin = 0.05f;
   unsigned long long pull_reverse = 0;  // levels whose pull probes in-neighbours from the back
-  uint32_t pull_words = 2;              // bitmap words per warp step of a short-circuit pull
+  uint32_t pull_words = 4;              // bitmap words per warp step of a short-circuit pull
   float* features = nullptr;
   uint32_t last_iterations = 0;
   bool fresh = false;  // initialised but not run: depths not written yet
