@@ -475,6 +475,8 @@ sg_status sg_bc_batch_destroy(sg_bc_batch h);
 sg_status sg_bc_batch_run_async(sg_bc_batch h, const uint32_t* host_sources, uint32_t k, int accumulate);
 sg_status sg_bc_batch_run(sg_bc_batch h, const uint32_t* host_sources, uint32_t k, int accumulate,
                           sg_bc_batch_details* details);
+/* As sg_sssp_set_launch. */
+sg_status sg_bc_batch_set_launch(sg_bc_batch h, void* stream, uint32_t max_ctas);
 sg_status sg_bc_batch_get(sg_bc_batch h, float* host_bc);
 sg_status sg_bc_batch_bc_device(sg_bc_batch h, const float** dev_bc);
 /* Log of the last batch: forward levels first (strategy 0: marked sparse

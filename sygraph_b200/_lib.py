@@ -192,6 +192,7 @@ SIGNATURES = {
     "sg_bc_batch_run_async": (st, [vp, u32p, C.c_uint32, C.c_int]),
     "sg_bc_batch_run": (st, [vp, u32p, C.c_uint32, C.c_int, C.POINTER(BcBatchDetails)]),
     "sg_bc_batch_get": (st, [vp, f32p]),
+    "sg_bc_batch_set_launch": (st, [vp, vp, C.c_uint32]),
     "sg_bc_batch_bc_device": (st, [vp, C.POINTER(vp)]),
     "sg_bc_batch_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
     "sg_bc_batched": (st, [vp, u32p, C.c_uint32, f32p]),

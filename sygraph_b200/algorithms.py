@@ -90,6 +90,10 @@ class BFS:
         """Bit L: level L's pull probes in-neighbours from the back."""
         call("sg_bfs_set_pull_order", self.handle, int(reverse_levels))
 
+    def set_launch(self, max_ctas: int = 0, stream=None) -> None:
+        """Persistent grid cap (0: every SM) and stream of this instance."""
+        call("sg_bfs_set_launch", self.handle, stream, int(max_ctas))
+
     def log_features(self, enable: bool = True) -> None:
         call("sg_bfs_log_features", self.handle, int(enable))
 
@@ -148,6 +152,9 @@ class MultiBFS:
         call("sg_msbfs_level_records", self.handle, recs, _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
         return [{k: getattr(recs[i], k) for k, _ in _lib.LevelRecord._fields_} for i in range(cnt.value)]
 
+    def set_launch(self, max_ctas: int = 0, stream=None) -> None:
+        call("sg_msbfs_set_launch", self.handle, stream, int(max_ctas))
+
     def getDistances(self) -> np.ndarray:
         """k x n depths (row s: depths from sources[s])."""
         out = np.empty((self.k, self.G.getVertexCount()), np.uint32)
@@ -192,6 +199,9 @@ class SSSP:
     def set_pull(self, ratio: int) -> None:
         """Pull iterations when frontier out-degree * ratio > m (0: push only)."""
         call("sg_sssp_set_pull", self.handle, int(ratio))
+
+    def set_launch(self, max_ctas: int = 0, stream=None) -> None:
+        call("sg_sssp_set_launch", self.handle, stream, int(max_ctas))
 
     def set_delta(self, delta: float) -> None:
         """Near-far threshold step (0: the reference's frontier Bellman-Ford)."""
@@ -290,6 +300,9 @@ class BatchedBC:
         out = np.empty(self.G.getVertexCount(), np.float32)
         call("sg_bc_batch_get", self.handle, out.ctypes.data_as(C.POINTER(C.c_float)))
         return out
+
+    def set_launch(self, max_ctas: int = 0, stream=None) -> None:
+        call("sg_bc_batch_set_launch", self.handle, stream, int(max_ctas))
 
     def level_records(self) -> list[dict]:
         recs = (_lib.LevelRecord * _lib.SG_MAX_LOGGED_LEVELS)()

@@ -537,6 +537,8 @@ using namespace sgb;
 
 struct sg_bc_batch_s {
   sg_graph g = nullptr;
+  cudaStream_t stream = nullptr;  // launches and copies (the graph's stream unless set)
+  uint32_t max_ctas = 0;
   uint32_t w0 = 0, cap_levels = 0, last_k = 0;
   unsigned long long* seen = nullptr;
   unsigned long long* hist = nullptr;
@@ -597,8 +599,8 @@ uint32_t bcb_max_levels(sg_bc_batch h) {
 
 sg_status bcb_launch(sg_bc_batch h, uint32_t k, int accumulate) {
   sg_graph g = h->g;
-  SG_CUDA(cudaMemsetAsync(h->bar, 0, sizeof(*h->bar), g->stream));
-  SG_CUDA(cudaMemsetAsync(h->result, 0, 4 * sizeof(unsigned long long), g->stream));
+  SG_CUDA(cudaMemsetAsync(h->bar, 0, sizeof(*h->bar), h->stream));
+  SG_CUDA(cudaMemsetAsync(h->result, 0, 4 * sizeof(unsigned long long), h->stream));
   bcb::Params P;
   P.n = g->n;
   P.w0 = h->w0;
@@ -628,7 +630,7 @@ sg_status bcb_launch(sg_bc_batch h, uint32_t k, int accumulate) {
   P.bar = h->bar;
   P.log = h->log;
   P.result = h->result;
-  return eng::launch_persistent(bcb::bc_batch_kernel, P, 2, g->stream);
+  return eng::launch_persistent(bcb::bc_batch_kernel, P, 2, h->stream, h->max_ctas);
 }
 
 }  // namespace
@@ -642,6 +644,7 @@ sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* o
   *out = nullptr;
   sg_bc_batch h = new sg_bc_batch_s();
   h->g = g;
+  h->stream = g->stream;
   h->w0 = div_up(g->n, 32);
   // at most m / kMarkDeg vertices have a degree >= kMarkDeg (>= kCtaDeg too)
   h->big_cap = (uint32_t)std::min<uint64_t>(g->n, g->m / bcb::kMarkDeg + 2);
@@ -675,7 +678,7 @@ sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* o
 
 sg_status sg_bc_batch_destroy(sg_bc_batch h) {
   if (h) {
-    cudaStreamSynchronize(h->g->stream);
+    cudaStreamSynchronize(h->stream);
     bcb_release(h);
   }
   return SG_OK;
@@ -686,7 +689,7 @@ sg_status sg_bc_batch_run_async(sg_bc_batch h, const uint32_t* host_sources, uin
   SG_REQUIRE(h && host_sources, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(k >= 1 && k <= 64, SG_ERR_INVALID, "a batch holds 1 to 64 sources");
   for (uint32_t i = 0; i < k; i++) SG_REQUIRE(host_sources[i] < h->g->n, SG_ERR_INVALID, "source out of range");
-  SG_CUDA(cudaMemcpyAsync(h->sources, host_sources, sizeof(uint32_t) * k, cudaMemcpyHostToDevice, h->g->stream));
+  SG_CUDA(cudaMemcpyAsync(h->sources, host_sources, sizeof(uint32_t) * k, cudaMemcpyHostToDevice, h->stream));
   h->last_k = k;
   return bcb_launch(h, k, accumulate);
 }
@@ -698,9 +701,9 @@ sg_status sg_bc_batch_run(sg_bc_batch h, const uint32_t* host_sources, uint32_t 
   for (;;) {
     unsigned long long r[4];
     sygraph::detail::GridBarrier b;
-    SG_CUDA(cudaMemcpyAsync(r, h->result, sizeof(r), cudaMemcpyDeviceToHost, h->g->stream));
-    SG_CUDA(cudaMemcpyAsync(&b, h->bar, sizeof(b), cudaMemcpyDeviceToHost, h->g->stream));
-    SG_CUDA(cudaStreamSynchronize(h->g->stream));
+    SG_CUDA(cudaMemcpyAsync(r, h->result, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    SG_CUDA(cudaMemcpyAsync(&b, h->bar, sizeof(b), cudaMemcpyDeviceToHost, h->stream));
+    SG_CUDA(cudaStreamSynchronize(h->stream));
     if (b.error) return fail(SG_ERR_TIMEOUT, "batched BC: a grid barrier wait ran out");
     if (r[1]) {
       // deeper than the history: enlarge it (bc is untouched before the backward sweep) and run again
@@ -721,10 +724,19 @@ sg_status sg_bc_batch_run(sg_bc_batch h, const uint32_t* host_sources, uint32_t 
   }
 }
 
+sg_status sg_bc_batch_set_launch(sg_bc_batch h, void* stream, uint32_t max_ctas) {
+  clear_error();
+  SG_REQUIRE(h, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t)stream : h->g->stream;
+  h->max_ctas = max_ctas;
+  return SG_OK;
+}
+
 sg_status sg_bc_batch_get(sg_bc_batch h, float* host_bc) {
   SG_REQUIRE(h && host_bc, SG_ERR_INVALID, "NULL argument");
-  SG_CUDA(cudaMemcpyAsync(host_bc, h->bc, sizeof(float) * h->g->n, cudaMemcpyDeviceToHost, h->g->stream));
-  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  SG_CUDA(cudaMemcpyAsync(host_bc, h->bc, sizeof(float) * h->g->n, cudaMemcpyDeviceToHost, h->stream));
+  SG_CUDA(cudaStreamSynchronize(h->stream));
   return SG_OK;
 }
 
@@ -736,7 +748,7 @@ sg_status sg_bc_batch_bc_device(sg_bc_batch h, const float** dev_bc) {
 
 sg_status sg_bc_batch_level_records(sg_bc_batch h, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
   SG_REQUIRE(h && count, SG_ERR_INVALID, "NULL argument");
-  SG_CUDA(cudaStreamSynchronize(h->g->stream));
+  SG_CUDA(cudaStreamSynchronize(h->stream));
   unsigned long long it = 0;
   if (h->last_k) SG_CUDA(cudaMemcpy(&it, h->result + 3, sizeof(it), cudaMemcpyDeviceToHost));
   uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
