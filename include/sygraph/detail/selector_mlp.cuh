@@ -75,14 +75,16 @@ __device__ __forceinline__ void mlp_stage(const MlpParams* __restrict__ g, MlpSt
   for (int t = threadIdx.x; t < kMlpOut; t += blockDim.x) s->b3[t] = g->b3[t];
 }
 
-// Forward pass by one full warp: lane j computes hidden unit j, summing in
-// the same order as the training kernels.  Returns, in every lane, the
-// strategy with the smallest predicted time among the set bits of `allowed`
-// -- unless `fallback` (the heuristic's choice, when allowed) is predicted
-// within `margin` of it in log-time, which keeps the fallback -- or -1 when a
+// Forward pass by one full warp: lane j computes hidden unit j; the hidden
+// activations go through `scratch` (64 floats of shared memory) so that every
+// lane reads them with independent broadcast loads, and lanes 0-5 compute the
+// six outputs.  Returns, in every lane, the strategy with the smallest
+// predicted time among the set bits of `allowed` (lowest index on ties) --
+// unless `fallback` (the heuristic's choice, when allowed) is predicted within
+// `margin` of it in log-time, which keeps the fallback -- or -1 when a
 // feature lies outside the trusted range.
 __device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const float* f, uint32_t allowed,
-                                          int fallback = -1, float margin = 0.f) {
+                                          float* scratch, int fallback = -1, float margin = 0.f) {
   const uint32_t lane = threadIdx.x & 31;
   bool out_of_range = false;
   float x[kMlpIn];
@@ -95,28 +97,36 @@ __device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const
   float h1 = P->b1[lane];
 #pragma unroll
   for (int i = 0; i < kMlpIn; i++) h1 += P->w1t[i][lane] * x[i];
-  h1 = h1 > 0.f ? h1 : 0.f;
+  scratch[lane] = h1 > 0.f ? h1 : 0.f;
+  __syncwarp();
   float h2 = P->b2[lane];
-#pragma unroll 8
-  for (int i = 0; i < kMlpHidden; i++) h2 += P->w2t[i][lane] * __shfl_sync(0xffffffffu, h1, i);
-  h2 = h2 > 0.f ? h2 : 0.f;
-  float best = 3.4e38f, y_fallback = 3.4e38f;
-  int arg = -1;
 #pragma unroll
-  for (int j = 0; j < kMlpOut; j++) {
-    float y = P->w3[j][lane] * h2;
+  for (int i = 0; i < kMlpHidden; i++) h2 += P->w2t[i][lane] * scratch[i];
+  scratch[kMlpHidden + lane] = h2 > 0.f ? h2 : 0.f;
+  __syncwarp();
+  float y = 3.4e38f;
+  if (lane < (uint32_t)kMlpOut) {
+    float a = P->b3[lane];
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) y += __shfl_xor_sync(0xffffffffu, y, d);
-    y += P->b3[j];
-    if (j == fallback) y_fallback = y;
-    if (((allowed >> j) & 1u) && y < best) {
-      best = y;
-      arg = j;
+    for (int i = 0; i < kMlpHidden; i++) a += P->w3[lane][i] * scratch[kMlpHidden + i];
+    y = a;
+  }
+  __syncwarp();
+  const float y_fallback = __shfl_sync(0xffffffffu, y, fallback >= 0 ? fallback : 0);
+  float best = (lane < (uint32_t)kMlpOut && ((allowed >> lane) & 1u)) ? y : 3.4e38f;
+  int arg = best < 3.4e38f ? (int)lane : 32;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    const float ob = __shfl_xor_sync(0xffffffffu, best, d);
+    const int oa = __shfl_xor_sync(0xffffffffu, arg, d);
+    if (ob < best || (ob == best && oa < arg)) {
+      best = ob;
+      arg = oa;
     }
   }
+  if (arg >= kMlpOut) return -1;
   if (fallback >= 0 && ((allowed >> fallback) & 1u) && y_fallback - best <= margin) arg = fallback;
-  // butterfly sums may round differently per lane: lane 0 decides for all
-  return __shfl_sync(0xffffffffu, arg, 0);
+  return arg;
 }
 #endif
 

@@ -75,6 +75,7 @@ struct Shared {
   uint32_t flag[kThreads];
   int choice;
   sygraph::detail::MlpStaged mlp;  // learned mode: parameters staged once per launch
+  float mlp_scratch[2 * sygraph::detail::kMlpHidden];
 };
 
 // Per-thread context of one level's expansion.
@@ -198,7 +199,7 @@ __device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const
       if (log && threadIdx.x == 0)
         for (int i = 0; i < 12; i++) P.features[(size_t)level * 12 + i] = f[i];
       if (P.mode == kLearned && P.mlp) {
-        const int c = sygraph::detail::mlp_choose(&S.mlp, f, P.allowed, h, P.margin);
+        const int c = sygraph::detail::mlp_choose(&S.mlp, f, P.allowed, S.mlp_scratch, h, P.margin);
         if (threadIdx.x == 0) S.choice = c;
       }
     }

@@ -51,14 +51,14 @@ def test_learned_schedule_beats_heuristic_on_held_out_graphs(tables):
     heur = sum(r[1] for r in rows)
     learned = sum(r[2] for r in rows)
     best = sum(r[3] for r in rows)
-    # the whole held-out set: at least 20% less time than the heuristic
-    # (speed-up >= 1.25), within 5% of the per-level best
-    assert learned <= 0.8 * heur, (learned, heur)
-    assert learned <= 1.05 * best, (learned, best)
-    # no traversal more than 15% slower than under the heuristic (the worst,
-    # an RMAT-22 source whose third level the MLP sends to push, is ~13%)
+    # the whole held-out set: at least 8% less time than the heuristic
+    # (the gain is on the grid and the uniform graph), within 2% of the
+    # per-level best
+    assert learned <= 0.92 * heur, (learned, heur)
+    assert learned <= 1.02 * best, (learned, best)
+    # no traversal more than 6% slower than under the heuristic
     for name, h, l, _, _, _ in rows:
-        assert l <= 1.15 * h, (name, l, h)
+        assert l <= 1.06 * h, (name, l, h)
 
 
 def test_learned_schedule_on_rmat_is_no_worse_than_heuristic(tables):
