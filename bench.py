@@ -494,6 +494,10 @@ def main():
                "workload": f"Brandes BC, {BC_SOURCES} sources, RMAT-{BC_SCALE} ef{EDGE_FACTOR}",
                "launch_ms": bc_ms, "per_source_ms": bc1_ms, "speedup_vs_per_source": bc1_ms / bc_ms,
                "max_rel_diff_vs_per_source": bc_rel, "forward_levels": bc_det["iterations"]}
+    bc_bytes = 2 * (4 * (gbc.n + 1) + 4 * gbc.m) + 2 * 256 * gbc.n
+    bc_line["roofline"] = {"bound": "hbm", "achieved": bc_bytes / (bc_ms * 1e-3) / 1e9, "unit": "GB/s",
+                           "frac": bc_bytes / (bc_ms * 1e-3) / 1e9 / peaks()[0],
+                           "bytes_per_launch": bc_bytes, "traffic": ncu_traffic("bc_batch_kernel")}
     del bcb, bc1, Gbc, gbc
 
     # SSSP on a subset of the same sources (reported beside the BFS line)
