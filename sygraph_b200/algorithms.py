@@ -115,7 +115,7 @@ class BFS:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.sg_bfs_destroy(h)
             self.handle = None
 
@@ -163,7 +163,7 @@ class MultiBFS:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.sg_msbfs_destroy(h)
             self.handle = None
 
@@ -218,7 +218,7 @@ class SSSP:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.sg_sssp_destroy(h)
             self.handle = None
 
@@ -312,7 +312,7 @@ class BatchedBC:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.sg_bc_batch_destroy(h)
             self.handle = None
 

@@ -144,7 +144,7 @@ class DeviceArray:
 
     def __del__(self):
         p = getattr(self, "ptr", None)
-        if p:
+        if p and lib is not None:
             lib.sg_free_device(C.c_void_p(p))
             self.ptr = None
 
@@ -196,7 +196,7 @@ class Graph:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.sg_graph_destroy(h)
             self.handle = None
 
@@ -287,7 +287,7 @@ class Frontier:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.sg_frontier_destroy(h)
             self.handle = None
 

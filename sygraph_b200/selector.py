@@ -106,6 +106,6 @@ class Mlp:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.sg_mlp_destroy(h)
             self.handle = None

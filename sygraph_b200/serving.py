@@ -38,7 +38,7 @@ class PinnedBuffer:
         self.array = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(self.nbytes,)).view(self.dtype)[:n]
 
     def __del__(self):
-        if getattr(self, "ptr", None):
+        if getattr(self, "ptr", None) and lib is not None:
             lib.sg_free_host_pinned(self.ptr)
             self.ptr = None
 
@@ -82,7 +82,7 @@ class Server:
 
     def close(self) -> None:
         h = getattr(self, "handle", None)
-        if h:
+        if h and lib is not None:
             lib.sg_server_destroy(h)
             self.handle = None
 
