@@ -29,7 +29,7 @@ namespace bfs {
 
 using namespace eng;
 
-__global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
+__global__ void __launch_bounds__(kBfsThreads, 1) bfs_kernel(Params P) {
   __shared__ Shared S;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
@@ -62,7 +62,10 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
     }
     P.cnt[gtid] = z;
   }
-  if (threadIdx.x == 0) S.hn = 0;
+  if (threadIdx.x == 0) {
+    S.hn = 0;
+    S.acc[0] = S.acc[1] = S.acc[2] = S.acc[3] = 0ull;
+  }
   if (P.mode == kLearned && P.mlp) sygraph::detail::mlp_stage(P.mlp, &S.mlp);
   if (!grid_sync(P.bar)) return;
 
@@ -121,10 +124,26 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
       if ((s >> lane) & 1u) st_cg(fb_zero + j * 32 + lane, 0u);
       if (lane == 0) st_cg(sm_zero + j, 0u);
     }
+    // level totals: warp sums into shared accumulators, one global atomic per
+    // counter and CTA after the barrier below
+    {
+      unsigned long long v4[4] = {L.n_new, L.deg_new, L.wnz, L.snz};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        v4[k] = sygraph::detail::warp_sum(v4[k]);
+        if (lane == 0 && v4[k]) atomicAdd(&S.acc[k], v4[k]);
+      }
+    }
     // staged heavy vertices: one atomic per CTA reserves entries and chunks
     __syncthreads();
-    {
-      const uint32_t nb = min(S.hn, kHeavyBuf);
+    if (threadIdx.x == 0) {
+      if (S.acc[0]) atomicAdd(&C->new_count, S.acc[0]);
+      if (S.acc[1]) atomicAdd(&C->new_deg, S.acc[1]);
+      if (S.acc[2]) atomicAdd(&C->words_nz, S.acc[2]);
+      if (S.acc[3]) atomicAdd(&C->sum_nz, S.acc[3]);
+      S.acc[0] = S.acc[1] = S.acc[2] = S.acc[3] = 0ull;  // next added to after the grid barrier
+    }
+    if (const uint32_t nb = min(S.hn, kHeavyBuf)) {  // block-uniform; most levels stage none
       const uint32_t k0 = 2 * threadIdx.x;
       uint32_t my = 0;
       if (k0 < nb) my += bfs_chunks(S.hd[k0]);
@@ -146,16 +165,6 @@ __global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params P) {
         }
       }
       if (threadIdx.x == 0) S.hn = 0;
-    }
-    {
-      unsigned long long v4[4] = {L.n_new, L.deg_new, L.wnz, L.snz};
-      block_sum4(v4, S);
-      if (threadIdx.x == 0) {
-        if (v4[0]) atomicAdd(&C->new_count, v4[0]);
-        if (v4[1]) atomicAdd(&C->new_deg, v4[1]);
-        if (v4[2]) atomicAdd(&C->words_nz, v4[2]);
-        if (v4[3]) atomicAdd(&C->sum_nz, v4[3]);
-      }
     }
     if (!grid_sync(P.bar)) return;
 
@@ -311,7 +320,7 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.schedule = b->schedule_len ? b->schedule : nullptr;
   P.schedule_len = b->schedule_len;
   SG_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(*b->bar), b->stream));
-  return eng::launch_persistent(bfs::bfs_kernel, P, 2, b->stream, b->max_ctas);
+  return eng::launch_persistent(bfs::bfs_kernel, P, 1, b->stream, b->max_ctas, nullptr, bfs::kBfsThreads);
 }
 
 static sg_status bfs_collect(sg_bfs b, sg_bfs_details* details) {
@@ -678,7 +687,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   SG_CUDA(cudaMemsetAsync(P.bar, 0, sizeof(sygraph::detail::GridBarrier), s));
   bfs::no_in_edges_kernel<<<grid_for((uint64_t)w0 * 32, 256), 256, 0, s>>>(dev_inv_row_offsets, n, w0, no_in);
   SG_CHECK_LAUNCH();
-  SG_TRY(eng::launch_persistent(bfs::bfs_kernel, P, 2, s));
+  SG_TRY(eng::launch_persistent(bfs::bfs_kernel, P, 1, s, 0, nullptr, bfs::kBfsThreads));
   unsigned long long it = 0;
   uint32_t err = 0;
   SG_CUDA(cudaMemcpyAsync(&it, P.result, sizeof(it), cudaMemcpyDeviceToHost, s));

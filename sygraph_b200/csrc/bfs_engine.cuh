@@ -19,6 +19,9 @@ constexpr uint32_t kHeavy = 256;      // degree from which a vertex is expanded 
 constexpr uint32_t kHeavyBuf = 1024;  // per-CTA staging of newly discovered heavy vertices
 constexpr uint32_t kBfsChunk = 64;    // edges per heavy-vertex chunk (one warp, two steps)
 constexpr int kLearned = 3;           // mode: the MLP picks each level's strategy
+// One 1024-thread CTA per SM: half the CTAs of the other engines for the same
+// threads, so a level's grid barrier and per-CTA counter atomics cost less.
+constexpr uint32_t kBfsThreads = 1024;
 
 __device__ __forceinline__ uint32_t bfs_chunks(uint32_t deg) { return (deg + kBfsChunk - 1) / kBfsChunk; }
 
@@ -66,13 +69,14 @@ struct Params {
 struct Shared {
   uint32_t scan[32];
   unsigned long long red[32][4];
+  unsigned long long acc[4];  // per-level totals of the CTA (new vertices, their degree, words, summary bits)
   uint32_t hv[kHeavyBuf];
   uint32_t hd[kHeavyBuf];
   uint32_t hn;
   uint32_t base_e, base_c;
-  uint32_t beg[kThreads];
-  uint32_t incl[kThreads];
-  uint32_t flag[kThreads];
+  uint32_t beg[kBfsThreads];
+  uint32_t incl[kBfsThreads];
+  uint32_t flag[kBfsThreads];
   int choice;
   sygraph::detail::MlpStaged mlp;  // learned mode: parameters staged once per launch
   float mlp_scratch[2 * sygraph::detail::kMlpHidden];

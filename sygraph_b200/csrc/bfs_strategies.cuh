@@ -1,13 +1,15 @@
 // The expansion strategies of the BFS engine (bfs.cu), one call per level.
 //   push/warp : warps take summary words, expand the frontier's light vertices
 //               32 at a time, edge-parallel by a shuffle scan
-//   push/CTA  : a CTA takes 16 frontier words (512 candidates), scans their
+//   push/CTA  : a CTA takes one frontier word per warp (32 words, 1024
+//               candidates), scans their
 //               degrees across the block and walks the combined edge range
 //               (shared-memory binary search from edge rank to source)
-//   pull/warp : one warp per 32 unvisited vertices, each lane scans its own
-//               in-edges with the next column index prefetched; the warp
-//               helps with long lists
-//   pull/CTA  : a CTA takes 512 unvisited candidates and walks all their
+//   pull/warp : a warp takes four bitmap words (128 unvisited candidates,
+//               first probes of all four in flight together), each lane scans
+//               its own in-edges with the next column index prefetched; the
+//               warp helps with long lists
+//   pull/CTA  : a CTA takes one word per warp of unvisited candidates and walks all their
 //               in-edges edge-parallel, with a per-candidate done flag
 // Heavy vertices (degree >= kHeavy) of a push level are expanded from the
 // heavy list in kBfsChunk-edge chunks by both push strategies.
@@ -110,12 +112,16 @@ __device__ __forceinline__ void push_cta(Level& L, const uint32_t* fb_cur, const
   const Params& P = *L.P;
   Shared& S = *L.S;
   const uint32_t t = threadIdx.x, lane = t & 31, wl = t >> 5;
-  const uint32_t ngroups = (P.w0 + 15) / 16;
+  // a CTA takes as many bitmap words as it has warps (16 or 32: a group never
+  // straddles a summary word)
+  const uint32_t wg = blockDim.x >> 5;
+  const uint32_t ngroups = (P.w0 + wg - 1) / wg;
   for (uint32_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
-    const uint32_t s16 = (ld_cg(sm_cur + (g >> 1)) >> ((g & 1) * 16)) & 0xffffu;
-    if (!s16) continue;  // the same for every thread of the CTA
-    const uint32_t w = g * 16 + wl;
-    const uint32_t word = (((s16 >> wl) & 1u) && w < P.w0) ? ld_cg(fb_cur + w) : 0u;
+    const uint32_t first = g * wg;
+    const uint32_t sg = (ld_cg(sm_cur + (first >> 5)) >> (first & 31)) & (wg == 32 ? 0xffffffffu : ((1u << wg) - 1u));
+    if (!sg) continue;  // the same for every thread of the CTA
+    const uint32_t w = first + wl;
+    const uint32_t word = (((sg >> wl) & 1u) && w < P.w0) ? ld_cg(fb_cur + w) : 0u;
     const bool act = (word >> lane) & 1u;
     const uint32_t v = w * 32 + lane;
     const uint32_t beg = act ? P.ro[v] : 0u;
@@ -274,11 +280,12 @@ __device__ __forceinline__ void pull_cta(Level& L, const uint32_t* fb_cur, bool 
   const Params& P = *L.P;
   Shared& S = *L.S;
   const uint32_t t = threadIdx.x, lane = t & 31, wl = t >> 5;
-  const uint32_t ngroups = (P.w0 + 15) / 16;
+  const uint32_t wg = blockDim.x >> 5;
+  const uint32_t ngroups = (P.w0 + wg - 1) / wg;
   const bool same = P.iro == P.ro;
   volatile uint32_t* flag = S.flag;
   for (uint32_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
-    const uint32_t w = g * 16 + wl;
+    const uint32_t w = g * wg + wl;
     const uint32_t vw = w < P.w0 ? ld_cg(P.visited + w) : 0xffffffffu;
     const uint32_t cand = w < P.w0 ? (~vw & valid_bits(w, P.w0, P.n)) : 0u;
     if (!__syncthreads_or(cand != 0)) continue;

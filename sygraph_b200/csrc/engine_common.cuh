@@ -235,19 +235,19 @@ __device__ __forceinline__ uint32_t valid_bits(uint32_t wi, uint32_t w0, uint32_
 // streams can be resident at the same time).
 template <typename Params>
 inline sg_status launch_persistent(void (*kernel)(Params), const Params& p, int blocks_per_sm, cudaStream_t stream,
-                                   unsigned max_grid = 0, unsigned* grid_out = nullptr) {
+                                   unsigned max_grid = 0, unsigned* grid_out = nullptr, unsigned threads = kThreads) {
   int dev = 0, coop = 0;
   SG_CUDA(cudaGetDevice(&dev));
   SG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   SG_REQUIRE(coop, SG_ERR_UNSUPPORTED, "device does not support cooperative launch");
   int occ = 0;
-  SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, 0));
+  SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, (int)threads, 0));
   SG_REQUIRE(occ > 0, SG_ERR_CUDA, "engine kernel does not fit on an SM");
   const int per_sm = occ < blocks_per_sm ? occ : blocks_per_sm;
   unsigned grid = (unsigned)(per_sm * device_props().sm_count);
   if (max_grid && max_grid < grid) grid = max_grid;
   void* args[] = {(void*)&p};
-  SG_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(kThreads), args, 0, stream));
+  SG_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(threads), args, 0, stream));
   count_launch();
   if (grid_out) *grid_out = grid;
   return SG_OK;

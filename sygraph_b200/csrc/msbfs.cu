@@ -416,8 +416,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
       }
     }
     __syncthreads();
-    {
-      const uint32_t nb = min(S.hn, kHeavyBuf);
+    if (const uint32_t nb = min(S.hn, kHeavyBuf)) {  // block-uniform; most levels stage none
       const uint32_t k0 = 2 * threadIdx.x;
       uint32_t my = 0;
       if (k0 < nb) my += chunks_of(S.hd[k0]);

@@ -14,7 +14,6 @@ from pathlib import Path
 
 import numpy as np
 
-from . import _lib
 from ._lib import call, lib
 from .core import DeviceArray
 
