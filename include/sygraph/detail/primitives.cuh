@@ -167,28 +167,56 @@ struct GridBarrier {
 
 constexpr uint64_t kBarrierSpinLimit = 1ull << 24;  // ~16M polls x >=64 ns sleep: over a second
 
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void red_add_release(uint32_t* p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Top bit of the generation word: some block's wait ran out.
+constexpr uint32_t kBarrierFailed = 0x80000000u;
+
 // Returns false when the barrier timed out (here or in another block).
+//
+// Thread 0 of each block reads the generation (it cannot advance before this
+// block arrives), then arrives with one acq_rel atomic on the count: release
+// for this block's writes (ordered before it by __syncthreads), acquire for
+// the last arriver, whose atomic reads the chain of every earlier arrival.
+// The last arriver resets the count and bumps the generation with a release
+// add; the others spin on an acquire load of it, so every block leaves with
+// all writes of the phase visible.  A block whose wait runs out sets the
+// generation's top bit (and the error word the host reads), which ends every
+// other wait at once and fails every later barrier of the launch.
 __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
   __shared__ uint32_t s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t ok = 1;
-    const uint32_t gen = ld_acquire(&bar->generation);
-    __threadfence();
-    const uint32_t arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      bar->count = 0;
-      __threadfence();
-      st_release(&bar->generation, gen + 1);
+    const uint32_t gen = ld_relaxed(&bar->generation);
+    if (gen & kBarrierFailed) {
+      ok = 0;
+    } else if (atom_add_acq_rel(&bar->count, 1u) == gridDim.x - 1) {
+      bar->count = 0;  // ordered before the release below
+      red_add_release(&bar->generation, 1u);
     } else {
       uint64_t spins = 0;
-      while (ld_acquire(&bar->generation) == gen) {
-        if (++spins > kBarrierSpinLimit) {
-          atomicExch(&bar->error, 1u);
-          ok = 0;
+      for (;;) {
+        const uint32_t g = ld_acquire(&bar->generation);
+        if (g != gen) {
+          if (g & kBarrierFailed) ok = 0;
           break;
         }
-        if ((spins & 255u) == 0 && ld_volatile(&bar->error)) {
+        if (++spins > kBarrierSpinLimit) {
+          atomicOr(&bar->generation, kBarrierFailed);
+          atomicExch(&bar->error, 1u);
           ok = 0;
           break;
         }
@@ -197,8 +225,6 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
         if (spins > 512) __nanosleep(spins > 4096 ? 256 : 32);
       }
     }
-    __threadfence();
-    if (ld_volatile(&bar->error)) ok = 0;
     s_ok = ok;
   }
   __syncthreads();
