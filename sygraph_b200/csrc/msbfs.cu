@@ -9,8 +9,10 @@
 // "done" bitmap of vertices every source has reached.  Per level:
 //   push: for every active v and edge (v,u): new = F[v] & ~seen[u];
 //         atomicOr on seen[u] claims the bits, atomicOr on F'[u] publishes them
-//   pull: for every u not done: OR the frontier masks of its in-neighbours,
-//         stopping once every missing source is covered; u owns seen[u]
+//   pull: every u not done ORs the frontier masks of its in-neighbours:
+//         light u by a warp per word, the word's in-lists walked
+//         edge-parallel into per-owner shared slots (u owns seen[u]); heavy u
+//         by static in-list chunks, each applied like a push relaxation
 // No depth is stored during the traversal.  When F_{L-1} is cleared, each
 // active vertex folds its mask into the depth bit-planes: plane b holds, per
 // source bit, bit b of the vertex's depth, so v's planes get F_{L-1}[v] OR-ed
@@ -32,6 +34,8 @@ using namespace eng;
 
 constexpr uint32_t kHeavy = 256;
 constexpr uint32_t kHeavyBuf = 1024;
+constexpr uint32_t kPullHeavyIn = 256;  // in-degree from which a pulled vertex goes by chunks
+constexpr uint32_t kPullChunkIn = 256;  // in-edges per chunk
 using u64 = unsigned long long;
 
 struct LevelCounters {
@@ -65,6 +69,9 @@ struct Params {
   uint32_t heavy_cap;
   LevelCounters* cnt;
   GridBarrier* bar;
+  const uint32_t* pull_chunk_v;    // in-degree >= kPullHeavyIn: (vertex, first edge) of each
+  const uint32_t* pull_chunk_beg;  //   kPullChunkIn-edge chunk of its in-list, built at set-up
+  uint32_t pull_chunks;
   u64* planes;       // n_planes * n: bit b of each (source, vertex) depth
   uint32_t n_planes;
   uint32_t* depth;   // k * n, source-major, written after the last level
@@ -75,6 +82,7 @@ struct Params {
 struct Shared {
   uint32_t scan[32];
   u64 red[32];
+  u64 acc[kThreads];  // pull: per-warp OR accumulators of the word's 32 vertices
   uint32_t hv[kHeavyBuf];
   uint32_t hd[kHeavyBuf];
   uint32_t hn;
@@ -319,50 +327,47 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
         }
       }
     } else {
+      // pull: candidates OR the frontier masks of their in-neighbours.  Light
+      // candidates: a warp per word, the word's in-lists walked edge-parallel
+      // (coalesced column loads), masks OR-ed into the owner's shared slot;
+      // the owner alone writes seen / F' of its vertex.  Heavy candidates: the
+      // static chunk list, each chunk's OR applied like a push relaxation.
       n_pull++;
       const bool same = P.iro == P.ro;
+      u64* acc_slot = S.acc + (threadIdx.x & ~31u);
       for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
         const uint32_t dw = ld_cg(P.done + wi);
         const uint32_t cand = ~dw & valid_bits(wi, w0, n);
         if (!cand) continue;
         const uint32_t u = wi * 32 + lane;
         const bool mine = (cand >> lane) & 1u;
-        const u64 su = mine ? ld_cg(P.seen + u) : P.all;
         const uint32_t beg = mine ? P.iro[u] : 0u;
         const uint32_t end = mine ? P.iro[u + 1] : 0u;
-        u64 acc = 0;
-        uint32_t e = beg;
-        const uint32_t lim = min(end, beg + kPullSerial);
-        while (e < lim && (acc | su) != P.all) {
-          const uint32_t c0 = P.icol[e];
-          const uint32_t c1 = e + 1 < lim ? P.icol[e + 1] : c0;
-          acc |= F_cur[c0] | F_cur[c1];
-          e += 2;
-        }
-        if (e > lim) e = lim;
-        uint32_t left = __ballot_sync(kFullMask, mine && (acc | su) != P.all && e < end);
-        while (left) {
-          const uint32_t j = __ffs(left) - 1;
-          left &= left - 1;
-          const uint32_t jb = __shfl_sync(kFullMask, e, j);
-          const uint32_t je = __shfl_sync(kFullMask, end, j);
-          const u64 sj = shfl64(su | acc, j);
-          u64 part = 0;
-          for (uint32_t eb = jb; eb < je; eb += 32) {
-            const uint32_t ee = eb + lane;
-            if (ee < je) part |= F_cur[P.icol[ee]];
-            // warp OR-reduce, stop once everything missing is covered
-            u64 r = part;
-#pragma unroll
-            for (int d = 16; d > 0; d >>= 1) r |= ((u64)__shfl_xor_sync(kFullMask, (uint32_t)(r >> 32), d) << 32) |
-                                                   __shfl_xor_sync(kFullMask, (uint32_t)r, d);
-            part = r;
-            if ((part | sj) == P.all) break;
+        const bool light = mine && end - beg < kPullHeavyIn;
+        const uint32_t dg = light ? end - beg : 0u;
+        const uint32_t incl = warp_inclusive_scan(dg);
+        const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+        if (!total) continue;
+        const uint32_t excl = incl - dg;
+        acc_slot[lane] = 0ull;
+        __syncwarp();
+        for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+          const uint32_t r = r0 + lane;
+          const bool act = r < total;
+          const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+          const uint32_t ob = __shfl_sync(kFullMask, beg, o);
+          const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+          if (act) {
+            const u64 f = F_cur[P.icol[ob + (r - oe)]];
+            if (f) atomicOr(acc_slot + o, f);
           }
-          if (lane == j) acc |= part;
         }
+        __syncwarp();
+        const u64 acc = light ? acc_slot[lane] : 0ull;
+        __syncwarp();
+        const u64 su = light ? ld_cg(P.seen + u) : P.all;
         const u64 nw = acc & ~su;
-        const bool got = mine && nw != 0;
+        const bool got = light && nw != 0;
         const uint32_t du = got ? (same ? end - beg : P.ro[u + 1] - P.ro[u]) : 0u;
         if (got) {
           st_cg(P.seen + u, su | nw);
@@ -373,15 +378,24 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
           if ((su | nw) == P.all) L.done_deg += du;
           if (du >= kHeavy) L.add_heavy(u, du);
         }
+        // heavy vertices of the same word update these words by atomics too
         const uint32_t gmask = __ballot_sync(kFullMask, got);
-        const uint32_t dmask = __ballot_sync(kFullMask, mine && (su | nw) == P.all);
+        const uint32_t dmask = __ballot_sync(kFullMask, got && (su | nw) == P.all);
         if (lane == 0) {
-          if (gmask) {
-            st_cg(L.fa_next + wi, gmask);
-            atomicOr(L.sm_next + (wi >> 5), 1u << (wi & 31));
-          }
-          if (dmask) st_cg(P.done + wi, dw | dmask);
+          if (gmask && atomicOr(L.fa_next + wi, gmask) == 0) atomicOr(L.sm_next + (wi >> 5), 1u << (wi & 31));
+          if (dmask) atomicOr(P.done + wi, dmask);
         }
+      }
+      for (uint32_t c = gwarp; c < P.pull_chunks; c += nwarps) {
+        const uint32_t v = P.pull_chunk_v[c];
+        if (ld_cg(P.done + (v >> 5)) & (1u << (v & 31))) continue;
+        const uint32_t cb = P.pull_chunk_beg[c];
+        const uint32_t ce = min(P.iro[v + 1], cb + kPullChunkIn);
+        u64 part = 0;
+        for (uint32_t e = cb + lane; e < ce; e += 32) part |= F_cur[P.icol[e]];
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) part |= shfl64(part, lane ^ d);
+        if (lane == 0 && part) L.visit_push(v, part);
       }
     }
     // plane b is first folded at level 2^b + 1: zero it now
@@ -529,6 +543,8 @@ struct sg_msbfs_s {
   uint32_t* sources = nullptr;
   unsigned long long* planes = nullptr;
   uint32_t n_planes = 0;
+  uint32_t *pull_chunk_v = nullptr, *pull_chunk_beg = nullptr;
+  uint32_t pull_chunks = 0;
   uint32_t* depth = nullptr;
   ms::LevelCounters* cnt = nullptr;
   sygraph::detail::GridBarrier* bar = nullptr;
@@ -549,6 +565,8 @@ static void msbfs_release(sg_msbfs h) {
   dev_free(h->heavy_s);
   dev_free(h->sources);
   dev_free(h->planes);
+  dev_free(h->pull_chunk_v);
+  dev_free(h->pull_chunk_beg);
   dev_free(h->depth);
   dev_free(h->cnt);
   dev_free(h->bar);
@@ -585,6 +603,34 @@ sg_status sg_msbfs_create(sg_graph g, uint32_t max_sources, sg_msbfs* out) {
       (s = dev_alloc(&h->result, 8))) {
     msbfs_release(h);
     return s;
+  }
+  {
+    // static chunk list of the in-lists pulled by chunks (in-degree >= kPullHeavyIn)
+    std::vector<uint32_t> iro((size_t)g->n + 1), cv, cb;
+    if (cudaMemcpy(iro.data(), g->inv.ro, sizeof(uint32_t) * iro.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cudaGetLastError();
+      msbfs_release(h);
+      return fail(SG_ERR_CUDA, "multi-source BFS set-up: reading the in-edge offsets failed");
+    }
+    for (uint32_t v = 0; v < g->n; v++)
+      if (iro[v + 1] - iro[v] >= ms::kPullHeavyIn)
+        for (uint32_t e = iro[v]; e < iro[v + 1]; e += ms::kPullChunkIn) {
+          cv.push_back(v);
+          cb.push_back(e);
+        }
+    if (!cv.empty()) {
+      if ((s = dev_alloc(&h->pull_chunk_v, cv.size())) || (s = dev_alloc(&h->pull_chunk_beg, cb.size()))) {
+        msbfs_release(h);
+        return s;
+      }
+      if (cudaMemcpy(h->pull_chunk_v, cv.data(), 4 * cv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(h->pull_chunk_beg, cb.data(), 4 * cb.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        msbfs_release(h);
+        return fail(SG_ERR_CUDA, "multi-source BFS set-up: uploading the chunk list failed");
+      }
+      h->pull_chunks = (uint32_t)cv.size();
+    }
   }
   ms::no_in_edges_kernel<<<grid_for((uint64_t)h->w0 * 32, 256), 256, 0, g->stream>>>(g->inv.ro, g->n, h->w0, h->no_in);
   if (cudaGetLastError() != cudaSuccess) {
@@ -640,6 +686,9 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
   P.heavy_cap = h->heavy_cap;
   P.cnt = h->cnt;
   P.bar = h->bar;
+  P.pull_chunk_v = h->pull_chunk_v;
+  P.pull_chunk_beg = h->pull_chunk_beg;
+  P.pull_chunks = h->pull_chunks;
   P.planes = h->planes;
   P.n_planes = h->n_planes;
   P.depth = h->depth;
