@@ -437,9 +437,8 @@ sg_status sg_sssp_set_pull(sg_sssp s, uint32_t ratio);
  * improved, device timestamps), as sg_bfs_level_records. */
 sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count);
 /* Stream of this instance's launches and copies (NULL: the graph's stream)
- * and a cap on its persistent grid in CTAs (0: every SM; a BFS CTA is 1024
- * threads and one fills an SM, the other engines' CTAs are 512 threads, two
- * per SM), so that several instances
+ * and a cap on its persistent grid in CTAs of 512 threads (0: two per SM on
+ * every SM), so that several instances
  * can share the GPU.  Waits for work queued on the previous stream.  The
  * stream must stay valid until the instance is destroyed or given another. */
 sg_status sg_sssp_set_launch(sg_sssp s, void* stream, uint32_t max_ctas);

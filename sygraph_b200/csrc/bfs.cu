@@ -29,7 +29,7 @@ namespace bfs {
 
 using namespace eng;
 
-__global__ void __launch_bounds__(kBfsThreads, 1) bfs_kernel(Params P) {
+__global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
   __shared__ Shared S;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
@@ -320,7 +320,7 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.schedule = b->schedule_len ? b->schedule : nullptr;
   P.schedule_len = b->schedule_len;
   SG_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(*b->bar), b->stream));
-  return eng::launch_persistent(bfs::bfs_kernel, P, 1, b->stream, b->max_ctas, nullptr, bfs::kBfsThreads);
+  return eng::launch_persistent(bfs::bfs_kernel, P, 2, b->stream, b->max_ctas, nullptr, bfs::kBfsThreads);
 }
 
 static sg_status bfs_collect(sg_bfs b, sg_bfs_details* details) {
@@ -687,7 +687,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   SG_CUDA(cudaMemsetAsync(P.bar, 0, sizeof(sygraph::detail::GridBarrier), s));
   bfs::no_in_edges_kernel<<<grid_for((uint64_t)w0 * 32, 256), 256, 0, s>>>(dev_inv_row_offsets, n, w0, no_in);
   SG_CHECK_LAUNCH();
-  SG_TRY(eng::launch_persistent(bfs::bfs_kernel, P, 1, s, 0, nullptr, bfs::kBfsThreads));
+  SG_TRY(eng::launch_persistent(bfs::bfs_kernel, P, 2, s, 0, nullptr, bfs::kBfsThreads));
   unsigned long long it = 0;
   uint32_t err = 0;
   SG_CUDA(cudaMemcpyAsync(&it, P.result, sizeof(it), cudaMemcpyDeviceToHost, s));

@@ -19,9 +19,10 @@ constexpr uint32_t kHeavy = 256;      // degree from which a vertex is expanded 
 constexpr uint32_t kHeavyBuf = 1024;  // per-CTA staging of newly discovered heavy vertices
 constexpr uint32_t kBfsChunk = 64;    // edges per heavy-vertex chunk (one warp, two steps)
 constexpr int kLearned = 3;           // mode: the MLP picks each level's strategy
-// One 1024-thread CTA per SM: half the CTAs of the other engines for the same
-// threads, so a level's grid barrier and per-CTA counter atomics cost less.
-constexpr uint32_t kBfsThreads = 1024;
+// Two 512-thread CTAs per SM, as the other engines: one 1024-thread CTA per SM
+// halves the barrier arrivals but was within 1% on RMAT-22, and whole-SM CTAs
+// cannot share SMs with the half-SM CTAs of concurrent launches (serving).
+constexpr uint32_t kBfsThreads = 512;
 
 __device__ __forceinline__ uint32_t bfs_chunks(uint32_t deg) { return (deg + kBfsChunk - 1) / kBfsChunk; }
 

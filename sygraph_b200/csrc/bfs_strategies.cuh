@@ -1,7 +1,7 @@
 // The expansion strategies of the BFS engine (bfs.cu), one call per level.
 //   push/warp : warps take summary words, expand the frontier's light vertices
 //               32 at a time, edge-parallel by a shuffle scan
-//   push/CTA  : a CTA takes one frontier word per warp (32 words, 1024
+//   push/CTA  : a CTA takes one frontier word per warp (16 words, 512
 //               candidates), scans their
 //               degrees across the block and walks the combined edge range
 //               (shared-memory binary search from edge rank to source)

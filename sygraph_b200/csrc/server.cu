@@ -183,8 +183,7 @@ sg_status get_workspace(sg_server_s* s, uint32_t slot, uint32_t graph, int kind,
   if (kind == kWsBfs) {
     sg_bfs b = nullptr;
     st = sg_bfs_create(g, &b);
-    // the BFS engine runs one 1024-thread CTA per SM, the others two of 512
-    if (st == SG_OK) st = sg_bfs_set_launch(b, sl.stream, std::max<uint32_t>(1, ctas / 2));
+    if (st == SG_OK) st = sg_bfs_set_launch(b, sl.stream, ctas);
     w.handle = b;
   } else if (kind == kWsBatch) {
     sg_msbfs h = nullptr;
