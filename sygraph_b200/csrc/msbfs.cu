@@ -10,7 +10,9 @@
 //   push: for every active v and edge (v,u): new = F[v] & ~seen[u];
 //         atomicOr on seen[u] claims the bits, atomicOr on F'[u] publishes them
 //   pull: every u not done ORs the frontier masks of its in-neighbours:
-//         light u by a warp per word, the word's in-lists walked
+//         light u by a warp per word, each lane first probing a few
+//         in-neighbours serially (stopping once every missing source is
+//         covered), then the rest of the still-open lists walked
 //         edge-parallel into per-owner shared slots (u owns seen[u]); heavy u
 //         by static in-list chunks, each applied like a push relaxation
 // No depth is stored during the traversal.  When F_{L-1} is cleared, each
@@ -36,6 +38,7 @@ constexpr uint32_t kHeavy = 256;
 constexpr uint32_t kHeavyBuf = 1024;
 constexpr uint32_t kPullHeavyIn = 256;  // in-degree from which a pulled vertex goes by chunks
 constexpr uint32_t kPullChunkIn = 256;  // in-edges per chunk
+constexpr uint32_t kPullProbe = 8;      // serial early-exit probes before the edge-parallel scan
 using u64 = unsigned long long;
 
 struct LevelCounters {
@@ -344,29 +347,39 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
         const uint32_t beg = mine ? P.iro[u] : 0u;
         const uint32_t end = mine ? P.iro[u + 1] : 0u;
         const bool light = mine && end - beg < kPullHeavyIn;
-        const uint32_t dg = light ? end - beg : 0u;
+        if (!__any_sync(kFullMask, light)) continue;
+        const u64 su = light ? ld_cg(P.seen + u) : P.all;
+        // phase 1: a few serial probes; a vertex that every missing source
+        // reaches through its first in-neighbours stops here
+        u64 acc = 0;
+        uint32_t e = beg;
+        const uint32_t lim = light ? min(end, beg + kPullProbe) : beg;
+        while (e < lim && (acc | su) != P.all) acc |= F_cur[P.icol[e++]];
+        // phase 2: the rest of the still-open lists, edge-parallel into shared slots
+        const bool open = light && (acc | su) != P.all && e < end;
+        const uint32_t dg = open ? end - e : 0u;
         const uint32_t incl = warp_inclusive_scan(dg);
         const uint32_t total = __shfl_sync(kFullMask, incl, 31);
-        if (!total) continue;
-        const uint32_t excl = incl - dg;
-        acc_slot[lane] = 0ull;
-        __syncwarp();
-        for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-          const uint32_t r = r0 + lane;
-          const bool act = r < total;
-          const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
-          const uint32_t ob = __shfl_sync(kFullMask, beg, o);
-          const uint32_t oe = __shfl_sync(kFullMask, excl, o);
-          if (act) {
-            const u64 f = F_cur[P.icol[ob + (r - oe)]];
-            if (f) atomicOr(acc_slot + o, f);
+        if (total) {
+          const uint32_t excl = incl - dg;
+          acc_slot[lane] = acc;
+          __syncwarp();
+          for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+            const uint32_t r = r0 + lane;
+            const bool act = r < total;
+            const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+            const uint32_t ob = __shfl_sync(kFullMask, e, o);
+            const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+            if (act) {
+              const u64 f = F_cur[P.icol[ob + (r - oe)]];
+              if (f) atomicOr(acc_slot + o, f);
+            }
           }
+          __syncwarp();
+          acc = acc_slot[lane];
+          __syncwarp();
         }
-        __syncwarp();
-        const u64 acc = light ? acc_slot[lane] : 0ull;
-        __syncwarp();
-        const u64 su = light ? ld_cg(P.seen + u) : P.all;
-        const u64 nw = acc & ~su;
+        const u64 nw = light ? (acc & ~su) : 0ull;
         const bool got = light && nw != 0;
         const uint32_t du = got ? (same ? end - beg : P.ro[u + 1] - P.ro[u]) : 0u;
         if (got) {
