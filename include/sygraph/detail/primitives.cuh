@@ -159,70 +159,67 @@ __device__ __forceinline__ uint32_t atomic_min_nonneg(uint32_t* p, uint32_t v) {
 // GPU.  The grid must be co-resident (cooperative launch).
 // ---------------------------------------------------------------------------
 struct GridBarrier {
-  uint32_t count;
-  uint32_t generation;
-  uint32_t error;
+  unsigned long long count;  // arrivals since the launch began; top bit: a wait ran out
+  uint32_t error;            // read by the host after the launch
   uint32_t pad;
 };
 
 constexpr uint64_t kBarrierSpinLimit = 1ull << 24;  // ~16M polls x >=64 ns sleep: over a second
+constexpr unsigned long long kBarrierFailed = 1ull << 63;
 
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
-  uint32_t old;
-  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+__device__ __forceinline__ unsigned long long atom_add_acq_rel(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
   return old;
 }
-__device__ __forceinline__ void red_add_release(uint32_t* p, uint32_t v) {
-  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
 }
-
-// Top bit of the generation word: some block's wait ran out.
-constexpr uint32_t kBarrierFailed = 0x80000000u;
 
 // Returns false when the barrier timed out (here or in another block).
 //
-// Thread 0 of each block reads the generation (it cannot advance before this
-// block arrives), then arrives with one acq_rel atomic on the count: release
-// for this block's writes (ordered before it by __syncthreads), acquire for
-// the last arriver, whose atomic reads the chain of every earlier arrival.
-// The last arriver resets the count and bumps the generation with a release
-// add; the others spin on an acquire load of it, so every block leaves with
-// all writes of the phase visible.  A block whose wait runs out sets the
-// generation's top bit (and the error word the host reads), which ends every
-// other wait at once and fails every later barrier of the launch.
+// The count starts at zero for each launch (the host clears it) and only
+// grows: thread 0 of each block arrives with one acq_rel atomic (release for
+// this block's writes, ordered before it by __syncthreads), and the value it
+// returns names the phase, so the block waits until the count reaches the
+// phase's end, (old / gridDim.x + 1) * gridDim.x, with acquire loads.  Every
+// arrival is a read-modify-write of the same word, so the value a waiter
+// reads carries the release of every earlier arrival.  The last arriver
+// needs no wait and no second write: its own atomic completes the phase.  A
+// block whose wait runs out sets the count's top bit (and the error word),
+// which ends every other wait at once and fails every later barrier of the
+// launch.
 __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
   __shared__ uint32_t s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t ok = 1;
-    const uint32_t gen = ld_relaxed(&bar->generation);
-    if (gen & kBarrierFailed) {
+    const unsigned long long old = atom_add_acq_rel(&bar->count, 1ull);
+    if (old & kBarrierFailed) {
       ok = 0;
-    } else if (atom_add_acq_rel(&bar->count, 1u) == gridDim.x - 1) {
-      bar->count = 0;  // ordered before the release below
-      red_add_release(&bar->generation, 1u);
     } else {
-      uint64_t spins = 0;
-      for (;;) {
-        const uint32_t g = ld_acquire(&bar->generation);
-        if (g != gen) {
-          if (g & kBarrierFailed) ok = 0;
-          break;
+      const unsigned long long target = (old / gridDim.x + 1) * gridDim.x;
+      if (old + 1 != target) {
+        uint64_t spins = 0;
+        for (;;) {
+          const unsigned long long c = ld_acquire(&bar->count);
+          if (c & kBarrierFailed) {
+            ok = 0;
+            break;
+          }
+          if (c >= target) break;
+          if (++spins > kBarrierSpinLimit) {
+            atomicOr(&bar->count, kBarrierFailed);
+            atomicExch(&bar->error, 1u);
+            ok = 0;
+            break;
+          }
+          // poll back-to-back first (a barrier normally completes within a few
+          // microseconds), then back off
+          if (spins > 512) __nanosleep(spins > 4096 ? 256 : 32);
         }
-        if (++spins > kBarrierSpinLimit) {
-          atomicOr(&bar->generation, kBarrierFailed);
-          atomicExch(&bar->error, 1u);
-          ok = 0;
-          break;
-        }
-        // poll back-to-back first (a barrier normally completes within a few
-        // microseconds), then back off
-        if (spins > 512) __nanosleep(spins > 4096 ? 256 : 32);
       }
     }
     s_ok = ok;

@@ -187,8 +187,8 @@ sg_status sg_bc(sg_graph g, const uint32_t* host_sources, uint32_t k, float* hos
     if (e != cudaSuccess) st = cuda_fail(e, "memset", __FILE__, __LINE__);
   }
   for (uint32_t i = 0; i < k && st == SG_OK; i++) {
-    // count and generation restart per launch; the error flag persists
-    cudaError_t e = cudaMemsetAsync(ws.bar, 0, 2 * sizeof(uint32_t), s);
+    // the arrival count restarts per launch; the error flag persists
+    cudaError_t e = cudaMemsetAsync(&ws.bar->count, 0, sizeof(ws.bar->count), s);
     if (e != cudaSuccess) {
       st = cuda_fail(e, "memset", __FILE__, __LINE__);
       break;

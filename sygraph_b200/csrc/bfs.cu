@@ -69,6 +69,9 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
   if (P.mode == kLearned && P.mlp) sygraph::detail::mlp_stage(P.mlp, &S.mlp);
   if (!grid_sync(P.bar)) return;
 
+  // heavy list of the frontier being expanded, read with the level's other
+  // counters right after each barrier
+  unsigned long long heavy_packed = ld_cg(&P.cnt[2].heavy_packed);
   unsigned long long unexplored = P.m - deg_src;
   unsigned long long frontier_size = 1, frontier_deg = deg_src, prev_size = 1;
   unsigned long long visited_vertices = 1;
@@ -85,7 +88,6 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
   for (;; level++) {
     if (P.schedule && level < P.schedule_len && P.schedule[level] >= 0) strategy = P.schedule[level];
     LevelCounters* C = P.cnt + (level % 3);
-    const LevelCounters* Cprev = P.cnt + ((level + 2) % 3);
     const uint32_t* fb_cur = P.fb + (size_t)(level % 3) * w0;
     uint32_t* fb_zero = P.fb + (size_t)((level + 2) % 3) * w0;
     const uint32_t* sm_cur = P.sm + (size_t)(level % 3) * w1;
@@ -101,12 +103,11 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
             P.heavy_v + (size_t)(par ^ 1) * P.heavy_cap, P.heavy_s + (size_t)(par ^ 1) * P.heavy_cap, level + 1};
     if (strategy < 2) {
       n_push++;
-      const unsigned long long hp = ld_cg(&Cprev->heavy_packed);
-      const uint32_t n_heavy = (uint32_t)(hp >> 32), n_chunks = (uint32_t)hp;
+      const uint32_t n_heavy = (uint32_t)(heavy_packed >> 32), n_chunks = (uint32_t)heavy_packed;
       const uint32_t* hv = P.heavy_v + (size_t)par * P.heavy_cap;
       const uint32_t* hs = P.heavy_s + (size_t)par * P.heavy_cap;
       if (strategy == 0)
-        push_warp(L, fb_cur, sm_cur, hv, hs, n_heavy, n_chunks);
+        push_warp(L, fb_cur, sm_cur, fb_zero, sm_zero, hv, hs, n_heavy, n_chunks);
       else
         push_cta(L, fb_cur, sm_cur, hv, hs, n_heavy, n_chunks);
     } else {
@@ -117,8 +118,9 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
       else
         pull_warp(L, fb_cur, sc, level < 64 && ((P.pull_reverse >> level) & 1ull));
     }
-    // clear F_{L-1}: only the words its summary flags
-    for (uint32_t j = gwarp; j < w1; j += nwarps) {
+    // clear F_{L-1}: only the words its summary flags (push/warp did it with
+    // its own summary scan)
+    for (uint32_t j = gwarp; strategy != 0 && j < w1; j += nwarps) {
       const uint32_t s = ld_cg(sm_zero + j);
       if (!s) continue;
       if ((s >> lane) & 1u) st_cg(fb_zero + j * 32 + lane, 0u);
@@ -170,6 +172,9 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
 
     const unsigned long long next_size = ld_cg(&C->new_count);
     const unsigned long long next_deg = ld_cg(&C->new_deg);
+    const unsigned long long words_nz = ld_cg(&C->words_nz);
+    const unsigned long long sum_nz = ld_cg(&C->sum_nz);
+    heavy_packed = ld_cg(&C->heavy_packed);
     unexplored -= next_deg;
     visited_vertices += next_size;
     if (gtid == 0 && level < kMaxLog) {
@@ -190,7 +195,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     frontier_deg = next_deg;
     if (next_size == 0) break;
     FeatureInputs x{(double)next_size, (double)next_deg, (double)unexplored, (double)visited_vertices,
-                    (double)ld_cg(&C->words_nz), (double)ld_cg(&C->sum_nz), (double)prev_size, strategy >= 2};
+                    (double)words_nz, (double)sum_nz, (double)prev_size, strategy >= 2};
     // (float)(uint32) casts: the reference's uint32 degree sums (bfs.hpp:327-330)
     strategy = decide(P, S, strategy, x, level + 1, (float)(uint32_t)next_deg, (float)(uint32_t)unexplored,
                       next_size);

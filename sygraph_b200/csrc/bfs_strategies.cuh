@@ -71,9 +71,11 @@ __device__ __forceinline__ void push_heavy(Level& L, const uint32_t* hv, const u
   (void)n_chunks;
 }
 
+// Also clears F_{L-1} (fb_zero / sm_zero): its summary word is read with the
+// frontier's, so the clear adds no dependent load to the level.
 __device__ __forceinline__ void push_warp(Level& L, const uint32_t* fb_cur, const uint32_t* sm_cur,
-                                          const uint32_t* hv, const uint32_t* hs, uint32_t n_heavy,
-                                          uint32_t n_chunks) {
+                                          uint32_t* fb_zero, uint32_t* sm_zero, const uint32_t* hv,
+                                          const uint32_t* hs, uint32_t n_heavy, uint32_t n_chunks) {
   const Params& P = *L.P;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -81,6 +83,11 @@ __device__ __forceinline__ void push_warp(Level& L, const uint32_t* fb_cur, cons
   const uint32_t w1 = P.w1;
   for (uint32_t unit = gwarp; unit < w1; unit += nwarps) {
     const uint32_t s = ld_cg(sm_cur + unit);
+    const uint32_t z = ld_cg(sm_zero + unit);
+    if (z) {
+      if ((z >> lane) & 1u) st_cg(fb_zero + unit * 32 + lane, 0u);
+      if (lane == 0) st_cg(sm_zero + unit, 0u);
+    }
     if (!s) continue;
     const uint32_t bits = ((s >> lane) & 1u) ? ld_cg(fb_cur + unit * 32 + lane) : 0u;
     const uint32_t c = __popc(bits);

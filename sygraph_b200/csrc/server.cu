@@ -210,7 +210,7 @@ sg_status get_workspace(sg_server_s* s, uint32_t slot, uint32_t graph, int kind,
   return SG_OK;
 }
 
-constexpr float kBatchAlpha = 1.0f, kBatchBeta = 24.0f;  // batched BFS direction switch
+constexpr float kBatchAlpha = 4.0f, kBatchBeta = 24.0f;  // batched BFS direction switch (bench.py MS_ALPHA)
 constexpr float kAlpha = 15.0f, kBeta = 24.0f;           // single BFS: the reference heuristic
 
 sg_status launch(sg_server_s* s, uint32_t si, const std::vector<uint64_t>& tickets, uint32_t graph, int kind,
