@@ -427,14 +427,31 @@ sg_status sg_sssp_run(sg_sssp s, uint64_t* iterations);
  * same fixed point); the iteration count and the work are not.  0 (the
  * default) is the reference's frontier Bellman-Ford. */
 sg_status sg_sssp_set_delta(sg_sssp s, double delta);
+/* With near-far bucketing: once a refill leaves fewer than fraction * n
+ * vertices waiting beyond the threshold, the next refill takes all of them
+ * and the rest runs as plain frontier Bellman-Ford (every edge).  The sparse
+ * end of the distance range then takes a few iterations instead of one bucket
+ * per delta.  Default 1/4; 0 keeps bucketing to the end. */
+sg_status sg_sssp_set_tail(sg_sssp s, double fraction);
+/* With near-far bucketing, on graphs whose weighted rows are symmetric
+ * (every edge's reverse present with the same weight; checked once per
+ * graph): a bucket whose heavy edges number more than m / ratio relaxes them
+ * by pull, each vertex beyond the bucket scanning its weight-sorted row up
+ * to the first weight that can no longer improve it.  Default 8; 0 always
+ * pushes. */
+sg_status sg_sssp_set_heavy_pull(sg_sssp s, uint32_t ratio);
 /* Pull iterations (not in the reference): an iteration whose frontier
  * out-degree times `ratio` exceeds the edge count runs as one pull sweep
  * (every vertex takes the minimum over its in-neighbours in the frontier, no
  * atomics) instead of a push.  Distances are unchanged; 0 (the default) is
  * push only, as the reference. */
 sg_status sg_sssp_set_pull(sg_sssp s, uint32_t ratio);
-/* Per-iteration log of the last run (frontier size and out-degree, vertices
- * improved, device timestamps), as sg_bfs_level_records. */
+/* Per-step log of the last run (frontier size and out-degree, vertices
+ * improved, device timestamps), as sg_bfs_level_records.  strategy: 0 push
+ * iteration, 2 pull sweep; with near-far bucketing also 4, the heavy-edge
+ * phase of a bucket (frontier_size = the bucket's vertices), and 5, a refill
+ * pass (frontier_size = vertices moved to the frontier, next_size = vertices
+ * left beyond the threshold). */
 sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count);
 /* Stream of this instance's launches and copies (NULL: the graph's stream)
  * and a cap on its persistent grid in CTAs of 512 threads (0: two per SM on

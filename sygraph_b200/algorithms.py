@@ -207,6 +207,16 @@ class SSSP:
         """Near-far threshold step (0: the reference's frontier Bellman-Ford)."""
         call("sg_sssp_set_delta", self.handle, float(delta))
 
+    def set_tail(self, fraction: float) -> None:
+        """Near-far: once fewer than fraction * n vertices wait beyond the
+        threshold, finish with plain Bellman-Ford (0: bucket to the end)."""
+        call("sg_sssp_set_tail", self.handle, float(fraction))
+
+    def set_heavy_pull(self, ratio: int) -> None:
+        """Near-far on symmetric weighted graphs: a bucket's heavy edges go by
+        pull when they number more than m / ratio (0: always push)."""
+        call("sg_sssp_set_heavy_pull", self.handle, int(ratio))
+
     def getDistances(self) -> np.ndarray:
         dt = np.float32 if self.G.value_type == WEIGHT_F32 else np.uint32
         out = np.empty(self.G.getVertexCount(), dt)

@@ -70,6 +70,27 @@ sg_status graph_weight_sorted(sg_graph g) {
   SG_CUDA(cudaMemcpy(ro.data(), g->fwd.ro, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost));
   SG_CUDA(cudaMemcpy(col.data(), g->fwd.col, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
   SG_CUDA(cudaMemcpy(val.data(), g->fwd.val, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
+  // symmetric weighted adjacency: each row sorted by column and every edge's
+  // reverse present with the same weight (binary search in the other row)
+  bool sym = true;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(&& : sym)
+  for (int64_t v = 0; v < (int64_t)n; v++) {
+    if (!sym) continue;
+    for (uint32_t i = ro[v]; i < ro[v + 1]; i++) {
+      if (i + 1 < ro[v + 1] && col[i] >= col[i + 1]) {
+        sym = false;
+        break;
+      }
+      const uint32_t u = col[i];
+      const uint32_t* b = col.data() + ro[u];
+      const uint32_t* e = col.data() + ro[u + 1];
+      const uint32_t* f = std::lower_bound(b, e, (uint32_t)v);
+      if (f == e || *f != (uint32_t)v || val[f - col.data()] != val[i]) {
+        sym = false;
+        break;
+      }
+    }
+  }
 #pragma omp parallel
   {
     std::vector<uint64_t> key;
@@ -103,6 +124,7 @@ sg_status graph_weight_sorted(sg_graph g) {
   }
   g->wcol = wc;
   g->wval = wv;
+  g->wsym = sym;
   g->bytes += 8ull * m;
   return SG_OK;
 }

@@ -49,6 +49,21 @@ struct Queues {
 
 __device__ __forceinline__ uint32_t chunks_of(uint32_t deg) { return (deg + kChunk - 1) / kChunk; }
 
+// Position of the k-th (0-based) set bit of x.
+__device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t s = 16; s > 0; s >>= 1) {
+    const uint32_t low = __popc(x & ((1u << s) - 1u));
+    if (k >= low) {
+      k -= low;
+      x >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
 using sygraph::detail::block_excl_scan;
 using sygraph::detail::block_sum;
 
@@ -62,14 +77,19 @@ struct RowRange {
   __device__ __forceinline__ uint32_t end(uint32_t v) const { return hi[v + shift]; }
 };
 
-// Bitmap -> queues.  Each CTA owns a contiguous range of bitmap words, counts
-// the vertices there by class, reserves its slots with one atomic per list
-// and writes them in vertex order.  When `accumulate` is given, each word is
-// also OR-ed into it (one thread per word).
+// Bitmap -> queues.  Each CTA owns a contiguous range of bitmap words and
+// takes them 32 words per warp: the warp ranks the set bits of its words and
+// every lane takes every 32nd rank, so the row-range loads of a dense word go
+// out together instead of one latency per set bit.  A first pass counts each
+// lane's vertices by class; one block scan and one atomic per list reserve
+// the slots; a second pass repeats the same rank walk and writes them.  When
+// `accumulate` is given, each word is also OR-ed into it (one thread per
+// word).
 __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb, uint32_t w0, RowRange R,
                                                  Counters* C, Queues q, uint32_t* s_scan,
                                                  uint32_t* accumulate = nullptr) {
   __shared__ uint32_t s_base_small, s_base_big, s_base_chunk;
+  const uint32_t lane = threadIdx.x & 31;
   const uint32_t per_block = (w0 + gridDim.x - 1) / gridDim.x;
   const uint32_t wbeg = blockIdx.x * per_block;
   const uint32_t wend = min(w0, wbeg + per_block);
@@ -77,24 +97,39 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
     const uint32_t wi = base + threadIdx.x;
     const uint32_t bits = wi < wend ? ld_cg(fb + wi) : 0u;
     if (accumulate && bits) st_cg(accumulate + wi, ld_cg(accumulate + wi) | bits);
+    const uint32_t c = __popc(bits);
+    const uint32_t incl = warp_inclusive_scan(c);
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    const uint32_t excl = incl - c;
+    const uint32_t w_first = base + (threadIdx.x & ~31u);  // the warp's first word
+    // vertex of rank r (< total) among the warp's set bits
+    auto vertex_of = [&](uint32_t r) {
+      const uint32_t o = warp_owner_of_rank(incl, r);
+      const uint32_t ob = __shfl_sync(kFullMask, bits, o);
+      const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+      return (w_first + o) * 32 + select_bit(ob, r - oe);
+    };
     uint32_t n_small = 0, n_big = 0, n_chunk = 0;
     unsigned long long fdeg = 0;
-    for (uint32_t b = bits; b; b &= b - 1) {
-      const uint32_t v = wi * 32 + __ffs(b) - 1;
-      const uint32_t d = R.end(v) - R.beg(v);
-      fdeg += d;
-      if (d < kSmallDeg) {
-        n_small++;
-      } else {
-        n_big++;
-        n_chunk += chunks_of(d);
+    for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      const uint32_t v = vertex_of(min(r, total - 1));
+      if (r < total) {
+        const uint32_t d = R.end(v) - R.beg(v);
+        fdeg += d;
+        if (d < kSmallDeg) {
+          n_small++;
+        } else {
+          n_big++;
+          n_chunk += chunks_of(d);
+        }
       }
     }
     uint32_t t_pack, t_chunk;
     const uint32_t e_pack = block_excl_scan(n_small | (n_big << 16), &t_pack, s_scan);
     const uint32_t e_chunk = block_excl_scan(n_chunk, &t_chunk, s_scan);
     fdeg = sygraph::detail::warp_sum(fdeg);
-    if ((threadIdx.x & 31) == 0 && fdeg) atomicAdd(&C->frontier_deg, fdeg);
+    if (lane == 0 && fdeg) atomicAdd(&C->frontier_deg, fdeg);
     if (threadIdx.x == 0) {
       const uint32_t ts = t_pack & 0xffffu, tb = t_pack >> 16;
       s_base_small = ts ? atomicAdd(&C->small_tail, ts) : 0u;
@@ -108,16 +143,19 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
     uint32_t ps = s_base_small + (e_pack & 0xffffu);
     uint32_t pb = s_base_big + (e_pack >> 16);
     uint32_t pc = s_base_chunk + e_chunk;
-    for (uint32_t b = bits; b; b &= b - 1) {
-      const uint32_t v = wi * 32 + __ffs(b) - 1;
-      const uint32_t d = R.end(v) - R.beg(v);
-      if (d < kSmallDeg) {
-        q.small[ps++] = v;
-      } else {
-        q.big[pb] = v;
-        q.big_start[pb] = pc;
-        pb++;
-        pc += chunks_of(d);
+    for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      const uint32_t v = vertex_of(min(r, total - 1));
+      if (r < total) {
+        const uint32_t d = R.end(v) - R.beg(v);
+        if (d < kSmallDeg) {
+          q.small[ps++] = v;
+        } else {
+          q.big[pb] = v;
+          q.big_start[pb] = pc;
+          pb++;
+          pc += chunks_of(d);
+        }
       }
     }
     __syncthreads();
@@ -208,21 +246,6 @@ __device__ __forceinline__ void push_expand(const uint32_t* __restrict__ ro, con
                                             Queues q, uint32_t n_small, uint32_t n_big, uint32_t n_chunks,
                                             Visitor& vis) {
   push_expand(RowRange{ro, ro, 1}, col, q, n_small, n_big, n_chunks, vis);
-}
-
-// Position of the k-th (0-based) set bit of x.
-__device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t k) {
-  uint32_t pos = 0;
-#pragma unroll
-  for (uint32_t s = 16; s > 0; s >>= 1) {
-    const uint32_t low = __popc(x & ((1u << s) - 1u));
-    if (k >= low) {
-      k -= low;
-      x >>= s;
-      pos += s;
-    }
-  }
-  return pos;
 }
 
 __device__ __forceinline__ uint32_t valid_bits(uint32_t wi, uint32_t w0, uint32_t n) {

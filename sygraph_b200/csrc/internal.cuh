@@ -115,6 +115,9 @@ struct sg_graph_s {
   // built on first use (graph_weight_sorted), row offsets are fwd.ro
   uint32_t* wcol = nullptr;
   void* wval = nullptr;
+  // set with wcol: rows sorted by column and every edge (u, v, w) has its
+  // reverse (v, u, w), so a row also lists the vertex's in-edges
+  bool wsym = false;
   std::mutex wsort_mu;
   uint32_t n = 0;
   uint64_t m = 0;

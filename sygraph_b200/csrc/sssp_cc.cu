@@ -25,8 +25,7 @@ using namespace eng;
 // Near-far bookkeeping of one refill pass (three rotating slots).
 struct Refill {
   unsigned long long moved, remaining;
-  unsigned long long moved_deg;  // out-degree sum of the vertices moved to the frontier
-  uint32_t far_min;              // bit pattern of the smallest distance left in the far set
+  uint32_t far_min;  // bit pattern of the smallest distance left in the far set
   uint32_t pad;
 };
 
@@ -47,37 +46,258 @@ struct SsspParams {
   const uint32_t* split;  // delta-stepping: first edge of weight >= delta in each weight-sorted row
   const uint32_t* wcol;   // weight-sorted rows (same row offsets)
   const W* wval;
+  uint32_t tail;  // far set below this many vertices: the rest runs as plain Bellman-Ford
+  // heavy phase by pull when its push would relax more than m / heavy_pull
+  // edges (0: always push); only where a row's out-edges are its in-edges
+  uint32_t heavy_pull;
 };
 
+// Edge relaxation of the SSSP push steps, kU edges per lane at a time: the
+// column and weight loads of all kU edges go out together, then their
+// distance probes, then the atomicMins that improve, then the bitmap marks,
+// so a warp waits about four memory latencies per 32 * kU edges instead of
+// four per 32.  nd = d[v] + w with atomicMin on d[u] (non-negative floats
+// order as their bit patterns); an improved u joins the next frontier, or,
+// under near-far bucketing with nd at or beyond the threshold, the far set.
+constexpr int kU = 4;
+
 template <typename W>
-struct SsspVisitor : NextFrontier {
-  using src_t = W;
+struct SsspRelax {
   W* dist;
   const W* w;
+  const uint32_t* col;
   uint32_t* far;
+  uint32_t* fb_next;
   const uint32_t* ro;
   W threshold;
   bool bucketed;
+  bool want_deg;  // sum the out-degree of new frontier vertices (only a pull decision reads it)
+  uint32_t n_new = 0;
   unsigned long long deg_new = 0;
-  __device__ __forceinline__ void mark(uint32_t u) {
-    const uint32_t b = 1u << (u & 31);
-    if (!(atomicOr(fb_next + (u >> 5), b) & b)) {
-      n_new++;
-      deg_new += ro[u + 1] - ro[u];
+
+  __device__ __forceinline__ void relax(const uint32_t (&e)[kU], const W (&dv)[kU], uint32_t act) {
+    uint32_t u[kU];
+    W nd[kU], cur[kU], old[kU];
+#pragma unroll
+    for (int k = 0; k < kU; k++) {
+      u[k] = 0;
+      nd[k] = W(0);
+      if ((act >> k) & 1u) {
+        u[k] = col[e[k]];
+        nd[k] = dv[k] + w[e[k]];
+      }
     }
-  }
-  __device__ __forceinline__ W src(uint32_t v) const { return ld_cg(dist + v); }
-  __device__ __forceinline__ bool visit(uint32_t u, uint32_t e, W dv, uint32_t) {
-    const W nd = dv + w[e];
-    if (!(nd < ld_cg(dist + u))) return false;
-    if (!(nd < sygraph::detail::atomic_min_nonneg(dist + u, nd))) return false;
-    if (bucketed && !(nd < threshold)) {
-      atomicOr(far + (u >> 5), 1u << (u & 31));
-      return false;
+#pragma unroll
+    for (int k = 0; k < kU; k++) cur[k] = ((act >> k) & 1u) ? ld_cg(dist + u[k]) : W(0);
+    uint32_t imp = 0;
+#pragma unroll
+    for (int k = 0; k < kU; k++)
+      if (((act >> k) & 1u) && nd[k] < cur[k]) imp |= 1u << k;
+    if (!imp) return;
+#pragma unroll
+    for (int k = 0; k < kU; k++) old[k] = ((imp >> k) & 1u) ? sygraph::detail::atomic_min_nonneg(dist + u[k], nd[k]) : W(0);
+    uint32_t prev[kU];
+    uint32_t marked = 0;
+#pragma unroll
+    for (int k = 0; k < kU; k++) {
+      prev[k] = 0;
+      if (((imp >> k) & 1u) && nd[k] < old[k]) {
+        const uint32_t b = 1u << (u[k] & 31);
+        if (bucketed && !(nd[k] < threshold)) {
+          atomicOr(far + (u[k] >> 5), b);
+        } else {
+          prev[k] = atomicOr(fb_next + (u[k] >> 5), b);
+          marked |= 1u << k;
+        }
+      }
     }
-    return true;
+#pragma unroll
+    for (int k = 0; k < kU; k++)
+      if (((marked >> k) & 1u) && !(prev[k] & (1u << (u[k] & 31)))) {
+        n_new++;
+        if (want_deg) deg_new += ro[u[k] + 1] - ro[u[k]];
+      }
   }
 };
+
+// Last entry of the increasing list big_start[0, n) that is <= c (the list
+// starts at 0): a warp-wide 32-ary search, one load per lane per round.
+__device__ __forceinline__ uint32_t warp_find_chunk_owner(const uint32_t* big_start, uint32_t n, uint32_t c) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t step = (hi - lo + 31) / 32;
+    const uint32_t idx = lo + lane * step;
+    const bool le = idx < hi && ld_cg(big_start + idx) <= c;
+    const uint32_t m = __ballot_sync(kFullMask, le);  // a prefix of the lanes; lane 0 always
+    const uint32_t k = 31 - __clz(m);
+    lo += k * step;
+    hi = min(hi, lo + step);
+  }
+  return lo;
+}
+
+// Push expansion of one SSSP step over the compacted queues.  Small vertices
+// (row range < kSmallDeg) go 32 per warp, their edges ranked across the warp;
+// big vertices are cut in kChunk-edge chunks, and each warp takes a
+// contiguous run of chunks: one owner search, then the owners advance.
+template <typename W>
+__device__ __forceinline__ void sssp_expand(RowRange R, Queues q, uint32_t n_small, uint32_t n_big, uint32_t n_chunks,
+                                            SsspRelax<W>& X) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n_groups = (n_small + 31) / 32;
+  for (uint32_t unit = gwarp; unit < n_groups; unit += nwarps) {
+    const uint32_t idx = unit * 32 + lane;
+    const bool valid = idx < n_small;
+    const uint32_t v = valid ? ld_cg(q.small + idx) : 0u;
+    const uint32_t beg = valid ? R.beg(v) : 0u;
+    const uint32_t deg = valid ? R.end(v) - beg : 0u;
+    const W dv = valid ? ld_cg(X.dist + v) : W(0);
+    const uint32_t incl = warp_inclusive_scan(deg);
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    const uint32_t excl = incl - deg;
+    for (uint32_t r0 = 0; r0 < total; r0 += 32 * kU) {
+      uint32_t e[kU];
+      W d[kU];
+      uint32_t act = 0;
+#pragma unroll
+      for (int k = 0; k < kU; k++) {
+        const uint32_t r = r0 + k * 32 + lane;
+        const bool a = r < total;
+        const uint32_t o = warp_owner_of_rank(incl, a ? r : total - 1);
+        const uint32_t ob = __shfl_sync(kFullMask, beg, o);
+        const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+        d[k] = __shfl_sync(kFullMask, dv, o);
+        e[k] = ob + (r - oe);
+        act |= (uint32_t)a << k;
+      }
+      X.relax(e, d, act);
+    }
+  }
+  if (!n_chunks) return;
+  const uint32_t per = (n_chunks + nwarps - 1) / nwarps;
+  const uint32_t c_lo = gwarp * per;
+  const uint32_t c_hi = min(n_chunks, c_lo + per);
+  if (c_lo >= c_hi) return;
+  uint32_t ent = warp_find_chunk_owner(q.big_start, n_big, c_lo);
+  uint32_t v = ld_cg(q.big + ent);
+  uint32_t first = ld_cg(q.big_start + ent);
+  uint32_t next = ent + 1 < n_big ? ld_cg(q.big_start + ent + 1) : n_chunks;
+  uint32_t vb = R.beg(v), ve = R.end(v);
+  W dv = ld_cg(X.dist + v);
+  for (uint32_t c = c_lo; c < c_hi; c++) {
+    while (c >= next) {  // the run crossed into the next big vertex
+      ent++;
+      v = ld_cg(q.big + ent);
+      first = next;
+      next = ent + 1 < n_big ? ld_cg(q.big_start + ent + 1) : n_chunks;
+      vb = R.beg(v);
+      ve = R.end(v);
+      dv = ld_cg(X.dist + v);
+    }
+    const uint32_t cb = vb + (c - first) * kChunk;
+    const uint32_t ce = min(ve, cb + kChunk);
+    for (uint32_t eb = cb; eb < ce; eb += 32 * kU) {
+      uint32_t e[kU];
+      W d[kU];
+      uint32_t act = 0;
+#pragma unroll
+      for (int k = 0; k < kU; k++) {
+        e[k] = eb + k * 32 + lane;
+        d[k] = dv;
+        act |= (uint32_t)(e[k] < ce) << k;
+      }
+      X.relax(e, d, act);
+    }
+  }
+}
+
+// Heavy phase of the bucket [lo, threshold) by pull, for graphs whose rows
+// list in-edges as well as out-edges (undirected, symmetric weights): every
+// vertex u beyond the threshold takes the minimum over its neighbours c in
+// the bucket of d[c] + w.  An improvement can only come through an edge of
+// weight >= delta from a bucket vertex (its light edges were relaxed while
+// the bucket ran), and d[c] >= lo, so u's weight-sorted row is scanned from
+// the lightest edge and the scan stops at the first weight with lo + w >=
+// best (rounding is monotone: no later edge gives less).  u alone writes
+// d[u], so there are no atomics; improved vertices join the far set.  Lanes
+// scan their own rows kP edges per step; rows of kPullLong edges or more
+// are walked by the whole warp, 32 edges per step.
+constexpr uint32_t kP = 4;
+constexpr uint32_t kPullLong = 256;
+
+template <typename W>
+__device__ __forceinline__ void sssp_pull_heavy(const SsspParams<W>& P, W lo, W threshold) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n = P.L.n, w0 = P.L.w0;
+  const uint32_t* ro = P.L.ro;
+  for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+    const uint32_t u = wi * 32 + lane;
+    const W d0 = u < n ? ld_cg(P.dist + u) : W(0);
+    const bool cand = u < n && threshold < d0;
+    if (!__any_sync(kFullMask, cand)) continue;
+    const uint32_t beg = cand ? ro[u] : 0u, end = cand ? ro[u + 1] : 0u;
+    const bool is_long = end - beg >= kPullLong;
+    W best = d0;
+    uint32_t e = beg;
+    bool open = cand && !is_long && beg < end;
+    while (__any_sync(kFullMask, open)) {
+      if (open) {
+        W wv[kP], dc[kP];
+        uint32_t cv[kP];
+        bool inb[kP];
+#pragma unroll
+        for (uint32_t k = 0; k < kP; k++) {
+          const bool ok = e + k < end;
+          wv[k] = ok ? P.wval[e + k] : W(0);
+          cv[k] = ok ? P.wcol[e + k] : 0u;
+          inb[k] = ok;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kP; k++) inb[k] = inb[k] && lo + wv[k] < best && bit_test_ro(P.bucket, cv[k]);
+#pragma unroll
+        for (uint32_t k = 0; k < kP; k++) dc[k] = inb[k] ? ld_cg(P.dist + cv[k]) : W(0);
+#pragma unroll
+        for (uint32_t k = 0; k < kP; k++)
+          if (inb[k]) {
+            const W c = dc[k] + wv[k];
+            if (c < best) best = c;
+          }
+        e += kP;
+        open = e < end && lo + wv[kP - 1] < best;
+      }
+    }
+    // long rows: one at a time, the warp's 32 lanes on consecutive edges
+    for (uint32_t lm = __ballot_sync(kFullMask, cand && is_long); lm; lm &= lm - 1) {
+      const uint32_t o = __ffs(lm) - 1;
+      const uint32_t ob = __shfl_sync(kFullMask, beg, o), oe = __shfl_sync(kFullMask, end, o);
+      W ob_best = __shfl_sync(kFullMask, best, o);
+      for (uint32_t eb = ob; eb < oe; eb += 32) {
+        const uint32_t x = eb + lane;
+        const W w = x < oe ? P.wval[x] : W(0);
+        W c = max_weight<W>();
+        if (x < oe && lo + w < ob_best) {
+          const uint32_t cc = P.wcol[x];
+          if (bit_test_ro(P.bucket, cc)) c = ld_cg(P.dist + cc) + w;
+        }
+        c = warp_min_w(c);
+        if (c < ob_best) ob_best = c;
+        // the step's heaviest edge (lane 31; the row's last when it ends here)
+        const W w_last = __shfl_sync(kFullMask, w, min(31u, oe - 1 - eb));
+        if (!(lo + w_last < ob_best)) break;  // uniform: every lane holds the same values
+      }
+      if (lane == o) best = ob_best;
+    }
+    const bool improved = cand && best < d0;
+    if (improved) st_cg(P.dist + u, best);
+    const uint32_t im = __ballot_sync(kFullMask, improved);
+    if (lane == 0 && im) atomicOr(P.far + wi, im);
+  }
+}
 
 // The SSSP level loop: per iteration, push (compact the frontier, expand it
 // with atomicMin relaxations) or, when the frontier's out-degree is a large
@@ -113,17 +333,19 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
       if (!grid_sync(S.bar)) return 0;
       ns = ld_cg(&C->small_tail);
       bp = ld_cg(&C->big_packed);
-      SsspVisitor<W> v;
-      v.fb_next = fb_next;
-      v.dist = P.dist;
-      v.w = bucketed ? P.wval : P.w;
-      v.far = P.far;
-      v.ro = S.ro;
-      v.threshold = threshold;
-      v.bucketed = bucketed;
-      push_expand(R, bucketed ? P.wcol : S.col, S.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
-      n_new = v.n_new;
-      deg_new = v.deg_new;
+      SsspRelax<W> X;
+      X.dist = P.dist;
+      X.w = bucketed ? P.wval : P.w;
+      X.col = bucketed ? P.wcol : S.col;
+      X.far = P.far;
+      X.fb_next = fb_next;
+      X.ro = S.ro;
+      X.threshold = threshold;
+      X.bucketed = bucketed;
+      X.want_deg = !bucketed && P.pull_ratio;
+      sssp_expand(R, S.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, X);
+      n_new = X.n_new;
+      deg_new = X.deg_new;
     } else {
       sssp_pull_sweep(P.pull, fb_cur, fb_next, threshold, bucketed, n_new, deg_new, s_best);
     }
@@ -184,20 +406,45 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   // Near-far: vertices improved to a distance below the threshold stay in the
   // frontier, the others wait in the far set; when the near frontier is empty
   // the threshold moves up by delta (or to the far set's minimum) and the far
-  // vertices below it become the next frontier.  Every improved vertex is
-  // relaxed again before the end, so the fixed point is Bellman-Ford's.
+  // vertices below it become the next frontier.  Once half the vertices are
+  // settled and a refill leaves fewer than P.tail vertices in the far set, the
+  // next refill takes all of them and the rest runs as plain frontier
+  // Bellman-Ford (every edge, no far set): the last, sparse stretch of
+  // distances then costs a few iterations instead of one bucket per delta.  Every improved vertex is relaxed again before the
+  // end, so the fixed point is Bellman-Ford's.
   W threshold = P.delta;
+  W lo = W(0);  // the current bucket is [lo, threshold)
   unsigned long long total = 0;
   uint32_t pass = 0;
   PushLoop loop = P.L;
   unsigned long long fdeg0 = P.L.ro[src + 1] - P.L.ro[src];
+  bool near_far = bucketed;
+  unsigned long long far_left = ~0ull;  // far vertices the last refill left
+  unsigned long long settled = 0;       // vertices of finished buckets
+  uint32_t records = 0;                 // log entries written: iterations, heavy phases, refills
+  // one log entry for a heavy phase (strategy 4) or a refill pass (5)
+  auto log_phase = [&](uint32_t kind, uint64_t t0, unsigned long long size, unsigned long long next) {
+    if (P.L.log && gtid == 0 && records < kMaxLog) {
+      sg_level_record r = {};
+      r.level = records;
+      r.strategy = kind;
+      r.frontier_size = (uint32_t)size;
+      r.next_size = (uint32_t)next;
+      r.t_start_ns = t0;
+      r.t_end_ns = sygraph::detail::global_timer_ns();
+      P.L.log[records] = r;
+    }
+    records++;
+  };
   for (;;) {
-    loop.log_base = (uint32_t)min(total, (unsigned long long)kMaxLog);
-    const uint32_t levels = sssp_levels(P, loop, threshold, bucketed, fdeg0, s_scan, s_red, s_best);
+    loop.log_base = min(records, kMaxLog);
+    const uint32_t levels = sssp_levels(P, loop, threshold, near_far, fdeg0, s_scan, s_red, s_best);
     if (!levels) return;
     total += levels;
-    if (!bucketed) break;
+    records += levels;
+    if (!near_far) break;
     {
+      const uint64_t t0 = (P.L.log && gtid == 0) ? sygraph::detail::global_timer_ns() : 0;
       // heavy edges (w >= delta) of the bucket's vertices, relaxed once with
       // their final distances: they land at or beyond the threshold (far)
       Counters* Ch = P.L.cnt + (levels % 3);  // zeroed by the last level, unused since
@@ -206,17 +453,27 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       if (!grid_sync(P.L.bar)) return;
       const uint32_t ns = ld_cg(&Ch->small_tail);
       const unsigned long long bp = ld_cg(&Ch->big_packed);
-      SsspVisitor<W> v;
-      v.fb_next = P.L.fb + (size_t)((levels + 1) % 3) * w0;
-      v.dist = P.dist;
-      v.w = P.wval;
-      v.far = P.far;
-      v.ro = P.L.ro;
-      v.threshold = threshold;
-      v.bucketed = true;
-      push_expand(Rh, P.wcol, P.L.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, v);
-      for (uint32_t i = gtid; i < w0; i += nthreads) st_cg(P.bucket + i, 0u);
+      settled += ns + (uint32_t)(bp >> 32);
+      // pull when the push would relax a large share of the edges
+      const bool pull_heavy = P.heavy_pull && ld_cg(&Ch->frontier_deg) * P.heavy_pull > P.m;
+      if (pull_heavy) {
+        sssp_pull_heavy(P, lo, threshold);
+      } else {
+        SsspRelax<W> X;
+        X.dist = P.dist;
+        X.w = P.wval;
+        X.col = P.wcol;
+        X.far = P.far;
+        X.fb_next = P.L.fb + (size_t)((levels + 1) % 3) * w0;
+        X.ro = P.L.ro;
+        X.threshold = threshold;
+        X.bucketed = true;
+        X.want_deg = false;
+        sssp_expand(Rh, P.L.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, X);
+      }
+      // the bucket bitmap is cleared by the refill (the pull reads it until the barrier)
       if (!grid_sync(P.L.bar)) return;
+      log_phase(pull_heavy ? 6 : 4, t0, ns + (bp >> 32), 0);
     }
     bool refilled = false;
     for (;;) {
@@ -231,48 +488,62 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
         Counters z = {};
         P.L.cnt[gtid] = z;
       }
-      const W next_t = threshold + P.delta;
-      unsigned long long moved = 0, remaining = 0, mdeg = 0;
+      // (only once half the vertices are settled: early on the far set is
+      // small because little has been reached yet)
+      const bool tail = far_left < P.tail && 2 * settled >= n;
+      const uint64_t t0 = (P.L.log && gtid == 0) ? sygraph::detail::global_timer_ns() : 0;
+      const W next_t = tail ? max_weight<W>() : threshold + P.delta;
+      unsigned long long moved = 0, remaining = 0;
       uint32_t fmin = 0xffffffffu;
       for (uint32_t i = gtid; i < w0; i += nthreads) {
         const uint32_t f = ld_cg(P.far + i);
         uint32_t near = 0;
-        for (uint32_t b = f; b; b &= b - 1) {
-          const uint32_t bit = __ffs(b) - 1;
-          const W d = ld_cg(P.dist + i * 32 + bit);
-          if (d < next_t) {
-            near |= 1u << bit;
-            const uint32_t v = i * 32 + bit;
-            mdeg += P.L.ro[v + 1] - P.L.ro[v];
-          } else
-            fmin = min(fmin, order_bits<W>(d));
+        // the word's far distances, 16 loads in flight at a time
+#pragma unroll
+        for (uint32_t h = 0; h < 32; h += 16) {
+          const uint32_t fh = (f >> h) & 0xffffu;
+          if (!fh) continue;
+          W d[16];
+#pragma unroll
+          for (uint32_t k = 0; k < 16; k++) d[k] = ((fh >> k) & 1u) ? ld_cg(P.dist + i * 32 + h + k) : W(0);
+#pragma unroll
+          for (uint32_t k = 0; k < 16; k++) {
+            if (!((fh >> k) & 1u)) continue;
+            if (d[k] < next_t)
+              near |= 1u << (h + k);
+            else
+              fmin = min(fmin, order_bits<W>(d[k]));
+          }
         }
         st_cg(P.L.fb + i, near);
         st_cg(P.L.fb + w0 + i, 0u);
         st_cg(P.L.fb + 2 * w0 + i, 0u);
+        st_cg(P.bucket + i, 0u);
         if (f) st_cg(P.far + i, f & ~near);
         moved += __popc(near);
         remaining += __popc(f & ~near);
       }
       const unsigned long long mv = block_sum<unsigned long long>(moved, s_red);
       const unsigned long long rm = block_sum<unsigned long long>(remaining, s_red);
-      const unsigned long long md = block_sum<unsigned long long>(mdeg, s_red);
       fmin = sygraph::detail::warp_min(fmin);
       if ((threadIdx.x & 31) == 0 && fmin != 0xffffffffu) atomicMin(&R->far_min, fmin);
       if (threadIdx.x == 0) {
         if (mv) atomicAdd(&R->moved, mv);
         if (rm) atomicAdd(&R->remaining, rm);
-        if (md) atomicAdd(&R->moved_deg, md);
       }
       if (!grid_sync(P.L.bar)) return;
       pass++;
+      lo = threshold;
       threshold = next_t;
+      far_left = ld_cg(&R->remaining);
+      log_phase(5, t0, ld_cg(&R->moved), far_left);
+      if (tail) near_far = false;
       if (ld_cg(&R->moved)) {
-        fdeg0 = ld_cg(&R->moved_deg);
+        fdeg0 = 0;  // not summed: only a pull decision reads it, and pull is off with the light / heavy split
         refilled = true;
         break;
       }
-      if (!ld_cg(&R->remaining)) break;
+      if (!far_left) break;
       // nothing below the new threshold: jump to the far set's minimum
       const W m = from_order_bits<W>(ld_cg(&R->far_min));
       if (threshold < m) threshold = m;
@@ -282,6 +553,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   if (gtid == 0) {
     P.result[0] = total;
     P.result[1] = pass;
+    P.result[2] = records;
   }
 }
 
@@ -402,6 +674,8 @@ struct sg_sssp_s {
   double split_delta = -1.0;
   Refill* refill = nullptr;
   double delta = 0.0;  // near-far threshold step; 0 = the reference's frontier Bellman-Ford
+  double tail = 0.25;  // far-set fraction of n below which the rest runs as plain Bellman-Ford
+  uint32_t heavy_pull = 8;  // heavy phase by pull when its push would relax more than m / heavy_pull edges
   uint32_t pull_ratio = 0;  // pull iterations when frontier out-degree * ratio > m; 0 = push only
   uint32_t* heavy_v = nullptr;      // vertices of in-degree >= kPullHeavy
   uint32_t* heavy_first = nullptr;  // their first chunk index
@@ -475,6 +749,8 @@ static sg_status sssp_launch(sg_sssp s) {
     P.split = s->split;
     P.wcol = g->wcol;
     P.wval = (const float*)g->wval;
+    P.tail = (uint32_t)(s->tail * g->n);
+    P.heavy_pull = g->wsym ? s->heavy_pull : 0u;
     return launch_persistent(sssp_kernel<float>, P, 2, s->stream, s->max_ctas);
   }
   const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
@@ -487,6 +763,8 @@ static sg_status sssp_launch(sg_sssp s) {
   P.split = s->split;
   P.wcol = g->wcol;
   P.wval = (const uint32_t*)g->wval;
+  P.tail = (uint32_t)(s->tail * g->n);
+  P.heavy_pull = g->wsym ? s->heavy_pull : 0u;
   return launch_persistent(sssp_kernel<uint32_t>, P, 2, s->stream, s->max_ctas);
 }
 
@@ -591,8 +869,8 @@ extern "C" {
 sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count) {
   SG_REQUIRE(s && count, SG_ERR_INVALID, "NULL argument");
   SG_CUDA(cudaStreamSynchronize(s->stream));
-  unsigned long long it = 0;
-  SG_CUDA(cudaMemcpy(&it, s->ws.result, sizeof(it), cudaMemcpyDeviceToHost));
+  unsigned long long it = 0;  // log entries of the last run
+  SG_CUDA(cudaMemcpy(&it, s->ws.result + 2, sizeof(it), cudaMemcpyDeviceToHost));
   uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
   if (k > cap) k = cap;
   if (host_records && k) SG_CUDA(cudaMemcpy(host_records, s->log, sizeof(sg_level_record) * k, cudaMemcpyDeviceToHost));
@@ -606,6 +884,21 @@ sg_status sg_sssp_set_launch(sg_sssp s, void* stream, uint32_t max_ctas) {
   SG_CUDA(cudaStreamSynchronize(s->stream));
   s->stream = stream ? (cudaStream_t)stream : s->g->stream;
   s->max_ctas = max_ctas;
+  return SG_OK;
+}
+
+sg_status sg_sssp_set_heavy_pull(sg_sssp s, uint32_t ratio) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  s->heavy_pull = ratio;
+  return SG_OK;
+}
+
+sg_status sg_sssp_set_tail(sg_sssp s, double fraction) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  SG_REQUIRE(fraction >= 0.0 && fraction <= 1.0, SG_ERR_INVALID, "tail fraction must be in [0, 1]");
+  s->tail = fraction;
   return SG_OK;
 }
 

@@ -39,6 +39,15 @@ __device__ __forceinline__ W from_order_bits(uint32_t b) {
     return (W)b;
 }
 
+// A threshold above every distance (+inf for floats).
+template <typename W>
+__device__ __forceinline__ W max_weight() {
+  if constexpr (sizeof(W) == 4 && W(0.5) != W(0))
+    return __uint_as_float(0x7f800000u);
+  else
+    return (W)0xffffffffu;
+}
+
 template <typename W>
 __device__ __forceinline__ W warp_min_w(W x) {
 #pragma unroll

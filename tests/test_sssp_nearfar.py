@@ -42,11 +42,83 @@ def test_nearfar_u32_grid_and_unreachable(sg, oracle, delta):
     assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gd, 7))
 
 
+@pytest.mark.parametrize("tail", [0.0, 1 / 64, 0.25, 1.0])
+@pytest.mark.parametrize("delta", [0.02, 0.1])
+def test_nearfar_bellman_ford_tail(sg, oracle, rmat, delta, tail):
+    """Finishing with plain Bellman-Ford once the far set is small (any
+    fraction, including 1: as soon as half the vertices are settled) keeps
+    the distances; the log shows the buckets' heavy phases (push 4, pull 6)
+    and refills (5)."""
+    g = rmat(14, perm_seed=5)
+    s = sg.algorithms.SSSP(sg.graph.build.fromCSR(g))
+    s.set_delta(delta)
+    s.set_tail(tail)
+    for src in [int(x) for x in sg.io.sample_sources(g, 3, seed=6)]:
+        s.init(src)
+        it = s.run()
+        assert np.array_equal(s.getDistances().view(np.uint32), oracle.sssp_dijkstra(g, src).view(np.uint32))
+        kinds = [r["strategy"] for r in s.level_records()]
+        assert kinds.count(0) == it and (4 in kinds or 6 in kinds) and 5 in kinds
+    gg = sg.io.grid(64, 0.02, seed=2, weight_seed=3, value_type=sg.WEIGHT_U32)
+    s2 = sg.algorithms.SSSP(sg.graph.build.fromCSR(gg))
+    s2.set_delta(int(delta * 640))
+    s2.set_tail(tail)
+    s2.init(100)
+    s2.run()
+    assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gg, 100))
+
+
+@pytest.mark.parametrize("ratio", [0, 1, 8, 1 << 30])
+def test_nearfar_heavy_pull(sg, oracle, rmat, ratio):
+    """Heavy phases by pull (a bucket pulls when its heavy edges number more
+    than m / ratio: never at 0, every bucket with a heavy edge at 2^30) or by
+    push give the oracle's distances; graphs with asymmetric weights stay on
+    push."""
+    g = rmat(15, perm_seed=7)
+    s = sg.algorithms.SSSP(sg.graph.build.fromCSR(g))
+    s.set_heavy_pull(ratio)
+    for delta in (0.03, 0.2):
+        s.set_delta(delta)
+        for src in [int(x) for x in sg.io.sample_sources(g, 2, seed=8)]:
+            s.init(src)
+            s.run()
+            assert np.array_equal(s.getDistances().view(np.uint32), oracle.sssp_dijkstra(g, src).view(np.uint32))
+            kinds = {r["strategy"] for r in s.level_records()}
+            if ratio == 1 << 30:  # any bucket with a heavy edge pulls
+                assert 6 in kinds
+            if ratio == 0:
+                assert 6 not in kinds
+    gg = sg.io.grid(64, 0.02, seed=4, weight_seed=5, value_type=sg.WEIGHT_U32)
+    s2 = sg.algorithms.SSSP(sg.graph.build.fromCSR(gg))
+    s2.set_heavy_pull(ratio)
+    s2.set_delta(16)
+    s2.init(77)
+    s2.run()
+    assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gg, 77))
+    # asymmetric weights on an undirected-looking edge set: pull must not run
+    rng = np.random.default_rng(9)
+    n = 3000
+    a = rng.integers(0, n, 20000)
+    b = rng.integers(0, n, 20000)
+    w = (rng.integers(1, 1 << 24, 40000) / float(1 << 24)).astype(np.float32)
+    ga = sg.io.fromCOO(n, np.concatenate([a, b]), np.concatenate([b, a]), w, dedupe=True, drop_self_loops=True)
+    s3 = sg.algorithms.SSSP(sg.graph.build.fromCSR(ga, sg.Properties(directed=True, weighted=True)))
+    s3.set_heavy_pull(1 << 30)
+    s3.set_delta(0.05)
+    s3.init(1)
+    s3.run()
+    assert np.array_equal(s3.getDistances().view(np.uint32), oracle.sssp_dijkstra(ga, 1).view(np.uint32))
+    assert 6 not in {r["strategy"] for r in s3.level_records()}
+
+
 def test_nearfar_argument_checks_and_reset(sg, oracle, rmat):
     g = rmat(10)
     s = sg.algorithms.SSSP(sg.graph.build.fromCSR(g))
     with pytest.raises(sg._lib.SygraphError):
         s.set_delta(-1.0)
+    for bad in (-0.1, 1.5):
+        with pytest.raises(sg._lib.SygraphError):
+            s.set_tail(bad)
     s.set_delta(0.2)
     s.init(3)
     s.run()
