@@ -440,6 +440,11 @@ sg_status sg_sssp_set_tail(sg_sssp s, double fraction);
  * to the first weight that can no longer improve it.  Default 8; 0 always
  * pushes. */
 sg_status sg_sssp_set_heavy_pull(sg_sssp s, uint32_t ratio);
+/* Same graphs: an iteration of a bucket whose frontier holds more than
+ * n / ratio vertices relaxes the light edges by pull (each vertex scans the
+ * light prefix of its weight-sorted row, frontier neighbours only, up to the
+ * first weight that can no longer improve it).  Default 0 (always push). */
+sg_status sg_sssp_set_light_pull(sg_sssp s, uint32_t ratio);
 /* Pull iterations (not in the reference): an iteration whose frontier
  * out-degree times `ratio` exceeds the edge count runs as one pull sweep
  * (every vertex takes the minimum over its in-neighbours in the frontier, no

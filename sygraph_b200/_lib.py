@@ -184,6 +184,7 @@ SIGNATURES = {
     "sg_sssp_set_delta": (st, [vp, C.c_double]),
     "sg_sssp_set_tail": (st, [vp, C.c_double]),
     "sg_sssp_set_heavy_pull": (st, [vp, C.c_uint32]),
+    "sg_sssp_set_light_pull": (st, [vp, C.c_uint32]),
     "sg_sssp_set_pull": (st, [vp, C.c_uint32]),
     "sg_sssp_level_records": (st, [vp, C.POINTER(LevelRecord), C.c_uint32, u32p]),
     "sg_sssp_set_launch": (st, [vp, vp, C.c_uint32]),

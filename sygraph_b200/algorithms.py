@@ -217,6 +217,12 @@ class SSSP:
         pull when they number more than m / ratio (0: always push)."""
         call("sg_sssp_set_heavy_pull", self.handle, int(ratio))
 
+    def set_light_pull(self, ratio: int) -> None:
+        """Near-far on symmetric weighted graphs: an iteration whose frontier
+        holds more than n / ratio vertices relaxes light edges by pull (0:
+        always push)."""
+        call("sg_sssp_set_light_pull", self.handle, int(ratio))
+
     def getDistances(self) -> np.ndarray:
         dt = np.float32 if self.G.value_type == WEIGHT_F32 else np.uint32
         out = np.empty(self.G.getVertexCount(), dt)

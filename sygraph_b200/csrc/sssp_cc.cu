@@ -50,6 +50,9 @@ struct SsspParams {
   // heavy phase by pull when its push would relax more than m / heavy_pull
   // edges (0: always push); only where a row's out-edges are its in-edges
   uint32_t heavy_pull;
+  // light iteration by pull when its frontier holds more than n / light_pull
+  // vertices (0: always push); same condition on the graph
+  uint32_t light_pull;
 };
 
 // Edge relaxation of the SSSP push steps, kU edges per lane at a time: the
@@ -214,33 +217,49 @@ __device__ __forceinline__ void sssp_expand(RowRange R, Queues q, uint32_t n_sma
   }
 }
 
-// Heavy phase of the bucket [lo, threshold) by pull, for graphs whose rows
-// list in-edges as well as out-edges (undirected, symmetric weights): every
-// vertex u beyond the threshold takes the minimum over its neighbours c in
-// the bucket of d[c] + w.  An improvement can only come through an edge of
-// weight >= delta from a bucket vertex (its light edges were relaxed while
-// the bucket ran), and d[c] >= lo, so u's weight-sorted row is scanned from
-// the lightest edge and the scan stops at the first weight with lo + w >=
-// best (rounding is monotone: no later edge gives less).  u alone writes
-// d[u], so there are no atomics; improved vertices join the far set.  Lanes
-// scan their own rows kP edges per step; rows of kPullLong edges or more
-// are walked by the whole warp, 32 edges per step.
+// Pull steps of near-far bucketing, for graphs whose rows list in-edges as
+// well as out-edges (undirected, symmetric weights), over the bucket [lo,
+// threshold).  Every candidate vertex u takes the minimum of d[c] + w over
+// its neighbours c in a member bitmap, scanning its weight-sorted row from
+// the lightest edge; since d[c] >= lo for every member, the scan stops at the
+// first weight with lo + w >= best (rounding is monotone: no later edge
+// gives less).  u alone writes d[u]: no atomics on distances.
+//   heavy phase (kLight false): members = the bucket, candidates = vertices
+//     beyond the threshold, the whole row.  Only an edge of weight >= delta
+//     can improve u (the bucket's light edges were relaxed while it ran);
+//     improved vertices join the far set.
+//   light iteration (kLight true): members = the frontier, candidates =
+//     vertices above lo, the light prefix of the row (weights < delta);
+//     improved vertices join the next frontier below the threshold, the far
+//     set otherwise, and the frontier joins the bucket.  The frontier's own
+//     distances may drop during the sweep: any value read is an upper bound,
+//     and a vertex that dropped is in the next frontier, so its neighbours
+//     see the final value then.
+// Lanes scan their own rows kP edges per step; rows of kPullLong edges or
+// more are walked by the whole warp, 32 edges per step.
 constexpr uint32_t kP = 4;
 constexpr uint32_t kPullLong = 256;
 
-template <typename W>
-__device__ __forceinline__ void sssp_pull_heavy(const SsspParams<W>& P, W lo, W threshold) {
+template <typename W, bool kLight>
+__device__ __forceinline__ uint32_t sssp_pull_scan(const SsspParams<W>& P, const uint32_t* member, uint32_t* fb_next,
+                                                   W lo, W threshold) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t n = P.L.n, w0 = P.L.w0;
   const uint32_t* ro = P.L.ro;
+  uint32_t n_new = 0;
   for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+    if (kLight && lane == 0) {  // the frontier joins the bucket (its heavy edges wait)
+      const uint32_t fw = ld_cg(member + wi);
+      if (fw) st_cg(P.bucket + wi, ld_cg(P.bucket + wi) | fw);
+    }
     const uint32_t u = wi * 32 + lane;
     const W d0 = u < n ? ld_cg(P.dist + u) : W(0);
-    const bool cand = u < n && threshold < d0;
+    const bool cand = u < n && (kLight ? lo < d0 : threshold < d0);
     if (!__any_sync(kFullMask, cand)) continue;
-    const uint32_t beg = cand ? ro[u] : 0u, end = cand ? ro[u + 1] : 0u;
+    const uint32_t beg = cand ? ro[u] : 0u;
+    const uint32_t end = cand ? (kLight ? P.split[u] : ro[u + 1]) : 0u;
     const bool is_long = end - beg >= kPullLong;
     W best = d0;
     uint32_t e = beg;
@@ -258,7 +277,7 @@ __device__ __forceinline__ void sssp_pull_heavy(const SsspParams<W>& P, W lo, W 
           inb[k] = ok;
         }
 #pragma unroll
-        for (uint32_t k = 0; k < kP; k++) inb[k] = inb[k] && lo + wv[k] < best && bit_test_ro(P.bucket, cv[k]);
+        for (uint32_t k = 0; k < kP; k++) inb[k] = inb[k] && lo + wv[k] < best && bit_test_ro(member, cv[k]);
 #pragma unroll
         for (uint32_t k = 0; k < kP; k++) dc[k] = inb[k] ? ld_cg(P.dist + cv[k]) : W(0);
 #pragma unroll
@@ -282,7 +301,7 @@ __device__ __forceinline__ void sssp_pull_heavy(const SsspParams<W>& P, W lo, W 
         W c = max_weight<W>();
         if (x < oe && lo + w < ob_best) {
           const uint32_t cc = P.wcol[x];
-          if (bit_test_ro(P.bucket, cc)) c = ld_cg(P.dist + cc) + w;
+          if (bit_test_ro(member, cc)) c = ld_cg(P.dist + cc) + w;
         }
         c = warp_min_w(c);
         if (c < ob_best) ob_best = c;
@@ -294,9 +313,18 @@ __device__ __forceinline__ void sssp_pull_heavy(const SsspParams<W>& P, W lo, W 
     }
     const bool improved = cand && best < d0;
     if (improved) st_cg(P.dist + u, best);
-    const uint32_t im = __ballot_sync(kFullMask, improved);
-    if (lane == 0 && im) atomicOr(P.far + wi, im);
+    const bool near = kLight && improved && best < threshold;
+    const uint32_t fm = __ballot_sync(kFullMask, improved && !near);
+    const uint32_t nm = __ballot_sync(kFullMask, near);
+    if (lane == 0) {
+      if (fm) atomicOr(P.far + wi, fm);
+      if (nm) {
+        st_cg(fb_next + wi, nm);  // cleared before this step; this warp is its only writer
+        n_new += __popc(nm);
+      }
+    }
   }
+  return n_new;
 }
 
 // The SSSP level loop: per iteration, push (compact the frontier, expand it
@@ -304,9 +332,9 @@ __device__ __forceinline__ void sssp_pull_heavy(const SsspParams<W>& P, W lo, W 
 // part of the edges, one pull sweep.  Returns the number of iterations, or 0
 // when a barrier timed out.  `fdeg0` is the out-degree of the first frontier.
 template <typename W>
-__device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const PushLoop& S, W threshold, bool bucketed,
-                                                unsigned long long fdeg0, uint32_t* s_scan, unsigned long long* s_red,
-                                                uint32_t* s_best) {
+__device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const PushLoop& S, W lo, W threshold,
+                                                bool bucketed, unsigned long long fdeg0, unsigned long long fsize0,
+                                                uint32_t* s_scan, unsigned long long* s_red, uint32_t* s_best) {
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
   for (uint32_t level = 0;; level++) {
@@ -316,6 +344,7 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
     uint32_t* fb_next = S.fb + (size_t)((level + 1) % 3) * S.w0;
     uint32_t* fb_zero = S.fb + (size_t)((level + 2) % 3) * S.w0;
     const unsigned long long fdeg = level ? ld_cg(&Cprev->new_deg) : fdeg0;
+    const unsigned long long fsize = level ? ld_cg(&Cprev->new_count) : fsize0;
     if (gtid == 0) {
       Counters z = {};
       S.cnt[(level + 1) % 3] = z;
@@ -323,10 +352,14 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
     const uint64_t t0 = (S.log && gtid == 0) ? sygraph::detail::global_timer_ns() : 0;
     // pull sweeps relax every edge: not with the light / heavy split
     const bool pull = !bucketed && P.pull_ratio && fdeg * P.pull_ratio > P.m;
+    // a large frontier of a bucket: its light edges by pull, one barrier
+    const bool pull_light = bucketed && P.light_pull && fsize * P.light_pull > S.n;
     unsigned long long n_new = 0, deg_new = 0;
     uint32_t ns = 0;
     unsigned long long bp = 0;
-    if (!pull) {
+    if (pull_light) {
+      n_new = sssp_pull_scan<W, true>(P, fb_cur, fb_next, lo, threshold);
+    } else if (!pull) {
       // bucketed: light edges only, the prefix of each weight-sorted row
       const RowRange R = bucketed ? RowRange{S.ro, P.split, 0} : RowRange{S.ro, S.ro, 1};
       compact_frontier(fb_cur, S.w0, R, C, S.q, s_scan, bucketed ? P.bucket : nullptr);
@@ -360,8 +393,8 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
     if (S.log && gtid == 0 && S.log_base + level < kMaxLog) {
       sg_level_record r = {};
       r.level = S.log_base + level;
-      r.strategy = pull ? 2u : 0u;
-      r.frontier_size = pull ? 0u : ns + (uint32_t)(bp >> 32);
+      r.strategy = (pull || pull_light) ? 2u : 0u;
+      r.frontier_size = pull ? 0u : pull_light ? (uint32_t)fsize : ns + (uint32_t)(bp >> 32);
       r.frontier_degree = fdeg;
       r.next_size = (uint32_t)ld_cg(&C->new_count);
       r.t_start_ns = t0;
@@ -418,6 +451,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   uint32_t pass = 0;
   PushLoop loop = P.L;
   unsigned long long fdeg0 = P.L.ro[src + 1] - P.L.ro[src];
+  unsigned long long fsize0 = 1;  // vertices of the first frontier of the next bucket
   bool near_far = bucketed;
   unsigned long long far_left = ~0ull;  // far vertices the last refill left
   unsigned long long settled = 0;       // vertices of finished buckets
@@ -438,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   };
   for (;;) {
     loop.log_base = min(records, kMaxLog);
-    const uint32_t levels = sssp_levels(P, loop, threshold, near_far, fdeg0, s_scan, s_red, s_best);
+    const uint32_t levels = sssp_levels(P, loop, lo, threshold, near_far, fdeg0, fsize0, s_scan, s_red, s_best);
     if (!levels) return;
     total += levels;
     records += levels;
@@ -457,7 +491,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       // pull when the push would relax a large share of the edges
       const bool pull_heavy = P.heavy_pull && ld_cg(&Ch->frontier_deg) * P.heavy_pull > P.m;
       if (pull_heavy) {
-        sssp_pull_heavy(P, lo, threshold);
+        sssp_pull_scan<W, false>(P, P.bucket, nullptr, lo, threshold);
       } else {
         SsspRelax<W> X;
         X.dist = P.dist;
@@ -540,6 +574,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       if (tail) near_far = false;
       if (ld_cg(&R->moved)) {
         fdeg0 = 0;  // not summed: only a pull decision reads it, and pull is off with the light / heavy split
+        fsize0 = ld_cg(&R->moved);
         refilled = true;
         break;
       }
@@ -676,6 +711,10 @@ struct sg_sssp_s {
   double delta = 0.0;  // near-far threshold step; 0 = the reference's frontier Bellman-Ford
   double tail = 0.25;  // far-set fraction of n below which the rest runs as plain Bellman-Ford
   uint32_t heavy_pull = 8;  // heavy phase by pull when its push would relax more than m / heavy_pull edges
+  // light iteration by pull when its frontier holds more than n / light_pull
+  // vertices; off by default: on RMAT-22 the warps holding the low-id hubs'
+  // long light prefixes made each pull iteration take milliseconds
+  uint32_t light_pull = 0;
   uint32_t pull_ratio = 0;  // pull iterations when frontier out-degree * ratio > m; 0 = push only
   uint32_t* heavy_v = nullptr;      // vertices of in-degree >= kPullHeavy
   uint32_t* heavy_first = nullptr;  // their first chunk index
@@ -751,6 +790,7 @@ static sg_status sssp_launch(sg_sssp s) {
     P.wval = (const float*)g->wval;
     P.tail = (uint32_t)(s->tail * g->n);
     P.heavy_pull = g->wsym ? s->heavy_pull : 0u;
+    P.light_pull = g->wsym ? s->light_pull : 0u;
     return launch_persistent(sssp_kernel<float>, P, 2, s->stream, s->max_ctas);
   }
   const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
@@ -765,6 +805,7 @@ static sg_status sssp_launch(sg_sssp s) {
   P.wval = (const uint32_t*)g->wval;
   P.tail = (uint32_t)(s->tail * g->n);
   P.heavy_pull = g->wsym ? s->heavy_pull : 0u;
+  P.light_pull = g->wsym ? s->light_pull : 0u;
   return launch_persistent(sssp_kernel<uint32_t>, P, 2, s->stream, s->max_ctas);
 }
 
@@ -891,6 +932,13 @@ sg_status sg_sssp_set_heavy_pull(sg_sssp s, uint32_t ratio) {
   clear_error();
   SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
   s->heavy_pull = ratio;
+  return SG_OK;
+}
+
+sg_status sg_sssp_set_light_pull(sg_sssp s, uint32_t ratio) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  s->light_pull = ratio;
   return SG_OK;
 }
 

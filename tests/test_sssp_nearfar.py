@@ -58,7 +58,7 @@ def test_nearfar_bellman_ford_tail(sg, oracle, rmat, delta, tail):
         it = s.run()
         assert np.array_equal(s.getDistances().view(np.uint32), oracle.sssp_dijkstra(g, src).view(np.uint32))
         kinds = [r["strategy"] for r in s.level_records()]
-        assert kinds.count(0) == it and (4 in kinds or 6 in kinds) and 5 in kinds
+        assert kinds.count(0) + kinds.count(2) == it and (4 in kinds or 6 in kinds) and 5 in kinds
     gg = sg.io.grid(64, 0.02, seed=2, weight_seed=3, value_type=sg.WEIGHT_U32)
     s2 = sg.algorithms.SSSP(sg.graph.build.fromCSR(gg))
     s2.set_delta(int(delta * 640))
@@ -68,15 +68,18 @@ def test_nearfar_bellman_ford_tail(sg, oracle, rmat, delta, tail):
     assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gg, 100))
 
 
+@pytest.mark.parametrize("light", [0, 16, 1 << 30])
 @pytest.mark.parametrize("ratio", [0, 1, 8, 1 << 30])
-def test_nearfar_heavy_pull(sg, oracle, rmat, ratio):
+def test_nearfar_heavy_pull(sg, oracle, rmat, ratio, light):
     """Heavy phases by pull (a bucket pulls when its heavy edges number more
     than m / ratio: never at 0, every bucket with a heavy edge at 2^30) or by
-    push give the oracle's distances; graphs with asymmetric weights stay on
+    push, and light iterations by pull (frontier above n / light) or push,
+    give the oracle's distances; graphs with asymmetric weights stay on
     push."""
     g = rmat(15, perm_seed=7)
     s = sg.algorithms.SSSP(sg.graph.build.fromCSR(g))
     s.set_heavy_pull(ratio)
+    s.set_light_pull(light)
     for delta in (0.03, 0.2):
         s.set_delta(delta)
         for src in [int(x) for x in sg.io.sample_sources(g, 2, seed=8)]:
@@ -88,9 +91,14 @@ def test_nearfar_heavy_pull(sg, oracle, rmat, ratio):
                 assert 6 in kinds
             if ratio == 0:
                 assert 6 not in kinds
+            if light == 1 << 30:  # every bucket iteration pulls
+                assert 2 in kinds
+            if light == 0:
+                assert 2 not in kinds
     gg = sg.io.grid(64, 0.02, seed=4, weight_seed=5, value_type=sg.WEIGHT_U32)
     s2 = sg.algorithms.SSSP(sg.graph.build.fromCSR(gg))
     s2.set_heavy_pull(ratio)
+    s2.set_light_pull(light)
     s2.set_delta(16)
     s2.init(77)
     s2.run()
@@ -104,11 +112,12 @@ def test_nearfar_heavy_pull(sg, oracle, rmat, ratio):
     ga = sg.io.fromCOO(n, np.concatenate([a, b]), np.concatenate([b, a]), w, dedupe=True, drop_self_loops=True)
     s3 = sg.algorithms.SSSP(sg.graph.build.fromCSR(ga, sg.Properties(directed=True, weighted=True)))
     s3.set_heavy_pull(1 << 30)
+    s3.set_light_pull(1 << 30)
     s3.set_delta(0.05)
     s3.init(1)
     s3.run()
     assert np.array_equal(s3.getDistances().view(np.uint32), oracle.sssp_dijkstra(ga, 1).view(np.uint32))
-    assert 6 not in {r["strategy"] for r in s3.level_records()}
+    assert not {2, 6} & {r["strategy"] for r in s3.level_records()}
 
 
 def test_nearfar_argument_checks_and_reset(sg, oracle, rmat):
