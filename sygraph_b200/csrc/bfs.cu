@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     if (P.mode == kLearned) strategy = d;
   }
 
+  const bool want_words = (P.mode == kLearned && P.mlp) || P.features;
   uint32_t level = 0;
   for (;; level++) {
     if (P.schedule && level < P.schedule_len && P.schedule[level] >= 0) strategy = P.schedule[level];
@@ -100,7 +101,8 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     const uint64_t t0 = gtid == 0 ? sygraph::detail::global_timer_ns() : 0;
 
     Level L{&P, &S, C, P.fb + (size_t)((level + 1) % 3) * w0, P.sm + (size_t)((level + 1) % 3) * w1,
-            P.heavy_v + (size_t)(par ^ 1) * P.heavy_cap, P.heavy_s + (size_t)(par ^ 1) * P.heavy_cap, level + 1};
+            P.heavy_v + (size_t)(par ^ 1) * P.heavy_cap, P.heavy_s + (size_t)(par ^ 1) * P.heavy_cap, level + 1,
+            want_words, frontier_deg < kDirectClaimDeg};
     if (strategy < 2) {
       n_push++;
       const uint32_t n_heavy = (uint32_t)(heavy_packed >> 32), n_chunks = (uint32_t)heavy_packed;

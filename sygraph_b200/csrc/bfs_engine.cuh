@@ -19,6 +19,7 @@ constexpr uint32_t kHeavy = 256;      // degree from which a vertex is expanded 
 constexpr uint32_t kHeavyBuf = 1024;  // per-CTA staging of newly discovered heavy vertices
 constexpr uint32_t kBfsChunk = 64;    // edges per heavy-vertex chunk (one warp, two steps)
 constexpr int kLearned = 3;           // mode: the MLP picks each level's strategy
+constexpr unsigned long long kDirectClaimDeg = 1u << 16;  // push frontier degree below which claims skip the pre-load
 // Two 512-thread CTAs per SM, as the other engines: one 1024-thread CTA per SM
 // halves the barrier arrivals but was within 1% on RMAT-22, and whole-SM CTAs
 // cannot share SMs with the half-SM CTAs of concurrent launches (serving).
@@ -93,6 +94,12 @@ struct Level {
   uint32_t* hv_next;
   uint32_t* hs_next;
   uint32_t next_depth;
+  // count the next frontier's non-zero bitmap and summary words (selector
+  // features): only then do the bitmap atomics wait for their old values
+  bool want_words;
+  // claim without the plain pre-load (small frontiers: their neighbours are
+  // mostly unvisited, and the load would add a round trip to each discovery)
+  bool direct_claim;
   uint32_t n_new = 0, wnz = 0, snz = 0;
   unsigned long long deg_new = 0;
 
@@ -114,13 +121,26 @@ struct Level {
     deg_new += du;
     if (du >= kHeavy) add_heavy(u, du);
   }
-  // push: claim u through the visited bitmap
+  // push: claim u through the visited bitmap (on large frontiers a plain
+  // load first skips the atomic when u is visibly visited); u's row offsets
+  // are loaded together
+  // with the claiming atomic, so a discovery waits one round trip, not two
   __device__ __forceinline__ void visit_push(uint32_t u) {
-    if (!sygraph::detail::bit_set_once(P->visited, u)) return;
-    const uint32_t du = P->ro[u + 1] - P->ro[u];
-    if (atomicOr(fb_next + (u >> 5), 1u << (u & 31)) == 0) {
-      wnz++;
-      if (atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31)) == 0) snz++;
+    const uint32_t bit = 1u << (u & 31);
+    uint32_t* vword = P->visited + (u >> 5);
+    if (!direct_claim && (ld_cg(vword) & bit)) return;
+    const uint32_t old = atomicOr(vword, bit);
+    const uint32_t r0 = P->ro[u], r1 = P->ro[u + 1];
+    if (old & bit) return;
+    const uint32_t du = r1 - r0;
+    if (want_words) {
+      if (atomicOr(fb_next + (u >> 5), 1u << (u & 31)) == 0) {
+        wnz++;
+        if (atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31)) == 0) snz++;
+      }
+    } else {  // results unused: fire-and-forget reductions
+      atomicOr(fb_next + (u >> 5), 1u << (u & 31));
+      atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31));
     }
     discovered(u, du);
   }
@@ -129,7 +149,11 @@ struct Level {
     st_cg(P->visited + wi, vw | fmask);
     st_cg(fb_next + wi, fmask);
     wnz++;
-    if (atomicOr(sm_next + (wi >> 5), 1u << (wi & 31)) == 0) snz++;
+    if (want_words) {
+      if (atomicOr(sm_next + (wi >> 5), 1u << (wi & 31)) == 0) snz++;
+    } else {
+      atomicOr(sm_next + (wi >> 5), 1u << (wi & 31));
+    }
   }
 };
 

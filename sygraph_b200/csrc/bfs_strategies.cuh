@@ -155,62 +155,58 @@ __device__ __forceinline__ uint32_t probe_pos(uint32_t beg, uint32_t end, uint32
   return reverse ? end - 1 - k : beg + k;
 }
 
-// Rest of a short-circuit pull of word wi after its first probe: unresolved
-// lanes probe the next in-neighbours serially (next column index loaded while
-// the current bit is tested) up to kPullSerial, the warp scans longer lists
-// together; then the word's new vertices are published.
-__device__ __forceinline__ void pull_word_finish(Level& L, const uint32_t* fb_cur, uint32_t wi, uint32_t vw, bool mine,
-                                                 uint32_t v, uint32_t beg, uint32_t end, bool found, bool reverse) {
-  const Params& P = *L.P;
+// Short-circuit pull of the still-open lists of one bitmap word, after the
+// serial probes: the lanes' remaining in-neighbours are ranked across the
+// warp and scanned kPullWin windows of 32 at a time (coalesced column loads,
+// then the frontier tests); a hit marks its owner (one warp OR-reduction per
+// window batch), edges of owners already found are not loaded, and the scan
+// ends once every open list has a hit.  Returns this lane's result.
+__device__ __forceinline__ bool pull_word_scan(const Params& P, const uint32_t* fb_cur, bool open, uint32_t b,
+                                               uint32_t e, bool reverse) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t deg = end - beg;
-  const uint32_t lim = min(deg, kPullSerial);
-  if (mine && !found && lim > 1) {
-    uint32_t k = 1;
-    uint32_t c = P.icol[probe_pos(beg, end, k, reverse)];
-    for (;;) {
-      const uint32_t cn = k + 1 < lim ? P.icol[probe_pos(beg, end, k + 1, reverse)] : 0u;
-      if (bit_test_ro(fb_cur, c)) {
-        found = true;
-        break;
-      }
-      if (++k >= lim) break;
-      c = cn;
+  const uint32_t rem = open ? e - b - kPullProbes : 0u;  // open: more than kPullProbes in-neighbours
+  const uint32_t incl = warp_inclusive_scan(rem);
+  const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+  const uint32_t excl = incl - rem;
+  const uint32_t need = __ballot_sync(kFullMask, open);
+  uint32_t hitm = 0;
+  for (uint32_t r0 = 0; r0 < total; r0 += 32 * kPullWin) {
+    uint32_t col[kPullWin], own[kPullWin];
+    bool act[kPullWin];
+#pragma unroll
+    for (int k = 0; k < kPullWin; k++) {
+      const uint32_t r = r0 + k * 32 + lane;
+      const bool in = r < total;
+      const uint32_t o = warp_owner_of_rank(incl, in ? r : total - 1);
+      const uint32_t ob = __shfl_sync(kFullMask, b, o);
+      const uint32_t oe = __shfl_sync(kFullMask, e, o);
+      const uint32_t ox = __shfl_sync(kFullMask, excl, o);
+      own[k] = o;
+      act[k] = in && !((hitm >> o) & 1u);
+      col[k] = act[k] ? P.icol[probe_pos(ob, oe, kPullProbes + (r - ox), reverse)] : 0u;
     }
+    uint32_t bits = 0;
+#pragma unroll
+    for (int k = 0; k < kPullWin; k++)
+      if (act[k] && bit_test_ro(fb_cur, col[k])) bits |= 1u << own[k];
+    hitm |= __reduce_or_sync(kFullMask, bits);
+    if ((hitm & need) == need) break;
   }
-  uint32_t left = __ballot_sync(kFullMask, mine && !found && lim < deg);
-  while (left) {
-    const uint32_t j = __ffs(left) - 1;
-    left &= left - 1;
-    const uint32_t jb = __shfl_sync(kFullMask, beg, j);
-    const uint32_t je = __shfl_sync(kFullMask, end, j);
-    bool hit = false;
-    for (uint32_t kb = kPullSerial; kb < je - jb; kb += 32) {
-      const uint32_t kk = kb + lane;
-      const bool h = kk < je - jb && bit_test_ro(fb_cur, P.icol[probe_pos(jb, je, kk, reverse)]);
-      if (__any_sync(kFullMask, h)) {
-        hit = true;
-        break;
-      }
-    }
-    if (lane == j) found = hit;
-  }
-  const uint32_t fmask = __ballot_sync(kFullMask, found);
-  if (fmask) {
-    if (found) L.discovered(v, P.iro == P.ro ? deg : (P.ro[v + 1] - P.ro[v]));
-    if (lane == 0) L.publish_word(wi, vw, fmask);
-  }
+  return (hitm >> lane) & 1u;
 }
 
-// Short-circuit pull, U bitmap words per warp step: the candidates and first
-// probes of all U words are issued before any word is finished, so U x 32
-// first-neighbour loads are in flight per warp.
+// Short-circuit pull, U bitmap words per warp step.  Every candidate first
+// probes up to kPullProbes in-neighbours serially, the probes of all U words
+// issued together (U column loads in flight per lane); vertices still open
+// after that (mostly those with no frontier neighbour at all, whose whole
+// list must be read) are finished edge-parallel, word by word.
 template <int U>
 __device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, bool reverse) {
   const Params& P = *L.P;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool same = P.iro == P.ro;
   for (uint32_t wbase = gwarp; wbase < P.w0; wbase += U * nwarps) {
     uint32_t vw[U], cd[U], b[U], e[U];
     bool f[U];
@@ -229,17 +225,36 @@ __device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, boo
       const bool m = (cd[k] >> lane) & 1u;
       b[k] = m ? P.iro[v] : 0u;
       e[k] = m ? P.iro[v + 1] : 0u;
+      f[k] = false;
     }
-    uint32_t x[U];
+    for (uint32_t j = 0; j < kPullProbes; j++) {
+      uint32_t x[U];
+      bool a[U];
 #pragma unroll
-    for (int k = 0; k < U; k++) x[k] = e[k] > b[k] ? P.icol[probe_pos(b[k], e[k], 0, reverse)] : 0u;
+      for (int k = 0; k < U; k++) {
+        a[k] = !f[k] && b[k] + j < e[k];
+        x[k] = a[k] ? P.icol[probe_pos(b[k], e[k], j, reverse)] : 0u;
+      }
+      bool more = false;
 #pragma unroll
-    for (int k = 0; k < U; k++) f[k] = e[k] > b[k] && bit_test_ro(fb_cur, x[k]);
+      for (int k = 0; k < U; k++) {
+        if (a[k]) f[k] = bit_test_ro(fb_cur, x[k]);
+        more |= !f[k] && b[k] + j + 1 < e[k];
+      }
+      if (!__any_sync(kFullMask, more)) break;
+    }
 #pragma unroll
     for (int k = 0; k < U; k++) {
-      if (!cd[k]) continue;
+      if (!cd[k]) continue;  // uniform
       const uint32_t w = wbase + k * nwarps;
-      pull_word_finish(L, fb_cur, w, vw[k], (cd[k] >> lane) & 1u, w * 32 + lane, b[k], e[k], f[k], reverse);
+      const bool open = !f[k] && e[k] - b[k] > kPullProbes;
+      if (__any_sync(kFullMask, open)) f[k] = pull_word_scan(P, fb_cur, open, b[k], e[k], reverse) || f[k];
+      const uint32_t fmask = __ballot_sync(kFullMask, f[k]);
+      if (fmask) {
+        const uint32_t v = w * 32 + lane;
+        if (f[k]) L.discovered(v, same ? e[k] - b[k] : (P.ro[v + 1] - P.ro[v]));
+        if (lane == 0) L.publish_word(w, vw[k], fmask);
+      }
     }
   }
 }

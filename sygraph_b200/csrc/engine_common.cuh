@@ -26,7 +26,9 @@ using sygraph::detail::warp_owner_of_rank;
 constexpr uint32_t kThreads = 512;     // threads per engine CTA
 constexpr uint32_t kSmallDeg = 64;     // degree below which a vertex joins a 32-vertex warp group
 constexpr uint32_t kChunk = 256;       // edges per work chunk of a high-degree vertex (one warp)
-constexpr uint32_t kPullSerial = 32;   // edges a pull lane scans alone before the warp helps
+constexpr uint32_t kPullSerial = 32;   // edges a pull lane scans alone before the warp helps (per-source BC)
+constexpr uint32_t kPullProbes = 8;    // in-neighbours a BFS pull lane probes alone before the warp scans the rest
+constexpr int kPullWin = 4;            // 32-edge windows in flight in a warp's edge-parallel pull scan
 constexpr uint32_t kMaxLog = SG_MAX_LOGGED_LEVELS;
 
 // Per-level counters, three rotating slots (a slot is reset two levels
