@@ -144,6 +144,45 @@ struct Level {
     }
     discovered(u, du);
   }
+  // push of K candidate targets at once (bit k of `act`: u[k] is valid): the
+  // pre-loads, then the claiming atomics with the row offsets, of all K go
+  // out together, so K edges cost the round trips of one
+  template <int K>
+  __device__ __forceinline__ void visit_push_n(const uint32_t (&u)[K], uint32_t act) {
+    if (!direct_claim) {
+      uint32_t w[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) w[k] = ((act >> k) & 1u) ? ld_cg(P->visited + (u[k] >> 5)) : 0u;
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        if ((w[k] >> (u[k] & 31)) & 1u) act &= ~(1u << k);
+    }
+    uint32_t old[K], r0[K], r1[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      old[k] = 0xffffffffu;
+      r0[k] = r1[k] = 0;
+      if ((act >> k) & 1u) {
+        old[k] = atomicOr(P->visited + (u[k] >> 5), 1u << (u[k] & 31));
+        r0[k] = P->ro[u[k]];
+        r1[k] = P->ro[u[k] + 1];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if ((old[k] >> (u[k] & 31)) & 1u) continue;
+      if (want_words) {
+        if (atomicOr(fb_next + (u[k] >> 5), 1u << (u[k] & 31)) == 0) {
+          wnz++;
+          if (atomicOr(sm_next + (u[k] >> 10), 1u << ((u[k] >> 5) & 31)) == 0) snz++;
+        }
+      } else {
+        atomicOr(fb_next + (u[k] >> 5), 1u << (u[k] & 31));
+        atomicOr(sm_next + (u[k] >> 10), 1u << ((u[k] >> 5) & 31));
+      }
+      discovered(u[k], r1[k] - r0[k]);
+    }
+  }
   // pull: a warp publishes the vertices of word wi it found (lane 0 calls)
   __device__ __forceinline__ void publish_word(uint32_t wi, uint32_t vw, uint32_t fmask) {
     st_cg(P->visited + wi, vw | fmask);

@@ -38,13 +38,19 @@ __device__ __forceinline__ void expand_group(Level& L, uint32_t beg, uint32_t de
   const uint32_t incl = warp_inclusive_scan(deg);
   const uint32_t total = __shfl_sync(kFullMask, incl, 31);
   const uint32_t excl = incl - deg;
-  for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-    const uint32_t r = r0 + lane;
-    const bool act = r < total;
-    const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
-    const uint32_t ob = __shfl_sync(kFullMask, beg, o);
-    const uint32_t oe = __shfl_sync(kFullMask, excl, o);
-    if (act) L.visit_push(L.P->col[ob + (r - oe)]);
+  for (uint32_t r0 = 0; r0 < total; r0 += 64) {
+    uint32_t u[2], act = 0;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const uint32_t r = r0 + k * 32 + lane;
+      const bool a = r < total;
+      const uint32_t o = warp_owner_of_rank(incl, a ? r : total - 1);
+      const uint32_t ob = __shfl_sync(kFullMask, beg, o);
+      const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+      u[k] = a ? L.P->col[ob + (r - oe)] : 0u;
+      act |= (uint32_t)a << k;
+    }
+    L.visit_push_n<2>(u, act);
   }
 }
 
@@ -58,14 +64,20 @@ __device__ __forceinline__ void push_heavy(Level& L, const uint32_t* hv, const u
   for (uint32_t unit = gwarp; unit < units_end; unit += nwarps) {
     if (unit < first_unit) continue;
     const uint32_t c = unit - first_unit;
-    const uint32_t ent = find_chunk_owner(hs, n_heavy, c);
+    const uint32_t ent = warp_find_owner(hs, n_heavy, c);
     const uint32_t v = ld_cg(hv + ent);
     const uint32_t first = ld_cg(hs + ent);
     const uint32_t cb = P.ro[v] + (c - first) * kBfsChunk;
     const uint32_t ce = min(P.ro[v + 1], cb + kBfsChunk);
-    for (uint32_t eb = cb; eb < ce; eb += 32) {
-      const uint32_t e = eb + lane;
-      if (e < ce) L.visit_push(P.col[e]);
+    for (uint32_t eb = cb; eb < ce; eb += 64) {
+      uint32_t u[2], act = 0;
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const uint32_t e = eb + k * 32 + lane;
+        u[k] = e < ce ? P.col[e] : 0u;
+        act |= (uint32_t)(e < ce) << k;
+      }
+      L.visit_push_n<2>(u, act);
     }
   }
   (void)n_chunks;

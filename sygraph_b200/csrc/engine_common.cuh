@@ -177,6 +177,23 @@ __device__ __forceinline__ uint32_t find_chunk_owner(const uint32_t* big_start, 
   return lo;
 }
 
+// Last entry of the increasing list start[0, n) that is <= c (start[0] <=
+// c): a warp-wide 32-ary search, one load per lane per round (one round for
+// up to 32 entries).  Called by the whole warp.
+__device__ __forceinline__ uint32_t warp_find_owner(const uint32_t* start, uint32_t n, uint32_t c) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t step = (hi - lo + 31) / 32;
+    const uint32_t idx = lo + lane * step;
+    const bool le = idx < hi && ld_cg(start + idx) <= c;
+    const uint32_t m = __ballot_sync(kFullMask, le);  // a prefix of the lanes; lane 0 always
+    lo += (31 - __clz(m)) * step;
+    hi = min(hi, lo + step);
+  }
+  return lo;
+}
+
 // Degree-bucketed push expansion over the queues of one frontier.  Work units
 // are 32-vertex groups of small vertices (edge-parallel inside the warp by a
 // shuffle scan) and kChunk-edge chunks of big vertices; warps take units

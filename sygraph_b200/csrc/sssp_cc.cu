@@ -123,23 +123,6 @@ struct SsspRelax {
   }
 };
 
-// Last entry of the increasing list big_start[0, n) that is <= c (the list
-// starts at 0): a warp-wide 32-ary search, one load per lane per round.
-__device__ __forceinline__ uint32_t warp_find_chunk_owner(const uint32_t* big_start, uint32_t n, uint32_t c) {
-  const uint32_t lane = threadIdx.x & 31;
-  uint32_t lo = 0, hi = n;
-  while (hi - lo > 1) {
-    const uint32_t step = (hi - lo + 31) / 32;
-    const uint32_t idx = lo + lane * step;
-    const bool le = idx < hi && ld_cg(big_start + idx) <= c;
-    const uint32_t m = __ballot_sync(kFullMask, le);  // a prefix of the lanes; lane 0 always
-    const uint32_t k = 31 - __clz(m);
-    lo += k * step;
-    hi = min(hi, lo + step);
-  }
-  return lo;
-}
-
 // Push expansion of one SSSP step over the compacted queues.  Small vertices
 // (row range < kSmallDeg) go 32 per warp, their edges ranked across the warp;
 // big vertices are cut in kChunk-edge chunks, and each warp takes a
@@ -184,7 +167,7 @@ __device__ __forceinline__ void sssp_expand(RowRange R, Queues q, uint32_t n_sma
   const uint32_t c_lo = gwarp * per;
   const uint32_t c_hi = min(n_chunks, c_lo + per);
   if (c_lo >= c_hi) return;
-  uint32_t ent = warp_find_chunk_owner(q.big_start, n_big, c_lo);
+  uint32_t ent = warp_find_owner(q.big_start, n_big, c_lo);
   uint32_t v = ld_cg(q.big + ent);
   uint32_t first = ld_cg(q.big_start + ent);
   uint32_t next = ent + 1 < n_big ? ld_cg(q.big_start + ent + 1) : n_chunks;
