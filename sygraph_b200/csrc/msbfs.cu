@@ -361,18 +361,34 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
         const uint32_t incl = warp_inclusive_scan(dg);
         const uint32_t total = __shfl_sync(kFullMask, incl, 31);
         if (total) {
+          // kPullWin windows of 32 edges in flight: column loads, then mask
+          // loads; each window's masks are OR-reduced per owner (a window's
+          // lanes of one owner are one match group) and the group's first
+          // lane adds the result to the owner's shared slot
           const uint32_t excl = incl - dg;
           acc_slot[lane] = acc;
           __syncwarp();
-          for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-            const uint32_t r = r0 + lane;
-            const bool act = r < total;
-            const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
-            const uint32_t ob = __shfl_sync(kFullMask, e, o);
-            const uint32_t oe = __shfl_sync(kFullMask, excl, o);
-            if (act) {
-              const u64 f = F_cur[P.icol[ob + (r - oe)]];
-              if (f) atomicOr(acc_slot + o, f);
+          for (uint32_t r0 = 0; r0 < total; r0 += 32 * kPullWin) {
+            uint32_t c[kPullWin], own[kPullWin];
+#pragma unroll
+            for (int k = 0; k < kPullWin; k++) {
+              const uint32_t r = r0 + k * 32 + lane;
+              const bool act = r < total;
+              const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
+              const uint32_t ob = __shfl_sync(kFullMask, e, o);
+              const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+              own[k] = act ? o : 32u;  // 32: no owner, a group of its own
+              c[k] = act ? P.icol[ob + (r - oe)] : 0u;
+            }
+            u64 f[kPullWin];
+#pragma unroll
+            for (int k = 0; k < kPullWin; k++) f[k] = own[k] < 32 ? F_cur[c[k]] : 0ull;
+#pragma unroll
+            for (int k = 0; k < kPullWin; k++) {
+              const uint32_t g = __match_any_sync(kFullMask, own[k]);
+              const uint32_t lo = __reduce_or_sync(g, (uint32_t)f[k]);
+              const uint32_t hi = __reduce_or_sync(g, (uint32_t)(f[k] >> 32));
+              if (own[k] < 32 && lane == __ffs(g) - 1 && (lo | hi)) atomicOr(acc_slot + own[k], ((u64)hi << 32) | lo);
             }
           }
           __syncwarp();
