@@ -138,6 +138,50 @@ struct Level {
       if (du >= kHeavy) add_heavy(u, du);
     }
   }
+  // K edges (u[k] carrying mask fv[k]; bit k of `act` marks valid ones) at
+  // once: the seen probes, then the claiming atomics with the row offsets,
+  // then the frontier atomics of all K go out together
+  template <int K>
+  __device__ __forceinline__ void visit_push_n(const uint32_t (&u)[K], const u64 (&fv)[K], uint32_t act) {
+    u64 nb[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) nb[k] = ((act >> k) & 1u) ? fv[k] & ~ld_cg(P->seen + u[k]) : 0ull;
+    u64 nw[K], old[K];
+    uint32_t r0[K], r1[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      old[k] = 0;
+      r0[k] = r1[k] = 0;
+      if (nb[k]) {
+        old[k] = atomicOr(P->seen + u[k], nb[k]);
+        r0[k] = P->ro[u[k]];
+        r1[k] = P->ro[u[k] + 1];
+      }
+    }
+    u64 fo[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      nw[k] = nb[k] & ~old[k];
+      fo[k] = nw[k] ? atomicOr(F_next + u[k], nw[k]) : ~0ull;
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (!nw[k]) continue;
+      const uint32_t du = r1[k] - r0[k];
+      reached += (u64)__popcll(nw[k]) * du;
+      if ((old[k] | nw[k]) == P->all) {
+        done_deg += du;
+        atomicOr(P->done + (u[k] >> 5), 1u << (u[k] & 31));
+      }
+      if (fo[k] == 0) {  // first sources to reach u this level: u joins the frontier
+        atomicOr(fa_next + (u[k] >> 5), 1u << (u[k] & 31));
+        atomicOr(sm_next + (u[k] >> 10), 1u << ((u[k] >> 5) & 31));
+        n_new++;
+        deg_new += du;
+        if (du >= kHeavy) add_heavy(u[k], du);
+      }
+    }
+  }
 };
 
 __device__ __forceinline__ u64 shfl64(u64 x, uint32_t src) {
@@ -151,14 +195,21 @@ __device__ __forceinline__ void expand_group(Level& L, uint32_t beg, uint32_t de
   const uint32_t incl = warp_inclusive_scan(deg);
   const uint32_t total = __shfl_sync(kFullMask, incl, 31);
   const uint32_t excl = incl - deg;
-  for (uint32_t r0 = 0; r0 < total; r0 += 32) {
-    const uint32_t r = r0 + lane;
-    const bool act = r < total;
-    const uint32_t o = warp_owner_of_rank(incl, act ? r : total - 1);
-    const uint32_t ob = __shfl_sync(kFullMask, beg, o);
-    const uint32_t oe = __shfl_sync(kFullMask, excl, o);
-    const u64 of = shfl64(fv, o);
-    if (act) L.visit_push(L.P->col[ob + (r - oe)], of);
+  for (uint32_t r0 = 0; r0 < total; r0 += 64) {
+    uint32_t u[2], act = 0;
+    u64 f[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const uint32_t r = r0 + k * 32 + lane;
+      const bool a = r < total;
+      const uint32_t o = warp_owner_of_rank(incl, a ? r : total - 1);
+      const uint32_t ob = __shfl_sync(kFullMask, beg, o);
+      const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+      f[k] = shfl64(fv, o);
+      u[k] = a ? L.P->col[ob + (r - oe)] : 0u;
+      act |= (uint32_t)a << k;
+    }
+    L.visit_push_n<2>(u, f, act);
   }
 }
 
@@ -317,15 +368,22 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
           }
         } else {
           const uint32_t c = unit - w1;
-          const uint32_t ent = find_chunk_owner(hs_cur, n_heavy, c);
+          const uint32_t ent = warp_find_owner(hs_cur, n_heavy, c);
           const uint32_t v = ld_cg(hv_cur + ent);
           const uint32_t first = ld_cg(hs_cur + ent);
           const uint32_t cb = P.ro[v] + (c - first) * kChunk;
           const uint32_t ce = min(P.ro[v + 1], cb + kChunk);
           const u64 fv = F_cur[v];  // read-only until the next barrier: L1-cached
-          for (uint32_t eb = cb; eb < ce; eb += 32) {
-            const uint32_t e = eb + lane;
-            if (e < ce) L.visit_push(P.col[e], fv);
+          const u64 f2[2] = {fv, fv};
+          for (uint32_t eb = cb; eb < ce; eb += 64) {
+            uint32_t u[2], act = 0;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+              const uint32_t e = eb + k * 32 + lane;
+              u[k] = e < ce ? P.col[e] : 0u;
+              act |= (uint32_t)(e < ce) << k;
+            }
+            L.visit_push_n<2>(u, f2, act);
           }
         }
       }
