@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
   }
   if (threadIdx.x == 0) {
     S.hn = 0;
-    S.acc[0] = S.acc[1] = S.acc[2] = S.acc[3] = 0ull;
+    S.acc[0] = S.acc[1] = 0ull;
   }
   if (P.mode == kLearned && P.mlp) sygraph::detail::mlp_stage(P.mlp, &S.mlp);
   if (!grid_sync(P.bar)) return;
@@ -79,12 +79,11 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
   // level 0: the mode's first choice (the reference starts in push unless pull-only)
   int strategy = P.mode == SG_BFS_PULL ? 2 : 0;
   {
-    FeatureInputs x{1.0, (double)deg_src, (double)unexplored, 1.0, 1.0, 1.0, 1.0, 0};
+    FeatureInputs x{1.0, (double)deg_src, (double)unexplored, 1.0, 1.0, 0};
     const int d = decide(P, S, 0, x, 0, 0.f, 1.f, 1);
     if (P.mode == kLearned) strategy = d;
   }
 
-  const bool want_words = (P.mode == kLearned && P.mlp) || P.features;
   uint32_t level = 0;
   for (;; level++) {
     if (P.schedule && level < P.schedule_len && P.schedule[level] >= 0) strategy = P.schedule[level];
@@ -102,7 +101,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
 
     Level L{&P, &S, C, P.fb + (size_t)((level + 1) % 3) * w0, P.sm + (size_t)((level + 1) % 3) * w1,
             P.heavy_v + (size_t)(par ^ 1) * P.heavy_cap, P.heavy_s + (size_t)(par ^ 1) * P.heavy_cap, level + 1,
-            want_words, frontier_deg < kDirectClaimDeg};
+            frontier_deg < kDirectClaimDeg};
     if (strategy < 2) {
       n_push++;
       const uint32_t n_heavy = (uint32_t)(heavy_packed >> 32), n_chunks = (uint32_t)heavy_packed;
@@ -131,11 +130,11 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     // level totals: warp sums into shared accumulators, one global atomic per
     // counter and CTA after the barrier below
     {
-      unsigned long long v4[4] = {L.n_new, L.deg_new, L.wnz, L.snz};
+      unsigned long long v2[2] = {L.n_new, L.deg_new};
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        v4[k] = sygraph::detail::warp_sum(v4[k]);
-        if (lane == 0 && v4[k]) atomicAdd(&S.acc[k], v4[k]);
+      for (int k = 0; k < 2; k++) {
+        v2[k] = sygraph::detail::warp_sum(v2[k]);
+        if (lane == 0 && v2[k]) atomicAdd(&S.acc[k], v2[k]);
       }
     }
     // staged heavy vertices: one atomic per CTA reserves entries and chunks
@@ -143,9 +142,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     if (threadIdx.x == 0) {
       if (S.acc[0]) atomicAdd(&C->new_count, S.acc[0]);
       if (S.acc[1]) atomicAdd(&C->new_deg, S.acc[1]);
-      if (S.acc[2]) atomicAdd(&C->words_nz, S.acc[2]);
-      if (S.acc[3]) atomicAdd(&C->sum_nz, S.acc[3]);
-      S.acc[0] = S.acc[1] = S.acc[2] = S.acc[3] = 0ull;  // next added to after the grid barrier
+      S.acc[0] = S.acc[1] = 0ull;  // next added to after the grid barrier
     }
     if (const uint32_t nb = min(S.hn, kHeavyBuf)) {  // block-uniform; most levels stage none
       const uint32_t k0 = 2 * threadIdx.x;
@@ -174,8 +171,6 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
 
     const unsigned long long next_size = ld_cg(&C->new_count);
     const unsigned long long next_deg = ld_cg(&C->new_deg);
-    const unsigned long long words_nz = ld_cg(&C->words_nz);
-    const unsigned long long sum_nz = ld_cg(&C->sum_nz);
     heavy_packed = ld_cg(&C->heavy_packed);
     unexplored -= next_deg;
     visited_vertices += next_size;
@@ -197,7 +192,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     frontier_deg = next_deg;
     if (next_size == 0) break;
     FeatureInputs x{(double)next_size, (double)next_deg, (double)unexplored, (double)visited_vertices,
-                    (double)words_nz, (double)sum_nz, (double)prev_size, strategy >= 2};
+                    (double)prev_size, strategy >= 2};
     // (float)(uint32) casts: the reference's uint32 degree sums (bfs.hpp:327-330)
     strategy = decide(P, S, strategy, x, level + 1, (float)(uint32_t)next_deg, (float)(uint32_t)unexplored,
                       next_size);

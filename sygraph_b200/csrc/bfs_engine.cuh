@@ -31,9 +31,7 @@ struct LevelCounters {
   unsigned long long heavy_packed;  // (entries << 32) | chunks of the heavy list being built
   unsigned long long new_count;     // vertices that joined the next frontier
   unsigned long long new_deg;       // their forward degrees
-  unsigned long long words_nz;      // non-zero words of the next frontier bitmap
-  unsigned long long sum_nz;        // non-zero words of its summary
-  unsigned long long pad[3];
+  unsigned long long pad[5];
 };
 
 struct Params {
@@ -71,7 +69,7 @@ struct Params {
 struct Shared {
   uint32_t scan[32];
   unsigned long long red[32][4];
-  unsigned long long acc[4];  // per-level totals of the CTA (new vertices, their degree, words, summary bits)
+  unsigned long long acc[2];  // per-level totals of the CTA (new vertices, their degree)
   uint32_t hv[kHeavyBuf];
   uint32_t hd[kHeavyBuf];
   uint32_t hn;
@@ -94,13 +92,10 @@ struct Level {
   uint32_t* hv_next;
   uint32_t* hs_next;
   uint32_t next_depth;
-  // count the next frontier's non-zero bitmap and summary words (selector
-  // features): only then do the bitmap atomics wait for their old values
-  bool want_words;
   // claim without the plain pre-load (small frontiers: their neighbours are
   // mostly unvisited, and the load would add a round trip to each discovery)
   bool direct_claim;
-  uint32_t n_new = 0, wnz = 0, snz = 0;
+  uint32_t n_new = 0;
   unsigned long long deg_new = 0;
 
   __device__ __forceinline__ void add_heavy(uint32_t u, uint32_t du) {
@@ -133,15 +128,8 @@ struct Level {
     const uint32_t r0 = P->ro[u], r1 = P->ro[u + 1];
     if (old & bit) return;
     const uint32_t du = r1 - r0;
-    if (want_words) {
-      if (atomicOr(fb_next + (u >> 5), 1u << (u & 31)) == 0) {
-        wnz++;
-        if (atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31)) == 0) snz++;
-      }
-    } else {  // results unused: fire-and-forget reductions
-      atomicOr(fb_next + (u >> 5), 1u << (u & 31));
-      atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31));
-    }
+    atomicOr(fb_next + (u >> 5), 1u << (u & 31));  // results unused: fire-and-forget reductions
+    atomicOr(sm_next + (u >> 10), 1u << ((u >> 5) & 31));
     discovered(u, du);
   }
   // push of K candidate targets at once (bit k of `act`: u[k] is valid): the
@@ -171,15 +159,8 @@ struct Level {
 #pragma unroll
     for (int k = 0; k < K; k++) {
       if ((old[k] >> (u[k] & 31)) & 1u) continue;
-      if (want_words) {
-        if (atomicOr(fb_next + (u[k] >> 5), 1u << (u[k] & 31)) == 0) {
-          wnz++;
-          if (atomicOr(sm_next + (u[k] >> 10), 1u << ((u[k] >> 5) & 31)) == 0) snz++;
-        }
-      } else {
-        atomicOr(fb_next + (u[k] >> 5), 1u << (u[k] & 31));
-        atomicOr(sm_next + (u[k] >> 10), 1u << ((u[k] >> 5) & 31));
-      }
+      atomicOr(fb_next + (u[k] >> 5), 1u << (u[k] & 31));
+      atomicOr(sm_next + (u[k] >> 10), 1u << ((u[k] >> 5) & 31));
       discovered(u[k], r1[k] - r0[k]);
     }
   }
@@ -187,12 +168,7 @@ struct Level {
   __device__ __forceinline__ void publish_word(uint32_t wi, uint32_t vw, uint32_t fmask) {
     st_cg(P->visited + wi, vw | fmask);
     st_cg(fb_next + wi, fmask);
-    wnz++;
-    if (want_words) {
-      if (atomicOr(sm_next + (wi >> 5), 1u << (wi & 31)) == 0) snz++;
-    } else {
-      atomicOr(sm_next + (wi >> 5), 1u << (wi & 31));
-    }
+    atomicOr(sm_next + (wi >> 5), 1u << (wi & 31));
   }
 };
 
@@ -221,8 +197,6 @@ struct FeatureInputs {
   double nd;     // frontier degree sum
   double ud;     // unexplored degree (unvisited vertices)
   double vis;    // visited vertices
-  double wnz;    // non-zero frontier bitmap words
-  double snz;    // non-zero summary words
   double prev;   // previous frontier size
   int cur_pull;  // direction of the level that produced this frontier
 };
@@ -235,8 +209,11 @@ __device__ __forceinline__ void compute_features(const Params& P, const FeatureI
   f[3] = (float)x.nd / m;
   f[4] = (float)x.ud / m;
   f[5] = (n - (float)x.vis) / n;
-  f[6] = (float)x.wnz / (float)P.w0;
-  f[7] = (float)x.snz / (float)P.w1;
+  // expected occupancy of the frontier bitmap and of its summary for a
+  // frontier of this size spread at random (the words are not counted: that
+  // would make every bitmap atomic wait for its old value)
+  f[6] = 1.f - expf(-(float)x.ns / (float)P.w0);
+  f[7] = 1.f - expf(-(float)x.ns / (32.f * (float)P.w1));
   f[8] = log2f(1.f + (float)x.nd / fmaxf(1.f, (float)x.ns)) / 16.f;
   f[9] = log2f(1.f + m / n) / 8.f;
   f[10] = x.cur_pull ? 1.f : 0.f;

@@ -5,8 +5,9 @@ Strategies (the MLP's six outputs): 0 push/warp, 1 push/CTA, 2 pull/warp,
 3 pull/CTA, 4 pull_all/warp, 5 pull_all/CTA.  Features (twelve, computed on
 the device at every level end, the same way for training and inference):
 log and linear frontier size, log and linear frontier degree, unexplored
-degree fraction, unvisited fraction, level-0 and summary bitmap occupancy,
-mean frontier degree, graph mean degree, current direction, frontier growth."""
+degree fraction, unvisited fraction, the level-0 and summary bitmap occupancy
+a frontier of that size would have if spread at random, mean frontier
+degree, graph mean degree, current direction, frontier growth."""
 from __future__ import annotations
 
 import ctypes as C

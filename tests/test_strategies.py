@@ -173,6 +173,11 @@ def test_feature_log_matches_level_records(sg, rmat):
     for i, r in enumerate(recs):
         # feature 1: frontier size / n of the level the features choose for
         assert F[i, 1] == pytest.approx(r["frontier_size"] / n, rel=1e-5)
+        # features 6, 7: bitmap / summary occupancy of a randomly spread frontier of that size
+        w0 = (n + 31) // 32
+        w1 = (w0 + 31) // 32
+        assert F[i, 6] == pytest.approx(1 - np.exp(-r["frontier_size"] / w0), rel=1e-4, abs=1e-6)
+        assert F[i, 7] == pytest.approx(1 - np.exp(-r["frontier_size"] / (32 * w1)), rel=1e-4, abs=1e-6)
         if i > 0:
             assert F[i, 10] == (1.0 if recs[i - 1]["strategy"] >= 2 else 0.0)
 
