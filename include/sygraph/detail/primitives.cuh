@@ -161,7 +161,7 @@ __device__ __forceinline__ uint32_t atomic_min_nonneg(uint32_t* p, uint32_t v) {
 struct GridBarrier {
   unsigned long long count;  // arrivals since the launch began; top bit: a wait ran out
   uint32_t error;            // read by the host after the launch
-  uint32_t pad;
+  uint32_t exits;            // blocks past their last barrier (grid_exit)
 };
 
 constexpr uint64_t kBarrierSpinLimit = 1ull << 24;  // ~16M polls x >=64 ns sleep: over a second
@@ -191,7 +191,7 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
 // block whose wait runs out sets the count's top bit (and the error word),
 // which ends every other wait at once and fails every later barrier of the
 // launch.
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, uint64_t spin_limit = kBarrierSpinLimit) {
   __shared__ uint32_t s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -210,7 +210,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
             break;
           }
           if (c >= target) break;
-          if (++spins > kBarrierSpinLimit) {
+          if (++spins > spin_limit) {
             atomicOr(&bar->count, kBarrierFailed);
             atomicExch(&bar->error, 1u);
             ok = 0;
@@ -226,6 +226,19 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// Called once by every block at the end of a launch that completed all its
+// barriers: the last block out returns the barrier to its launch state
+// (count and exits zero), so the next launch needs no host-side reset.
+// Every other block has passed its last wait before it arrives here.  A
+// launch that left through a failed barrier skips this, and its count keeps
+// the failure bit until the host clears it.
+__device__ __forceinline__ void grid_exit(GridBarrier* bar) {
+  if (threadIdx.x == 0 && atomicAdd(&bar->exits, 1u) == gridDim.x - 1) {
+    bar->count = 0;
+    bar->exits = 0;
+  }
 }
 
 }  // namespace detail

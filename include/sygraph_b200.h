@@ -111,6 +111,15 @@ sg_status sg_free_host_pinned(void* host_ptr);
 sg_status sg_memcpy(void* dst, const void* src, uint64_t bytes, int kind, void* stream);
 sg_status sg_memset(void* dev_ptr, int value, uint64_t bytes, void* stream);
 /* A non-blocking stream (does not synchronise with the legacy default stream). */
+/* Diagnostic of the bounded grid barrier every fused engine uses (not in the
+ * reference): launches `blocks` (1-64) cooperative blocks, all of which but
+ * `skip_block` (none when it is >= blocks) wait at one grid barrier polling
+ * at most `spin_limit` (1 - 2^20) times.  *timed_out = blocks whose wait ran
+ * out, *error_flag = the barrier's error word the engines report as
+ * SG_ERR_TIMEOUT.  A block that never arrives makes every other block give up
+ * and return; no wait is unbounded. */
+sg_status sg_debug_barrier_check(uint32_t blocks, uint32_t skip_block, uint64_t spin_limit, uint32_t* timed_out,
+                                 uint32_t* error_flag);
 sg_status sg_stream_create(void** stream);
 sg_status sg_stream_destroy(void* stream);
 sg_status sg_stream_synchronize(void* stream);

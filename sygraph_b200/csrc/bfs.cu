@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     P.result[3] = visited_vertices;
     P.result[4] = P.m - unexplored;
   }
+  sygraph::detail::grid_exit(P.bar);
 }
 
 __global__ void fill_depth_kernel(uint32_t* depth, uint32_t n, uint32_t src) {
@@ -258,6 +259,10 @@ struct sg_bfs_s {
   float* features = nullptr;
   uint32_t last_iterations = 0;
   bool fresh = false;  // initialised but not run: depths not written yet
+  // the grid barrier needs a reset before the next launch: set at creation
+  // and when a launch reported a barrier timeout (a completed launch resets
+  // it itself, grid_exit)
+  bool bar_reset = true;
 };
 
 static sg_status bfs_materialise(sg_bfs b) {
@@ -321,7 +326,10 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.result = b->result;
   P.schedule = b->schedule_len ? b->schedule : nullptr;
   P.schedule_len = b->schedule_len;
-  SG_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(*b->bar), b->stream));
+  if (b->bar_reset) {
+    SG_CUDA(cudaMemsetAsync(b->bar, 0, sizeof(*b->bar), b->stream));
+    b->bar_reset = false;
+  }
   return eng::launch_persistent(bfs::bfs_kernel, P, 2, b->stream, b->max_ctas, nullptr, bfs::kBfsThreads);
 }
 
@@ -331,7 +339,10 @@ static sg_status bfs_collect(sg_bfs b, sg_bfs_details* details) {
   SG_CUDA(cudaMemcpyAsync(res, b->result, sizeof(res), cudaMemcpyDeviceToHost, b->stream));
   SG_CUDA(cudaMemcpyAsync(&bar, b->bar, sizeof(bar), cudaMemcpyDeviceToHost, b->stream));
   SG_CUDA(cudaStreamSynchronize(b->stream));
-  if (bar.error) return fail(SG_ERR_TIMEOUT, "BFS engine: a grid barrier wait ran out");
+  if (bar.error) {
+    b->bar_reset = true;
+    return fail(SG_ERR_TIMEOUT, "BFS engine: a grid barrier wait ran out");
+  }
   b->last_iterations = (uint32_t)res[0];
   if (details) {
     memset(details, 0, sizeof(*details));
@@ -454,6 +465,7 @@ sg_status sgb::bfs_launch_status(sg_bfs b) {
   uint32_t err = 0;
   SG_CUDA(cudaMemcpyAsync(&err, &b->bar->error, sizeof(err), cudaMemcpyDeviceToHost, b->stream));
   SG_CUDA(cudaStreamSynchronize(b->stream));
+  if (err) b->bar_reset = true;
   return err ? fail(SG_ERR_TIMEOUT, "BFS engine: a grid barrier wait ran out") : SG_OK;
 }
 

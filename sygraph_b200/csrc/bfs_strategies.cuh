@@ -83,8 +83,10 @@ __device__ __forceinline__ void push_heavy(Level& L, const uint32_t* hv, const u
   (void)n_chunks;
 }
 
-// Also clears F_{L-1} (fb_zero / sm_zero): its summary word is read with the
-// frontier's, so the clear adds no dependent load to the level.
+// A warp takes a summary unit of 32 bitmap words and loads the words
+// directly (one round trip, not summary then words: the 128-byte load costs
+// the same when the unit is empty), and clears the unit of F_{L-1} (fb_zero
+// / sm_zero) with plain stores.
 __device__ __forceinline__ void push_warp(Level& L, const uint32_t* fb_cur, const uint32_t* sm_cur,
                                           uint32_t* fb_zero, uint32_t* sm_zero, const uint32_t* hv,
                                           const uint32_t* hs, uint32_t n_heavy, uint32_t n_chunks) {
@@ -92,16 +94,14 @@ __device__ __forceinline__ void push_warp(Level& L, const uint32_t* fb_cur, cons
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t w1 = P.w1;
+  const uint32_t w0 = P.w0, w1 = P.w1;
+  (void)sm_cur;
   for (uint32_t unit = gwarp; unit < w1; unit += nwarps) {
-    const uint32_t s = ld_cg(sm_cur + unit);
-    const uint32_t z = ld_cg(sm_zero + unit);
-    if (z) {
-      if ((z >> lane) & 1u) st_cg(fb_zero + unit * 32 + lane, 0u);
-      if (lane == 0) st_cg(sm_zero + unit, 0u);
-    }
-    if (!s) continue;
-    const uint32_t bits = ((s >> lane) & 1u) ? ld_cg(fb_cur + unit * 32 + lane) : 0u;
+    const uint32_t wi = unit * 32 + lane;
+    const uint32_t bits = wi < w0 ? ld_cg(fb_cur + wi) : 0u;
+    if (wi < w0) st_cg(fb_zero + wi, 0u);
+    if (lane == 0) st_cg(sm_zero + unit, 0u);
+    if (!__any_sync(kFullMask, bits)) continue;
     const uint32_t c = __popc(bits);
     const uint32_t incl = warp_inclusive_scan(c);
     const uint32_t total = __shfl_sync(kFullMask, incl, 31);

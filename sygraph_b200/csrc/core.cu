@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "sygraph/detail/primitives.cuh"
 
 namespace sgb {
 
@@ -131,6 +132,16 @@ sg_status graph_weight_sorted(sg_graph g) {
 
 }  // namespace sgb
 
+// Diagnostic of the bounded grid barrier: every block but `skip_block`
+// (none when it is >= the grid) waits at one barrier with `limit` polls;
+// blocks whose wait ran out count themselves in *out.
+__global__ void barrier_check_kernel(sygraph::detail::GridBarrier* bar, uint32_t skip_block, uint64_t limit,
+                                     uint32_t* out) {
+  if (blockIdx.x == skip_block) return;  // never arrives
+  const bool ok = sygraph::detail::grid_sync(bar, limit);
+  if (threadIdx.x == 0 && !ok) atomicAdd(out, 1u);
+}
+
 using namespace sgb;
 
 extern "C" {
@@ -216,6 +227,39 @@ sg_status sg_memset(void* dev_ptr, int value, uint64_t bytes, void* stream) {
   SG_REQUIRE(dev_ptr, SG_ERR_INVALID, "NULL pointer in sg_memset");
   SG_CUDA(cudaMemsetAsync(dev_ptr, value, bytes, (cudaStream_t)stream));
   return SG_OK;
+}
+
+sg_status sg_debug_barrier_check(uint32_t blocks, uint32_t skip_block, uint64_t spin_limit, uint32_t* timed_out,
+                                 uint32_t* error_flag) {
+  clear_error();
+  SG_REQUIRE(timed_out && error_flag, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(blocks >= 1 && blocks <= 64, SG_ERR_INVALID, "blocks must be in [1, 64]");
+  SG_REQUIRE(spin_limit >= 1 && spin_limit <= (1ull << 20), SG_ERR_INVALID, "spin_limit must be in [1, 2^20]");
+  int coop = 0, dev = 0;
+  SG_CUDA(cudaGetDevice(&dev));
+  SG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  SG_REQUIRE(coop, SG_ERR_UNSUPPORTED, "device cannot launch cooperative kernels");
+  sygraph::detail::GridBarrier* bar = nullptr;
+  uint32_t* out = nullptr;
+  SG_TRY(dev_alloc(&bar, 1));
+  sg_status st = dev_alloc(&out, 1);
+  cudaError_t e = cudaSuccess;
+  if (st == SG_OK) {
+    e = cudaMemset(bar, 0, sizeof(*bar));
+    if (e == cudaSuccess) e = cudaMemset(out, 0, sizeof(uint32_t));
+    void* args[] = {&bar, &skip_block, &spin_limit, &out};
+    if (e == cudaSuccess)
+      e = cudaLaunchCooperativeKernel((const void*)barrier_check_kernel, dim3(blocks), dim3(64), args, 0, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    sygraph::detail::GridBarrier hb = {};
+    if (e == cudaSuccess) e = cudaMemcpy(&hb, bar, sizeof(hb), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(timed_out, out, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    *error_flag = hb.error;
+    if (e != cudaSuccess) st = cuda_fail(e, "barrier check", __FILE__, __LINE__);
+  }
+  dev_free(bar);
+  dev_free(out);
+  return st;
 }
 
 sg_status sg_stream_create(void** stream) {
