@@ -286,6 +286,7 @@ def serving_bench(sg, torch) -> dict:
     gids = [srv.add_graph(G) for G in Gs]
     warm = serving.make_workload(sizes, 200.0, 1.0, 0.7, seed=5)
     serving.run_open_loop(srv, gids, warm)
+    serving.warm_up(srv, gids, sizes, SERVE_SLOTS)
     out = {"graphs": [f"RMAT-{s}" for s in SERVE_SCALES], "slots": SERVE_SLOTS, "sssp_delta": SSSP_DELTA,
            "mix": "70% BFS / 30% SSSP", "runs": []}
     for qps in SERVE_QPS:

@@ -94,36 +94,49 @@ __device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const
     x[i] = (f[i] - P->mean[i]) * P->inv_std[i];
   }
   if (out_of_range) return -1;
-  float h1 = P->b1[lane];
+  // independent partial sums break the dependent FMA chains
+  float a0 = P->b1[lane], a1 = 0.f;
 #pragma unroll
-  for (int i = 0; i < kMlpIn; i++) h1 += P->w1t[i][lane] * x[i];
+  for (int i = 0; i < kMlpIn; i += 2) {
+    a0 += P->w1t[i][lane] * x[i];
+    a1 += P->w1t[i + 1][lane] * x[i + 1];
+  }
+  const float h1 = a0 + a1;
   scratch[lane] = h1 > 0.f ? h1 : 0.f;
   __syncwarp();
-  float h2 = P->b2[lane];
+  float c[4] = {P->b2[lane], 0.f, 0.f, 0.f};
 #pragma unroll
-  for (int i = 0; i < kMlpHidden; i++) h2 += P->w2t[i][lane] * scratch[i];
+  for (int i = 0; i < kMlpHidden; i += 4)
+#pragma unroll
+    for (int k = 0; k < 4; k++) c[k] += P->w2t[i + k][lane] * scratch[i + k];
+  const float h2 = (c[0] + c[1]) + (c[2] + c[3]);
   scratch[kMlpHidden + lane] = h2 > 0.f ? h2 : 0.f;
   __syncwarp();
   float y = 3.4e38f;
   if (lane < (uint32_t)kMlpOut) {
-    float a = P->b3[lane];
+    float d[4] = {P->b3[lane], 0.f, 0.f, 0.f};
 #pragma unroll
-    for (int i = 0; i < kMlpHidden; i++) a += P->w3[lane][i] * scratch[kMlpHidden + i];
-    y = a;
+    for (int i = 0; i < kMlpHidden; i += 4)
+#pragma unroll
+      for (int k = 0; k < 4; k++) d[k] += P->w3[lane][i + k] * scratch[kMlpHidden + i + k];
+    y = (d[0] + d[1]) + (d[2] + d[3]);
   }
   __syncwarp();
   const float y_fallback = __shfl_sync(0xffffffffu, y, fallback >= 0 ? fallback : 0);
+  // argmin over lanes 0-7 (the six outputs; the others hold +inf)
   float best = (lane < (uint32_t)kMlpOut && ((allowed >> lane) & 1u)) ? y : 3.4e38f;
   int arg = best < 3.4e38f ? (int)lane : 32;
 #pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    const float ob = __shfl_xor_sync(0xffffffffu, best, d);
-    const int oa = __shfl_xor_sync(0xffffffffu, arg, d);
+  for (int dd = 4; dd > 0; dd >>= 1) {
+    const float ob = __shfl_xor_sync(0xffffffffu, best, dd);
+    const int oa = __shfl_xor_sync(0xffffffffu, arg, dd);
     if (ob < best || (ob == best && oa < arg)) {
       best = ob;
       arg = oa;
     }
   }
+  best = __shfl_sync(0xffffffffu, best, 0);
+  arg = __shfl_sync(0xffffffffu, arg, 0);
   if (arg >= kMlpOut) return -1;
   if (fallback >= 0 && ((allowed >> fallback) & 1u) && y_fallback - best <= margin) arg = fallback;
   return arg;

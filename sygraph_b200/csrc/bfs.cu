@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     S.acc[0] = S.acc[1] = 0ull;
   }
   if (P.mode == kLearned && P.mlp) sygraph::detail::mlp_stage(P.mlp, &S.mlp);
+  if (threadIdx.x == 0) S.fk = feature_const(P);
   if (!grid_sync(P.bar)) return;
 
   // heavy list of the frontier being expanded, read with the level's other

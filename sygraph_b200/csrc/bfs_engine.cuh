@@ -66,6 +66,13 @@ struct Params {
   float* features;                        // optional log: 12 floats per level decision
 };
 
+// Per-launch constants of the features (reciprocals and logarithms of the
+// graph's sizes), computed once so a level's features need no division by
+// them.
+struct FeatureConst {
+  float inv_log_n, inv_n, inv_log_m, inv_m, inv_w0, inv_sw1, f9;
+};
+
 struct Shared {
   uint32_t scan[32];
   unsigned long long red[32][4];
@@ -80,6 +87,7 @@ struct Shared {
   int choice;
   sygraph::detail::MlpStaged mlp;  // learned mode: parameters staged once per launch
   float mlp_scratch[2 * sygraph::detail::kMlpHidden];
+  FeatureConst fk;  // set once per launch
 };
 
 // Per-thread context of one level's expansion.
@@ -201,23 +209,31 @@ struct FeatureInputs {
   int cur_pull;  // direction of the level that produced this frontier
 };
 
-__device__ __forceinline__ void compute_features(const Params& P, const FeatureInputs& x, float f[12]) {
+__device__ __forceinline__ FeatureConst feature_const(const Params& P) {
   const float n = (float)P.n, m = (float)(P.m ? P.m : 1);
-  f[0] = log2f(1.f + (float)x.ns) / log2f(1.f + n);
-  f[1] = (float)x.ns / n;
-  f[2] = log2f(1.f + (float)x.nd) / log2f(1.f + m);
-  f[3] = (float)x.nd / m;
-  f[4] = (float)x.ud / m;
-  f[5] = (n - (float)x.vis) / n;
+  return FeatureConst{1.f / log2f(1.f + n), 1.f / n, 1.f / log2f(1.f + m), 1.f / m, 1.f / (float)P.w0,
+                      1.f / (32.f * (float)P.w1), log2f(1.f + m / n) / 8.f};
+}
+
+__device__ __forceinline__ void compute_features(const Params& P, const FeatureConst& k, const FeatureInputs& x,
+                                                 float f[12]) {
+  const float ns = (float)x.ns, nd = (float)x.nd;
+  const float lns = log2f(1.f + ns);
+  f[0] = lns * k.inv_log_n;
+  f[1] = ns * k.inv_n;
+  f[2] = log2f(1.f + nd) * k.inv_log_m;
+  f[3] = nd * k.inv_m;
+  f[4] = (float)x.ud * k.inv_m;
+  f[5] = ((float)P.n - (float)x.vis) * k.inv_n;
   // expected occupancy of the frontier bitmap and of its summary for a
   // frontier of this size spread at random (the words are not counted: that
   // would make every bitmap atomic wait for its old value)
-  f[6] = 1.f - expf(-(float)x.ns / (float)P.w0);
-  f[7] = 1.f - expf(-(float)x.ns / (32.f * (float)P.w1));
-  f[8] = log2f(1.f + (float)x.nd / fmaxf(1.f, (float)x.ns)) / 16.f;
-  f[9] = log2f(1.f + m / n) / 8.f;
+  f[6] = 1.f - expf(-ns * k.inv_w0);
+  f[7] = 1.f - expf(-ns * k.inv_sw1);
+  f[8] = log2f(1.f + nd / fmaxf(1.f, ns)) / 16.f;
+  f[9] = k.f9;
   f[10] = x.cur_pull ? 1.f : 0.f;
-  f[11] = fminf(16.f, fmaxf(-16.f, log2f((1.f + (float)x.ns) / (1.f + (float)x.prev)))) / 16.f;
+  f[11] = fminf(16.f, fmaxf(-16.f, lns - log2f(1.f + (float)x.prev))) / 16.f;
 }
 
 // Strategy of the next level, identical in every CTA (same inputs, same
@@ -240,7 +256,7 @@ __device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const
   if (P.mode == kLearned && P.mlp || log) {
     if (threadIdx.x < 32) {
       float f[12];
-      compute_features(P, x, f);
+      compute_features(P, S.fk, x, f);
       if (log && threadIdx.x == 0)
         for (int i = 0; i < 12; i++) P.features[(size_t)level * 12 + i] = f[i];
       if (P.mode == kLearned && P.mlp) {
@@ -248,9 +264,8 @@ __device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const
         if (threadIdx.x == 0) S.choice = c;
       }
     }
-    __syncthreads();
+    __syncthreads();  // S.choice is written again only after the next grid barrier
     if (P.mode == kLearned && P.mlp && S.choice >= 0) h = S.choice;
-    __syncthreads();
   }
   return h;
 }

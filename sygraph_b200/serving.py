@@ -119,6 +119,18 @@ def percentiles(lat_ms) -> dict:
     return {"p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)), "mean_ms": float(a.mean())}
 
 
+def warm_up(srv: Server, gids, graph_sizes, slots: int, batch: int = 64, seed: int = 0) -> None:
+    """Creates every workspace a run may need before it is timed: for each
+    graph, `slots` x `batch` BFS queries at once (a batched launch lands on
+    every slot) and `slots` SSSP queries, then waits for all of them."""
+    rng = np.random.default_rng(seed)
+    for gi, n in zip(gids, graph_sizes):
+        tickets = [srv.submit(gi, "bfs", int(rng.integers(0, n))) for _ in range(slots * batch)]
+        tickets += [srv.submit(gi, "sssp", int(rng.integers(0, n))) for _ in range(slots)]
+        for t in tickets:
+            srv.wait(t)
+
+
 def run_open_loop(srv: Server, gids, wl: Workload, outs=None) -> dict:
     """Submits each query at its arrival time (busy-waiting the host clock),
     waits for all, returns throughput and latency percentiles."""
