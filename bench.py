@@ -263,7 +263,7 @@ def profile_case(kind: str) -> None:
 
 
 SERVE_SCALES = (14, 16, 18, 20, 21, 22, 22, 23)
-SERVE_QPS = (1000.0, 3000.0)
+SERVE_QPS = (1000.0, 3000.0, 6000.0)
 SERVE_SECONDS = 2.0
 SERVE_SLOTS = 4
 SSSP_DELTA = 0.1
