@@ -11,7 +11,8 @@ value  = GTEPS = sum over the step's traversals of the edges incident to
          reached vertices / device time (CUDA events), all ranks.
 e2e    = the same metric through the C ABI with host buffers: the source ids
          are copied from pinned host memory and every depth array is read back
-         to pinned host memory inside the timed region.
+         to pinned host memory inside the timed region (two instances on two
+         streams, each traversal's copy overlapping the next traversal).
 roofline: the BFS kernel against the measured HBM copy bandwidth, with
          B = 4(n+1) + 4m + 4n algorithmic bytes per traversal.
 cpu_baseline: the oracle's OpenMP frontier BFS on the host cores, a bounded
@@ -395,36 +396,65 @@ def main():
     import ctypes as C
     hp_src = C.c_void_p()
     sg._lib.call("sg_malloc_host_pinned", 4 * len(srcs), C.byref(hp_src))
-    hp_dst = C.c_void_p()
-    sg._lib.call("sg_malloc_host_pinned", 4 * n, C.byref(hp_dst))
     dsrc = C.c_void_p()
     sg._lib.call("sg_malloc_device", 4 * len(srcs), C.byref(dsrc))
     np.ctypeslib.as_array(C.cast(hp_src, C.POINTER(C.c_uint32)), shape=(len(srcs),))[:] = srcs
     host_src = np.ctypeslib.as_array(C.cast(hp_src, C.POINTER(C.c_uint32)), shape=(len(srcs),))
-    out_ptr = C.cast(hp_dst, C.POINTER(C.c_uint32))
+
+    # two instances on two streams: traversal i's depth copy (on its stream,
+    # after its kernel) overlaps traversal i+1's kernel on the other stream;
+    # each instance's next kernel waits for its previous copy by stream order
+    streams, insts, hp_out, d_depth = [], [], [], []
+    for _ in range(2):
+        st = C.c_void_p()
+        sg._lib.call("sg_stream_create", C.byref(st))
+        streams.append(st)
+        inst = sg.algorithms.BFS(G)
+        inst.set_launch(0, st)
+        insts.append(inst)
+        hp = C.c_void_p()
+        sg._lib.call("sg_malloc_host_pinned", 4 * n, C.byref(hp))
+        hp_out.append(hp)
+        dd = C.POINTER(C.c_uint32)()
+        sg._lib.call("sg_bfs_distances_device", inst.handle, C.byref(dd))
+        d_depth.append(dd)
 
     def e2e_step():
-        sg._lib.call("sg_memcpy", dsrc, hp_src, 4 * len(srcs), 0, None)
+        sg._lib.call("sg_memcpy", dsrc, hp_src, 4 * len(srcs), 0, streams[0])
         for i in range(len(srcs)):
-            sg._lib.call("sg_bfs_init", bfs.handle, int(host_src[i]))
-            sg._lib.call("sg_bfs_run_async", bfs.handle, 2, ALPHA, BETA)
-            sg._lib.call("sg_bfs_get_distances", bfs.handle, out_ptr)
+            k = i & 1
+            sg._lib.call("sg_bfs_init", insts[k].handle, int(host_src[i]))
+            sg._lib.call("sg_bfs_run_async", insts[k].handle, 2, ALPHA, BETA)
+            sg._lib.call("sg_memcpy_async", hp_out[k], d_depth[k], 4 * n, 1, streams[k])
+        for st in streams:
+            sg._lib.call("sg_stream_synchronize", st)
 
     for _ in range(2):
         e2e_step()
+    # the copied-back depths are the traversal's (the last source's, on its instance)
+    last = np.ctypeslib.as_array(C.cast(hp_out[(len(srcs) - 1) & 1], C.POINTER(C.c_uint32)), shape=(n,))
+    insts[(len(srcs) - 1) & 1].init(int(srcs[-1]))
+    insts[(len(srcs) - 1) & 1].run(2, ALPHA, BETA)
+    assert np.array_equal(last, insts[(len(srcs) - 1) & 1].getDistances())
     barrier()
     e_steps = max(2, args.steps // 2)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
     for _ in range(e_steps):
         e2e_step()
-    b.record()
+    b.record()  # after both streams were synchronised on the host
     barrier()
     e2e_ms = replicas.max_over_ranks(a.elapsed_time(b), device="cuda")
     e2e_val = step_edges * world * e_steps / (e2e_ms * 1e-3) / 1e9
     sg._lib.call("sg_free_host_pinned", hp_src)
-    sg._lib.call("sg_free_host_pinned", hp_dst)
     sg._lib.call("sg_free_device", dsrc)
+    for hp in hp_out:
+        sg._lib.call("sg_free_host_pinned", hp)
+    for x in insts:  # back on the graph's stream before the streams go
+        x.set_launch(0, None)
+    del insts, inst, d_depth
+    for st in streams:
+        sg._lib.call("sg_stream_destroy", st)
 
     # learned selector (committed model) on the same sources, and on a held-out
     # 4096 x 4096 grid with 2% long-range pairs, against the reference heuristic

@@ -109,6 +109,10 @@ sg_status sg_malloc_host_pinned(uint64_t bytes, void** host_ptr);
 sg_status sg_free_host_pinned(void* host_ptr);
 /* kind: 0 host->device, 1 device->host, 2 device->device, 3 default (unified addressing) */
 sg_status sg_memcpy(void* dst, const void* src, uint64_t bytes, int kind, void* stream);
+/* As sg_memcpy, enqueued on `stream` only (no synchronisation for any kind):
+ * for pipelines that overlap a result's copy with the next launch; the
+ * caller synchronises the stream before reading a device->host copy. */
+sg_status sg_memcpy_async(void* dst, const void* src, uint64_t bytes, int kind, void* stream);
 sg_status sg_memset(void* dev_ptr, int value, uint64_t bytes, void* stream);
 /* A non-blocking stream (does not synchronise with the legacy default stream). */
 /* Diagnostic of the bounded grid barrier every fused engine uses (not in the

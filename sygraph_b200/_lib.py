@@ -106,6 +106,7 @@ SIGNATURES = {
     "sg_malloc_host_pinned": (st, [C.c_uint64, C.POINTER(vp)]),
     "sg_free_host_pinned": (st, [vp]),
     "sg_memcpy": (st, [vp, vp, C.c_uint64, C.c_int, vp]),
+    "sg_memcpy_async": (st, [vp, vp, C.c_uint64, C.c_int, vp]),
     "sg_memset": (st, [vp, C.c_int, C.c_uint64, vp]),
     "sg_debug_barrier_check": (st, [C.c_uint32, C.c_uint32, C.c_uint64, u32p, u32p]),
     "sg_stream_create": (st, [C.POINTER(vp)]),

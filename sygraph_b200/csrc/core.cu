@@ -222,6 +222,18 @@ sg_status sg_memcpy(void* dst, const void* src, uint64_t bytes, int kind, void* 
   return SG_OK;
 }
 
+sg_status sg_memcpy_async(void* dst, const void* src, uint64_t bytes, int kind, void* stream) {
+  if (bytes == 0) return SG_OK;
+  SG_REQUIRE(dst && src, SG_ERR_INVALID, "NULL pointer in sg_memcpy_async");
+  SG_REQUIRE(kind >= 0 && kind <= 3, SG_ERR_INVALID, "kind must be 0-3");
+  const cudaMemcpyKind k = kind == 0   ? cudaMemcpyHostToDevice
+                           : kind == 1 ? cudaMemcpyDeviceToHost
+                           : kind == 2 ? cudaMemcpyDeviceToDevice
+                                       : cudaMemcpyDefault;
+  SG_CUDA(cudaMemcpyAsync(dst, src, bytes, k, (cudaStream_t)stream));
+  return SG_OK;
+}
+
 sg_status sg_memset(void* dev_ptr, int value, uint64_t bytes, void* stream) {
   if (bytes == 0) return SG_OK;
   SG_REQUIRE(dev_ptr, SG_ERR_INVALID, "NULL pointer in sg_memset");
