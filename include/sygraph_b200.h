@@ -155,6 +155,21 @@ typedef struct {
 sg_status sg_graph_create_csr(const uint32_t* host_row_offsets, const uint32_t* host_column_indices,
                               const void* host_values, int value_type, uint32_t n, uint64_t m, uint32_t flags,
                               void* stream, sg_graph* out);
+/* Edge list -> device graph, built on the device (the step before the path;
+ * the reference builds on the host: io/read_csr.hpp:260-300 fromCOO,
+ * formats/csr.hpp:179-209 invert, graph_csr.hpp:394-426 upload).  The same
+ * CSR as sg_csr_from_edges followed by sg_graph_create_csr: symmetrize adds
+ * (v,u) for every edge (u,v) with u != v and makes the graph undirected,
+ * dedupe keeps the first of repeated pairs in edge order, drop_self_loops
+ * drops (v,v); rows sorted by column; values NULL or value_type
+ * SG_WEIGHT_NONE means every weight 1.  Without symmetrize the graph is
+ * directed and its inverse CSR is built too.  src / dst / values are device
+ * pointers when device_pointers, else host arrays (copied first).  Edge
+ * entries (2 * count when symmetrised) must be below 2^32; an endpoint >= n
+ * is SG_ERR_INVALID. */
+sg_status sg_graph_create_coo(const uint32_t* src, const uint32_t* dst, const void* values, int value_type,
+                              uint32_t n, uint64_t count, int symmetrize, int dedupe, int drop_self_loops,
+                              int device_pointers, void* stream, sg_graph* out);
 sg_status sg_graph_destroy(sg_graph g);
 sg_status sg_graph_info(sg_graph g, uint32_t* n, uint64_t* m, uint32_t* flags, int* value_type);
 /* GraphCSR::getDeviceGraph / getInverseDeviceGraph (graph_csr.hpp:300-320). */

@@ -115,6 +115,8 @@ SIGNATURES = {
     "sg_device_synchronize": (st, []),
     # graph
     "sg_graph_create_csr": (st, [u32p, u32p, vp, C.c_int, C.c_uint32, C.c_uint64, C.c_uint32, vp, C.POINTER(vp)]),
+    "sg_graph_create_coo": (st, [vp, vp, vp, C.c_int, C.c_uint32, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, vp,
+                                 C.POINTER(vp)]),
     "sg_graph_destroy": (st, [vp]),
     "sg_graph_info": (st, [vp, u32p, u64p, u32p, C.POINTER(C.c_int)]),
     "sg_graph_device_view": (st, [vp, C.c_int, C.POINTER(GraphView)]),

@@ -158,19 +158,45 @@ class Graph:
         h = C.c_void_p()
         call("sg_graph_create_csr", _ptr(csr.row_offsets), _ptr(csr.column_indices), _vptr(csr.values),
              csr.value_type, csr.n, csr.m, props.flags, stream, C.byref(h))
+        self._adopt(h, stream, csr)
+
+    def _adopt(self, h, stream, csr: CSR | None) -> None:
         self.handle = h
-        self.csr = csr
-        self.properties = props
         self.stream = stream
-        info_vt = C.c_int()
-        call("sg_graph_info", h, None, None, None, C.byref(info_vt))
-        self.value_type = info_vt.value
+        self._csr = csr
+        n, m, flags, vt = C.c_uint32(), C.c_uint64(), C.c_uint32(), C.c_int()
+        call("sg_graph_info", h, C.byref(n), C.byref(m), C.byref(flags), C.byref(vt))
+        self._n, self._m, self.value_type = n.value, m.value, vt.value
+        self.properties = Properties(directed=bool(flags.value & GRAPH_DIRECTED),
+                                     weighted=bool(flags.value & GRAPH_WEIGHTED))
+        if csr is not None:
+            self.properties = csr.properties if csr.properties.flags == flags.value else self.properties
+
+    @classmethod
+    def from_handle(cls, h, stream=None) -> "Graph":
+        """Wraps a graph the library built on the device; its host CSR is
+        copied back only when asked for (`csr`)."""
+        g = cls.__new__(cls)
+        g._adopt(h, stream, None)
+        return g
+
+    @property
+    def csr(self) -> CSR:
+        if self._csr is None:
+            ro = np.empty(self._n + 1, np.uint32)
+            col = np.empty(self._m, np.uint32)
+            val = np.empty(self._m, _NP_OF_WT[self.value_type])
+            call("sg_graph_copy_csr", self.handle, 0, _ptr(ro), _ptr(col), C.c_void_p(val.ctypes.data))
+            weighted = self.properties.weighted
+            self._csr = CSR(ro, col, val if weighted else None, self.value_type if weighted else None,
+                            self.properties)
+        return self._csr
 
     def getVertexCount(self) -> int:
-        return self.csr.n
+        return self._n
 
     def getEdgeCount(self) -> int:
-        return self.csr.m
+        return self._m
 
     def getDegree(self, v: int) -> int:
         return int(self.csr.row_offsets[v + 1] - self.csr.row_offsets[v])
@@ -206,6 +232,44 @@ class build:  # noqa: N801 - mirrors graph::build
     def fromCSR(csr: CSR, properties: Properties | None = None, stream=None) -> Graph:
         """graph::build::fromCSR (graph/build.hpp:31-41)."""
         return Graph(csr, properties, stream)
+
+    @staticmethod
+    def fromCOO(n: int, src, dst, values=None, value_type: int | None = None, symmetrize: bool = False,
+                dedupe: bool = False, drop_self_loops: bool = False, stream=None) -> Graph:
+        """Edge list -> device graph, built on the device (sg_graph_create_coo):
+        the same CSR as io.fromCOO + fromCSR.  src / dst / values are host
+        arrays, or DeviceArray objects already on the device."""
+        dev = isinstance(src, DeviceArray)
+        if dev:
+            count = int(np.prod(src.shape))
+            ps, pd = C.c_void_p(src.ptr), C.c_void_p(dst.ptr)
+            pv = C.c_void_p(values.ptr) if values is not None else None
+            if value_type is None:
+                value_type = WEIGHT_NONE if values is None else (WEIGHT_F32 if values.dtype == np.float32
+                                                                 else WEIGHT_U32)
+            keep = ()
+        else:
+            s_ = np.ascontiguousarray(src, np.uint32)
+            d_ = np.ascontiguousarray(dst, np.uint32)
+            if s_.size != d_.size:
+                raise ValueError("src and dst must have the same length")
+            count = s_.size
+            v_ = None
+            if values is not None:
+                values = np.asarray(values)
+                if value_type is None:
+                    value_type = WEIGHT_F32 if values.dtype.kind == "f" else WEIGHT_U32
+                v_ = np.ascontiguousarray(values, _NP_OF_WT[value_type])
+            elif value_type is None:
+                value_type = WEIGHT_NONE
+            ps, pd = C.c_void_p(s_.ctypes.data), C.c_void_p(d_.ctypes.data)
+            pv = None if v_ is None else C.c_void_p(v_.ctypes.data)
+            keep = (s_, d_, v_)
+        h = C.c_void_p()
+        call("sg_graph_create_coo", ps, pd, pv, value_type, int(n), int(count), int(symmetrize), int(dedupe),
+             int(drop_self_loops), int(dev), stream, C.byref(h))
+        del keep
+        return Graph.from_handle(h, stream)
 
 
 class Frontier:

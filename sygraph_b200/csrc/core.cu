@@ -144,6 +144,21 @@ __global__ void barrier_check_kernel(sygraph::detail::GridBarrier* bar, uint32_t
 
 using namespace sgb;
 
+void sgb::release_graph(sg_graph g) {
+  if (!g) return;
+  dev_free(g->wcol);
+  if (g->wval) cudaFree(g->wval);
+  if (g->owns_inverse) {
+    dev_free(g->inv.ro);
+    dev_free(g->inv.col);
+    if (g->inv.val) cudaFree(g->inv.val);
+  }
+  dev_free(g->fwd.ro);
+  dev_free(g->fwd.col);
+  if (g->fwd.val) cudaFree(g->fwd.val);
+  delete g;
+}
+
 extern "C" {
 
 const char* sg_last_error(void) { return t_last_error.c_str(); }
@@ -340,20 +355,6 @@ static sg_status build_inverse(sg_graph g, const uint32_t* h_ro, const uint32_t*
   return SG_OK;
 }
 
-static void release_graph(sg_graph g) {
-  if (!g) return;
-  dev_free(g->wcol);
-  if (g->wval) cudaFree(g->wval);
-  if (g->owns_inverse) {
-    dev_free(g->inv.ro);
-    dev_free(g->inv.col);
-    if (g->inv.val) cudaFree(g->inv.val);
-  }
-  dev_free(g->fwd.ro);
-  dev_free(g->fwd.col);
-  if (g->fwd.val) cudaFree(g->fwd.val);
-  delete g;
-}
 
 sg_status sg_graph_create_csr(const uint32_t* host_row_offsets, const uint32_t* host_column_indices,
                               const void* host_values, int value_type, uint32_t n, uint64_t m, uint32_t flags,

@@ -92,6 +92,8 @@ inline unsigned grid_for(uint64_t work_items, unsigned block, unsigned per_sm = 
 
 // Device address of an sg_mlp's parameter block (selector.cu).
 const void* mlp_device_params(sg_mlp h);
+// Frees a graph and every device array it owns.
+void release_graph(sg_graph g);
 // Builds g->wcol / g->wval once (weighted graphs only).
 sg_status graph_weight_sorted(sg_graph g);
 // SG_ERR_TIMEOUT when the last launch of the instance left its grid barrier's
