@@ -271,6 +271,46 @@ SSSP_DELTA = 0.1
 SSSP_PULL = 0  # pull iterations off: on RMAT they cost more than the pushes they replace
 
 
+def _edge_list(g, seed: int = 5):
+    """One direction (u < v) of each pair of a symmetric CSR, shuffled."""
+    ro, col = g.row_offsets, g.column_indices
+    src = np.repeat(np.arange(g.n, dtype=np.uint32), np.diff(ro))
+    keep = src < col
+    order = np.random.default_rng(seed).permutation(int(keep.sum()))
+    return src[keep][order], col[keep][order], g.values[keep][order]
+
+
+def construction_bench(sg, torch, g) -> dict:
+    def wall(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, r
+
+    s, d, w = _edge_list(g)
+    build = lambda a, b, c: sg.graph.build.fromCOO(g.n, a, b, c, symmetrize=True, dedupe=True,  # noqa: E731
+                                                   drop_self_loops=True)
+    t_host_arrays = min(wall(lambda: build(s, d, w))[0] for _ in range(3))
+    ds, dd, dw = sg.DeviceArray(s), sg.DeviceArray(d), sg.DeviceArray(w)
+    t_dev_arrays, G = wall(lambda: build(ds, dd, dw))
+    t_dev_arrays = min([t_dev_arrays] + [wall(lambda: build(ds, dd, dw))[0] for _ in range(2)])
+    same = bool(np.array_equal(G.csr.row_offsets, g.row_offsets) and np.array_equal(G.csr.column_indices,
+                                                                                      g.column_indices))
+    del G, ds, dd, dw
+    g20 = sg.io.rmat(20, EDGE_FACTOR, *RMAT_ABC, seed=1)
+    s2, d2, w2 = _edge_list(g20)
+    t_dev20 = min(wall(lambda: sg.graph.build.fromCOO(g20.n, s2, d2, w2, symmetrize=True, dedupe=True,
+                                                     drop_self_loops=True))[0] for _ in range(3))
+    t_host20 = wall(lambda: sg.graph.build.fromCSR(sg.io.fromCOO(g20.n, s2, d2, w2, symmetrize=True, dedupe=True,
+                                                                  drop_self_loops=True)))[0]
+    return {"workload": f"RMAT-{SCALE} edge list ({s.size} pairs, shuffled) -> symmetrised CSR (m {g.m})",
+            "device_ms_from_host_arrays": t_host_arrays * 1e3, "device_ms_from_device_arrays": t_dev_arrays * 1e3,
+            "identical_csr": same,
+            "rmat20": {"pairs": int(s2.size), "device_ms_from_host_arrays": t_dev20 * 1e3,
+                       "host_ms": t_host20 * 1e3, "speedup": t_host20 / t_dev20}}
+
+
 def serving_bench(sg, torch) -> dict:
     """Eight resident RMAT graphs (edge factor 16, float32 weights), Poisson
     BFS/SSSP queries (70/30, uniform graph and source) through the serving
@@ -532,6 +572,12 @@ def main():
                            "bytes_per_launch": bc_bytes, "traffic": ncu_traffic("bc_batch_kernel")}
     del bcb, bc1, Gbc, gbc
 
+    # graph construction on the device: the bench graph's edge list (one
+    # direction of each pair, shuffled, with its weights) -> symmetrised,
+    # de-duplicated CSR, checked equal to the generator's; the host path
+    # (sg_csr_from_edges + upload) timed on the RMAT-20 edge list only
+    construction = construction_bench(sg, torch, g)
+
     # SSSP on a subset of the same sources (reported beside the BFS line)
     sssp = sg.algorithms.SSSP(G)
     ss_edges, ss_ms = 0, 0.0
@@ -601,6 +647,7 @@ def main():
                                      "bytes_per_launch": ms_bytes, "traffic": ncu_traffic("msbfs_kernel")}},
             "learned": learned,
             "bc_batched": bc_line,
+            "construction": construction,
             "serving": serve,
             "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
                      "schedule": "frontier Bellman-Ford (the reference's)",
