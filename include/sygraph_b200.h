@@ -127,6 +127,12 @@ sg_status sg_debug_barrier_check(uint32_t blocks, uint32_t skip_block, uint64_t 
 sg_status sg_stream_create(void** stream);
 sg_status sg_stream_destroy(void* stream);
 sg_status sg_stream_synchronize(void* stream);
+/* Device timing for callers without a CUDA toolchain: an event recorded on
+ * `stream` (NULL: the legacy default stream), and the milliseconds between
+ * two recorded events (waits for `end`). */
+sg_status sg_event_record(void* stream, void** event);
+sg_status sg_event_elapsed_ms(void* start, void* end, float* ms);
+sg_status sg_event_destroy(void* event);
 sg_status sg_device_synchronize(void);
 /* Number of kernels this library has launched in this process (all entry
  * points, all devices); used to report launch counts. */

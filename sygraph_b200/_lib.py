@@ -109,6 +109,9 @@ SIGNATURES = {
     "sg_memcpy_async": (st, [vp, vp, C.c_uint64, C.c_int, vp]),
     "sg_memset": (st, [vp, C.c_int, C.c_uint64, vp]),
     "sg_debug_barrier_check": (st, [C.c_uint32, C.c_uint32, C.c_uint64, u32p, u32p]),
+    "sg_event_record": (st, [vp, C.POINTER(vp)]),
+    "sg_event_elapsed_ms": (st, [vp, vp, C.POINTER(C.c_float)]),
+    "sg_event_destroy": (st, [vp]),
     "sg_stream_create": (st, [C.POINTER(vp)]),
     "sg_stream_destroy": (st, [vp]),
     "sg_stream_synchronize": (st, [vp]),

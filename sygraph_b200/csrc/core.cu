@@ -289,6 +289,33 @@ sg_status sg_debug_barrier_check(uint32_t blocks, uint32_t skip_block, uint64_t 
   return st;
 }
 
+sg_status sg_event_record(void* stream, void** event) {
+  clear_error();
+  SG_REQUIRE(event, SG_ERR_INVALID, "NULL argument");
+  cudaEvent_t e = nullptr;
+  SG_CUDA(cudaEventCreate(&e));
+  const cudaError_t r = cudaEventRecord(e, (cudaStream_t)stream);
+  if (r != cudaSuccess) {
+    cudaEventDestroy(e);
+    return cuda_fail(r, "cudaEventRecord", __FILE__, __LINE__);
+  }
+  *event = e;
+  return SG_OK;
+}
+
+sg_status sg_event_elapsed_ms(void* start, void* end, float* ms) {
+  clear_error();
+  SG_REQUIRE(start && end && ms, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaEventSynchronize((cudaEvent_t)end));
+  SG_CUDA(cudaEventElapsedTime(ms, (cudaEvent_t)start, (cudaEvent_t)end));
+  return SG_OK;
+}
+
+sg_status sg_event_destroy(void* event) {
+  if (event) cudaEventDestroy((cudaEvent_t)event);
+  return SG_OK;
+}
+
 sg_status sg_stream_create(void** stream) {
   clear_error();
   SG_REQUIRE(stream, SG_ERR_INVALID, "NULL argument");
