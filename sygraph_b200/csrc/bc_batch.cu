@@ -43,7 +43,8 @@ namespace bcb {
 using namespace eng;
 using u64 = unsigned long long;
 
-constexpr uint32_t kCtaDeg = 1024;    // degree from which a vertex takes a whole CTA
+constexpr uint32_t kCtaDeg = 1024;    // degree from which a vertex is gathered in chunks by many warps
+constexpr uint32_t kChunkE = 1024;    // edges per chunk of such a vertex (one warp)
 constexpr uint32_t kMarkDeg = 256;    // frontier out-degree from which the whole grid marks its edges
 constexpr uint32_t kRow = 64;         // floats per sigma / q row
 constexpr uint32_t kUnroll = 8;       // row loads a warp keeps in flight
@@ -55,9 +56,10 @@ struct Counters {
   u64 reached;    // sum over (source, newly reached vertex) of its out-degree
   u64 new_deg;    // out-degree sum of the vertices that gained a source
   u64 done_in;    // in-degree sum of the vertices every source has now reached
-  uint32_t big;   // CTA-sized vertices of this phase (global list)
+  u64 big_packed; // (entries << 32) | chunks of this phase's chunked vertices
   uint32_t mark;  // high-degree vertices of the next frontier (mark list)
-  u64 pad[3];
+  uint32_t pad0;
+  u64 pad[2];
 };
 
 struct Params {
@@ -75,7 +77,11 @@ struct Params {
   uint32_t* act;        // cap_levels * w0: hist[L] != 0
   uint32_t* done;       // w0: every source reached (or no in-edge)
   uint32_t* cand;       // w0: marked candidates of a sparse level (zero between levels)
-  uint32_t* big;        // big_cap: CTA-sized vertices of the current phase
+  uint32_t* big;        // big_cap: chunked vertices of the current phase
+  uint32_t* big_first;  // big_cap: their first chunk index
+  float* part;          // chunk_cap * 64: per-chunk partial sums
+  u64* part_mask;       // chunk_cap: per-chunk source masks (forward)
+  uint32_t chunk_cap;
   uint32_t* mark;       // 2 * big_cap: frontier vertices of out-degree >= kMarkDeg, by level parity
   uint32_t big_cap;     // > (number of edges) / kMarkDeg
   const uint32_t* no_in_edges;
@@ -90,8 +96,6 @@ struct Params {
 };
 
 struct Shared {
-  float part[16][kRow];  // per-warp partial sums of a CTA-sized vertex
-  u64 mask[16];
   uint32_t scan[32];
   u64 red[32];
 };
@@ -241,42 +245,60 @@ __device__ __forceinline__ void backward_finish(const Params& P, uint32_t v, u64
   if (lane == 0) st_cg(P.bc + v, ld_cg(P.bc + v) + t);
 }
 
-// A CTA-sized vertex: the warps gather contiguous slices of its list and the
-// partial sums are added in warp order.  Called by every thread of the block.
+// Chunked vertices (degree >= kCtaDeg): every warp of the grid takes chunks
+// of kChunkE edges (its first owner by a warp-wide search, then the next
+// ones), gathers each into its own partial sums; after a grid barrier one
+// warp per vertex adds the partials in chunk order (a fixed order, so
+// repeated runs give the same bits) and finishes the vertex.
 template <bool kForward>
-__device__ __forceinline__ void cta_vertex(const Params& P, Shared& S, const u64* hist_src, u64* hist_N,
-                                           uint32_t* act_N, uint32_t* mark_N, Counters* C, uint32_t x, Local& loc) {
-  const uint32_t lane = threadIdx.x & 31, wl = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const uint32_t beg = kForward ? P.iro[x] : P.ro[x];
-  const uint32_t end = kForward ? P.iro[x + 1] : P.ro[x + 1];
-  const uint32_t deg = end - beg;
-  const uint32_t slice = ((deg + nw - 1) / nw + 31) & ~31u;
-  const uint32_t sb = min(end, beg + wl * slice), se = min(end, sb + slice);
-  const u64 sx = kForward ? ld_cg(P.seen + x) : ld_cg(hist_src + x);
-  float a0 = 0.f, a1 = 0.f;
-  u64 mk = 0;
-  if (kForward)
-    mk = forward_gather(P, hist_src, sb, se, sx, a0, a1);
-  else if (hist_N)
-    backward_gather(P, hist_N, sb, se, sx, a0, a1);
-  S.part[wl][2 * lane] = a0;
-  S.part[wl][2 * lane + 1] = a1;
-  if (lane == 0) S.mask[wl] = mk;
-  __syncthreads();
-  if (wl == 0) {
+__device__ __forceinline__ void gather_chunks(const Params& P, const u64* hist_src, const u64* hist_N, uint32_t n_big,
+                                              uint32_t n_chunks) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = gwarp; c < n_chunks; c += nwarps) {
+    const uint32_t ent = warp_find_owner(P.big_first, n_big, c);
+    const uint32_t x = ld_cg(P.big + ent);
+    const uint32_t first = ld_cg(P.big_first + ent);
+    const uint32_t beg = kForward ? P.iro[x] : P.ro[x];
+    const uint32_t end = kForward ? P.iro[x + 1] : P.ro[x + 1];
+    const uint32_t cb = beg + (c - first) * kChunkE, ce = min(end, cb + kChunkE);
+    const u64 sx = kForward ? ld_cg(P.seen + x) : ld_cg(hist_src + x);
+    float a0 = 0.f, a1 = 0.f;
+    u64 mk = 0;
+    if (kForward)
+      mk = forward_gather(P, hist_src, cb, ce, sx, a0, a1);
+    else
+      backward_gather(P, hist_N, cb, ce, sx, a0, a1);
+    __stcg(reinterpret_cast<float2*>(P.part + (size_t)c * kRow) + lane, make_float2(a0, a1));
+    if (lane == 0) st_cg(P.part_mask + c, mk);
+  }
+}
+
+template <bool kForward>
+__device__ __forceinline__ void finish_chunked(const Params& P, const u64* hist_src, u64* hist_N, uint32_t* act_N,
+                                               uint32_t* mark_N, Counters* C, uint32_t n_big, uint32_t n_chunks,
+                                               Local& loc) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t ent = gwarp; ent < n_big; ent += nwarps) {
+    const uint32_t x = ld_cg(P.big + ent);
+    const uint32_t c0 = ld_cg(P.big_first + ent);
+    const uint32_t c1 = ent + 1 < n_big ? ld_cg(P.big_first + ent + 1) : n_chunks;
     float t0 = 0.f, t1 = 0.f;
     u64 all = 0;
-    for (uint32_t w = 0; w < nw; w++) {
-      t0 += S.part[w][2 * lane];
-      t1 += S.part[w][2 * lane + 1];
-      all |= S.mask[w];
+    for (uint32_t c = c0; c < c1; c++) {
+      const float2 pr = __ldcg(reinterpret_cast<const float2*>(P.part + (size_t)c * kRow) + lane);
+      t0 += pr.x;
+      t1 += pr.y;
+      if (kForward) all |= ld_cg(P.part_mask + c);
     }
     if (kForward)
-      forward_finish(P, hist_N, act_N, mark_N, C, x, sx, all, t0, t1, loc);
+      forward_finish(P, hist_N, act_N, mark_N, C, x, ld_cg(P.seen + x), all, t0, t1, loc);
     else
-      backward_finish(P, x, sx, t0, t1);
+      backward_finish(P, x, ld_cg(hist_src + x), t0, t1);
   }
-  __syncthreads();
 }
 
 __device__ __forceinline__ void block_add(Local& loc, Shared& S, Counters* C) {
@@ -292,12 +314,17 @@ __device__ __forceinline__ void block_add(Local& loc, Shared& S, Counters* C) {
   }
 }
 
-// Appends CTA-sized vertex x to the phase's global list (processed after the
-// phase's light pass, CTAs taking entries round-robin); true when deferred.
+// Appends vertex x of degree >= kCtaDeg, with its first chunk index, to the
+// phase's chunked list (one atomic reserves the entry and its chunks, so the
+// first-chunk indices increase with the entries); true when deferred.
 // Warp-uniform.
 __device__ __forceinline__ bool defer_big(const Params& P, Counters* C, uint32_t x, uint32_t deg) {
   if (deg < kCtaDeg) return false;
-  if ((threadIdx.x & 31) == 0) P.big[atomicAdd(&C->big, 1u)] = x;
+  if ((threadIdx.x & 31) == 0) {
+    const u64 old = atomicAdd(&C->big_packed, (1ull << 32) | ((deg + kChunkE - 1) / kChunkE));
+    P.big[old >> 32] = x;
+    P.big_first[old >> 32] = (uint32_t)old;
+  }
   return true;
 }
 
@@ -438,9 +465,15 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
       }
     }
     if (!grid_sync(P.bar)) return;
-    const uint32_t nbig = ld_cg(&C->big);
-    for (uint32_t i = blockIdx.x; i < nbig; i += gridDim.x)
-      cta_vertex<true>(P, S, hist_L, hist_N, act_N, mark_N, C, ld_cg(P.big + i), loc);
+    {
+      const u64 bp = ld_cg(&C->big_packed);
+      const uint32_t nbig = (uint32_t)(bp >> 32), nch = (uint32_t)bp;
+      if (nbig) {  // grid-uniform
+        gather_chunks<true>(P, hist_L, nullptr, nbig, nch);
+        if (!grid_sync(P.bar)) return;
+        finish_chunked<true>(P, hist_L, hist_N, act_N, mark_N, C, nbig, nch, loc);
+      }
+    }
     block_add(loc, S, C);
     if (!grid_sync(P.bar)) return;
     const u64 next = ld_cg(&C->new_count);
@@ -497,10 +530,16 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
       }
     }
     if (!grid_sync(P.bar)) return;
-    const uint32_t nbig = ld_cg(&C->big);
-    for (uint32_t i = blockIdx.x; i < nbig; i += gridDim.x)
-      cta_vertex<false>(P, S, hist_B, const_cast<u64*>(hist_next), nullptr, nullptr, C, ld_cg(P.big + i), unused);
-    if (!grid_sync(P.bar)) return;
+    {
+      const u64 bp = ld_cg(&C->big_packed);
+      const uint32_t nbig = (uint32_t)(bp >> 32), nch = (uint32_t)bp;
+      if (nbig) {  // grid-uniform
+        gather_chunks<false>(P, hist_B, hist_next, nbig, nch);
+        if (!grid_sync(P.bar)) return;
+        finish_chunked<false>(P, hist_B, nullptr, nullptr, nullptr, C, nbig, nch, unused);
+        if (!grid_sync(P.bar)) return;
+      }
+    }
     if (gtid == 0 && n_log < kMaxLog) {
       sg_level_record r = {};
       r.level = Lb;
@@ -544,7 +583,10 @@ struct sg_bc_batch_s {
   unsigned long long* hist = nullptr;
   uint32_t *act = nullptr, *done = nullptr, *no_in = nullptr, *sources = nullptr;
   uint32_t* cand = nullptr;
-  uint32_t *big = nullptr, *mark = nullptr, big_cap = 0;
+  uint32_t *big = nullptr, *big_first = nullptr, *mark = nullptr, big_cap = 0;
+  float* part = nullptr;                // chunk partial sums of degree >= kCtaDeg vertices
+  unsigned long long* part_mask = nullptr;
+  uint32_t chunk_cap = 0;
   float *sigma = nullptr, *q = nullptr, *bc = nullptr;
   bcb::Counters* cnt = nullptr;
   sygraph::detail::GridBarrier* bar = nullptr;
@@ -566,6 +608,9 @@ void bcb_release(sg_bc_batch h) {
   dev_free(h->q);
   dev_free(h->cand);
   dev_free(h->big);
+  dev_free(h->big_first);
+  dev_free(h->part);
+  dev_free(h->part_mask);
   dev_free(h->mark);
   dev_free(h->bc);
   dev_free(h->cnt);
@@ -622,6 +667,10 @@ sg_status bcb_launch(sg_bc_batch h, uint32_t k, int accumulate) {
   P.q = h->q;
   P.cand = h->cand;
   P.big = h->big;
+  P.big_first = h->big_first;
+  P.part = h->part;
+  P.part_mask = h->part_mask;
+  P.chunk_cap = h->chunk_cap;
   P.mark = h->mark;
   P.big_cap = h->big_cap;
   P.bc = h->bc;
@@ -648,6 +697,8 @@ sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* o
   h->w0 = div_up(g->n, 32);
   // at most m / kMarkDeg vertices have a degree >= kMarkDeg (>= kCtaDeg too)
   h->big_cap = (uint32_t)std::min<uint64_t>(g->n, g->m / bcb::kMarkDeg + 2);
+  // chunks of the vertices of degree >= kCtaDeg: at most m / kChunkE + one per vertex
+  h->chunk_cap = (uint32_t)std::min<uint64_t>(0xffffffffu, g->m / bcb::kChunkE + h->big_cap);
   const uint64_t n = g->n;
   uint32_t levels = history_levels;
   if (!levels) levels = (uint32_t)std::max<uint64_t>(16, std::min<uint64_t>(256, (2ull << 30) / level_bytes(h)));
@@ -656,7 +707,9 @@ sg_status sg_bc_batch_create(sg_graph g, uint32_t history_levels, sg_bc_batch* o
   if ((s = dev_alloc(&h->seen, n)) || (s = dev_alloc(&h->done, h->w0)) || (s = dev_alloc(&h->no_in, h->w0)) ||
       (s = dev_alloc(&h->sources, 64)) || (s = dev_alloc(&h->sigma, n * bcb::kRow)) ||
       (s = dev_alloc(&h->q, n * bcb::kRow)) || (s = dev_alloc(&h->cand, h->w0)) ||
-      (s = dev_alloc(&h->big, h->big_cap)) || (s = dev_alloc(&h->mark, 2ull * h->big_cap)) || (s = dev_alloc(&h->bc, n)) || (s = dev_alloc(&h->cnt, 3)) ||
+      (s = dev_alloc(&h->big, h->big_cap)) || (s = dev_alloc(&h->big_first, h->big_cap)) ||
+      (s = dev_alloc(&h->part, (uint64_t)h->chunk_cap * bcb::kRow)) || (s = dev_alloc(&h->part_mask, h->chunk_cap)) ||
+      (s = dev_alloc(&h->mark, 2ull * h->big_cap)) || (s = dev_alloc(&h->bc, n)) || (s = dev_alloc(&h->cnt, 3)) ||
       (s = dev_alloc(&h->bar, 1)) || (s = dev_alloc(&h->log, SG_MAX_LOGGED_LEVELS)) ||
       (s = dev_alloc(&h->result, 4)) || (s = bcb_history(h, levels))) {
     bcb_release(h);
