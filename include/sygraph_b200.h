@@ -444,6 +444,10 @@ sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels);
  * default): more words put more first-neighbour probes in flight. */
 sg_status sg_bfs_set_pull_words(sg_bfs b, uint32_t words);
 sg_status sg_bfs_set_selector_margin(sg_bfs b, float margin);
+/* Learned mode: a frontier smaller than fraction * n keeps the heuristic's
+ * choice without an inference (when that choice is allowed).  Default 1e-3;
+ * 0 asks the MLP on every level. */
+sg_status sg_bfs_set_selector_min_frontier(sg_bfs b, float fraction);
 sg_status sg_bfs_log_features(sg_bfs b, int enable);
 sg_status sg_bfs_level_features(sg_bfs b, float* host_features, uint32_t cap_levels, uint32_t* count);
 

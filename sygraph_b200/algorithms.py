@@ -78,13 +78,18 @@ class BFS:
         s = np.ascontiguousarray(strategies if strategies is not None else [], np.int32)
         call("sg_bfs_set_schedule", self.handle, s.ctypes.data_as(C.POINTER(C.c_int)), s.size)
 
-    def set_selector(self, mlp, allowed: int = 0x3F, margin: float | None = None) -> None:
+    def set_selector(self, mlp, allowed: int = 0x3F, margin: float | None = None,
+                     min_frontier: float | None = None) -> None:
         """The MLP of bfs_direction.learned (None detaches it); `margin` is the
-        predicted log-time gain it needs to overrule the heuristic."""
+        predicted log-time gain it needs to overrule the heuristic, and
+        frontiers below `min_frontier` of the vertices keep the heuristic's
+        choice without an inference."""
         self._mlp = mlp  # keep the device parameters alive
         call("sg_bfs_set_selector", self.handle, mlp.handle if mlp is not None else None, allowed)
         if margin is not None:
             call("sg_bfs_set_selector_margin", self.handle, float(margin))
+        if min_frontier is not None:
+            call("sg_bfs_set_selector_min_frontier", self.handle, float(min_frontier))
 
     def set_pull_order(self, reverse_levels: int) -> None:
         """Bit L: level L's pull probes in-neighbours from the back."""

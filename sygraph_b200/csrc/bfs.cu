@@ -255,6 +255,7 @@ struct sg_bfs_s {
   const sygraph::detail::MlpParams* mlp = nullptr;  // not owned
   uint32_t allowed = 0x3f;
   float margin = 0.05f;
+  float min_frontier = 1e-3f;  // learned mode: frontiers below this fraction of n keep the heuristic
   unsigned long long pull_reverse = 0;  // levels whose pull probes in-neighbours from the back
   uint32_t pull_words = 4;              // bitmap words per warp step of a short-circuit pull
   float* features = nullptr;
@@ -310,6 +311,7 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.mlp = b->mlp;
   P.allowed = b->allowed;
   P.margin = b->margin;
+  P.min_frontier = b->min_frontier;
   P.pull_reverse = b->pull_reverse;
   P.pull_words = b->pull_words;
   P.features = b->features;
@@ -484,6 +486,14 @@ sg_status sg_bfs_set_pull_words(sg_bfs b, uint32_t words) {
   SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
   SG_REQUIRE(words == 2 || words == 4, SG_ERR_INVALID, "2 or 4 words per warp step");
   b->pull_words = words;
+  return SG_OK;
+}
+
+sg_status sg_bfs_set_selector_min_frontier(sg_bfs b, float fraction) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_REQUIRE(fraction >= 0.f && fraction <= 1.f, SG_ERR_INVALID, "fraction must be in [0, 1]");
+  b->min_frontier = fraction;
   return SG_OK;
 }
 
@@ -677,6 +687,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.mlp = nullptr;
   P.allowed = 0x3f;
   P.margin = 0.f;
+  P.min_frontier = 0.f;
   P.pull_reverse = 0;
   P.pull_words = 2;
   P.features = nullptr;

@@ -30,6 +30,9 @@ HYBRID_ALPHA, HYBRID_BETA = 15.0, 24.0
 # this much slower in log-time (chosen on the training tables: most of the
 # gain, no training traversal more than about 1% slower than the heuristic)
 MARGIN = 0.05
+# the engine skips the inference on frontiers below this fraction of n (the
+# heuristic's choice stands there), as kLearnedMinFrontier in the engine
+MIN_FRONTIER = 1e-3
 MAX_LEVELS = 4096
 
 # (name, generator, kwargs): RMAT skews and scales, grids with and without
@@ -144,11 +147,12 @@ def traversals(data: dict):
 
 
 def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.ndarray,
-                     allowed: int = 0x3F, margin: float = MARGIN) -> np.ndarray:
+                     allowed: int = 0x3F, margin: float = MARGIN, min_frontier: float = MIN_FRONTIER) -> np.ndarray:
     """The learned mode's schedule on a traversal: the MLP's argmin per level
     (`forward` maps a feature batch to predicted log-times) with the
     current-direction feature following its own previous choice, and the
-    heuristic where a feature leaves the trusted range, as the engine does."""
+    heuristic where a feature leaves the trusted range or the frontier is
+    below `min_frontier` of the vertices, as the engine does."""
     t0 = params.size - 4 * IN
     lo, hi = params[t0 + 2 * IN:t0 + 3 * IN], params[t0 + 3 * IN:t0 + 4 * IN]
     banned = [j for j in range(OUT) if not (allowed >> j) & 1]
@@ -158,7 +162,7 @@ def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.n
         f = np.array(F[L], np.float32)
         if L > 0:
             f[10] = 1.0 if prev >= 2 else 0.0
-        if np.any(f < lo) or np.any(f > hi):
+        if f[1] < min_frontier or np.any(f < lo) or np.any(f > hi):
             out[L] = heuristic[L]
         else:
             y = np.array(forward(f[None, :]), np.float64)[0]

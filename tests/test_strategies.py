@@ -118,7 +118,7 @@ def test_learned_mode_parity_and_mask(sg, oracle, graphs):
         bfs = sg.algorithms.BFS(G)
         for seed, allowed in ((1, 0x3F), (2, 0x03), (3, 0x0C), (4, 0x30), (5, 0x21)):
             m = _trusting_mlp(selector, seed)
-            bfs.set_selector(m, allowed, margin=0.0)  # plain argmin, checked below
+            bfs.set_selector(m, allowed, margin=0.0, min_frontier=0.0)  # plain argmin on every level, checked below
             bfs.log_features(True)
             for s in _sources(sg, g)[:2]:
                 bfs.init(s)
@@ -135,6 +135,29 @@ def test_learned_mode_parity_and_mask(sg, oracle, graphs):
                 got = np.array([r["strategy"] for r in recs])
                 best = y.min(1)
                 assert np.all(y[np.arange(len(got)), got] <= best + 1e-4 * (1 + np.abs(best)))
+
+
+def test_learned_mode_small_frontiers_keep_the_heuristic(sg, oracle, rmat):
+    """Frontiers below min_frontier * n take the heuristic's choice without an
+    inference (when it is allowed); 1.0 leaves every level to the heuristic."""
+    from sygraph_b200 import selector
+    g = rmat(14, perm_seed=7)
+    bfs = sg.algorithms.BFS(sg.graph.build.fromCSR(g))
+    s = int(np.argmax(g.degrees()))
+    ref, it, steps = oracle.bfs_frontier(g, s, 2, 15.0, 24.0)
+    bfs.set_selector(_trusting_mlp(selector, 9), margin=0.0, min_frontier=1.0)
+    bfs.init(s)
+    bfs.run(sg.algorithms.bfs_direction.learned, 15.0, 24.0)
+    assert np.array_equal(bfs.getDistances(), ref)
+    assert [r["strategy"] for r in bfs.level_records()] == [2 * x for x in steps]
+    # restricted to pull_all: the heuristic's push / pull is not allowed, so the MLP decides
+    bfs.set_selector(_trusting_mlp(selector, 9), allowed=0x30, margin=0.0, min_frontier=1.0)
+    bfs.init(s)
+    bfs.run(sg.algorithms.bfs_direction.learned, 15.0, 24.0)
+    assert np.array_equal(bfs.getDistances(), ref)
+    assert all(r["strategy"] in (4, 5) for r in bfs.level_records())
+    with pytest.raises(sg._lib.SygraphError):
+        bfs.set_selector(None, min_frontier=2.0)
 
 
 def test_learned_mode_falls_back_to_heuristic_outside_range(sg, oracle, rmat):
