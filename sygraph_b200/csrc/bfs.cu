@@ -40,7 +40,18 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
 
   // ---- init: depth = n+1 except the source; F_0 = {source}; vertices that no
   // edge reaches are pre-marked visited so pull never scans them.
-  for (uint32_t i = gtid; i < n; i += nthreads) st_cg(P.depth + i, i == src ? 0u : inf);
+  if ((reinterpret_cast<uintptr_t>(P.depth) & 15) == 0) {  // 16-byte stores
+    const uint32_t n4 = n / 4;
+    for (uint32_t i = gtid; i < n4; i += nthreads) {
+      const uint32_t b0 = 4 * i;
+      const uint4 v = make_uint4(b0 == src ? 0u : inf, b0 + 1 == src ? 0u : inf, b0 + 2 == src ? 0u : inf,
+                                 b0 + 3 == src ? 0u : inf);
+      st_cg(reinterpret_cast<uint4*>(P.depth) + i, v);
+    }
+    for (uint32_t i = 4 * n4 + gtid; i < n; i += nthreads) st_cg(P.depth + i, i == src ? 0u : inf);
+  } else {
+    for (uint32_t i = gtid; i < n; i += nthreads) st_cg(P.depth + i, i == src ? 0u : inf);
+  }
   for (uint32_t i = gtid; i < w0; i += nthreads) {
     const uint32_t b = (i == (src >> 5)) ? (1u << (src & 31)) : 0u;
     st_cg(P.visited + i, P.no_in_edges[i] | b);
@@ -120,13 +131,18 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
       else
         pull_warp(L, fb_cur, sc, level < 64 && ((P.pull_reverse >> level) & 1ull));
     }
-    // clear F_{L-1}: only the words its summary flags (push/warp did it with
-    // its own summary scan)
-    for (uint32_t j = gwarp; strategy != 0 && j < w1; j += nwarps) {
-      const uint32_t s = ld_cg(sm_zero + j);
-      if (!s) continue;
-      if ((s >> lane) & 1u) st_cg(fb_zero + j * 32 + lane, 0u);
-      if (lane == 0) st_cg(sm_zero + j, 0u);
+    // clear F_{L-1}: push/warp and the warp-mapped pulls cleared its words in
+    // their own word loops (their summary words here, no load needed); the
+    // CTA-mapped strategies clear the words its summary flags
+    if (strategy == 2 || strategy == 4) {
+      for (uint32_t j = gtid; j < w1; j += nthreads) st_cg(sm_zero + j, 0u);
+    } else if (strategy != 0) {
+      for (uint32_t j = gwarp; j < w1; j += nwarps) {
+        const uint32_t s = ld_cg(sm_zero + j);
+        if (!s) continue;
+        if ((s >> lane) & 1u) st_cg(fb_zero + j * 32 + lane, 0u);
+        if (lane == 0) st_cg(sm_zero + j, 0u);
+      }
     }
     // level totals: warp sums into shared accumulators, one global atomic per
     // counter and CTA after the barrier below

@@ -212,6 +212,13 @@ __device__ __forceinline__ bool pull_word_scan(const Params& P, const uint32_t* 
 // issued together (U column loads in flight per lane); vertices still open
 // after that (mostly those with no frontier neighbour at all, whose whole
 // list must be read) are finished edge-parallel, word by word.
+// F_{L-1}, the frontier bitmap two levels back (rotating buffers).
+__device__ __forceinline__ uint32_t* old_frontier(const Level& L) {
+  return L.P->fb + (size_t)((L.next_depth + 1) % 3) * L.P->w0;
+}
+
+// Also clears F_{L-1}: every word is visited once, and the store needs no
+// load of the old summary.
 template <int U>
 __device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, bool reverse) {
   const Params& P = *L.P;
@@ -220,6 +227,7 @@ __device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, boo
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const bool same = P.iro == P.ro;
   for (uint32_t wbase = gwarp; wbase < P.w0; wbase += U * nwarps) {
+    if (lane < (uint32_t)U && wbase + lane * nwarps < P.w0) st_cg(old_frontier(L) + wbase + lane * nwarps, 0u);
     uint32_t vw[U], cd[U], b[U], e[U];
     bool f[U];
     uint32_t any = 0;
@@ -286,6 +294,7 @@ __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool
   }
   // pull_all: every in-neighbour of every unvisited vertex is scanned
   for (uint32_t wi = gwarp; wi < P.w0; wi += nwarps) {
+    if (lane == 0) st_cg(old_frontier(L) + wi, 0u);
     const uint32_t vw = ld_cg(P.visited + wi);
     const uint32_t cand = ~vw & valid_bits(wi, P.w0, P.n);
     if (!cand) continue;
