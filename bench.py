@@ -198,6 +198,29 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def cc_fixed_point(csr, labels) -> bool:
+    """Max-label components on a symmetric graph, checked without a second
+    implementation: equal labels across every edge, every label at least the
+    vertex id, and every label the id of a vertex that carries it."""
+    ro = csr.row_offsets.astype(np.int64)
+    src = np.repeat(np.arange(csr.n, dtype=np.int64), np.diff(ro))
+    lab = labels.astype(np.int64)
+    return bool((lab[src] == lab[csr.column_indices]).all() and (lab >= np.arange(csr.n)).all()
+                and (lab[lab] == lab).all())
+
+
+def dag_wedges(csr) -> int:
+    """Sum over the degree-ordered DAG's edges (u,v) of d+(v): the set probes
+    of the triangle count (numpy, outside the timed region)."""
+    ro = csr.row_offsets.astype(np.int64)
+    col = csr.column_indices.astype(np.int64)
+    deg = np.diff(ro)
+    src = np.repeat(np.arange(csr.n, dtype=np.int64), deg)
+    keep = (deg[src] < deg[col]) | ((deg[src] == deg[col]) & (src < col))
+    dplus = np.bincount(src[keep], minlength=csr.n)
+    return int(dplus[col[keep]].sum())
+
+
 def _launch_ms(torch, fn) -> float:
     """Device time of what `fn` enqueues, by CUDA events on the current stream."""
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -229,6 +252,15 @@ def profile_case(kind: str) -> None:
     captures: the second launch is the one to capture (-s 1 -c 1 on the
     traversal kernel)."""
     import sygraph_b200 as sg
+    if kind in ("tc", "cc"):  # on the RMAT-20 graph only
+        gbc = sg.io.rmat(BC_SCALE, EDGE_FACTOR, *RMAT_ABC, seed=1)
+        Gbc = sg.graph.build.fromCSR(gbc)
+        a = sg.algorithms.TC(Gbc) if kind == "tc" else sg.algorithms.CC(Gbc)
+        for _ in range(2):
+            a.run()
+        out = {"triangles": a.getNumTriangles()} if kind == "tc" else {"sweeps": a.iterations}
+        print(json.dumps({"profile": kind, **out}))
+        return
     g, _ = make_graph(sg)
     src = int(sg.io.sample_sources(g, 1, seed=SOURCE_SEED)[0])
     G = sg.graph.build.fromCSR(g)
@@ -352,7 +384,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sub-benchmark")
     ap.add_argument("--sssp-sources", type=int, default=8)
-    ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs", "bc"], default=None,
+    ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs", "bc", "tc", "cc"], default=None,
                     help="profiling case: build the graph, run 2 traversals of one kind and exit (few launches)")
     args = ap.parse_args()
     world, rank, local = dist_init()
@@ -570,7 +602,36 @@ def main():
     bc_line["roofline"] = {"bound": "hbm", "achieved": bc_bytes / (bc_ms * 1e-3) / 1e9, "unit": "GB/s",
                            "frac": bc_bytes / (bc_ms * 1e-3) / 1e9 / peaks()[0],
                            "bytes_per_launch": bc_bytes, "traffic": ncu_traffic("bc_batch_kernel")}
-    del bcb, bc1, Gbc, gbc
+    # CC and TC on the same RMAT-20 graph, through their instances (which own
+    # their workspaces): device time of run_async, median of five after one
+    # warm-up run
+    cc = sg.algorithms.CC(Gbc)
+    cc.run()
+    cc_ok = cc_fixed_point(gbc, cc.getLabels())
+    cc_ms = float(np.median([_launch_ms(torch, cc.run_async) for _ in range(5)]))
+    cc_bytes = 4 * (gbc.n + 1) + 4 * gbc.m + 8 * gbc.n
+    cc_line = {"workload": f"max-label propagation, RMAT-{BC_SCALE} ef{EDGE_FACTOR}", "ms": cc_ms,
+               "sweeps": cc.iterations, "gteps": gbc.m / (cc_ms * 1e-3) / 1e9, "labels_fixed_point": cc_ok,
+               "roofline": {"bound": "hbm", "bytes_one_sweep": cc_bytes, "unit": "GB/s",
+                            "achieved": cc_bytes / (cc_ms * 1e-3) / 1e9,
+                            "frac": cc_bytes / (cc_ms * 1e-3) / 1e9 / peaks()[0]},
+               "note": "achieved counts one full sweep's bytes over the whole run (every sweep after the first "
+                       "touches only the vertices whose label changed)"}
+    tc = sg.algorithms.TC(Gbc)
+    tc.run()
+    tc_ms = float(np.median([_launch_ms(torch, tc.run_async) for _ in range(5)]))
+    tri = tc.getNumTriangles()
+    probes = dag_wedges(gbc)
+    tc_bytes = 4 * (gbc.n + 1) + 4 * gbc.m // 2
+    tc_line = {"workload": f"triangle count on the degree-ordered DAG, RMAT-{BC_SCALE} ef{EDGE_FACTOR}",
+               "ms": tc_ms, "triangles": tri, "dag_edges": gbc.m // 2, "set_probes": probes,
+               "probes_per_s": probes / (tc_ms * 1e-3), "dag_edges_per_s": (gbc.m // 2) / (tc_ms * 1e-3),
+               "roofline": {"bound": "hbm", "bytes": tc_bytes, "unit": "GB/s",
+                            "achieved": tc_bytes / (tc_ms * 1e-3) / 1e9,
+                            "frac": tc_bytes / (tc_ms * 1e-3) / 1e9 / peaks()[0]},
+               "note": "DAG build (keep bits, scan, compaction) plus the hash-set intersections, one run; "
+                       "set_probes = sum over DAG edges (u,v) of d+(v), the rows streamed from L2"}
+    del bcb, bc1, cc, tc, Gbc, gbc
 
     # graph construction on the device: the bench graph's edge list (one
     # direction of each pair, shuffled, with its weights) -> symmetrised,
@@ -648,6 +709,8 @@ def main():
             "learned": learned,
             "bc_batched": bc_line,
             "construction": construction,
+            "cc": cc_line,
+            "tc": tc_line,
             "serving": serve,
             "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
                      "schedule": "frontier Bellman-Ford (the reference's)",

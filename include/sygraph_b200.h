@@ -508,7 +508,18 @@ sg_status sg_sssp_distances_device(sg_sssp s, const void** dev_dist);
 sg_status sg_run_sssp(sg_graph g, uint32_t source, void* host_dist, uint64_t* iterations);
 
 /* CC(G) + init + run (algorithms/cc.hpp:82-169): maximum-label propagation
- * with atomicMax; labels[v] = max id over the vertices reaching v. */
+ * with atomicMax; labels[v] = max id over the vertices reaching v.  The
+ * instance owns the label array and the engine's workspace (cc.hpp:54), so
+ * that runs allocate nothing; runs are enqueued on the graph's stream. */
+typedef struct sg_cc_s* sg_cc_handle;
+sg_status sg_cc_create(sg_graph g, sg_cc_handle* out);
+sg_status sg_cc_destroy(sg_cc_handle c);
+sg_status sg_cc_run_async(sg_cc_handle c);
+/* iterations = propagation levels, the first one over every vertex */
+sg_status sg_cc_run(sg_cc_handle c, uint64_t* iterations);
+sg_status sg_cc_get_labels(sg_cc_handle c, uint32_t* host_labels);
+sg_status sg_cc_labels_device(sg_cc_handle c, const uint32_t** dev_labels);
+/* One-shot: create, run, copy the labels (when non-NULL), destroy. */
 sg_status sg_cc(sg_graph g, uint32_t* host_labels, uint64_t* iterations);
 
 /* BC(G) + init(source) + run (algorithms/bc.hpp:86-200) for each of k
@@ -546,10 +557,22 @@ sg_status sg_bc_batch_level_records(sg_bc_batch h, sg_level_record* host_records
 /* One-shot: any number of sources, in batches of 64. */
 sg_status sg_bc_batched(sg_graph g, const uint32_t* host_sources, uint32_t k, float* host_bc);
 
-/* TC(G) + init + run + getNumTriangles (algorithms/tc.hpp:58-138), exact:
- * degree-ordered DAG and sorted-list segmented intersection, uint64.  When
- * host_per_vertex is non-NULL it receives getNumTriangles(v): for every edge
- * (u,v) with u < v, |N(u) n N(v)| added to u. */
+/* TC(G) + init + run + getNumTriangles (algorithms/tc.hpp:58-138), exact,
+ * uint64: every run orients the edges into the degree-ordered DAG and
+ * intersects N+(u) with N+(v) for every DAG edge through shared-memory hash
+ * sets.  Rows need not be sorted.  getNumTriangles(v), the per-vertex count,
+ * is for every edge (u,v) with u < v, |N(u) n N(v)| added to u.  The instance
+ * owns the DAG and the work lists (about 4m + 20n bytes), so that runs
+ * allocate nothing; runs are enqueued on the graph's stream. */
+typedef struct sg_tc_s* sg_tc_handle;
+sg_status sg_tc_create(sg_graph g, sg_tc_handle* out);
+sg_status sg_tc_destroy(sg_tc_handle t);
+/* per_vertex != 0 also accumulates the per-vertex counts (8n more bytes) */
+sg_status sg_tc_run_async(sg_tc_handle t, int per_vertex);
+sg_status sg_tc_run(sg_tc_handle t, int per_vertex, uint64_t* total);
+sg_status sg_tc_get_total(sg_tc_handle t, uint64_t* total);
+sg_status sg_tc_get_per_vertex(sg_tc_handle t, uint64_t* host_per_vertex);
+/* One-shot; host_per_vertex may be NULL. */
 sg_status sg_tc(sg_graph g, uint64_t* total, uint64_t* host_per_vertex);
 
 /* -------------------------------------------------------------- serving -- */

@@ -222,8 +222,20 @@ SIGNATURES = {
     "sg_sssp_distances_device": (st, [vp, C.POINTER(vp)]),
     "sg_run_sssp": (st, [vp, C.c_uint32, vp, u64p]),
     "sg_cc": (st, [vp, u32p, u64p]),
+    "sg_cc_create": (st, [vp, C.POINTER(vp)]),
+    "sg_cc_destroy": (st, [vp]),
+    "sg_cc_run_async": (st, [vp]),
+    "sg_cc_run": (st, [vp, u64p]),
+    "sg_cc_get_labels": (st, [vp, u32p]),
+    "sg_cc_labels_device": (st, [vp, C.POINTER(vp)]),
     "sg_bc": (st, [vp, u32p, C.c_uint32, f32p]),
     "sg_tc": (st, [vp, u64p, u64p]),
+    "sg_tc_create": (st, [vp, C.POINTER(vp)]),
+    "sg_tc_destroy": (st, [vp]),
+    "sg_tc_run_async": (st, [vp, C.c_int]),
+    "sg_tc_run": (st, [vp, C.c_int, u64p]),
+    "sg_tc_get_total": (st, [vp, u64p]),
+    "sg_tc_get_per_vertex": (st, [vp, u64p]),
     # host graph I/O
     "sg_rmat_generate": (st, [C.POINTER(RmatParams), C.POINTER(HostCSR)]),
     "sg_grid_generate": (st, [C.c_uint32, C.c_double, C.c_uint64, C.c_uint64, C.c_int, C.POINTER(HostCSR)]),

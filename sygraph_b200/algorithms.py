@@ -245,24 +245,45 @@ class SSSP:
 
 
 class CC:
-    """algorithms::CC (cc.hpp:74-192): labels[v] = max id over the vertices reaching v."""
+    """algorithms::CC (cc.hpp:74-192): labels[v] = max id over the vertices reaching v.
+    The instance owns the labels and the engine workspace, so runs allocate nothing."""
 
     def __init__(self, G: Graph):
         self.G = G
-        self.labels = None
+        h = C.c_void_p()
+        call("sg_cc_create", G.handle, C.byref(h))
+        self.handle = h
         self.iterations = 0
+        self._labels = None
 
     def init(self, source: int = 0) -> None:
         self.source = source
 
     def run(self) -> None:
-        self.labels = np.empty(self.G.getVertexCount(), np.uint32)
         it = C.c_uint64()
-        call("sg_cc", self.G.handle, _ptr(self.labels), C.byref(it))
+        call("sg_cc_run", self.handle, C.byref(it))
         self.iterations = it.value
+        self._labels = None
+
+    def run_async(self) -> None:
+        """Enqueue a run on the graph's stream; getLabels() waits for it."""
+        call("sg_cc_run_async", self.handle)
+        self._labels = None
 
     def getLabels(self) -> np.ndarray:
-        return self.labels
+        if self._labels is None:
+            out = np.empty(self.G.getVertexCount(), np.uint32)
+            call("sg_cc_get_labels", self.handle, _ptr(out))
+            self._labels = out
+        return self._labels
+
+    labels = property(getLabels)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and lib is not None:  # module globals are gone at interpreter exit
+            lib.sg_cc_destroy(h)
+            self.handle = None
 
 
 class BC:
@@ -339,10 +360,14 @@ class BatchedBC:
 
 
 class TC:
-    """algorithms::TC (tc.hpp:473-565), exact."""
+    """algorithms::TC (tc.hpp:473-565), exact.  The instance owns the DAG and
+    the work lists, so runs allocate nothing."""
 
     def __init__(self, G: Graph):
         self.G = G
+        h = C.c_void_p()
+        call("sg_tc_create", G.handle, C.byref(h))
+        self.handle = h
         self.total = None
         self.per_vertex = None
 
@@ -351,14 +376,32 @@ class TC:
 
     def run(self, per_vertex: bool = False) -> None:
         tot = C.c_uint64()
-        pv = np.zeros(self.G.getVertexCount(), np.uint64) if per_vertex else None
-        call("sg_tc", self.G.handle, C.byref(tot), pv.ctypes.data_as(C.POINTER(C.c_uint64)) if pv is not None else None)
+        call("sg_tc_run", self.handle, int(per_vertex), C.byref(tot))
         self.total = tot.value
-        self.per_vertex = pv
+        self.per_vertex = None
+        if per_vertex:
+            pv = np.zeros(self.G.getVertexCount(), np.uint64)
+            call("sg_tc_get_per_vertex", self.handle, pv.ctypes.data_as(C.POINTER(C.c_uint64)))
+            self.per_vertex = pv
+
+    def run_async(self, per_vertex: bool = False) -> None:
+        """Enqueue a run on the graph's stream; getNumTriangles() waits for it."""
+        call("sg_tc_run_async", self.handle, int(per_vertex))
+        self.total = None
 
     def getNumTriangles(self, v: int | None = None) -> int:
         if v is None:
+            if self.total is None:
+                tot = C.c_uint64()
+                call("sg_tc_get_total", self.handle, C.byref(tot))
+                self.total = tot.value
             return int(self.total)
         if self.per_vertex is None:
             self.run(per_vertex=True)
         return int(self.per_vertex[v])
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and lib is not None:  # module globals are gone at interpreter exit
+            lib.sg_tc_destroy(h)
+            self.handle = None

@@ -677,6 +677,14 @@ struct PushWorkspace {
 
 using namespace sgb;
 
+struct sg_cc_s {
+  sg_graph g = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t* labels = nullptr;
+  bool ran = false;
+  PushWorkspace ws;
+};
+
 struct sg_sssp_s {
   sg_graph g = nullptr;
   cudaStream_t stream = nullptr;
@@ -990,30 +998,71 @@ sg_status sg_run_sssp(sg_graph g, uint32_t source, void* host_dist, uint64_t* it
   return st;
 }
 
-sg_status sg_cc(sg_graph g, uint32_t* host_labels, uint64_t* iterations) {
+sg_status sg_cc_destroy(sg_cc_handle c) {
+  if (c) {
+    cudaStreamSynchronize(c->stream);
+    c->ws.release();
+    dev_free(c->labels);
+    delete c;
+  }
+  return SG_OK;
+}
+
+sg_status sg_cc_create(sg_graph g, sg_cc_handle* out) {
   clear_error();
-  SG_REQUIRE(g, SG_ERR_INVALID, "graph is NULL");
+  SG_REQUIRE(g && out, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(g->n > 0, SG_ERR_INVALID, "graph has no vertices");
-  PushWorkspace ws;
-  uint32_t* labels = nullptr;
-  sg_status st = ws.alloc(g->n);
-  if (st == SG_OK) st = dev_alloc(&labels, g->n);
-  if (st == SG_OK) {
-    cudaError_t e = cudaMemsetAsync(ws.bar, 0, sizeof(GridBarrier), g->stream);
-    if (e != cudaSuccess) st = cuda_fail(e, "memset", __FILE__, __LINE__);
+  *out = nullptr;
+  sg_cc_handle c = new sg_cc_s();
+  c->g = g;
+  c->stream = g->stream;
+  sg_status st = c->ws.alloc(g->n);
+  if (st == SG_OK) st = dev_alloc(&c->labels, g->n);
+  if (st != SG_OK) {
+    sg_cc_destroy(c);
+    return st;
   }
-  if (st == SG_OK) {
-    CcParams P{ws.loop(g), labels, ws.result};
-    st = launch_persistent(cc_kernel, P, 2, g->stream);
-  }
-  if (st == SG_OK) st = ws.finish(g->stream, iterations);
-  if (st == SG_OK && host_labels) {
-    cudaError_t e = cudaMemcpy(host_labels, labels, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) st = cuda_fail(e, "labels copy", __FILE__, __LINE__);
-  }
-  cudaStreamSynchronize(g->stream);
-  ws.release();
-  dev_free(labels);
+  *out = c;
+  return SG_OK;
+}
+
+sg_status sg_cc_run_async(sg_cc_handle c) {
+  clear_error();
+  SG_REQUIRE(c, SG_ERR_INVALID, "cc is NULL");
+  SG_CUDA(cudaMemsetAsync(c->ws.bar, 0, sizeof(GridBarrier), c->stream));
+  CcParams P{c->ws.loop(c->g), c->labels, c->ws.result};
+  SG_TRY(launch_persistent(cc_kernel, P, 2, c->stream));
+  c->ran = true;
+  return SG_OK;
+}
+
+sg_status sg_cc_run(sg_cc_handle c, uint64_t* iterations) {
+  SG_TRY(sg_cc_run_async(c));
+  return c->ws.finish(c->stream, iterations);
+}
+
+sg_status sg_cc_get_labels(sg_cc_handle c, uint32_t* host_labels) {
+  clear_error();
+  SG_REQUIRE(c && host_labels, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(c->ran, SG_ERR_NOT_INITIALIZED, "CC not run");
+  SG_CUDA(cudaMemcpyAsync(host_labels, c->labels, sizeof(uint32_t) * c->g->n, cudaMemcpyDeviceToHost, c->stream));
+  SG_CUDA(cudaStreamSynchronize(c->stream));
+  return SG_OK;
+}
+
+sg_status sg_cc_labels_device(sg_cc_handle c, const uint32_t** dev_labels) {
+  clear_error();
+  SG_REQUIRE(c && dev_labels, SG_ERR_INVALID, "NULL argument");
+  *dev_labels = c->labels;
+  return SG_OK;
+}
+
+sg_status sg_cc(sg_graph g, uint32_t* host_labels, uint64_t* iterations) {
+  sg_cc_handle c = nullptr;
+  SG_TRY(sg_cc_create(g, &c));
+  sg_status st = sg_cc_run(c, iterations);
+  if (st == SG_OK && host_labels) st = sg_cc_get_labels(c, host_labels);
+  sg_cc_destroy(c);
   return st;
 }
 

@@ -4,13 +4,25 @@
 // full adjacency lists and adds its running count inside the merge loop
 // (tc.hpp:104), which over-counts.  Here:
 //   1. orient every edge from the endpoint with the smaller (degree, id) key
-//      (the degree-ordered DAG, out-degree O(sqrt m)); lists stay sorted;
-//   2. for every DAG edge (u,v), |N+(u) n N+(v)| by walking the shorter list
-//      and binary-searching the longer one (segmented intersection);
-//   3. each triangle is found exactly once; the total is a uint64 sum.
-// The reference's per-vertex convention (for every edge (u,v), u < v,
+//      (the degree-ordered DAG, out-degree at most sqrt(m)): one keep bit per
+//      edge, a scan of the per-word counts, and a stable compaction, so the
+//      DAG rows keep the order of the input rows;
+//   2. for every vertex u with d+(u) >= 2, N+(u) goes into a shared-memory
+//      hash set (four-slot buckets, at most half a key per bucket), and
+//      every row N+(v), v in N+(u), is streamed against it by whole warps
+//      (coalesced, eight loads in flight per lane): |N+(u) n N+(v)| summed;
+//   3. each triangle is found exactly once, from its lowest DAG vertex; the
+//      total is a uint64 sum.
+// The per-vertex convention of the reference (for every edge (u,v), u < v,
 // |N(u) n N(v)| is added to u) is recovered from the same enumeration: a
 // triangle a < b < c adds 2 to a and 1 to b.
+//
+// Work lists: vertices with d+(u) > 128 are counted by a whole block (one
+// 8192-bucket table; the flattened rows of N+(u) split evenly over the 32
+// warps), the rest by single warps (256-bucket tables), medium degrees
+// (33..128) before small ones so that the long counts start first.  A vertex
+// with d+(u) > 4096 (possible only when m > 2^24) is counted in pieces of
+// 4096 keys, which is exact for graphs without parallel edges.
 #include "internal.cuh"
 
 namespace sgb {
@@ -18,42 +30,107 @@ namespace {
 
 using sygraph::detail::block_sum;
 
+constexpr uint32_t kTcThreads = 1024, kTcWarps = kTcThreads / 32;
+constexpr uint32_t kWarpBuckets = 256;                       // one warp's table: 256 x 4 slots, 4 KB
+constexpr uint32_t kBlockBuckets = kWarpBuckets * kTcWarps;  // the block's table: 8192 buckets, 128 KB
+constexpr uint32_t kWarpMaxDeg = kWarpBuckets / 2;           // d+(u) counted by one warp
+constexpr uint32_t kSmallMaxDeg = 32;
+constexpr uint32_t kBlockMaxDeg = kBlockBuckets / 2;  // keys of one block table (4 * kTcThreads)
+constexpr uint32_t kEmptySlot = 0xffffffffu;          // never a vertex id (n < 2^32)
+constexpr uint32_t kRowUnroll = 8;                    // row loads in flight per lane
+
+struct TcCounters {
+  uint32_t n_list[3];  // heavy, medium, small
+  uint32_t next[3];    // next unclaimed entry of each list
+  unsigned long long total;
+};
+
 __device__ __forceinline__ bool dag_before(uint32_t du, uint32_t u, uint32_t dv, uint32_t v) {
   return du < dv || (du == dv && u < v);
 }
 
-__global__ void __launch_bounds__(256) dag_count_kernel(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
-                                                        uint32_t n, uint32_t* __restrict__ cnt) {
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
-    const uint32_t b = ro[u], e = ro[u + 1], du = e - b;
-    uint32_t c = 0;
-    for (uint32_t i = b; i < e; i++) {
-      const uint32_t v = col[i];
-      if (dag_before(du, u, ro[v + 1] - ro[v], v)) c++;
+// Keep bit of every edge, one thread per 32-edge word: the thread finds the
+// source of its first edge by binary search on the row offsets and walks on.
+__global__ void __launch_bounds__(256) dag_flags_kernel(const uint32_t* __restrict__ ro,
+                                                        const uint32_t* __restrict__ col, uint32_t n, uint32_t m,
+                                                        uint32_t nw, uint32_t* __restrict__ keep,
+                                                        uint32_t* __restrict__ cnt) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid == 0) cnt[nw] = 0;  // the scan's last input: its output is the DAG size
+  for (uint32_t w = tid; w < nw; w += gridDim.x * blockDim.x) {
+    const uint32_t e0 = w * 32u, e1 = (uint32_t)min((uint64_t)e0 + 32u, (uint64_t)m);
+    uint32_t lo = 0, hi = n - 1;  // last u with ro[u] <= e0: the source of edge e0
+    while (lo < hi) {
+      const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+      if (ro[mid] <= e0)
+        lo = mid;
+      else
+        hi = mid - 1;
     }
-    cnt[u] = c;
-  }
-}
-
-__global__ void __launch_bounds__(256) dag_fill_kernel(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
-                                                       uint32_t n, const uint32_t* __restrict__ dro,
-                                                       uint32_t* __restrict__ dcol, uint32_t* __restrict__ dsrc) {
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
-    const uint32_t b = ro[u], e = ro[u + 1], du = e - b;
-    uint32_t p = dro[u];
-    for (uint32_t i = b; i < e; i++) {
-      const uint32_t v = col[i];
-      if (dag_before(du, u, ro[v + 1] - ro[v], v)) {
-        dcol[p] = v;
-        dsrc[p] = u;
-        p++;
+    uint32_t u = lo, rb = ro[u], re = ro[u + 1], bits = 0;
+    for (uint32_t e = e0; e < e1; e++) {
+      while (re <= e) {  // rows without edges are skipped
+        u++;
+        rb = re;
+        re = ro[u + 1];
       }
+      const uint32_t v = col[e];
+      if (dag_before(re - rb, u, ro[v + 1] - ro[v], v)) bits |= 1u << (e - e0);
+    }
+    keep[w] = bits;
+    cnt[w] = __popc(bits);
+  }
+}
+
+// Number of DAG edges among the first e edges of the input CSR.
+__device__ __forceinline__ uint32_t dag_prefix(const uint32_t* keep, const uint32_t* wpre, uint32_t e) {
+  const uint32_t r = e & 31u;
+  return wpre[e >> 5] + (r ? __popc(keep[e >> 5] & ((1u << r) - 1u)) : 0u);
+}
+
+// Stable compaction of the kept edges into the DAG's columns, the DAG's row
+// offsets, and the three work lists (warp-aggregated appends).
+__global__ void __launch_bounds__(256) dag_fill_kernel(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
+                                                       uint32_t n, uint32_t nw, const uint32_t* __restrict__ keep,
+                                                       const uint32_t* __restrict__ wpre, uint32_t* __restrict__ dro,
+                                                       uint32_t* __restrict__ dcol, uint32_t* __restrict__ lists,
+                                                       TcCounters* __restrict__ C) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+  for (uint32_t w = tid; w < nw; w += nthreads) {
+    uint32_t bits = keep[w], p = wpre[w];
+    const uint32_t* src = col + (uint64_t)w * 32u;
+    while (bits) {
+      const uint32_t j = __ffs(bits) - 1u;
+      bits &= bits - 1u;
+      dcol[p++] = src[j];
+    }
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = tid - lane; base < n; base += nthreads) {  // whole warps, for the ballots
+    const uint32_t u = base + lane;
+    uint32_t d = 0;
+    if (u < n) {
+      const uint32_t a = dag_prefix(keep, wpre, ro[u]), b = dag_prefix(keep, wpre, ro[u + 1]);
+      dro[u] = a;
+      if (u == n - 1) dro[n] = b;
+      d = b - a;
+    }
+    const int kind = d < 2 ? -1 : d <= kSmallMaxDeg ? 2 : d <= kWarpMaxDeg ? 1 : 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const uint32_t mask = __ballot_sync(0xffffffffu, kind == k);
+      if (!mask) continue;
+      const uint32_t leader = __ffs(mask) - 1u;
+      uint32_t at = 0;
+      if (lane == leader) at = atomicAdd(&C->n_list[k], (uint32_t)__popc(mask));
+      at = __shfl_sync(0xffffffffu, at, leader);
+      if (kind == k) lists[(uint64_t)k * n + at + __popc(mask & ((1u << lane) - 1u))] = u;
     }
   }
 }
 
-// Exclusive scan in three passes: per-block sums, a scan of those, then the
-// per-block scan with its offset.  kItems values per block.
+// Exclusive scan in three passes: per-tile sums, a scan of those, then the
+// per-tile scan with its offset.  kScanItems values per thread.
 constexpr uint32_t kScanThreads = 256, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
 
 __global__ void __launch_bounds__(kScanThreads) scan_tile_sums(const uint32_t* in, uint32_t n, uint32_t* tile_sums) {
@@ -102,65 +179,268 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(const uint32_t* in, u
   }
 }
 
-template <bool kPerVertex>
-__global__ void __launch_bounds__(256) tc_count_kernel(const uint32_t* __restrict__ dro,
-                                                       const uint32_t* __restrict__ dcol,
-                                                       const uint32_t* __restrict__ dsrc, uint64_t dm,
-                                                       unsigned long long* total,
-                                                       unsigned long long* __restrict__ per_vertex) {
-  __shared__ unsigned long long s_red[32];
-  unsigned long long acc = 0;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dm; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t u = dsrc[i], v = dcol[i];
-    uint32_t xb = dro[u], xe = dro[u + 1], yb = dro[v], ye = dro[v + 1];
-    if (xe - xb > ye - yb) {
-      uint32_t t = xb; xb = yb; yb = t;
-      t = xe; xe = ye; ye = t;
+// Hash set in shared memory: buckets of four slots, read with one 16-byte
+// load.  A key goes to the first empty slot at or after the first slot of
+// its bucket (linear probing over slots), so every bucket fills as a prefix:
+// a bucket whose last slot is empty ends a lookup.  At most half a key per
+// bucket, so about one lookup in 400 reads a second bucket.
+__device__ __forceinline__ uint32_t bucket_of(uint32_t key, uint32_t shift) { return (key * 0x9E3779B1u) >> shift; }
+
+__device__ __forceinline__ void set_insert(uint4* tab, uint32_t key, uint32_t shift, uint32_t bmask) {
+  uint32_t h = bucket_of(key, shift);
+  for (;;) {  // ends: at most half a key per bucket
+    uint32_t* slot = reinterpret_cast<uint32_t*>(tab + h);
+#pragma unroll
+    for (uint32_t i = 0; i < 4; i++) {
+      const uint32_t prev = atomicCAS(slot + i, kEmptySlot, key);
+      if (prev == kEmptySlot || prev == key) return;
     }
-    uint32_t lo = yb;
-    for (uint32_t e = xb; e < xe && lo < ye; e++) {
-      const uint32_t key = dcol[e];
-      uint32_t l = lo, h = ye;
-      while (l < h) {
-        const uint32_t mid = (l + h) >> 1;
-        if (dcol[mid] < key)
-          l = mid + 1;
-        else
-          h = mid;
+    h = (h + 1u) & bmask;
+  }
+}
+
+__device__ __forceinline__ bool set_has(const uint4* tab, uint32_t key, uint32_t shift, uint32_t bmask) {
+  uint32_t h = bucket_of(key, shift);
+  for (;;) {
+    const uint4 x = tab[h];
+    if ((x.x == key) | (x.y == key) | (x.z == key) | (x.w == key)) return true;
+    if (x.w == kEmptySlot) return false;
+    h = (h + 1u) & bmask;
+  }
+}
+
+// log2 of the bucket count for `keys` keys: at least two buckets per key,
+// at least eight buckets, at most 2^max_log2.
+__device__ __forceinline__ uint32_t log2_buckets(uint32_t keys, uint32_t max_log2) {
+  const uint32_t want = keys <= 4u ? 8u : 2u * keys;
+  const uint32_t lg = 32u - __clz(want - 1u);
+  return lg < max_log2 ? lg : max_log2;
+}
+
+__device__ __forceinline__ void set_clear(uint4* tab, uint32_t buckets, uint32_t first, uint32_t step) {
+  for (uint32_t s = first; s < buckets; s += step) tab[s] = make_uint4(kEmptySlot, kEmptySlot, kEmptySlot, kEmptySlot);
+}
+
+struct TcParams {
+  const uint32_t* dro;
+  const uint32_t* dcol;
+  const uint32_t* lists;
+  TcCounters* C;
+  unsigned long long* per_vertex;
+  uint32_t n;
+};
+
+template <bool kPerVertex>
+__device__ __forceinline__ void add_triangle(unsigned long long* pv, uint32_t a, uint32_t b, uint32_t c) {
+  if (kPerVertex) {
+    uint32_t t;
+    if (a > b) { t = a; a = b; b = t; }
+    if (b > c) { t = b; b = c; c = t; }
+    if (a > b) { t = a; a = b; b = t; }
+    atomicAdd(pv + a, 2ull);
+    atomicAdd(pv + b, 1ull);
+  }
+}
+
+// Lookups of dcol[e], dcol[e + 32], ... below `end` (this lane's share of a
+// row segment of N+(v)); kRowUnroll loads in flight.
+template <bool kPerVertex>
+__device__ __forceinline__ uint32_t probe_segment(const TcParams& P, const uint4* tab, uint32_t shift, uint32_t bmask,
+                                                  uint32_t u, uint32_t v, uint32_t e, uint32_t end) {
+  uint32_t hits = 0;
+  for (; e + 32u * (kRowUnroll - 1) < end; e += 32u * kRowUnroll) {
+    uint32_t w[kRowUnroll];
+#pragma unroll
+    for (uint32_t q = 0; q < kRowUnroll; q++) w[q] = P.dcol[e + 32u * q];
+#pragma unroll
+    for (uint32_t q = 0; q < kRowUnroll; q++) {
+      if (set_has(tab, w[q], shift, bmask)) {
+        hits++;
+        add_triangle<kPerVertex>(P.per_vertex, u, v, w[q]);
       }
-      if (l < ye && dcol[l] == key) {
-        acc++;
-        if (kPerVertex) {
-          uint32_t a = u, b = v, c = key, t;
-          if (a > b) { t = a; a = b; b = t; }
-          if (b > c) { t = b; b = c; c = t; }
-          if (a > b) { t = a; a = b; b = t; }
-          atomicAdd(per_vertex + a, 2ull);
-          atomicAdd(per_vertex + b, 1ull);
+    }
+  }
+  if (e < end) {  // fewer than kRowUnroll loads left for this lane
+    uint32_t w[kRowUnroll];
+#pragma unroll
+    for (uint32_t q = 0; q < kRowUnroll; q++) w[q] = e + 32u * q < end ? P.dcol[e + 32u * q] : 0u;
+#pragma unroll
+    for (uint32_t q = 0; q < kRowUnroll; q++) {
+      if (e + 32u * q < end && set_has(tab, w[q], shift, bmask)) {
+        hits++;
+        add_triangle<kPerVertex>(P.per_vertex, u, v, w[q]);
+      }
+    }
+  }
+  return hits;
+}
+
+// One warp streams the rows N+(v), v = N+(u)[j] for j = j0, j0 + jstride,
+// ... (N+(u) = dcol[b, b + d)), against the table, 32 row bounds loaded at a
+// time; returns its lane's hits.
+template <bool kPerVertex>
+__device__ __forceinline__ uint32_t count_rows(const TcParams& P, const uint4* tab, uint32_t shift, uint32_t bmask,
+                                               uint32_t u, uint32_t b, uint32_t d, uint32_t j0, uint32_t jstride) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t hits = 0;
+  for (uint32_t jb = j0; jb < d; jb += 32u * jstride) {
+    const uint32_t j = jb + lane * jstride;
+    uint32_t v = 0, vb = 0, ve = 0;
+    if (j < d) {
+      v = P.dcol[b + j];
+      vb = P.dro[v];
+      ve = P.dro[v + 1];
+    }
+    const uint32_t rows = __popc(__ballot_sync(0xffffffffu, j < d));  // a prefix of the lanes
+    for (uint32_t k = 0; k < rows; k++) {
+      const uint32_t rb = __shfl_sync(0xffffffffu, vb, k), re = __shfl_sync(0xffffffffu, ve, k);
+      const uint32_t rv = kPerVertex ? __shfl_sync(0xffffffffu, v, k) : 0u;
+      hits += probe_segment<kPerVertex>(P, tab, shift, bmask, u, rv, rb + lane, re);
+    }
+  }
+  return hits;
+}
+
+// Shared memory of the counting kernel: the table (the block's for heavy
+// vertices, 32 warp slices otherwise), then the row starts and the prefix of
+// the row lengths of a heavy vertex's rows.
+constexpr size_t kTcSmem = sizeof(uint4) * kBlockBuckets + sizeof(uint32_t) * (2 * kBlockMaxDeg + 1);
+
+template <bool kPerVertex>
+__global__ void __launch_bounds__(kTcThreads, 1) tc_hash_kernel(TcParams P) {
+  extern __shared__ uint4 s_tab[];  // kBlockBuckets, then s_vb and s_pre
+  uint32_t* s_vb = reinterpret_cast<uint32_t*>(s_tab + kBlockBuckets);
+  uint32_t* s_pre = s_vb + kBlockMaxDeg;
+  __shared__ uint32_t s_next, s_scan[32];
+  __shared__ unsigned long long s_red[32];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  unsigned long long acc = 0;
+  // heavy vertices: one block each, the whole table
+  const uint32_t n_heavy = P.C->n_list[0];
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(&P.C->next[0], 1u);
+    __syncthreads();
+    const uint32_t i = s_next;
+    if (i >= n_heavy) break;
+    const uint32_t u = P.lists[i], b = P.dro[u], d = P.dro[u + 1] - b;
+    if (d <= kBlockMaxDeg) {
+      // the flattened rows of N+(u) in 32 equal shares, one per warp
+      const uint32_t lg = log2_buckets(d, 13u), shift = 32u - lg, bmask = (1u << lg) - 1u;
+      set_clear(s_tab, 1u << lg, threadIdx.x, kTcThreads);
+      __syncthreads();
+      uint32_t len[4], sum = 0;
+#pragma unroll
+      for (uint32_t q = 0; q < 4; q++) {  // d <= 4 * kTcThreads
+        const uint32_t j = 4u * threadIdx.x + q;
+        len[q] = 0;
+        if (j < d) {
+          const uint32_t v = P.dcol[b + j], vb = P.dro[v];
+          set_insert(s_tab, v, shift, bmask);
+          len[q] = P.dro[v + 1] - vb;
+          s_vb[j] = vb;
         }
-        l++;
+        sum += len[q];
       }
-      lo = l;
+      uint32_t total;
+      uint32_t run = sygraph::detail::block_excl_scan(sum, &total, s_scan);
+#pragma unroll
+      for (uint32_t q = 0; q < 4; q++) {
+        const uint32_t j = 4u * threadIdx.x + q;
+        if (j < d) s_pre[j] = run;
+        run += len[q];
+      }
+      if (threadIdx.x == 0) s_pre[d] = total;
+      __syncthreads();
+      const uint32_t lo = (uint32_t)((uint64_t)total * warp / kTcWarps);
+      const uint32_t hi = (uint32_t)((uint64_t)total * (warp + 1) / kTcWarps);
+      if (lo < hi) {
+        uint32_t r = 0, top = d;  // last row with s_pre[r] <= lo
+        while (r < top) {
+          const uint32_t mid = (r + top + 1) >> 1;
+          if (s_pre[mid] <= lo)
+            r = mid;
+          else
+            top = mid - 1;
+        }
+        for (uint32_t pos = lo; pos < hi;) {
+          while (s_pre[r + 1] <= pos) r++;  // rows without out-edges
+          const uint32_t rend = min(hi, s_pre[r + 1]);
+          const uint32_t base = s_vb[r] - s_pre[r];  // dcol index of flattened position 0 of row r (mod 2^32)
+          const uint32_t rv = kPerVertex ? P.dcol[b + r] : 0u;
+          acc += probe_segment<kPerVertex>(P, s_tab, shift, bmask, u, rv, base + pos + lane, base + rend);
+          pos = rend;
+        }
+      }
+    } else {
+      // pieces of kBlockMaxDeg keys, every row against each piece
+      for (uint32_t off = 0; off < d; off += kBlockMaxDeg) {
+        const uint32_t kd = min(kBlockMaxDeg, d - off);
+        const uint32_t lg = log2_buckets(kd, 13u), shift = 32u - lg, bmask = (1u << lg) - 1u;
+        set_clear(s_tab, 1u << lg, threadIdx.x, kTcThreads);
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < kd; j += kTcThreads) set_insert(s_tab, P.dcol[b + off + j], shift, bmask);
+        __syncthreads();
+        acc += count_rows<kPerVertex>(P, s_tab, shift, bmask, u, b, d, warp, kTcWarps);
+        __syncthreads();
+      }
+    }
+    __syncthreads();  // the table is reused
+  }
+  // medium, then small vertices: one warp each, a 256-bucket slice of the table
+  uint4* tab = s_tab + warp * kWarpBuckets;
+#pragma unroll 1
+  for (uint32_t k = 1; k < 3; k++) {
+    const uint32_t cnt = P.C->n_list[k], grab = k == 1 ? 1u : 8u;
+    const uint32_t* list = P.lists + (uint64_t)k * P.n;
+    for (;;) {
+      uint32_t i0 = 0;
+      if (lane == 0) i0 = atomicAdd(&P.C->next[k], grab);
+      i0 = __shfl_sync(0xffffffffu, i0, 0);
+      if (i0 >= cnt) break;
+      const uint32_t i1 = min(i0 + grab, cnt);
+      for (uint32_t i = i0; i < i1; i++) {
+        const uint32_t u = list[i], b = P.dro[u], d = P.dro[u + 1] - b;
+        const uint32_t lg = log2_buckets(d, 8u), shift = 32u - lg, bmask = (1u << lg) - 1u;
+        __syncwarp();  // the previous vertex's lookups are done
+        set_clear(tab, 1u << lg, lane, 32u);
+        __syncwarp();
+        for (uint32_t j = lane; j < d; j += 32u) set_insert(tab, P.dcol[b + j], shift, bmask);
+        __syncwarp();
+        acc += count_rows<kPerVertex>(P, tab, shift, bmask, u, b, d, 0u, 1u);
+      }
     }
   }
   acc = block_sum(acc, s_red);
-  if (threadIdx.x == 0 && acc) atomicAdd(total, acc);
+  if (threadIdx.x == 0 && acc) atomicAdd(&P.C->total, acc);
+}
+
+template <bool kPerVertex>
+sg_status launch_count(const TcParams& P, cudaStream_t s) {
+  static bool configured = false;  // the attribute is per kernel; setting it twice is harmless
+  if (!configured) {
+    SG_CUDA(cudaFuncSetAttribute(tc_hash_kernel<kPerVertex>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    configured = true;
+  }
+  int occ = 0;
+  SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tc_hash_kernel<kPerVertex>, (int)kTcThreads, kTcSmem));
+  SG_REQUIRE(occ > 0, SG_ERR_CUDA, "triangle-count kernel does not fit on an SM");
+  tc_hash_kernel<kPerVertex><<<(unsigned)(occ * device_props().sm_count), kTcThreads, kTcSmem, s>>>(P);
+  SG_CUDA(cudaGetLastError());
+  count_launch();
+  return SG_OK;
 }
 
 }  // namespace
 
-sg_status exclusive_scan_u32(const uint32_t* in, uint32_t n, uint32_t* out, cudaStream_t s) {
+// Exclusive scan of n values into out, with tile_sums holding
+// div_up(n, 2048) words; enqueued on s only.
+sg_status exclusive_scan_u32(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* tile_sums, cudaStream_t s) {
   const uint32_t tiles = div_up(n ? n : 1, kScanTile);
-  uint32_t* tile = nullptr;
-  SG_TRY(dev_alloc(&tile, tiles));
-  scan_tile_sums<<<tiles, kScanThreads, 0, s>>>(in, n, tile);
-  scan_tile_offsets<<<1, 1024, 0, s>>>(tile, tiles);
-  scan_tiles<<<tiles, kScanThreads, 0, s>>>(in, n, tile, out);
-  cudaError_t e = cudaGetLastError();
+  scan_tile_sums<<<tiles, kScanThreads, 0, s>>>(in, n, tile_sums);
+  scan_tile_offsets<<<1, 1024, 0, s>>>(tile_sums, tiles);
+  scan_tiles<<<tiles, kScanThreads, 0, s>>>(in, n, tile_sums, out);
   count_launch(3);
-  cudaStreamSynchronize(s);
-  cudaFree(tile);
-  if (e != cudaSuccess) return cuda_fail(e, "scan launch", __FILE__, __LINE__);
+  SG_CUDA(cudaGetLastError());
   return SG_OK;
 }
 
@@ -168,59 +448,127 @@ sg_status exclusive_scan_u32(const uint32_t* in, uint32_t n, uint32_t* out, cuda
 
 using namespace sgb;
 
+struct sg_tc_s {
+  sg_graph g = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t nw = 0;  // 32-edge words of the input CSR
+  uint32_t* keep = nullptr;
+  uint32_t* cnt = nullptr;   // nw + 1
+  uint32_t* wpre = nullptr;  // nw + 1
+  uint32_t* tiles = nullptr;
+  uint32_t* dro = nullptr;   // n + 1
+  uint32_t* dcol = nullptr;  // up to m
+  uint32_t* lists = nullptr; // 3 n
+  TcCounters* counters = nullptr;
+  unsigned long long* pv = nullptr;  // n, allocated on the first per-vertex run
+  bool ran = false, ran_per_vertex = false;
+};
+
 extern "C" {
+
+sg_status sg_tc_destroy(sg_tc_handle t) {
+  if (t) {
+    cudaStreamSynchronize(t->stream);
+    dev_free(t->keep);
+    dev_free(t->cnt);
+    dev_free(t->wpre);
+    dev_free(t->tiles);
+    dev_free(t->dro);
+    dev_free(t->dcol);
+    dev_free(t->lists);
+    dev_free(t->counters);
+    dev_free(t->pv);
+    delete t;
+  }
+  return SG_OK;
+}
+
+sg_status sg_tc_create(sg_graph g, sg_tc_handle* out) {
+  clear_error();
+  SG_REQUIRE(g && out, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(g->n > 0, SG_ERR_INVALID, "graph has no vertices");
+  *out = nullptr;
+  sg_tc_handle t = new sg_tc_s();
+  t->g = g;
+  t->stream = g->stream;
+  const uint64_t n = g->n, m = g->m;
+  t->nw = (uint32_t)div_up(m, 32);
+  sg_status st;
+  if ((st = dev_alloc(&t->keep, t->nw)) || (st = dev_alloc(&t->cnt, (uint64_t)t->nw + 1)) ||
+      (st = dev_alloc(&t->wpre, (uint64_t)t->nw + 1)) ||
+      (st = dev_alloc(&t->tiles, div_up((uint64_t)t->nw + 1, kScanTile))) || (st = dev_alloc(&t->dro, n + 1)) ||
+      (st = dev_alloc(&t->dcol, m)) || (st = dev_alloc(&t->lists, 3 * n)) || (st = dev_alloc(&t->counters, 1))) {
+    sg_tc_destroy(t);
+    return st;
+  }
+  *out = t;
+  return SG_OK;
+}
+
+sg_status sg_tc_run_async(sg_tc_handle t, int per_vertex) {
+  clear_error();
+  SG_REQUIRE(t, SG_ERR_INVALID, "tc is NULL");
+  const sg_graph g = t->g;
+  const uint32_t n = g->n, m = (uint32_t)g->m;
+  cudaStream_t s = t->stream;
+  if (per_vertex && !t->pv) SG_TRY(dev_alloc(&t->pv, n));
+  SG_CUDA(cudaMemsetAsync(t->counters, 0, sizeof(TcCounters), s));
+  dag_flags_kernel<<<grid_for(t->nw ? t->nw : 1, 256, 8), 256, 0, s>>>(g->fwd.ro, g->fwd.col, n, m, t->nw, t->keep,
+                                                                       t->cnt);
+  SG_CUDA(cudaGetLastError());
+  count_launch();
+  SG_TRY(exclusive_scan_u32(t->cnt, t->nw + 1, t->wpre, t->tiles, s));
+  dag_fill_kernel<<<grid_for(std::max<uint64_t>(t->nw, n), 256, 8), 256, 0, s>>>(
+      g->fwd.ro, g->fwd.col, n, t->nw, t->keep, t->wpre, t->dro, t->dcol, t->lists, t->counters);
+  SG_CUDA(cudaGetLastError());
+  count_launch();
+  TcParams P{t->dro, t->dcol, t->lists, t->counters, t->pv, n};
+  if (per_vertex) {
+    SG_CUDA(cudaMemsetAsync(t->pv, 0, sizeof(unsigned long long) * n, s));
+    SG_TRY(launch_count<true>(P, s));
+  } else {
+    SG_TRY(launch_count<false>(P, s));
+  }
+  t->ran = true;
+  t->ran_per_vertex = per_vertex != 0;
+  return SG_OK;
+}
+
+sg_status sg_tc_get_total(sg_tc_handle t, uint64_t* total) {
+  clear_error();
+  SG_REQUIRE(t && total, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(t->ran, SG_ERR_NOT_INITIALIZED, "triangle count not run");
+  unsigned long long v = 0;
+  SG_CUDA(cudaMemcpyAsync(&v, &t->counters->total, sizeof(v), cudaMemcpyDeviceToHost, t->stream));
+  SG_CUDA(cudaStreamSynchronize(t->stream));
+  *total = v;
+  return SG_OK;
+}
+
+sg_status sg_tc_run(sg_tc_handle t, int per_vertex, uint64_t* total) {
+  SG_TRY(sg_tc_run_async(t, per_vertex));
+  if (total) return sg_tc_get_total(t, total);
+  SG_CUDA(cudaStreamSynchronize(t->stream));
+  return SG_OK;
+}
+
+sg_status sg_tc_get_per_vertex(sg_tc_handle t, uint64_t* host_per_vertex) {
+  clear_error();
+  SG_REQUIRE(t && host_per_vertex, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(t->ran_per_vertex, SG_ERR_NOT_INITIALIZED, "no per-vertex triangle count run");
+  SG_CUDA(cudaMemcpyAsync(host_per_vertex, t->pv, sizeof(uint64_t) * t->g->n, cudaMemcpyDeviceToHost, t->stream));
+  SG_CUDA(cudaStreamSynchronize(t->stream));
+  return SG_OK;
+}
 
 sg_status sg_tc(sg_graph g, uint64_t* total, uint64_t* host_per_vertex) {
   clear_error();
   SG_REQUIRE(g && total, SG_ERR_INVALID, "NULL argument");
-  const uint32_t n = g->n;
-  cudaStream_t s = g->stream;
-  uint32_t *cnt = nullptr, *dro = nullptr, *dcol = nullptr, *dsrc = nullptr;
-  unsigned long long *tot = nullptr, *pv = nullptr;
-  sg_status st = SG_OK;
-  do {
-    if ((st = dev_alloc(&cnt, (uint64_t)n + 1)) || (st = dev_alloc(&dro, (uint64_t)n + 1)) ||
-        (st = dev_alloc(&tot, 1)))
-      break;
-    cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * ((uint64_t)n + 1), s);
-    if (e != cudaSuccess) { st = cuda_fail(e, "memset", __FILE__, __LINE__); break; }
-    dag_count_kernel<<<grid_for(n, 256, 16), 256, 0, s>>>(g->fwd.ro, g->fwd.col, n, cnt);
-    if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "dag count", __FILE__, __LINE__); break; }
-    count_launch();
-    if ((st = exclusive_scan_u32(cnt, n + 1, dro, s))) break;
-    uint32_t dm = 0;
-    e = cudaMemcpy(&dm, dro + n, sizeof(uint32_t), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) { st = cuda_fail(e, "dag size", __FILE__, __LINE__); break; }
-    if ((st = dev_alloc(&dcol, dm)) || (st = dev_alloc(&dsrc, dm))) break;
-    dag_fill_kernel<<<grid_for(n, 256, 16), 256, 0, s>>>(g->fwd.ro, g->fwd.col, n, dro, dcol, dsrc);
-    if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "dag fill", __FILE__, __LINE__); break; }
-    count_launch();
-    if ((e = cudaMemsetAsync(tot, 0, sizeof(*tot), s)) != cudaSuccess) { st = cuda_fail(e, "memset", __FILE__, __LINE__); break; }
-    if (host_per_vertex) {
-      if ((st = dev_alloc(&pv, n))) break;
-      if ((e = cudaMemsetAsync(pv, 0, sizeof(*pv) * n, s)) != cudaSuccess) { st = cuda_fail(e, "memset", __FILE__, __LINE__); break; }
-      tc_count_kernel<true><<<grid_for(dm, 256, 16), 256, 0, s>>>(dro, dcol, dsrc, dm, tot, pv);
-    } else {
-      tc_count_kernel<false><<<grid_for(dm, 256, 16), 256, 0, s>>>(dro, dcol, dsrc, dm, tot, nullptr);
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "tc count", __FILE__, __LINE__); break; }
-    count_launch();
-    unsigned long long t = 0;
-    if ((e = cudaMemcpyAsync(&t, tot, sizeof(t), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-        (host_per_vertex && (e = cudaMemcpyAsync(host_per_vertex, pv, sizeof(*pv) * n, cudaMemcpyDeviceToHost, s)) != cudaSuccess) ||
-        (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-      st = cuda_fail(e, "tc copy", __FILE__, __LINE__);
-      break;
-    }
-    *total = t;
-  } while (0);
-  cudaStreamSynchronize(s);
-  dev_free(cnt);
-  dev_free(dro);
-  dev_free(dcol);
-  dev_free(dsrc);
-  dev_free(tot);
-  dev_free(pv);
+  sg_tc_handle t = nullptr;
+  SG_TRY(sg_tc_create(g, &t));
+  sg_status st = sg_tc_run(t, host_per_vertex != nullptr, total);
+  if (st == SG_OK && host_per_vertex) st = sg_tc_get_per_vertex(t, host_per_vertex);
+  sg_tc_destroy(t);
   return st;
 }
 

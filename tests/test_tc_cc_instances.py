@@ -1,0 +1,102 @@
+"""Triangle counting and connected components through their instances, against
+the oracle: block-table vertices (DAG out-degree above 256), unsorted rows,
+self-loops and parallel edges, graphs without edges, and repeated runs."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _edges(g):
+    ro = g.row_offsets.astype(np.int64)
+    return np.repeat(np.arange(g.n, dtype=np.uint32), np.diff(ro)), g.column_indices
+
+
+def _check_tc(sg, oracle, g):
+    tc = sg.algorithms.TC(sg.graph.build.fromCSR(g))
+    tc.run(per_vertex=True)
+    tot, pv = oracle.tc_dag(g, per_vertex=True)
+    assert tc.getNumTriangles() == tot
+    assert np.array_equal(tc.per_vertex, pv)
+    return tc
+
+
+def test_tc_clique_block_tables(sg, oracle):
+    # K_600: DAG out-degrees 0..599, so block tables (> 256), warp tables
+    # (33..256) and the small list (2..32) all count
+    k = 600
+    iu, ju = np.triu_indices(k, 1)
+    g = sg.io.fromCOO(k, iu, ju, symmetrize=True, dedupe=True)
+    tc = _check_tc(sg, oracle, g)
+    assert tc.getNumTriangles() == k * (k - 1) * (k - 2) // 6
+
+
+def test_tc_planted_clique_rmat(sg, oracle, rmat):
+    g = rmat(13)
+    s, d = _edges(g)
+    members = np.random.default_rng(5).choice(g.n, 400, replace=False).astype(np.uint32)
+    iu, ju = np.triu_indices(members.size, 1)
+    h = sg.io.fromCOO(g.n, np.concatenate([s, members[iu]]), np.concatenate([d, members[ju]]), symmetrize=True,
+                      dedupe=True, drop_self_loops=True)
+    _check_tc(sg, oracle, h)
+    assert oracle.tc_edge_merge(h)[0] == oracle.tc_dag(h)[0]
+
+
+def test_tc_unsorted_rows(sg, oracle, rmat):
+    g = rmat(12)
+    ro = g.row_offsets.astype(np.int64)
+    col = g.column_indices.copy()
+    rng = np.random.default_rng(9)
+    for u in range(g.n):
+        rng.shuffle(col[ro[u]:ro[u + 1]])
+    h = sg.CSR(g.row_offsets, col)
+    tc = sg.algorithms.TC(sg.graph.build.fromCSR(h))
+    tc.run(per_vertex=True)
+    tot, pv = oracle.tc_dag(g, per_vertex=True)
+    assert tc.getNumTriangles() == tot
+    assert np.array_equal(tc.per_vertex, pv)
+
+
+def test_tc_self_loops_and_parallel_edges(sg, oracle):
+    rng = np.random.default_rng(11)
+    n = 300
+    s = rng.integers(0, n, 6000)
+    d = rng.integers(0, n, 6000)
+    s[:50] = d[:50]  # self-loops
+    g = sg.io.fromCOO(n, np.concatenate([s, s[:400]]), np.concatenate([d, d[:400]]), symmetrize=True)
+    assert (g.column_indices == np.repeat(np.arange(n), np.diff(g.row_offsets.astype(np.int64)))).any()
+    _check_tc(sg, oracle, g)
+
+
+@pytest.mark.parametrize("n", [1, 7])
+def test_tc_no_edges(sg, n):
+    g = sg.CSR(np.zeros(n + 1, np.uint32), np.zeros(0, np.uint32))
+    tc = sg.algorithms.TC(sg.graph.build.fromCSR(g))
+    tc.run(per_vertex=True)
+    assert tc.getNumTriangles() == 0
+    assert not tc.per_vertex.any()
+
+
+def test_tc_instance_reruns(sg, oracle, rmat):
+    g = rmat(14, perm_seed=6)
+    tot, pv = oracle.tc_dag(g, per_vertex=True)
+    tc = sg.algorithms.TC(sg.graph.build.fromCSR(g))
+    for per_vertex in (False, True, False, True):
+        tc.run(per_vertex=per_vertex)
+        assert tc.getNumTriangles() == tot
+        if per_vertex:
+            assert np.array_equal(tc.per_vertex, pv)
+    tc.run_async()
+    assert tc.getNumTriangles() == tot
+
+
+def test_cc_instance_reruns(sg, oracle, rmat):
+    g = rmat(14, perm_seed=8)
+    ref = oracle.cc_maxlabel(g)
+    cc = sg.algorithms.CC(sg.graph.build.fromCSR(g))
+    for _ in range(3):
+        cc.run()
+        assert cc.iterations > 0
+        assert np.array_equal(cc.getLabels(), ref)
+    cc.run_async()
+    assert np.array_equal(cc.labels, ref)
