@@ -560,10 +560,12 @@ sg_status sg_bc_batched(sg_graph g, const uint32_t* host_sources, uint32_t k, fl
 /* TC(G) + init + run + getNumTriangles (algorithms/tc.hpp:58-138), exact,
  * uint64: every run orients the edges into the degree-ordered DAG and
  * intersects N+(u) with N+(v) for every DAG edge through shared-memory hash
- * sets.  Rows need not be sorted.  getNumTriangles(v), the per-vertex count,
- * is for every edge (u,v) with u < v, |N(u) n N(v)| added to u.  The instance
- * owns the DAG and the work lists (about 4m + 20n bytes), so that runs
- * allocate nothing; runs are enqueued on the graph's stream. */
+ * sets, streaming the shorter row.  Rows need not be sorted; the graph must
+ * have no parallel edges (self-loops are ignored).
+ * getNumTriangles(v), the per-vertex count, is for every edge (u,v) with
+ * u < v, |N(u) n N(v)| added to u.  The instance owns the DAG, its reverse
+ * lists and the work lists (about 8m + 28n bytes), so that runs allocate
+ * nothing; runs are enqueued on the graph's stream. */
 typedef struct sg_tc_s* sg_tc_handle;
 sg_status sg_tc_create(sg_graph g, sg_tc_handle* out);
 sg_status sg_tc_destroy(sg_tc_handle t);
@@ -571,6 +573,10 @@ sg_status sg_tc_destroy(sg_tc_handle t);
 sg_status sg_tc_run_async(sg_tc_handle t, int per_vertex);
 sg_status sg_tc_run(sg_tc_handle t, int per_vertex, uint64_t* total);
 sg_status sg_tc_get_total(sg_tc_handle t, uint64_t* total);
+/* shorter != 0 (the default): every DAG edge streams the shorter of its two
+ * rows against the other's set (reverse lists built each run); 0: always the
+ * head's row against the tail's set (no reverse lists).  Same counts. */
+sg_status sg_tc_set_shorter_rows(sg_tc_handle t, int shorter);
 sg_status sg_tc_get_per_vertex(sg_tc_handle t, uint64_t* host_per_vertex);
 /* One-shot; host_per_vertex may be NULL. */
 sg_status sg_tc(sg_graph g, uint64_t* total, uint64_t* host_per_vertex);

@@ -235,6 +235,7 @@ SIGNATURES = {
     "sg_tc_run_async": (st, [vp, C.c_int]),
     "sg_tc_run": (st, [vp, C.c_int, u64p]),
     "sg_tc_get_total": (st, [vp, u64p]),
+    "sg_tc_set_shorter_rows": (st, [vp, C.c_int]),
     "sg_tc_get_per_vertex": (st, [vp, u64p]),
     # host graph I/O
     "sg_rmat_generate": (st, [C.POINTER(RmatParams), C.POINTER(HostCSR)]),

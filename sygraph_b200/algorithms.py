@@ -389,6 +389,10 @@ class TC:
         call("sg_tc_run_async", self.handle, int(per_vertex))
         self.total = None
 
+    def set_shorter_rows(self, shorter: bool = True) -> None:
+        """True (default): each DAG edge streams its shorter row; False: the head's row."""
+        call("sg_tc_set_shorter_rows", self.handle, int(shorter))
+
     def getNumTriangles(self, v: int | None = None) -> int:
         if v is None:
             if self.total is None:

@@ -5,24 +5,31 @@
 // (tc.hpp:104), which over-counts.  Here:
 //   1. orient every edge from the endpoint with the smaller (degree, id) key
 //      (the degree-ordered DAG, out-degree at most sqrt(m)): one keep bit per
-//      edge, a scan of the per-word counts, and a stable compaction, so the
-//      DAG rows keep the order of the input rows;
-//   2. for every vertex u with d+(u) >= 2, N+(u) goes into a shared-memory
-//      hash set (four-slot buckets, at most half a key per bucket), and
-//      every row N+(v), v in N+(u), is streamed against it by whole warps
-//      (coalesced, eight loads in flight per lane): |N+(u) n N+(v)| summed;
-//   3. each triangle is found exactly once, from its lowest DAG vertex; the
-//      total is a uint64 sum.
-// The per-vertex convention of the reference (for every edge (u,v), u < v,
-// |N(u) n N(v)| is added to u) is recovered from the same enumeration: a
-// triangle a < b < c adds 2 to a and 1 to b.
+//      edge, a scan of the per-word counts, and a stable compaction;
+//   2. every DAG edge a -> b needs |N+(a) n N+(b)|.  It is counted at the
+//      endpoint x with the longer row: x's row N+(x) goes into a
+//      shared-memory hash set (four-slot buckets, at most half a key per
+//      bucket) and the shorter row is streamed against it by whole warps
+//      (coalesced, eight loads in flight per lane).  So x streams its
+//      out-neighbours' rows no longer than its own, and the rows of the
+//      in-neighbours y with d+(y) < d+(x) (the reverse lists, built by a
+//      count, a scan and a fill);
+//   3. each triangle is found exactly once, through the edge between its two
+//      lowest DAG vertices; the total is a uint64 sum.
+// On RMAT-20 this streams sum over DAG edges of min(d+(a), d+(b)) = 1.97 G
+// elements instead of sum of d+(b) = 4.42 G.  The per-vertex convention of
+// the reference (for every edge (u,v), u < v, |N(u) n N(v)| is added to u)
+// is recovered from the same enumeration: a triangle a < b < c adds 2 to a
+// and 1 to b.
 //
-// Work lists: vertices with d+(u) > 128 are counted by a whole block (one
-// 8192-bucket table; the flattened rows of N+(u) split evenly over the 32
-// warps), the rest by single warps (256-bucket tables), medium degrees
-// (33..128) before small ones so that the long counts start first.  A vertex
-// with d+(u) > 4096 (possible only when m > 2^24) is counted in pieces of
-// 4096 keys, which is exact for graphs without parallel edges.
+// Work lists by an upper bound of each vertex's probes: the big ones (or
+// d+(x) > 128) are counted by a whole 256-thread block (one 2048-bucket
+// table; the flattened rows in 8 equal shares, one per warp), the rest by
+// single warps (256-bucket tables), medium before small so that the long
+// counts start first; four blocks share an SM.  A vertex with d+(x) > 1024
+// is counted in pieces of 1024 keys, each piece against all of x's rows.  The count is that of a graph without parallel
+// edges (the reference's sorted-list merge assumes none either); self-loops
+// are no DAG edges.
 #include "internal.cuh"
 
 namespace sgb {
@@ -30,12 +37,14 @@ namespace {
 
 using sygraph::detail::block_sum;
 
-constexpr uint32_t kTcThreads = 1024, kTcWarps = kTcThreads / 32;
+constexpr uint32_t kTcThreads = 256, kTcWarps = kTcThreads / 32;  // four blocks per SM
 constexpr uint32_t kWarpBuckets = 256;                       // one warp's table: 256 x 4 slots, 4 KB
-constexpr uint32_t kBlockBuckets = kWarpBuckets * kTcWarps;  // the block's table: 8192 buckets, 128 KB
+constexpr uint32_t kBlockBuckets = kWarpBuckets * kTcWarps;  // the block's table: 2048 buckets, 32 KB
 constexpr uint32_t kWarpMaxDeg = kWarpBuckets / 2;           // d+(u) counted by one warp
-constexpr uint32_t kSmallMaxDeg = 32;
-constexpr uint32_t kBlockMaxDeg = kBlockBuckets / 2;  // keys of one block table (4 * kTcThreads)
+constexpr uint64_t kWarpMaxWork = 1ull << 17;                // probe bound counted by one warp
+constexpr uint64_t kSmallMaxWork = 1ull << 11;               // medium above, small below
+constexpr uint32_t kBlockMaxDeg = kBlockBuckets / 2;  // keys of one block table
+constexpr uint32_t kBlockRows = 4 * kTcThreads;       // rows per balanced block pass
 constexpr uint32_t kEmptySlot = 0xffffffffu;          // never a vertex id (n < 2^32)
 constexpr uint32_t kRowUnroll = 8;                    // row loads in flight per lane
 
@@ -50,15 +59,32 @@ __device__ __forceinline__ bool dag_before(uint32_t du, uint32_t u, uint32_t dv,
 }
 
 // Keep bit of every edge, one thread per 32-edge word: the thread finds the
-// source of its first edge by binary search on the row offsets and walks on.
+// source of its first edge by binary search on the row offsets (kept in
+// wsrc for the compaction), loads the word's 32 columns and their 32 degrees
+// with every load in flight, then walks the rows.
 __global__ void __launch_bounds__(256) dag_flags_kernel(const uint32_t* __restrict__ ro,
                                                         const uint32_t* __restrict__ col, uint32_t n, uint32_t m,
                                                         uint32_t nw, uint32_t* __restrict__ keep,
-                                                        uint32_t* __restrict__ cnt) {
+                                                        uint32_t* __restrict__ cnt, uint32_t* __restrict__ wsrc) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid == 0) cnt[nw] = 0;  // the scan's last input: its output is the DAG size
   for (uint32_t w = tid; w < nw; w += gridDim.x * blockDim.x) {
-    const uint32_t e0 = w * 32u, e1 = (uint32_t)min((uint64_t)e0 + 32u, (uint64_t)m);
+    const uint32_t e0 = w * 32u, ne = (uint32_t)min((uint64_t)m - e0, (uint64_t)32u);
+    uint32_t v[32], dv[32];
+    if (ne == 32u) {  // col + e0 is 128-byte aligned
+      const uint4* c4 = reinterpret_cast<const uint4*>(col + e0);
+#pragma unroll
+      for (uint32_t k = 0; k < 8; k++) {
+        const uint4 t = c4[k];
+        v[4 * k] = t.x;
+        v[4 * k + 1] = t.y;
+        v[4 * k + 2] = t.z;
+        v[4 * k + 3] = t.w;
+      }
+    } else {
+#pragma unroll
+      for (uint32_t i = 0; i < 32; i++) v[i] = i < ne ? col[e0 + i] : 0u;
+    }
     uint32_t lo = 0, hi = n - 1;  // last u with ro[u] <= e0: the source of edge e0
     while (lo < hi) {
       const uint32_t mid = lo + ((hi - lo + 1) >> 1);
@@ -67,15 +93,20 @@ __global__ void __launch_bounds__(256) dag_flags_kernel(const uint32_t* __restri
       else
         hi = mid - 1;
     }
+#pragma unroll
+    for (uint32_t i = 0; i < 32; i++) dv[i] = i < ne ? ro[v[i] + 1] - ro[v[i]] : 0u;
+    wsrc[w] = lo;
     uint32_t u = lo, rb = ro[u], re = ro[u + 1], bits = 0;
-    for (uint32_t e = e0; e < e1; e++) {
-      while (re <= e) {  // rows without edges are skipped
-        u++;
-        rb = re;
-        re = ro[u + 1];
+#pragma unroll
+    for (uint32_t i = 0; i < 32; i++) {
+      if (i < ne) {
+        while (re <= e0 + i) {  // rows without edges are skipped
+          u++;
+          rb = re;
+          re = ro[u + 1];
+        }
+        if (dag_before(re - rb, u, dv[i], v[i])) bits |= 1u << i;
       }
-      const uint32_t v = col[e];
-      if (dag_before(re - rb, u, ro[v + 1] - ro[v], v)) bits |= 1u << (e - e0);
     }
     keep[w] = bits;
     cnt[w] = __popc(bits);
@@ -88,34 +119,70 @@ __device__ __forceinline__ uint32_t dag_prefix(const uint32_t* keep, const uint3
   return wpre[e >> 5] + (r ? __popc(keep[e >> 5] & ((1u << r) - 1u)) : 0u);
 }
 
-// Stable compaction of the kept edges into the DAG's columns, the DAG's row
-// offsets, and the three work lists (warp-aggregated appends).
+// Stable compaction of the kept edges into the DAG's columns (and each
+// edge's source) and the DAG's row offsets; zeroes the reverse counts.
 __global__ void __launch_bounds__(256) dag_fill_kernel(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
                                                        uint32_t n, uint32_t nw, const uint32_t* __restrict__ keep,
-                                                       const uint32_t* __restrict__ wpre, uint32_t* __restrict__ dro,
-                                                       uint32_t* __restrict__ dcol, uint32_t* __restrict__ lists,
-                                                       TcCounters* __restrict__ C) {
+                                                       const uint32_t* __restrict__ wpre,
+                                                       const uint32_t* __restrict__ wsrc, uint32_t* __restrict__ dro,
+                                                       uint32_t* __restrict__ dcol, uint32_t* __restrict__ dsrc,
+                                                       uint32_t* __restrict__ rcnt) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
   for (uint32_t w = tid; w < nw; w += nthreads) {
     uint32_t bits = keep[w], p = wpre[w];
-    const uint32_t* src = col + (uint64_t)w * 32u;
+    if (!bits) continue;
+    const uint32_t e0 = w * 32u;
+    uint32_t u = wsrc[w], re = ro[u + 1];
     while (bits) {
       const uint32_t j = __ffs(bits) - 1u;
       bits &= bits - 1u;
-      dcol[p++] = src[j];
+      while (re <= e0 + j) re = ro[++u + 1];  // rows without edges are skipped
+      dcol[p] = col[e0 + j];
+      dsrc[p++] = u;
     }
   }
-  const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t base = tid - lane; base < n; base += nthreads) {  // whole warps, for the ballots
-    const uint32_t u = base + lane;
-    uint32_t d = 0;
-    if (u < n) {
-      const uint32_t a = dag_prefix(keep, wpre, ro[u]), b = dag_prefix(keep, wpre, ro[u + 1]);
-      dro[u] = a;
-      if (u == n - 1) dro[n] = b;
-      d = b - a;
+  for (uint32_t u = tid; u <= n; u += nthreads) {
+    dro[u] = dag_prefix(keep, wpre, ro[u]);
+    rcnt[u] = 0;
+  }
+}
+
+// The reverse lists: for every DAG edge y -> x with d+(y) < d+(x), y joins
+// x's list (the edge's shorter row N+(y) is then streamed against x's set).
+// One thread per DAG edge; kFill = false counts, kFill = true places (rcnt
+// counted down to zero).
+template <bool kFill>
+__global__ void __launch_bounds__(256) rev_kernel(const uint32_t* __restrict__ dro, const uint32_t* __restrict__ dcol,
+                                                  const uint32_t* __restrict__ dsrc, const uint32_t* dm_ptr,
+                                                  uint32_t* __restrict__ rcnt, const uint32_t* __restrict__ rro,
+                                                  uint32_t* __restrict__ rcol) {
+  const uint32_t dm = *dm_ptr;  // DAG edges
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < dm; i += gridDim.x * blockDim.x) {
+    const uint32_t y = dsrc[i], x = dcol[i];
+    if (dro[y + 1] - dro[y] < dro[x + 1] - dro[x]) {
+      if (kFill)
+        rcol[rro[x] + atomicSub(rcnt + x, 1u) - 1u] = y;
+      else
+        atomicAdd(rcnt + x, 1u);
     }
-    const int kind = d < 2 ? -1 : d <= kSmallMaxDeg ? 2 : d <= kWarpMaxDeg ? 1 : 0;
+  }
+}
+
+// Work lists by an upper bound of the probes, (d+(x) + reverse count) *
+// d+(x): heavy (block) when d+(x) > kWarpMaxDeg or the bound exceeds
+// kWarpMaxWork, medium above kSmallMaxWork, small otherwise; d+(x) < 2 has
+// no triangle to count.  Warp-aggregated appends.
+__global__ void __launch_bounds__(256) classify_kernel(const uint32_t* __restrict__ dro, const uint32_t* __restrict__ rro,
+                                                       uint32_t n, uint32_t* __restrict__ lists,
+                                                       TcCounters* __restrict__ C) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
+  for (uint32_t base = tid - lane; base < n; base += gridDim.x * blockDim.x) {  // whole warps, for the ballots
+    const uint32_t x = base + lane;
+    int kind = -1;
+    if (x < n) {
+      const uint64_t d = dro[x + 1] - dro[x], r = rro[x + 1] - rro[x], bound = (d + r) * d;
+      if (d >= 2) kind = (d > kWarpMaxDeg || bound > kWarpMaxWork) ? 0 : bound > kSmallMaxWork ? 1 : 2;
+    }
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const uint32_t mask = __ballot_sync(0xffffffffu, kind == k);
@@ -124,7 +191,7 @@ __global__ void __launch_bounds__(256) dag_fill_kernel(const uint32_t* __restric
       uint32_t at = 0;
       if (lane == leader) at = atomicAdd(&C->n_list[k], (uint32_t)__popc(mask));
       at = __shfl_sync(0xffffffffu, at, leader);
-      if (kind == k) lists[(uint64_t)k * n + at + __popc(mask & ((1u << lane) - 1u))] = u;
+      if (kind == k) lists[(uint64_t)k * n + at + __popc(mask & ((1u << lane) - 1u))] = x;
     }
   }
 }
@@ -224,10 +291,13 @@ __device__ __forceinline__ void set_clear(uint4* tab, uint32_t buckets, uint32_t
 struct TcParams {
   const uint32_t* dro;
   const uint32_t* dcol;
+  const uint32_t* rro;
+  const uint32_t* rcol;
   const uint32_t* lists;
   TcCounters* C;
   unsigned long long* per_vertex;
   uint32_t n;
+  uint32_t shorter;  // 1: an out-row longer than x's own is left to its head's reverse list
 };
 
 template <bool kPerVertex>
@@ -242,13 +312,16 @@ __device__ __forceinline__ void add_triangle(unsigned long long* pv, uint32_t a,
   }
 }
 
-// Lookups of dcol[e], dcol[e + 32], ... below `end` (this lane's share of a
-// row segment of N+(v)); kRowUnroll loads in flight.
+// Lookups of the row segment dcol[sb, se) (warp-uniform bounds), one
+// element per lane and chunk of 32, kRowUnroll loads in flight; the last
+// chunks are skipped by uniform branches.  A hit w closes the triangle
+// {x, y, w}.
 template <bool kPerVertex>
 __device__ __forceinline__ uint32_t probe_segment(const TcParams& P, const uint4* tab, uint32_t shift, uint32_t bmask,
-                                                  uint32_t u, uint32_t v, uint32_t e, uint32_t end) {
-  uint32_t hits = 0;
-  for (; e + 32u * (kRowUnroll - 1) < end; e += 32u * kRowUnroll) {
+                                                  uint32_t x, uint32_t y, uint32_t sb, uint32_t se) {
+  const uint32_t lane = threadIdx.x & 31u, part = (se - sb) & 31u;  // lanes of the partial last chunk
+  uint32_t full = (se - sb) >> 5, e = sb + lane, hits = 0;
+  for (; full >= kRowUnroll; full -= kRowUnroll, e += 32u * kRowUnroll) {
     uint32_t w[kRowUnroll];
 #pragma unroll
     for (uint32_t q = 0; q < kRowUnroll; q++) w[q] = P.dcol[e + 32u * q];
@@ -256,46 +329,56 @@ __device__ __forceinline__ uint32_t probe_segment(const TcParams& P, const uint4
     for (uint32_t q = 0; q < kRowUnroll; q++) {
       if (set_has(tab, w[q], shift, bmask)) {
         hits++;
-        add_triangle<kPerVertex>(P.per_vertex, u, v, w[q]);
+        add_triangle<kPerVertex>(P.per_vertex, x, y, w[q]);
       }
     }
   }
-  if (e < end) {  // fewer than kRowUnroll loads left for this lane
-    uint32_t w[kRowUnroll];
+  // fewer than kRowUnroll full chunks left, then the partial one (q == full)
+  uint32_t w[kRowUnroll];
 #pragma unroll
-    for (uint32_t q = 0; q < kRowUnroll; q++) w[q] = e + 32u * q < end ? P.dcol[e + 32u * q] : 0u;
+  for (uint32_t q = 0; q < kRowUnroll; q++) {
+    if (q > full) break;
+    w[q] = (q < full || lane < part) ? P.dcol[e + 32u * q] : 0u;
+  }
 #pragma unroll
-    for (uint32_t q = 0; q < kRowUnroll; q++) {
-      if (e + 32u * q < end && set_has(tab, w[q], shift, bmask)) {
-        hits++;
-        add_triangle<kPerVertex>(P.per_vertex, u, v, w[q]);
-      }
+  for (uint32_t q = 0; q < kRowUnroll; q++) {
+    if (q > full) break;
+    if ((q < full || lane < part) && set_has(tab, w[q], shift, bmask)) {
+      hits++;
+      add_triangle<kPerVertex>(P.per_vertex, x, y, w[q]);
     }
   }
   return hits;
 }
 
-// One warp streams the rows N+(v), v = N+(u)[j] for j = j0, j0 + jstride,
-// ... (N+(u) = dcol[b, b + d)), against the table, 32 row bounds loaded at a
-// time; returns its lane's hits.
+// The rows x streams: the out-neighbours y of x with d+(y) <= d+(x) (row
+// index j < d), then x's reverse list (j >= d, d+(y) < d+(x) already).
+__device__ __forceinline__ uint32_t row_vertex(const TcParams& P, uint32_t b, uint32_t d, uint32_t rb, uint32_t j) {
+  return j < d ? P.dcol[b + j] : P.rcol[rb + (j - d)];
+}
+
+// One warp streams the rows j = j0, j0 + jstride, ... < rows of x against
+// the table, 32 row bounds loaded at a time; returns its lane's hits.
 template <bool kPerVertex>
 __device__ __forceinline__ uint32_t count_rows(const TcParams& P, const uint4* tab, uint32_t shift, uint32_t bmask,
-                                               uint32_t u, uint32_t b, uint32_t d, uint32_t j0, uint32_t jstride) {
+                                               uint32_t x, uint32_t b, uint32_t d, uint32_t rb, uint32_t rows,
+                                               uint32_t j0, uint32_t jstride) {
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t hits = 0;
-  for (uint32_t jb = j0; jb < d; jb += 32u * jstride) {
+  for (uint32_t jb = j0; jb < rows; jb += 32u * jstride) {
     const uint32_t j = jb + lane * jstride;
-    uint32_t v = 0, vb = 0, ve = 0;
-    if (j < d) {
-      v = P.dcol[b + j];
-      vb = P.dro[v];
-      ve = P.dro[v + 1];
+    uint32_t y = 0, vb = 0, ve = 0;
+    if (j < rows) {
+      y = row_vertex(P, b, d, rb, j);
+      vb = P.dro[y];
+      ve = P.dro[y + 1];
+      if (P.shorter && j < d && ve - vb > d) ve = vb;  // the edge's shorter row is x's own
     }
-    const uint32_t rows = __popc(__ballot_sync(0xffffffffu, j < d));  // a prefix of the lanes
-    for (uint32_t k = 0; k < rows; k++) {
-      const uint32_t rb = __shfl_sync(0xffffffffu, vb, k), re = __shfl_sync(0xffffffffu, ve, k);
-      const uint32_t rv = kPerVertex ? __shfl_sync(0xffffffffu, v, k) : 0u;
-      hits += probe_segment<kPerVertex>(P, tab, shift, bmask, u, rv, rb + lane, re);
+    for (uint32_t live = __ballot_sync(0xffffffffu, ve > vb); live; live &= live - 1u) {
+      const uint32_t k = __ffs(live) - 1u;
+      const uint32_t sb = __shfl_sync(0xffffffffu, vb, k), se = __shfl_sync(0xffffffffu, ve, k);
+      const uint32_t sy = kPerVertex ? __shfl_sync(0xffffffffu, y, k) : 0u;
+      hits += probe_segment<kPerVertex>(P, tab, shift, bmask, x, sy, sb, se);
     }
   }
   return hits;
@@ -303,14 +386,14 @@ __device__ __forceinline__ uint32_t count_rows(const TcParams& P, const uint4* t
 
 // Shared memory of the counting kernel: the table (the block's for heavy
 // vertices, 32 warp slices otherwise), then the row starts and the prefix of
-// the row lengths of a heavy vertex's rows.
-constexpr size_t kTcSmem = sizeof(uint4) * kBlockBuckets + sizeof(uint32_t) * (2 * kBlockMaxDeg + 1);
+// the row lengths of one balanced pass.
+constexpr size_t kTcSmem = sizeof(uint4) * kBlockBuckets + sizeof(uint32_t) * (2 * kBlockRows + 1);
 
 template <bool kPerVertex>
-__global__ void __launch_bounds__(kTcThreads, 1) tc_hash_kernel(TcParams P) {
+__global__ void __launch_bounds__(kTcThreads, 4) tc_hash_kernel(TcParams P) {
   extern __shared__ uint4 s_tab[];  // kBlockBuckets, then s_vb and s_pre
   uint32_t* s_vb = reinterpret_cast<uint32_t*>(s_tab + kBlockBuckets);
-  uint32_t* s_pre = s_vb + kBlockMaxDeg;
+  uint32_t* s_pre = s_vb + kBlockRows;
   __shared__ uint32_t s_next, s_scan[32];
   __shared__ unsigned long long s_red[32];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -322,69 +405,64 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_hash_kernel(TcParams P) {
     __syncthreads();
     const uint32_t i = s_next;
     if (i >= n_heavy) break;
-    const uint32_t u = P.lists[i], b = P.dro[u], d = P.dro[u + 1] - b;
-    if (d <= kBlockMaxDeg) {
-      // the flattened rows of N+(u) in 32 equal shares, one per warp
-      const uint32_t lg = log2_buckets(d, 13u), shift = 32u - lg, bmask = (1u << lg) - 1u;
+    const uint32_t x = P.lists[i], b = P.dro[x], d = P.dro[x + 1] - b;
+    const uint32_t rb = P.rro[x], rows = d + (P.rro[x + 1] - rb);
+    // the table holds N+(x), in pieces of kBlockMaxDeg keys when longer
+    for (uint32_t off = 0; off < d; off += kBlockMaxDeg) {
+      const uint32_t kd = min(kBlockMaxDeg, d - off);
+      const uint32_t lg = log2_buckets(kd, 11u), shift = 32u - lg, bmask = (1u << lg) - 1u;
       set_clear(s_tab, 1u << lg, threadIdx.x, kTcThreads);
       __syncthreads();
-      uint32_t len[4], sum = 0;
+      for (uint32_t j = threadIdx.x; j < kd; j += kTcThreads) set_insert(s_tab, P.dcol[b + off + j], shift, bmask);
+      // passes of kBlockRows rows: their flattened lengths in kTcWarps equal shares
+      for (uint32_t c0 = 0; c0 < rows; c0 += kBlockRows) {
+        const uint32_t cr = min(kBlockRows, rows - c0);
+        uint32_t len[4], sum = 0;
 #pragma unroll
-      for (uint32_t q = 0; q < 4; q++) {  // d <= 4 * kTcThreads
-        const uint32_t j = 4u * threadIdx.x + q;
-        len[q] = 0;
-        if (j < d) {
-          const uint32_t v = P.dcol[b + j], vb = P.dro[v];
-          set_insert(s_tab, v, shift, bmask);
-          len[q] = P.dro[v + 1] - vb;
-          s_vb[j] = vb;
+        for (uint32_t q = 0; q < 4; q++) {
+          const uint32_t jj = 4u * threadIdx.x + q;
+          len[q] = 0;
+          if (jj < cr) {
+            const uint32_t j = c0 + jj, y = row_vertex(P, b, d, rb, j), vb = P.dro[y];
+            len[q] = P.dro[y + 1] - vb;
+            if (P.shorter && j < d && len[q] > d) len[q] = 0;
+            s_vb[jj] = vb;
+          }
+          sum += len[q];
         }
-        sum += len[q];
-      }
-      uint32_t total;
-      uint32_t run = sygraph::detail::block_excl_scan(sum, &total, s_scan);
+        uint32_t total;  // block_excl_scan synchronises: the inserts above are complete after it
+        uint32_t run = sygraph::detail::block_excl_scan(sum, &total, s_scan);
 #pragma unroll
-      for (uint32_t q = 0; q < 4; q++) {
-        const uint32_t j = 4u * threadIdx.x + q;
-        if (j < d) s_pre[j] = run;
-        run += len[q];
-      }
-      if (threadIdx.x == 0) s_pre[d] = total;
-      __syncthreads();
-      const uint32_t lo = (uint32_t)((uint64_t)total * warp / kTcWarps);
-      const uint32_t hi = (uint32_t)((uint64_t)total * (warp + 1) / kTcWarps);
-      if (lo < hi) {
-        uint32_t r = 0, top = d;  // last row with s_pre[r] <= lo
-        while (r < top) {
-          const uint32_t mid = (r + top + 1) >> 1;
-          if (s_pre[mid] <= lo)
-            r = mid;
-          else
-            top = mid - 1;
+        for (uint32_t q = 0; q < 4; q++) {
+          const uint32_t jj = 4u * threadIdx.x + q;
+          if (jj < cr) s_pre[jj] = run;
+          run += len[q];
         }
-        for (uint32_t pos = lo; pos < hi;) {
-          while (s_pre[r + 1] <= pos) r++;  // rows without out-edges
-          const uint32_t rend = min(hi, s_pre[r + 1]);
-          const uint32_t base = s_vb[r] - s_pre[r];  // dcol index of flattened position 0 of row r (mod 2^32)
-          const uint32_t rv = kPerVertex ? P.dcol[b + r] : 0u;
-          acc += probe_segment<kPerVertex>(P, s_tab, shift, bmask, u, rv, base + pos + lane, base + rend);
-          pos = rend;
+        if (threadIdx.x == 0) s_pre[cr] = total;
+        __syncthreads();
+        const uint32_t lo = (uint32_t)((uint64_t)total * warp / kTcWarps);
+        const uint32_t hi = (uint32_t)((uint64_t)total * (warp + 1) / kTcWarps);
+        if (lo < hi) {
+          uint32_t r = 0, top = cr;  // last row with s_pre[r] <= lo
+          while (r < top) {
+            const uint32_t mid = (r + top + 1) >> 1;
+            if (s_pre[mid] <= lo)
+              r = mid;
+            else
+              top = mid - 1;
+          }
+          for (uint32_t pos = lo; pos < hi;) {
+            while (s_pre[r + 1] <= pos) r++;  // rows left out or without out-edges
+            const uint32_t rend = min(hi, s_pre[r + 1]);
+            const uint32_t base = s_vb[r] - s_pre[r];  // dcol index of flattened position 0 of row r (mod 2^32)
+            const uint32_t ry = kPerVertex ? row_vertex(P, b, d, rb, c0 + r) : 0u;
+            acc += probe_segment<kPerVertex>(P, s_tab, shift, bmask, x, ry, base + pos, base + rend);
+            pos = rend;
+          }
         }
-      }
-    } else {
-      // pieces of kBlockMaxDeg keys, every row against each piece
-      for (uint32_t off = 0; off < d; off += kBlockMaxDeg) {
-        const uint32_t kd = min(kBlockMaxDeg, d - off);
-        const uint32_t lg = log2_buckets(kd, 13u), shift = 32u - lg, bmask = (1u << lg) - 1u;
-        set_clear(s_tab, 1u << lg, threadIdx.x, kTcThreads);
-        __syncthreads();
-        for (uint32_t j = threadIdx.x; j < kd; j += kTcThreads) set_insert(s_tab, P.dcol[b + off + j], shift, bmask);
-        __syncthreads();
-        acc += count_rows<kPerVertex>(P, s_tab, shift, bmask, u, b, d, warp, kTcWarps);
-        __syncthreads();
+        __syncthreads();  // s_vb and s_pre are reused
       }
     }
-    __syncthreads();  // the table is reused
   }
   // medium, then small vertices: one warp each, a 256-bucket slice of the table
   uint4* tab = s_tab + warp * kWarpBuckets;
@@ -399,14 +477,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_hash_kernel(TcParams P) {
       if (i0 >= cnt) break;
       const uint32_t i1 = min(i0 + grab, cnt);
       for (uint32_t i = i0; i < i1; i++) {
-        const uint32_t u = list[i], b = P.dro[u], d = P.dro[u + 1] - b;
+        const uint32_t x = list[i], b = P.dro[x], d = P.dro[x + 1] - b;
+        const uint32_t rb = P.rro[x], rows = d + (P.rro[x + 1] - rb);
         const uint32_t lg = log2_buckets(d, 8u), shift = 32u - lg, bmask = (1u << lg) - 1u;
         __syncwarp();  // the previous vertex's lookups are done
         set_clear(tab, 1u << lg, lane, 32u);
         __syncwarp();
         for (uint32_t j = lane; j < d; j += 32u) set_insert(tab, P.dcol[b + j], shift, bmask);
         __syncwarp();
-        acc += count_rows<kPerVertex>(P, tab, shift, bmask, u, b, d, 0u, 1u);
+        acc += count_rows<kPerVertex>(P, tab, shift, bmask, x, b, d, rb, rows, 0u, 1u);
       }
     }
   }
@@ -453,15 +532,22 @@ struct sg_tc_s {
   cudaStream_t stream = nullptr;
   uint32_t nw = 0;  // 32-edge words of the input CSR
   uint32_t* keep = nullptr;
+  uint32_t* wsrc = nullptr;  // nw: source of each word's first edge
   uint32_t* cnt = nullptr;   // nw + 1
   uint32_t* wpre = nullptr;  // nw + 1
   uint32_t* tiles = nullptr;
   uint32_t* dro = nullptr;   // n + 1
   uint32_t* dcol = nullptr;  // up to m
+  uint32_t* dsrc = nullptr;  // up to m
+  uint32_t* rcnt = nullptr;  // n + 1
+  uint32_t* rro = nullptr;   // n + 1
+  uint32_t* rcol = nullptr;  // up to m
+  uint32_t* rtiles = nullptr;
   uint32_t* lists = nullptr; // 3 n
   TcCounters* counters = nullptr;
   unsigned long long* pv = nullptr;  // n, allocated on the first per-vertex run
   bool ran = false, ran_per_vertex = false;
+  bool shorter = true;  // stream each DAG edge's shorter row
 };
 
 extern "C" {
@@ -470,11 +556,17 @@ sg_status sg_tc_destroy(sg_tc_handle t) {
   if (t) {
     cudaStreamSynchronize(t->stream);
     dev_free(t->keep);
+    dev_free(t->wsrc);
     dev_free(t->cnt);
     dev_free(t->wpre);
     dev_free(t->tiles);
     dev_free(t->dro);
     dev_free(t->dcol);
+    dev_free(t->dsrc);
+    dev_free(t->rcnt);
+    dev_free(t->rro);
+    dev_free(t->rcol);
+    dev_free(t->rtiles);
     dev_free(t->lists);
     dev_free(t->counters);
     dev_free(t->pv);
@@ -494,10 +586,12 @@ sg_status sg_tc_create(sg_graph g, sg_tc_handle* out) {
   const uint64_t n = g->n, m = g->m;
   t->nw = (uint32_t)div_up(m, 32);
   sg_status st;
-  if ((st = dev_alloc(&t->keep, t->nw)) || (st = dev_alloc(&t->cnt, (uint64_t)t->nw + 1)) ||
+  if ((st = dev_alloc(&t->keep, t->nw)) || (st = dev_alloc(&t->wsrc, t->nw)) || (st = dev_alloc(&t->cnt, (uint64_t)t->nw + 1)) ||
       (st = dev_alloc(&t->wpre, (uint64_t)t->nw + 1)) ||
       (st = dev_alloc(&t->tiles, div_up((uint64_t)t->nw + 1, kScanTile))) || (st = dev_alloc(&t->dro, n + 1)) ||
-      (st = dev_alloc(&t->dcol, m)) || (st = dev_alloc(&t->lists, 3 * n)) || (st = dev_alloc(&t->counters, 1))) {
+      (st = dev_alloc(&t->dcol, m)) || (st = dev_alloc(&t->dsrc, m)) || (st = dev_alloc(&t->rcnt, n + 1)) || (st = dev_alloc(&t->rro, n + 1)) ||
+      (st = dev_alloc(&t->rcol, m)) || (st = dev_alloc(&t->rtiles, div_up(n + 1, kScanTile))) ||
+      (st = dev_alloc(&t->lists, 3 * n)) || (st = dev_alloc(&t->counters, 1))) {
     sg_tc_destroy(t);
     return st;
   }
@@ -514,15 +608,30 @@ sg_status sg_tc_run_async(sg_tc_handle t, int per_vertex) {
   if (per_vertex && !t->pv) SG_TRY(dev_alloc(&t->pv, n));
   SG_CUDA(cudaMemsetAsync(t->counters, 0, sizeof(TcCounters), s));
   dag_flags_kernel<<<grid_for(t->nw ? t->nw : 1, 256, 8), 256, 0, s>>>(g->fwd.ro, g->fwd.col, n, m, t->nw, t->keep,
-                                                                       t->cnt);
+                                                                       t->cnt, t->wsrc);
   SG_CUDA(cudaGetLastError());
   count_launch();
   SG_TRY(exclusive_scan_u32(t->cnt, t->nw + 1, t->wpre, t->tiles, s));
-  dag_fill_kernel<<<grid_for(std::max<uint64_t>(t->nw, n), 256, 8), 256, 0, s>>>(
-      g->fwd.ro, g->fwd.col, n, t->nw, t->keep, t->wpre, t->dro, t->dcol, t->lists, t->counters);
+  const unsigned vgrid = grid_for((uint64_t)n + 1, 256, 8), egrid = grid_for(m ? m : 1, 256, 8);
+  dag_fill_kernel<<<grid_for(std::max<uint64_t>(t->nw, (uint64_t)n + 1), 256, 8), 256, 0, s>>>(
+      g->fwd.ro, g->fwd.col, n, t->nw, t->keep, t->wpre, t->wsrc, t->dro, t->dcol, t->dsrc, t->rcnt);
   SG_CUDA(cudaGetLastError());
   count_launch();
-  TcParams P{t->dro, t->dcol, t->lists, t->counters, t->pv, n};
+  if (t->shorter) {  // the DAG size is read on the device: dro[n]
+    rev_kernel<false><<<egrid, 256, 0, s>>>(t->dro, t->dcol, t->dsrc, t->dro + n, t->rcnt, nullptr, nullptr);
+    SG_CUDA(cudaGetLastError());
+    count_launch();
+  }
+  SG_TRY(exclusive_scan_u32(t->rcnt, n + 1, t->rro, t->rtiles, s));
+  if (t->shorter) {
+    rev_kernel<true><<<egrid, 256, 0, s>>>(t->dro, t->dcol, t->dsrc, t->dro + n, t->rcnt, t->rro, t->rcol);
+    SG_CUDA(cudaGetLastError());
+    count_launch();
+  }
+  classify_kernel<<<vgrid, 256, 0, s>>>(t->dro, t->rro, n, t->lists, t->counters);
+  SG_CUDA(cudaGetLastError());
+  count_launch();
+  TcParams P{t->dro, t->dcol, t->rro, t->rcol, t->lists, t->counters, t->pv, n, t->shorter ? 1u : 0u};
   if (per_vertex) {
     SG_CUDA(cudaMemsetAsync(t->pv, 0, sizeof(unsigned long long) * n, s));
     SG_TRY(launch_count<true>(P, s));
@@ -531,6 +640,13 @@ sg_status sg_tc_run_async(sg_tc_handle t, int per_vertex) {
   }
   t->ran = true;
   t->ran_per_vertex = per_vertex != 0;
+  return SG_OK;
+}
+
+sg_status sg_tc_set_shorter_rows(sg_tc_handle t, int shorter) {
+  clear_error();
+  SG_REQUIRE(t, SG_ERR_INVALID, "tc is NULL");
+  t->shorter = shorter != 0;
   return SG_OK;
 }
 
