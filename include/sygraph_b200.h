@@ -507,15 +507,26 @@ sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist);
 sg_status sg_sssp_distances_device(sg_sssp s, const void** dev_dist);
 sg_status sg_run_sssp(sg_graph g, uint32_t source, void* host_dist, uint64_t* iterations);
 
-/* CC(G) + init + run (algorithms/cc.hpp:82-169): maximum-label propagation
- * with atomicMax; labels[v] = max id over the vertices reaching v.  The
- * instance owns the label array and the engine's workspace (cc.hpp:54), so
- * that runs allocate nothing; runs are enqueued on the graph's stream. */
+/* CC(G) + init + run (algorithms/cc.hpp:82-169): labels[v] = max id over the
+ * vertices reaching v.  The instance owns the label array and the engine's
+ * workspace (cc.hpp:54), so that runs allocate nothing; runs are enqueued on
+ * the graph's stream.  Methods: the reference's maximum-label propagation
+ * with atomicMax (SG_CC_PROPAGATION, every directed graph), or, on an
+ * undirected graph (whose rows hold every edge both ways), lock-free
+ * union-find in the Afforest order (two sampled neighbours per vertex, then
+ * the other edges of the vertices outside the largest component) followed by
+ * the largest id of each component (SG_CC_UNION_FIND): the same labels.
+ * SG_CC_AUTO picks union-find for undirected graphs. */
+#define SG_CC_AUTO 0
+#define SG_CC_PROPAGATION 1
+#define SG_CC_UNION_FIND 2
 typedef struct sg_cc_s* sg_cc_handle;
 sg_status sg_cc_create(sg_graph g, sg_cc_handle* out);
 sg_status sg_cc_destroy(sg_cc_handle c);
+sg_status sg_cc_set_method(sg_cc_handle c, int method);
 sg_status sg_cc_run_async(sg_cc_handle c);
-/* iterations = propagation levels, the first one over every vertex */
+/* iterations = propagation levels, the first one over every vertex (1 for
+ * union-find: one pass over the edges) */
 sg_status sg_cc_run(sg_cc_handle c, uint64_t* iterations);
 sg_status sg_cc_get_labels(sg_cc_handle c, uint32_t* host_labels);
 sg_status sg_cc_labels_device(sg_cc_handle c, const uint32_t** dev_labels);

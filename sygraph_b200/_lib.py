@@ -225,6 +225,7 @@ SIGNATURES = {
     "sg_cc_create": (st, [vp, C.POINTER(vp)]),
     "sg_cc_destroy": (st, [vp]),
     "sg_cc_run_async": (st, [vp]),
+    "sg_cc_set_method": (st, [vp, C.c_int]),
     "sg_cc_run": (st, [vp, u64p]),
     "sg_cc_get_labels": (st, [vp, u32p]),
     "sg_cc_labels_device": (st, [vp, C.POINTER(vp)]),

@@ -270,6 +270,13 @@ class CC:
         call("sg_cc_run_async", self.handle)
         self._labels = None
 
+    AUTO, PROPAGATION, UNION_FIND = 0, 1, 2
+
+    def set_method(self, method: int) -> None:
+        """AUTO (union-find on undirected graphs), PROPAGATION (the reference's
+        maximum-label propagation) or UNION_FIND; the labels are the same."""
+        call("sg_cc_set_method", self.handle, int(method))
+
     def getLabels(self) -> np.ndarray:
         if self._labels is None:
             out = np.empty(self.G.getVertexCount(), np.uint32)

@@ -621,6 +621,133 @@ __global__ void __launch_bounds__(kThreads, 2) cc_kernel(CcParams P) {
   if (gtid == 0) P.result[0] = levels;
 }
 
+// Connected components of an undirected graph by lock-free union-find, then
+// the largest id of each component as its label (the label propagation's
+// result).  Links put the larger root under the smaller, so a component's
+// root is its smallest id: on a power-law graph a hub, which stops changing
+// early, and every link CASes the thread's own root instead of a shared
+// one.  A failed link means another thread linked that root first, so every
+// retry follows progress of the whole grid: no thread waits on another.
+// Every access to the parent array that races with the links is a strong
+// relaxed one (coherent with the atomics), and the memory clobber keeps the
+// compiler from reusing or moving it.
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
+  for (;;) {
+    const uint32_t p = ld_relaxed(parent + x);
+    if (p == x) return x;
+    const uint32_t gp = ld_relaxed(parent + p);
+    if (gp != p) st_relaxed(parent + x, gp);  // path halving: gp is an ancestor of x
+    x = gp;
+  }
+}
+
+__device__ __forceinline__ void uf_unite(uint32_t* parent, uint32_t u, uint32_t v) {
+  for (;;) {
+    u = uf_find(parent, u);
+    v = uf_find(parent, v);
+    if (u == v) return;
+    if (u < v) {
+      const uint32_t t = u;
+      u = v;
+      v = t;
+    }
+    if (atomicCAS(parent + u, u, v) == u) return;  // larger root under the smaller
+  }
+}
+
+__global__ void __launch_bounds__(256) uf_init_kernel(uint32_t* __restrict__ parent, uint32_t* __restrict__ top,
+                                                      uint32_t n) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    parent[v] = v;
+    top[v] = v;
+  }
+}
+
+// Afforest-style order: every vertex first unites with its first kSampled
+// neighbours (one round per neighbour index), the trees are flattened, and
+// the root shared by most of 1024 sampled vertices is taken as the giant
+// component's; then only vertices outside it unite with their other
+// neighbours.  An edge skipped at an endpoint inside the giant component is
+// united from its other endpoint (the rows hold every edge both ways) unless
+// that endpoint is inside too.
+constexpr uint32_t kSampled = 2, kGiantSamples = 1024;
+
+__global__ void __launch_bounds__(256) uf_sample_kernel(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
+                                                        uint32_t n, uint32_t r, uint32_t* parent) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    const uint32_t b = ro[u];
+    if (ro[u + 1] - b > r) uf_unite(parent, u, col[b + r]);
+  }
+}
+
+// One block of kGiantSamples threads: the most frequent root among the
+// samples (ties to the larger id); the trees are flat when it runs.
+__global__ void __launch_bounds__(kGiantSamples) uf_giant_kernel(const uint32_t* parent, uint32_t n,
+                                                                 uint32_t* __restrict__ giant) {
+  __shared__ uint32_t s_root[kGiantSamples];
+  __shared__ unsigned long long s_best;
+  const uint32_t i = threadIdx.x;
+  s_root[i] = ld_relaxed(parent + (uint32_t)(((uint64_t)i * 2654435761u) % n));
+  if (i == 0) s_best = 0;
+  __syncthreads();
+  uint32_t c = 0;
+  for (uint32_t j = 0; j < kGiantSamples; j++) c += s_root[j] == s_root[i];
+  atomicMax(&s_best, ((unsigned long long)c << 32) | s_root[i]);
+  __syncthreads();
+  if (i == 0) *giant = (uint32_t)s_best;
+}
+
+__global__ void __launch_bounds__(256) uf_rest_kernel(const uint32_t* __restrict__ ro, const uint32_t* __restrict__ col,
+                                                      uint32_t n, const uint32_t* __restrict__ giant, uint32_t* parent) {
+  const uint32_t g = *giant;
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    if (ld_relaxed(parent + u) == g) continue;
+    const uint32_t e = ro[u + 1];
+    for (uint32_t i = ro[u] + kSampled; i < e; i++) uf_unite(parent, u, col[i]);
+  }
+}
+
+// Flattening: every vertex's parent becomes its root.  The walk only reads:
+// a path-halving store here could land after another vertex's root and
+// replace it with an ancestor short of the root.  The only stores are roots,
+// so every value read is still an ancestor.
+__global__ void __launch_bounds__(256) uf_flatten_kernel(uint32_t* parent, uint32_t n) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    uint32_t x = v;
+    for (uint32_t p = ld_relaxed(parent + x); p != x; p = ld_relaxed(parent + x)) x = p;
+    st_relaxed(parent + v, x);
+  }
+}
+
+// top[root] = largest id of the root's (flat) tree: one atomicMax per root
+// and warp.
+__global__ void __launch_bounds__(256) uf_top_kernel(const uint32_t* __restrict__ parent, uint32_t* top, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t v = base + lane;
+    const bool ok = v < n;
+    const uint32_t r = ok ? parent[v] : 0xffffffffu;
+    const uint32_t same = __match_any_sync(0xffffffffu, r);
+    const uint32_t mx = __reduce_max_sync(same, ok ? v : 0u);
+    if (ok && lane == __ffs(same) - 1u) atomicMax(top + r, mx);
+  }
+}
+
+// labels[v] = top[root(v)]; in place: each thread reads only its own parent.
+__global__ void __launch_bounds__(256) uf_label_kernel(uint32_t* parent, const uint32_t* __restrict__ top, uint32_t n) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) parent[v] = top[parent[v]];
+}
+
 }  // namespace
 
 // Workspace shared by the push engines: rotating bitmaps, queues, counters.
@@ -682,6 +809,8 @@ struct sg_cc_s {
   cudaStream_t stream = nullptr;
   uint32_t* labels = nullptr;
   bool ran = false;
+  int method = SG_CC_AUTO;
+  bool used_union_find = false;
   PushWorkspace ws;
 };
 
@@ -1026,18 +1155,54 @@ sg_status sg_cc_create(sg_graph g, sg_cc_handle* out) {
   return SG_OK;
 }
 
+sg_status sg_cc_set_method(sg_cc_handle c, int method) {
+  clear_error();
+  SG_REQUIRE(c, SG_ERR_INVALID, "cc is NULL");
+  SG_REQUIRE(method == SG_CC_AUTO || method == SG_CC_PROPAGATION || method == SG_CC_UNION_FIND, SG_ERR_INVALID,
+             "unknown CC method");
+  SG_REQUIRE(method != SG_CC_UNION_FIND || !(c->g->flags & SG_GRAPH_DIRECTED), SG_ERR_UNSUPPORTED,
+             "union-find components need an undirected graph");
+  c->method = method;
+  return SG_OK;
+}
+
 sg_status sg_cc_run_async(sg_cc_handle c) {
   clear_error();
   SG_REQUIRE(c, SG_ERR_INVALID, "cc is NULL");
-  SG_CUDA(cudaMemsetAsync(c->ws.bar, 0, sizeof(GridBarrier), c->stream));
-  CcParams P{c->ws.loop(c->g), c->labels, c->ws.result};
-  SG_TRY(launch_persistent(cc_kernel, P, 2, c->stream));
+  const sg_graph g = c->g;
+  c->used_union_find = c->method == SG_CC_UNION_FIND || (c->method == SG_CC_AUTO && !(g->flags & SG_GRAPH_DIRECTED));
+  if (c->used_union_find) {
+    const unsigned vgrid = grid_for(g->n, 256, 8);
+    // scratch from the push workspace, idle on this path: the giant root in
+    // the first queue's first word, the per-root largest ids in the second
+    uint32_t *giant = c->ws.q.small, *top = c->ws.q.big;
+    uf_init_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, top, g->n);
+    for (uint32_t r = 0; r < kSampled; r++)
+      uf_sample_kernel<<<vgrid, 256, 0, c->stream>>>(g->fwd.ro, g->fwd.col, g->n, r, c->labels);
+    uf_flatten_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, g->n);
+    uf_giant_kernel<<<1, kGiantSamples, 0, c->stream>>>(c->labels, g->n, giant);
+    uf_rest_kernel<<<vgrid, 256, 0, c->stream>>>(g->fwd.ro, g->fwd.col, g->n, giant, c->labels);
+    uf_flatten_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, g->n);
+    uf_top_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, top, g->n);
+    uf_label_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, top, g->n);
+    SG_CUDA(cudaGetLastError());
+    count_launch(6 + kSampled);
+  } else {
+    SG_CUDA(cudaMemsetAsync(c->ws.bar, 0, sizeof(GridBarrier), c->stream));
+    CcParams P{c->ws.loop(g), c->labels, c->ws.result};
+    SG_TRY(launch_persistent(cc_kernel, P, 2, c->stream));
+  }
   c->ran = true;
   return SG_OK;
 }
 
 sg_status sg_cc_run(sg_cc_handle c, uint64_t* iterations) {
   SG_TRY(sg_cc_run_async(c));
+  if (c->used_union_find) {
+    SG_CUDA(cudaStreamSynchronize(c->stream));
+    if (iterations) *iterations = 1;  // one pass over the edges (most skipped)
+    return SG_OK;
+  }
   return c->ws.finish(c->stream, iterations);
 }
 

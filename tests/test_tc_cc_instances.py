@@ -112,3 +112,40 @@ def test_tc_row_choice(sg, oracle, rmat, shorter):
     tc.run(per_vertex=True)
     assert tc.getNumTriangles() == tot
     assert np.array_equal(tc.per_vertex, pv)
+
+
+@pytest.mark.parametrize("method", [0, 1, 2])
+def test_cc_methods(sg, oracle, rmat, method):
+    for g in (rmat(13, perm_seed=2), sg.io.grid(64, 0.0, seed=1)):
+        cc = sg.algorithms.CC(sg.graph.build.fromCSR(g))
+        cc.set_method(method)
+        cc.run()
+        assert np.array_equal(cc.getLabels(), oracle.cc_maxlabel(g))
+        if method != 1:
+            assert cc.iterations == 1
+
+
+def test_cc_union_find_many_components(sg, oracle):
+    # a forest of paths and isolated vertices: many roots, long chains
+    rng = np.random.default_rng(13)
+    n = 50000
+    perm = rng.permutation(n).astype(np.uint32)
+    cut = np.sort(rng.choice(n - 1, 3000, replace=False))
+    s, d = perm[:-1], perm[1:]
+    keep = np.ones(n - 1, bool)
+    keep[cut] = False
+    g = sg.io.fromCOO(n, s[keep], d[keep], symmetrize=True, dedupe=True)
+    ref = oracle.cc_maxlabel(g)
+    cc = sg.algorithms.CC(sg.graph.build.fromCSR(g))
+    for _ in range(5):  # the links race; every run must give the same labels
+        cc.run()
+        assert np.array_equal(cc.getLabels(), ref)
+
+
+def test_cc_union_find_needs_undirected(sg, rmat):
+    cc = sg.algorithms.CC(sg.graph.build.fromCSR(rmat(10), sg.Properties(directed=True)))
+    with pytest.raises(Exception):
+        cc.set_method(2)
+    cc.set_method(0)
+    cc.run()
+    assert cc.iterations > 1
