@@ -639,7 +639,8 @@ def main():
                "probes_per_s": probes / (tc_ms * 1e-3), "dag_edges_per_s": (gbc.m // 2) / (tc_ms * 1e-3),
                "roofline": {"bound": "hbm", "bytes": tc_bytes, "unit": "GB/s",
                             "achieved": tc_bytes / (tc_ms * 1e-3) / 1e9,
-                            "frac": tc_bytes / (tc_ms * 1e-3) / 1e9 / peaks()[0]},
+                            "frac": tc_bytes / (tc_ms * 1e-3) / 1e9 / peaks()[0],
+                            "traffic": ncu_traffic("tc_hash_kernel")},
                "note": "DAG build (keep bits, scan, compaction, reverse lists) plus the hash-set intersections, "
                        "one run; set_probes = sum over DAG edges (a,b) of min(d+(a), d+(b)), the shorter rows "
                        "streamed from L2 (head rows only: set_probes_head_rows)"}
