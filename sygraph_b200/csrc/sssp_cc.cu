@@ -730,17 +730,29 @@ __global__ void __launch_bounds__(256) uf_flatten_kernel(uint32_t* parent, uint3
 }
 
 // top[root] = largest id of the root's (flat) tree: one atomicMax per root
-// and warp.
-__global__ void __launch_bounds__(256) uf_top_kernel(const uint32_t* __restrict__ parent, uint32_t* top, uint32_t n) {
-  const uint32_t lane = threadIdx.x & 31u;
+// and warp, and for the giant component's root one per block (through
+// shared memory), since most vertices carry it.
+__global__ void __launch_bounds__(256) uf_top_kernel(const uint32_t* __restrict__ parent, uint32_t* top, uint32_t n,
+                                                     const uint32_t* __restrict__ giant) {
+  __shared__ uint32_t s_giant_max;
+  const uint32_t lane = threadIdx.x & 31u, gr = *giant;
+  if (threadIdx.x == 0) s_giant_max = 0;
+  __syncthreads();
   for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x - lane; base < n; base += gridDim.x * blockDim.x) {
     const uint32_t v = base + lane;
     const bool ok = v < n;
     const uint32_t r = ok ? parent[v] : 0xffffffffu;
     const uint32_t same = __match_any_sync(0xffffffffu, r);
     const uint32_t mx = __reduce_max_sync(same, ok ? v : 0u);
-    if (ok && lane == __ffs(same) - 1u) atomicMax(top + r, mx);
+    if (ok && lane == __ffs(same) - 1u) {
+      if (r == gr)
+        atomicMax(&s_giant_max, mx);
+      else
+        atomicMax(top + r, mx);
+    }
   }
+  __syncthreads();
+  if (threadIdx.x == 0 && s_giant_max) atomicMax(top + gr, s_giant_max);
 }
 
 // labels[v] = top[root(v)]; in place: each thread reads only its own parent.
@@ -1183,7 +1195,7 @@ sg_status sg_cc_run_async(sg_cc_handle c) {
     uf_giant_kernel<<<1, kGiantSamples, 0, c->stream>>>(c->labels, g->n, giant);
     uf_rest_kernel<<<vgrid, 256, 0, c->stream>>>(g->fwd.ro, g->fwd.col, g->n, giant, c->labels);
     uf_flatten_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, g->n);
-    uf_top_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, top, g->n);
+    uf_top_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, top, g->n, giant);
     uf_label_kernel<<<vgrid, 256, 0, c->stream>>>(c->labels, top, g->n);
     SG_CUDA(cudaGetLastError());
     count_launch(6 + kSampled);

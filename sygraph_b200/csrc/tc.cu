@@ -26,7 +26,7 @@
 // d+(x) > 128) are counted by a whole 256-thread block (one 2048-bucket
 // table; the flattened rows in 8 equal shares, one per warp), the rest by
 // single warps (256-bucket tables), medium before small so that the long
-// counts start first; four blocks share an SM.  A vertex with d+(x) > 1024
+// counts start first; five blocks share an SM.  A vertex with d+(x) > 1024
 // is counted in pieces of 1024 keys, each piece against all of x's rows.  The count is that of a graph without parallel
 // edges (the reference's sorted-list merge assumes none either); self-loops
 // are no DAG edges.
@@ -37,7 +37,8 @@ namespace {
 
 using sygraph::detail::block_sum;
 
-constexpr uint32_t kTcThreads = 256, kTcWarps = kTcThreads / 32;  // four blocks per SM
+constexpr uint32_t kTcThreads = 256, kTcWarps = kTcThreads / 32;
+constexpr uint32_t kTcBlocksPerSm = 5;  // 5 x 41 KB of shared memory, 48 registers
 constexpr uint32_t kWarpBuckets = 256;                       // one warp's table: 256 x 4 slots, 4 KB
 constexpr uint32_t kBlockBuckets = kWarpBuckets * kTcWarps;  // the block's table: 2048 buckets, 32 KB
 constexpr uint32_t kWarpMaxDeg = kWarpBuckets / 2;           // d+(u) counted by one warp
@@ -390,7 +391,7 @@ __device__ __forceinline__ uint32_t count_rows(const TcParams& P, const uint4* t
 constexpr size_t kTcSmem = sizeof(uint4) * kBlockBuckets + sizeof(uint32_t) * (2 * kBlockRows + 1);
 
 template <bool kPerVertex>
-__global__ void __launch_bounds__(kTcThreads, 4) tc_hash_kernel(TcParams P) {
+__global__ void __launch_bounds__(kTcThreads, kTcBlocksPerSm) tc_hash_kernel(TcParams P) {
   extern __shared__ uint4 s_tab[];  // kBlockBuckets, then s_vb and s_pre
   uint32_t* s_vb = reinterpret_cast<uint32_t*>(s_tab + kBlockBuckets);
   uint32_t* s_pre = s_vb + kBlockRows;
