@@ -108,19 +108,32 @@ class CC {
 
  public:
   CC(GraphType& g) : _g(g) {}
-  void init(const vertex_t& source) { _source = source; }
-  void reset() { _labels.clear(); }
+  void init(const vertex_t& source) {
+    _source = source;
+    if (!_h) {
+      sg_cc_handle c = nullptr;
+      sygraph::detail::throw_if(sg_cc_create(_g.handle(), &c));
+      _h = std::shared_ptr<sg_cc_s>(c, [](sg_cc_handle x) { sg_cc_destroy(x); });
+    }
+  }
+  void reset() {
+    _labels.clear();
+    _h.reset();
+  }
   template <bool EnableProfiling = false>
   void run() {
-    _labels.resize(_g.getVertexCount());
+    if (!_h) init(_source);
     uint64_t it = 0;
-    sygraph::detail::throw_if(sg_cc(_g.handle(), reinterpret_cast<uint32_t*>(_labels.data()), &it));
+    sygraph::detail::throw_if(sg_cc_run(_h.get(), &it));
+    _labels.resize(_g.getVertexCount());
+    sygraph::detail::throw_if(sg_cc_get_labels(_h.get(), reinterpret_cast<uint32_t*>(_labels.data())));
   }
   const std::vector<vertex_t>& getLabels() const { return _labels; }
 
  private:
   GraphType& _g;
   vertex_t _source = 0;
+  std::shared_ptr<sg_cc_s> _h;
   std::vector<vertex_t> _labels;
 };
 
@@ -152,12 +165,24 @@ class TC {
 
  public:
   TC(GraphType& g) : _g(g) {}
-  void init() { _ran = false; }
-  void reset() { _ran = false; }
+  void init() {
+    _ran = false;
+    if (!_h) {
+      sg_tc_handle t = nullptr;
+      sygraph::detail::throw_if(sg_tc_create(_g.handle(), &t));
+      _h = std::shared_ptr<sg_tc_s>(t, [](sg_tc_handle x) { sg_tc_destroy(x); });
+    }
+  }
+  void reset() {
+    _ran = false;
+    _h.reset();
+  }
   template <bool EnableProfiling = false>
   void run() {
+    if (!_h) init();
+    sygraph::detail::throw_if(sg_tc_run(_h.get(), /*per_vertex=*/1, &_total));
     _per.resize(_g.getVertexCount());
-    sygraph::detail::throw_if(sg_tc(_g.handle(), &_total, _per.data()));
+    sygraph::detail::throw_if(sg_tc_get_per_vertex(_h.get(), _per.data()));
     _ran = true;
   }
   size_t getNumTriangles() const {
@@ -171,6 +196,7 @@ class TC {
 
  private:
   GraphType& _g;
+  std::shared_ptr<sg_tc_s> _h;
   bool _ran = false;
   uint64_t _total = 0;
   std::vector<uint64_t> _per;
