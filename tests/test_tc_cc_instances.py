@@ -149,3 +149,31 @@ def test_cc_union_find_needs_undirected(sg, rmat):
     cc.set_method(0)
     cc.run()
     assert cc.iterations > 1
+
+
+@pytest.mark.parametrize("shape", ["sorted_path", "reversed_path", "star", "two_hubs"])
+def test_cc_union_find_adversarial(sg, oracle, shape):
+    # shapes that make long parent chains or hot roots under min-linking
+    n = 1 << 20 if shape.endswith("path") else 1 << 16
+    ids = np.arange(n, dtype=np.uint32)
+    if shape == "sorted_path":
+        s, d = ids[:-1], ids[1:]
+    elif shape == "reversed_path":
+        s, d = ids[1:][::-1], ids[:-1][::-1]
+    elif shape == "star":
+        s, d = np.zeros(n - 1, np.uint32), ids[1:]
+    else:  # two hubs, every other vertex on one of them, the hubs unlinked
+        s = np.where(ids[2:] % 2 == 0, 0, 1).astype(np.uint32)
+        d = ids[2:]
+    g = sg.io.fromCOO(n, s, d, symmetrize=True, dedupe=True)
+    # closed forms (the oracle's propagation needs one pass per path vertex)
+    if shape == "two_hubs":
+        ref = np.where(ids % 2 == 0, n - 2, n - 1).astype(np.uint32)
+    else:
+        ref = np.full(n, n - 1, np.uint32)
+    if n <= 1 << 16:
+        assert np.array_equal(oracle.cc_maxlabel(g), ref)
+    cc = sg.algorithms.CC(sg.graph.build.fromCSR(g))
+    for _ in range(2):
+        cc.run()
+        assert np.array_equal(cc.getLabels(), ref)
