@@ -30,6 +30,25 @@ def test_tc_clique_block_tables(sg, oracle):
     assert tc.getNumTriangles() == k * (k - 1) * (k - 2) // 6
 
 
+def test_tc_clique_pieces(sg, oracle):
+    # K_1100: DAG out-degrees up to 1099 > 1024, so the largest vertices are
+    # counted in two pieces of their table, every row streamed against each
+    k = 1100
+    iu, ju = np.triu_indices(k, 1)
+    g = sg.io.fromCOO(k, iu, ju, symmetrize=True, dedupe=True)
+    for shorter in (True, False):
+        tc = sg.algorithms.TC(sg.graph.build.fromCSR(g))
+        tc.set_shorter_rows(shorter)
+        tc.run(per_vertex=True)
+        assert tc.getNumTriangles() == k * (k - 1) * (k - 2) // 6
+        # every vertex of a clique lies in C(k-1, 2) triangles; the per-vertex
+        # convention (2 to the lowest id, 1 to the middle one) gives
+        # 2*C(k-1-v, 2) + v*(k-1-v) for vertex v
+        v = np.arange(k, dtype=np.int64)
+        want = 2 * ((k - 1 - v) * (k - 2 - v) // 2) + v * (k - 1 - v)
+        assert np.array_equal(tc.per_vertex.astype(np.int64), want)
+
+
 def test_tc_planted_clique_rmat(sg, oracle, rmat):
     g = rmat(13)
     s, d = _edges(g)
