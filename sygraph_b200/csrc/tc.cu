@@ -496,11 +496,10 @@ __global__ void __launch_bounds__(kTcThreads, kTcBlocksPerSm) tc_hash_kernel(TcP
 
 template <bool kPerVertex>
 sg_status launch_count(const TcParams& P, cudaStream_t s) {
-  static bool configured = false;  // the attribute is per kernel; setting it twice is harmless
-  if (!configured) {
-    SG_CUDA(cudaFuncSetAttribute(tc_hash_kernel<kPerVertex>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-    configured = true;
-  }
+  // once per kernel (thread-safe static initialisation)
+  static const cudaError_t configured =
+      cudaFuncSetAttribute(tc_hash_kernel<kPerVertex>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  SG_CUDA(configured);
   int occ = 0;
   SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tc_hash_kernel<kPerVertex>, (int)kTcThreads, kTcSmem));
   SG_REQUIRE(occ > 0, SG_ERR_CUDA, "triangle-count kernel does not fit on an SM");
