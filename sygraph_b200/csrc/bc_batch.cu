@@ -57,8 +57,8 @@ struct Counters {
   u64 new_deg;    // out-degree sum of the vertices that gained a source
   u64 done_in;    // in-degree sum of the vertices every source has now reached
   u64 big_packed; // (entries << 32) | chunks of this phase's chunked vertices
-  uint32_t mark;  // high-degree vertices of the next frontier (mark list)
-  uint32_t pad0;
+  uint32_t mark;       // high-degree vertices of the next frontier (mark list)
+  uint32_t next_word;  // words of a dense level handed out so far
   u64 pad[2];
 };
 
@@ -95,10 +95,36 @@ struct Params {
   u64* result;          // [forward levels, overflow, reached_edges, log entries]
 };
 
+// Levels whose sizes are kept for the backward sweep's choice of word order.
+constexpr uint32_t kSizedLevels = 64;
+
 struct Shared {
   uint32_t scan[32];
   u64 red[32];
+  uint32_t level_size[kSizedLevels];  // vertices active at each depth (same in every block)
 };
+
+// Words of a dense level are handed out one at a time from a per-level
+// counter, the next one requested before the current one is processed (its
+// latency overlaps the work), so that warps drawing heavy words do not hold
+// up the level's barrier.  Sparse levels keep the static interleaving: most
+// of their words are empty and an atomic per word would cost more.
+template <class Fn>
+__device__ __forceinline__ void for_each_word(bool dynamic, uint32_t* counter, uint32_t w0, uint32_t gwarp,
+                                              uint32_t nwarps, Fn&& fn) {
+  if (!dynamic) {
+    for (uint32_t wi = gwarp; wi < w0; wi += nwarps) fn(wi);
+    return;
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t mine = lane == 0 ? atomicAdd(counter, 1u) : 0u;
+  uint32_t wi = __shfl_sync(kFullMask, mine, 0);
+  while (wi < w0) {
+    if (lane == 0) mine = atomicAdd(counter, 1u);
+    fn(wi);
+    wi = __shfl_sync(kFullMask, mine, 0);
+  }
+}
 
 struct Local {
   u64 new_count = 0, reached = 0, new_deg = 0, done_in = 0;
@@ -446,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
       if (!grid_sync(P.bar)) return;
     }
     Local loc;
-    for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+    for_each_word(!sparse, &C->next_word, w0, gwarp, nwarps, [&](uint32_t wi) {
       uint32_t cand = ~ld_cg(P.done + wi) & valid_bits(wi, w0, n);
       if (sparse) {
         const uint32_t c = ld_cg(P.cand + wi);
@@ -463,7 +489,7 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
         const u64 nm = forward_gather(P, hist_L, beg, end, su, a0, a1);
         forward_finish(P, hist_N, act_N, mark_N, C, u, su, nm, a0, a1, loc);
       }
-    }
+    });
     if (!grid_sync(P.bar)) return;
     {
       const u64 bp = ld_cg(&C->big_packed);
@@ -477,6 +503,7 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
     block_add(loc, S, C);
     if (!grid_sync(P.bar)) return;
     const u64 next = ld_cg(&C->new_count);
+    if (threadIdx.x == 0 && L + 1 < kSizedLevels) S.level_size[L + 1] = (uint32_t)min(next, (u64)0xffffffffu);
     reached_total += ld_cg(&C->reached);
     frontier_deg = ld_cg(&C->new_deg);
     undone_in -= ld_cg(&C->done_in);
@@ -516,7 +543,8 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
     const u64* hist_next = Lb < Lmax ? P.hist + (size_t)(Lb + 1) * n : nullptr;
     const uint32_t* act_B = P.act + (size_t)Lb * w0;
     Local unused;
-    for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+    const bool dense = Lb < kSizedLevels && S.level_size[Lb] > w0;  // block- and grid-uniform
+    for_each_word(dense, &C->next_word, w0, gwarp, nwarps, [&](uint32_t wi) {
       uint32_t word = ld_cg(act_B + wi);
       while (word) {
         const uint32_t v = wi * 32 + (__ffs(word) - 1);
@@ -528,7 +556,7 @@ __global__ void __launch_bounds__(kThreads, 2) bc_batch_kernel(Params P) {
         if (hist_next) backward_gather(P, hist_next, beg, end, fv, a0, a1);
         backward_finish(P, v, fv, a0, a1);
       }
-    }
+    });
     if (!grid_sync(P.bar)) return;
     {
       const u64 bp = ld_cg(&C->big_packed);
