@@ -41,14 +41,37 @@ constexpr uint32_t kPullChunkIn = 256;  // in-edges per chunk
 constexpr uint32_t kPullProbe = 8;      // serial early-exit probes before the edge-parallel scan
 using u64 = unsigned long long;
 
+// Words of a pull level beyond each warp's first are handed out by
+// kGrabDomains counters (warp w draws from counter w % kGrabDomains); the
+// warps of a launch are a multiple of it (16 per CTA).
+constexpr uint32_t kGrabDomains = 4;
+
 struct LevelCounters {
   u64 heavy_packed;
   u64 new_count;     // vertices that became active
   u64 new_deg;       // their degree sum
   u64 reached_edges; // sum over (source, newly reached vertex) of the vertex degree
   u64 done_deg;      // degree of vertices every source reached at this level
-  u64 pad[3];
+  uint32_t grab[kGrabDomains];  // words handed out by each domain's counter
+  u64 pad[1];
 };
+
+// Each warp's first word is its own (word = its warp index); the later ones
+// come from its domain's counter (word = nwarps + d + kGrabDomains * c), the
+// next one requested before the current word is processed, so that warps
+// that drew heavy words do not hold up the level's barrier.
+template <class Fn>
+__device__ __forceinline__ void for_each_word_balanced(uint32_t* grab, uint32_t w0, uint32_t gwarp, uint32_t nwarps,
+                                                       Fn&& fn) {
+  const uint32_t lane = threadIdx.x & 31u, d = gwarp % kGrabDomains;
+  uint32_t* counter = grab + d;
+  uint32_t nxt = lane == 0 ? atomicAdd(counter, 1u) : 0u;
+  for (uint32_t wi = gwarp; wi < w0;) {
+    fn(wi);
+    wi = nwarps + d + kGrabDomains * __shfl_sync(0xffffffffu, nxt, 0);
+    if (lane == 0) nxt = atomicAdd(counter, 1u);
+  }
+}
 
 struct Params {
   uint32_t n, w0, w1, k;
@@ -396,16 +419,16 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
       n_pull++;
       const bool same = P.iro == P.ro;
       u64* acc_slot = S.acc + (threadIdx.x & ~31u);
-      for (uint32_t wi = gwarp; wi < w0; wi += nwarps) {
+      for_each_word_balanced(C->grab, w0, gwarp, nwarps, [&](uint32_t wi) {
         const uint32_t dw = ld_cg(P.done + wi);
         const uint32_t cand = ~dw & valid_bits(wi, w0, n);
-        if (!cand) continue;
+        if (!cand) return;
         const uint32_t u = wi * 32 + lane;
         const bool mine = (cand >> lane) & 1u;
         const uint32_t beg = mine ? P.iro[u] : 0u;
         const uint32_t end = mine ? P.iro[u + 1] : 0u;
         const bool light = mine && end - beg < kPullHeavyIn;
-        if (!__any_sync(kFullMask, light)) continue;
+        if (!__any_sync(kFullMask, light)) return;
         const u64 su = light ? ld_cg(P.seen + u) : P.all;
         // phase 1: a few serial probes; a vertex that every missing source
         // reaches through its first in-neighbours stops here
@@ -472,7 +495,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
           if (gmask && atomicOr(L.fa_next + wi, gmask) == 0) atomicOr(L.sm_next + (wi >> 5), 1u << (wi & 31));
           if (dmask) atomicOr(P.done + wi, dmask);
         }
-      }
+      });
       for (uint32_t c = gwarp; c < P.pull_chunks; c += nwarps) {
         const uint32_t v = P.pull_chunk_v[c];
         if (ld_cg(P.done + (v >> 5)) & (1u << (v & 31))) continue;
