@@ -368,7 +368,8 @@ def run_cc(args) -> int:
         print(f"{'Vertex':<10}{'Label':<10}")
         for v in range(csr.n):
             print(f"{v:<10}{int(lab[v]):<10}")
-    _profile(args, "cc_kernel", tm.ms, csr.m)
+    # union-find on undirected graphs, the reference's propagation on directed ones
+    _profile(args, "cc_kernel" if G.properties.directed else "uf_*_kernel", tm.ms, csr.m)
     print(f"Total Host Time: {int(host_ms)} ms")
     return 0
 
@@ -415,7 +416,7 @@ def run_tc(args) -> int:
         _validate(lambda: tc.getNumTriangles() == cpu_tc(csr))
     if args.print:
         print(f"Total num triangles: {tc.getNumTriangles()}")
-    _profile(args, "tc_count_kernel", tm.ms, csr.m)
+    _profile(args, "tc_hash_kernel", tm.ms, csr.m)
     print(f"Total Host Time: {int(host_ms)} ms")
     return 0
 
