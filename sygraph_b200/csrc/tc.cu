@@ -9,7 +9,8 @@
 //   2. every DAG edge a -> b needs |N+(a) n N+(b)|.  It is counted at the
 //      endpoint x with the longer row: x's row N+(x) goes into a
 //      shared-memory hash set (four-slot buckets, at most half a key per
-//      bucket) and the shorter row is streamed against it by whole warps
+//      bucket, one in a warp's table for 129..256 keys) and the shorter
+//      row is streamed against it by whole warps
 //      (coalesced, eight loads in flight per lane).  So x streams its
 //      out-neighbours' rows no longer than its own, and the rows of the
 //      in-neighbours y with d+(y) < d+(x) (the reverse lists, built by a
@@ -23,10 +24,10 @@
 // and 1 to b.
 //
 // Work lists by an upper bound of each vertex's probes: the big ones (or
-// d+(x) > 128) are counted by a whole 256-thread block (one 2048-bucket
+// d+(x) > 256) are counted by a whole 256-thread block (one 2048-bucket
 // table; the flattened rows in 8 equal shares, one per warp), the rest by
-// single warps (256-bucket tables), medium before small so that the long
-// counts start first; five blocks share an SM.  A vertex with d+(x) > 1024
+// single warps (256-bucket tables, up to one key per bucket), medium before
+// small so that the long counts start first; five blocks share an SM.  A vertex with d+(x) > 1024
 // is counted in pieces of 1024 keys, each piece against all of x's rows.  The count is that of a graph without parallel
 // edges (the reference's sorted-list merge assumes none either); self-loops
 // are no DAG edges.
@@ -41,7 +42,7 @@ constexpr uint32_t kTcThreads = 256, kTcWarps = kTcThreads / 32;
 constexpr uint32_t kTcBlocksPerSm = 5;  // 5 x 41 KB of shared memory, 48 registers
 constexpr uint32_t kWarpBuckets = 256;                       // one warp's table: 256 x 4 slots, 4 KB
 constexpr uint32_t kBlockBuckets = kWarpBuckets * kTcWarps;  // the block's table: 2048 buckets, 32 KB
-constexpr uint32_t kWarpMaxDeg = kWarpBuckets / 2;           // d+(u) counted by one warp
+constexpr uint32_t kWarpMaxDeg = kWarpBuckets;               // d+(u) counted by one warp (<= 1 key per bucket)
 constexpr uint64_t kWarpMaxWork = 1ull << 17;                // probe bound counted by one warp
 constexpr uint64_t kSmallMaxWork = 1ull << 11;               // medium above, small below
 constexpr uint32_t kBlockMaxDeg = kBlockBuckets / 2;  // keys of one block table
@@ -251,12 +252,13 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles(const uint32_t* in, u
 // load.  A key goes to the first empty slot at or after the first slot of
 // its bucket (linear probing over slots), so every bucket fills as a prefix:
 // a bucket whose last slot is empty ends a lookup.  At most half a key per
-// bucket, so about one lookup in 400 reads a second bucket.
+// bucket (one in a warp's table holding 129 to 256 keys), so a few lookups
+// in a thousand read a second bucket.
 __device__ __forceinline__ uint32_t bucket_of(uint32_t key, uint32_t shift) { return (key * 0x9E3779B1u) >> shift; }
 
 __device__ __forceinline__ void set_insert(uint4* tab, uint32_t key, uint32_t shift, uint32_t bmask) {
   uint32_t h = bucket_of(key, shift);
-  for (;;) {  // ends: at most half a key per bucket
+  for (;;) {  // ends: at most one key per bucket, a quarter of the slots
     uint32_t* slot = reinterpret_cast<uint32_t*>(tab + h);
 #pragma unroll
     for (uint32_t i = 0; i < 4; i++) {
