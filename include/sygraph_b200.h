@@ -513,7 +513,7 @@ sg_status sg_run_sssp(sg_graph g, uint32_t source, void* host_dist, uint64_t* it
  * the graph's stream.  Methods: the reference's maximum-label propagation
  * with atomicMax (SG_CC_PROPAGATION, every directed graph), or, on an
  * undirected graph (whose rows hold every edge both ways), lock-free
- * union-find in the Afforest order (two sampled neighbours per vertex, then
+ * union-find in the Afforest order (one sampled neighbour per vertex, then
  * the other edges of the vertices outside the largest component) followed by
  * the largest id of each component (SG_CC_UNION_FIND): the same labels.
  * SG_CC_AUTO picks union-find for undirected graphs. */
