@@ -129,11 +129,26 @@ class GraphCSR {
   sg_graph handle() const { return _handle.get(); }
   const Queue& getQueue() const { return _queue; }
 
+  // 64 bytes of device memory owned by the graph, allocated on first use and
+  // released with the graph: the accumulator of compute::reduce, so repeated
+  // reductions allocate nothing.  Calls on one graph share it (they are
+  // ordered on the graph's queue).
+  static constexpr size_t kScratchBytes = 64;
+  void* scratch() const {
+    if (!_scratch) {
+      void* p = nullptr;
+      sygraph::detail::throw_if_cuda(cudaMalloc(&p, kScratchBytes), "cudaMalloc");
+      _scratch = std::shared_ptr<void>(p, [](void* q) { cudaFree(q); });
+    }
+    return _scratch.get();
+  }
+
  private:
   Queue _queue;
   formats::CSR<ValueT, IndexT, OffsetT> _csr;
   Properties _properties;
   std::shared_ptr<sg_graph_s> _handle;
+  mutable std::shared_ptr<void> _scratch;
 };
 
 }  // namespace detail

@@ -27,11 +27,22 @@ namespace sygraph {
 namespace operators {
 namespace detail {
 
-inline unsigned advance_grid(int expected_size) {
-  int dev = 0, sms = 148;
+// SM count of the current device, queried once per device and thread.
+inline unsigned sm_count() {
+  static thread_local int cached_dev = -1, cached_sms = 148;
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned full = (unsigned)sms * 8u;
+  if (dev != cached_dev) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0) cached_sms = sms;
+    else cudaGetLastError();
+    cached_dev = dev;
+  }
+  return (unsigned)cached_sms;
+}
+
+inline unsigned advance_grid(int expected_size) {
+  const unsigned full = sm_count() * 8u;
   if (expected_size > 0) {
     const unsigned want = (unsigned)(((uint64_t)expected_size + 255) / 256);
     return want < 1 ? 1 : (want < full ? want : full);
@@ -226,18 +237,20 @@ Event reduce(GraphT& graph, frontier::Frontier<T, FT>& f, R& accumulator, Lambda
   static_assert(FW == frontier::frontier_view::vertex, "Invalid frontier view for compute operation.");
   cudaStream_t s = graph.getQueue().stream();
   cudaEvent_t start = Event::mark(s);
+  static_assert(sizeof(R) <= GraphT::kScratchBytes, "reduction type larger than the graph's accumulator");
   f.computeActiveFrontier(false);
-  R* d = nullptr;
-  sygraph::detail::throw_if_cuda(cudaMalloc(&d, sizeof(R)), "cudaMalloc");
-  cudaMemsetAsync(d, 0, sizeof(R), s);
+  // the graph's preallocated accumulator: no allocation per call
+  R* d = static_cast<R*>(graph.scratch());
+  sygraph::detail::throw_if_cuda(cudaMemsetAsync(d, 0, sizeof(R), s), "cudaMemsetAsync");
   using A = detail::ReduceAdapter<R, std::decay_t<LambdaT>>;
   detail::reduce_kernel<R, A><<<operators::detail::advance_grid(-1), 256, 0, s>>>(
       f.getDeviceFrontier(), (uint32_t)graph.getVertexCount(), A{function}, d);
   sygraph::detail::throw_if_cuda(cudaGetLastError(), "reduce launch");
   R h{};
-  cudaMemcpyAsync(&h, d, sizeof(R), cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
-  cudaFree(d);
+  // the sum goes to a host reference, so the call waits for it, as the
+  // reference's reduction into a host buffer does
+  sygraph::detail::throw_if_cuda(cudaMemcpyAsync(&h, d, sizeof(R), cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync");
+  sygraph::detail::throw_if_cuda(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   accumulator += h;
   return Event(s, start);
 }

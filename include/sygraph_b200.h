@@ -356,15 +356,17 @@ sg_status sg_run_bfs(sg_graph g, uint32_t source, int direction, float alpha, fl
  * and passes in only input and output buffers.  The caller passes the device
  * CSR (forward, and the inverse CSR of a directed graph; NULL inverse means
  * the graph is undirected) and a device array of n depths (n+1 = unreached,
- * same values as sg_bfs_run).  All working memory is one static device array
- * of about 11 MB inside this library, held by every GPU that loads it until
- * the process exits; graphs above 2^22 vertices or 2^27 edges are rejected
- * with SG_ERR_INVALID.  The first call on a device looks up that array's
- * address (once per device); make that first call before any stream capture.
- * Every call shares the array: calls whose work overlaps on the GPU (other
- * streams, other threads) race and must be serialised by the caller.  The
- * call waits for the traversal to finish; *host_iterations (optional) gets
- * the number of BFS levels. */
+ * same values as sg_bfs_run).  m must equal row_offsets[n] of the forward
+ * and of the inverse CSR (read back and checked: SG_ERR_INVALID otherwise).
+ * All working memory is one static device array of about 11 MB inside this
+ * library, held by every GPU that loads it until the process exits; graphs
+ * above 2^22 vertices or 2^27 edges are rejected with SG_ERR_INVALID.  The
+ * first call on a device looks up that array's address (once per device);
+ * make that first call before any stream capture.  Every call shares the
+ * array: calls whose work overlaps on the GPU (other streams, other threads)
+ * race and must be serialised by the caller.  The call is synchronous: it
+ * waits on `stream` for the edge-count check and again for the traversal to
+ * finish; *host_iterations (optional) gets the number of BFS levels. */
 sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_column_indices,
                          const uint32_t* dev_inv_row_offsets, const uint32_t* dev_inv_column_indices, uint32_t n,
                          uint64_t m, uint32_t source, int direction, float alpha, float beta, uint32_t* dev_depth,

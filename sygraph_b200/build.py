@@ -30,7 +30,7 @@ CPP_TEST_BIN = CPP_TESTS / "bin"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a", "-ccbin", "/usr/bin/g++"]
 NVCC_FLAGS = [
     "-O3",
-    "-std=c++17",
+    "-std=c++20",
     "-lineinfo",
     "--expt-relaxed-constexpr",
     "--extended-lambda",
@@ -39,7 +39,7 @@ NVCC_FLAGS = [
     f"-I{INCLUDE}",
     f"-I{CSRC}",
 ]
-CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", f"-I{INCLUDE}", f"-I{CSRC}"]
+CXX_FLAGS = ["-O3", "-std=c++20", "-fPIC", "-fopenmp", f"-I{INCLUDE}", f"-I{CSRC}"]
 
 
 def nvcc() -> str:

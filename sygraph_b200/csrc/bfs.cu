@@ -19,6 +19,7 @@
 // One grid barrier per level; no host round trip until the traversal ends.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -371,9 +372,11 @@ static sg_status bfs_collect(sg_bfs b, sg_bfs_details* details) {
     details->visited_vertices = res[3];
     details->visited_edges = res[4];
     const uint32_t nlog = res[0] < SG_MAX_LOGGED_LEVELS ? (uint32_t)res[0] : SG_MAX_LOGGED_LEVELS;
-    std::vector<sg_level_record> recs(nlog ? nlog : 1);
+    // (a std::vector of this C struct trips an internal error of nvcc 12.9's
+    // front end under -std=c++20)
+    std::unique_ptr<sg_level_record[]> recs(new sg_level_record[nlog ? nlog : 1]);
     if (nlog) {
-      SG_CUDA(cudaMemcpy(recs.data(), b->log, sizeof(sg_level_record) * nlog, cudaMemcpyDeviceToHost));
+      SG_CUDA(cudaMemcpy(recs.get(), b->log, sizeof(sg_level_record) * nlog, cudaMemcpyDeviceToHost));
       for (uint32_t i = 0; i < nlog; i++) details->step_is_pull[i] = recs[i].strategy >= 2;
     }
   }
@@ -688,6 +691,17 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   unsigned char* base = nullptr;
   SG_TRY(scratch_base(&base));
   cudaStream_t s = (cudaStream_t)stream;
+  // The heavy-vertex lists in the static array are sized from m: a caller's
+  // m below the graph's real edge count would let them overflow into the
+  // regions after them, so m must be row_offsets[n] of both CSRs.
+  {
+    uint32_t last[2] = {0, 0};
+    SG_CUDA(cudaMemcpyAsync(&last[0], dev_row_offsets + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaMemcpyAsync(&last[1], dev_inv_row_offsets + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SG_CUDA(cudaStreamSynchronize(s));
+    SG_REQUIRE(last[0] == m && last[1] == m, SG_ERR_INVALID,
+               "sg_bfs_noalloc: m must equal row_offsets[n] of the forward and the inverse CSR");
+  }
   const uint32_t w0 = div_up(n, 32), w1 = div_up(w0, 32);
   bfs::Params P;
   P.n = n;
@@ -705,7 +719,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.margin = 0.f;
   P.min_frontier = 0.f;
   P.pull_reverse = 0;
-  P.pull_words = 2;
+  P.pull_words = 4;  // the instance default of sg_bfs_create
   P.features = nullptr;
   P.alpha = alpha;
   P.beta = beta;

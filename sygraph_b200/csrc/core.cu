@@ -395,8 +395,7 @@ sg_status sg_graph_create_csr(const uint32_t* host_row_offsets, const uint32_t* 
   SG_REQUIRE(n < 0xffffffffu, SG_ERR_INVALID, "vertex count must be below 2^32-1");
   SG_REQUIRE(value_type == SG_WEIGHT_NONE || value_type == SG_WEIGHT_F32 || value_type == SG_WEIGHT_U32,
              SG_ERR_INVALID, "unknown value_type");
-  SG_REQUIRE(host_row_offsets[0] == 0 && host_row_offsets[n] == m, SG_ERR_INVALID,
-             "row_offsets must start at 0 and end at m");
+  SG_TRY(check_csr(host_row_offsets, host_column_indices, n, m));
   sg_graph g = new sg_graph_s();
   g->n = n;
   g->m = m;

@@ -21,6 +21,26 @@
 namespace sgb {
 sg_status fail(sg_status s, const std::string& msg);
 void clear_error();
+
+// Structure check of a host CSR before anything indexes with it: offsets
+// start at 0, never decrease and end at m, and every column is a vertex id.
+// A graph that fails it would make every kernel read and write outside its
+// per-vertex arrays.  O(n + m), OpenMP.
+sg_status check_csr(const uint32_t* ro, const uint32_t* col, uint32_t n, uint64_t m) {
+  if (ro[0] != 0 || ro[n] != m) return fail(SG_ERR_INVALID, "row_offsets must start at 0 and end at m");
+  int64_t bad_row = -1, bad_edge = -1;
+#pragma omp parallel for schedule(static) reduction(max : bad_row)
+  for (int64_t v = 0; v < (int64_t)n; v++)
+    if (ro[v + 1] < ro[v]) bad_row = std::max(bad_row, v);
+  if (bad_row >= 0)
+    return fail(SG_ERR_INVALID, "row_offsets decrease at row " + std::to_string(bad_row));
+#pragma omp parallel for schedule(static) reduction(max : bad_edge)
+  for (int64_t e = 0; e < (int64_t)m; e++)
+    if (col[e] >= n) bad_edge = std::max(bad_edge, e);
+  if (bad_edge >= 0)
+    return fail(SG_ERR_INVALID, "column index out of range at edge " + std::to_string(bad_edge));
+  return SG_OK;
+}
 }  // namespace sgb
 
 namespace {
@@ -301,6 +321,8 @@ sg_status sg_csr_invert(const sg_host_csr* in, sg_host_csr* out) {
   if (!in || !out) return fail(SG_ERR_INVALID, "NULL argument");
   const uint32_t n = in->n;
   const uint64_t m = in->m;
+  if (!in->row_offsets || (m && !in->column_indices)) return fail(SG_ERR_INVALID, "NULL CSR array");
+  if (sgb::check_csr(in->row_offsets, in->column_indices, n, m) != SG_OK) return SG_ERR_INVALID;
   memset(out, 0, sizeof(*out));
   out->n = n;
   out->m = m;
@@ -393,9 +415,13 @@ sg_status sg_csr_read_binary(const char* path, int value_type, sg_host_csr* out)
   ok = fread(out->row_offsets, 4, rows, f) == rows && fread(out->column_indices, 4, nnz, f) == nnz &&
        fread(out->values, 4, nnz, f) == nnz;
   fclose(f);
-  if (!ok || out->row_offsets[0] != 0 || out->row_offsets[out->n] != nnz) {
+  if (!ok) {
     sg_host_csr_free(out);
     return fail(SG_ERR_INVALID, "malformed binary CSR body");
+  }
+  if (sgb::check_csr(out->row_offsets, out->column_indices, out->n, nnz) != SG_OK) {
+    sg_host_csr_free(out);
+    return SG_ERR_INVALID;  // the message names the first bad row or edge
   }
   if (value_type == SG_WEIGHT_NONE) {
     free(out->values);

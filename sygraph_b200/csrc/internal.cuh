@@ -21,6 +21,9 @@ void set_error(const std::string& msg);
 void clear_error();
 sg_status fail(sg_status s, const std::string& msg);
 sg_status cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+// Host CSR structure check (host_graph.cpp): offsets start at 0, never
+// decrease and end at m; every column is below n.
+sg_status check_csr(const uint32_t* ro, const uint32_t* col, uint32_t n, uint64_t m);
 
 // Every launch goes through this counter so callers can report how many of
 // this library's kernels ran in a timed region.

@@ -4,6 +4,8 @@
 // in place of sycl::queue.  Fixture matrices arrive on argv
 // (name=rows separated by ';') from tests/test_cpp_api.py.
 #include <array>
+#include <cstring>
+#include <limits>
 
 #include "test_utils.hpp"
 
@@ -89,6 +91,127 @@ uint32_t run_pull_case(GraphT& G, bool* active) {
   return two;
 }
 
+// sync::min / cas / load / store / atomicFetchAdd (sync/atomics.hpp:24-100):
+// every candidate is applied by 64 threads at once, so the minima are
+// contended; the expected values follow operator< (no store unless the
+// candidate is strictly less).
+template <typename T>
+__global__ void sync_min_kernel(T* targets, T* cand, const int* target_of, int k, int copies) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < k * copies) sync::min(targets + target_of[i / copies], cand + i / copies);
+}
+
+__global__ void sync_cas_kernel(uint32_t* word, uint32_t* won, uint32_t* seen) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t expected = 0;
+  if (sync::cas(word, expected, t + 1)) {
+    sync::atomicFetchAdd(won, 1u);
+    seen[t] = t + 1;
+  } else {
+    seen[t] = expected;  // the winner's value
+  }
+}
+
+__global__ void sync_add_kernel(float* acc, double* dacc, uint64_t* cnt) {
+  sync::atomicFetchAdd(acc, 1.0f);
+  sync::atomicFetchAdd(dacc, 0.5);
+  sync::atomicFetchAdd(cnt, (uint64_t)1);
+}
+
+__global__ void sync_load_store_kernel(uint64_t* p, uint64_t* out) {
+  if (threadIdx.x == 0) sync::store(p, sync::load(p) * 3 + 1);
+  __syncthreads();
+  if (threadIdx.x == 1) *out = sync::load(p);
+}
+
+template <typename T>
+bool same_bits(T a, T b) {
+  return std::memcmp(&a, &b, sizeof(T)) == 0;
+}
+
+template <typename T>
+void run_sync_min(Queue& q) {
+  const T inf = std::numeric_limits<T>::infinity(), nan = std::numeric_limits<T>::quiet_NaN();
+  // (target start, candidates) -> expected final value
+  struct Case {
+    T start;
+    std::vector<T> cand;
+    T want;
+  };
+  const std::vector<Case> cases{
+      {T(5), {T(-1), T(-2.5), T(3), T(-2.4), T(0.5)}, T(-2.5)},  // mixed sign
+      {T(-1), {T(-2), T(-0.5), T(4)}, T(-2)},                     // negative start
+      {T(0), {T(-0.0)}, T(0)},                                     // -0 is not below +0
+      {T(-0.0), {T(0)}, T(-0.0)},                                  // +0 is not below -0
+      {T(1), {T(-0.0)}, T(-0.0)},
+      {T(-3), {nan}, T(-3)},                                       // NaN is never less
+      {inf, {-inf, T(7)}, -inf},
+      {T(2), {T(3), T(4)}, T(2)},
+  };
+  const int copies = 64;
+  std::vector<T> cand_h;
+  std::vector<int> of_h;
+  for (size_t c = 0; c < cases.size(); ++c)
+    for (T x : cases[c].cand) {
+      cand_h.push_back(x);
+      of_h.push_back((int)c);
+    }
+  const int k = (int)cand_h.size();
+  T* targets = memory::detail::memoryAlloc<T, memory::space::shared>(cases.size(), q);
+  T* cand = memory::detail::memoryAlloc<T, memory::space::shared>(k, q);
+  int* of = memory::detail::memoryAlloc<int, memory::space::shared>(k, q);
+  for (size_t c = 0; c < cases.size(); ++c) targets[c] = cases[c].start;
+  for (int i = 0; i < k; ++i) {
+    cand[i] = cand_h[i];
+    of[i] = of_h[i];
+  }
+  sync_min_kernel<T><<<(k * copies + 255) / 256, 256>>>(targets, cand, of, k, copies);
+  EXPECT(cudaDeviceSynchronize() == cudaSuccess);
+  for (size_t c = 0; c < cases.size(); ++c) EXPECT(same_bits(targets[c], cases[c].want));
+  memory::detail::releaseUSM(targets, q);
+  memory::detail::releaseUSM(cand, q);
+  memory::detail::releaseUSM(of, q);
+}
+
+void run_sync_misc(Queue& q) {
+  // integers: hardware minimum, signed and unsigned
+  int* si = memory::detail::memoryAlloc<int, memory::space::shared>(1, q);
+  int* sc = memory::detail::memoryAlloc<int, memory::space::shared>(3, q);
+  int* of = memory::detail::memoryAlloc<int, memory::space::shared>(3, q);
+  si[0] = 5;
+  sc[0] = -7;
+  sc[1] = 3;
+  sc[2] = 10;
+  of[0] = of[1] = of[2] = 0;
+  sync_min_kernel<int><<<1, 192>>>(si, sc, of, 3, 64);
+  EXPECT(cudaDeviceSynchronize() == cudaSuccess);
+  EXPECT(si[0] == -7);
+  // compare-exchange: exactly one of 1024 threads wins, the others see its value
+  uint32_t* word = memory::detail::memoryAlloc<uint32_t, memory::space::shared>(2, q);
+  uint32_t* seen = memory::detail::memoryAlloc<uint32_t, memory::space::shared>(1024, q);
+  word[0] = word[1] = 0;
+  sync_cas_kernel<<<4, 256>>>(word, word + 1, seen);
+  EXPECT(cudaDeviceSynchronize() == cudaSuccess);
+  EXPECT(word[1] == 1 && word[0] != 0);
+  for (int t = 0; t < 1024; ++t) EXPECT(seen[t] == word[0]);
+  // fetch_add on float, double and 64-bit integers
+  float* acc = memory::detail::memoryAlloc<float, memory::space::shared>(1, q);
+  double* dacc = memory::detail::memoryAlloc<double, memory::space::shared>(1, q);
+  uint64_t* cnt = memory::detail::memoryAlloc<uint64_t, memory::space::shared>(3, q);
+  acc[0] = 0.0f;
+  dacc[0] = 0.0;
+  cnt[0] = 0;
+  sync_add_kernel<<<8, 256>>>(acc, dacc, cnt);
+  EXPECT(cudaDeviceSynchronize() == cudaSuccess);
+  EXPECT(acc[0] == 2048.0f && dacc[0] == 1024.0 && cnt[0] == 2048);
+  cnt[1] = 4;
+  sync_load_store_kernel<<<1, 32>>>(cnt + 1, cnt + 2);
+  EXPECT(cudaDeviceSynchronize() == cudaSuccess);
+  EXPECT(cnt[1] == 13 && cnt[2] == 13);
+  for (void* p : {(void*)si, (void*)sc, (void*)of, (void*)word, (void*)seen, (void*)acc, (void*)dacc, (void*)cnt})
+    memory::detail::releaseUSM(p, q);
+}
+
 int main(int argc, char** argv) {
   auto q = tests::makeQueue();
   const std::string symmetric_6nodes = tests::matrixArg(argc, argv, "symmetric_6nodes");
@@ -147,6 +270,11 @@ int main(int argc, char** argv) {
         graph, output, sum, SYGRAPH_LAMBDA(auto vertex, auto& acc) { acc += static_cast<uint32_t>(vertex); })
         .waitAndThrow();
     EXPECT(sum == 6);
+    // a second reduction reuses the graph's accumulator and adds again
+    operators::compute::reduce<frontier_view_t::vertex, operators::compute::plus<uint32_t>>(
+        graph, output, sum, SYGRAPH_LAMBDA(auto vertex, auto& acc) { acc += static_cast<uint32_t>(vertex); })
+        .waitAndThrow();
+    EXPECT(sum == 12);
     memory::detail::releaseUSM(seen, q);
     std::puts("filter_compute ok");
   }
@@ -236,6 +364,12 @@ int main(int argc, char** argv) {
     const std::vector<float> want{0, 3, 2, 1, 0};
     for (size_t i = 0; i < want.size(); ++i) EXPECT(std::abs(bc.getBC()[i] - want[i]) <= 1e-4f * (1 + want[i]));
     std::puts("bc ok");
+  }
+  {  // sync/atomics.hpp
+    run_sync_min<float>(q);
+    run_sync_min<double>(q);
+    run_sync_misc(q);
+    std::puts("sync ok");
   }
   std::puts("ALL OK");
   return 0;

@@ -3,9 +3,11 @@
 Reads SYgraph's test sources as text (nothing is compiled or run): the dense
 adjacency matrices of tests/include/test_utils.hpp and
 include/sygraph/io/matrices.hpp, and the answers its tests assert.  Each entry
-keeps the file:line it came from.  Run from the repository root:
+keeps the file:line it came from.  The committed kat.json is the
+authoritative fixture; it is regenerated only by hand, from the repository
+root, with the path of a SYgraph checkout:
 
-    python tests/golden/make_golden.py [/path/to/SYgraph]
+    python tests/golden/make_golden.py /path/to/SYgraph
 """
 from __future__ import annotations
 
@@ -14,7 +16,9 @@ import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if __name__ == "__main__" and len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py /path/to/SYgraph")
+REF = Path(sys.argv[1]) if len(sys.argv) > 1 else None
 OUT = Path(__file__).resolve().parent / "kat.json"
 
 

@@ -115,3 +115,43 @@ def test_argument_errors_without_gpu(sg):
     assert lib.sg_msbfs_create(None, 64, C.byref(out)) == sg._lib.SG_ERR_INVALID
     with pytest.raises(sg._lib.SygraphError):
         sg.io.rmat(0)
+
+
+def _create(sg, ro, col, flags):
+    lib = sg._lib.lib
+    out = C.c_void_p()
+    ro = np.ascontiguousarray(ro, np.uint32)
+    col = np.ascontiguousarray(col, np.uint32)
+    st = lib.sg_graph_create_csr(ro.ctypes.data_as(C.POINTER(C.c_uint32)), col.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                 None, 0, ro.size - 1, col.size, flags, None, C.byref(out))
+    return st, out
+
+
+@pytest.mark.parametrize("flags", [0, 1])  # undirected, directed
+def test_malformed_csr_is_rejected_before_upload(sg, flags):
+    """A column index >= n or decreasing offsets would make every kernel index
+    outside its per-vertex arrays: the graph is refused on the host."""
+    st, out = _create(sg, [0, 2, 3, 4], [1, 7, 0, 0], flags)  # column 7 with n = 3
+    assert st == sg._lib.SG_ERR_INVALID and not out.value
+    assert b"column index out of range at edge 1" in sg._lib.lib.sg_last_error()
+    st, out = _create(sg, [0, 3, 1, 4], [1, 2, 0, 1], flags)  # offsets 3 -> 1
+    assert st == sg._lib.SG_ERR_INVALID and not out.value
+    assert b"row_offsets decrease at row 1" in sg._lib.lib.sg_last_error()
+
+
+def test_malformed_binary_csr_is_rejected(sg, tmp_path):
+    g = sg.io.rmat(6, perm_seed=3)
+    good = tmp_path / "g.bin"
+    sg.io.toBinary(g, good)
+    raw = bytearray(good.read_bytes())
+    body = 32 + 4 * (g.n + 1)  # 32-byte header, then row offsets, then columns
+    bad_col = bytearray(raw)
+    bad_col[body:body + 4] = (g.n + 5).to_bytes(4, "little")
+    (tmp_path / "c.bin").write_bytes(bad_col)
+    with pytest.raises(sg._lib.SygraphError, match="column index out of range"):
+        sg.io.fromBinary(tmp_path / "c.bin")
+    bad_ro = bytearray(raw)
+    bad_ro[32 + 4 * 2:32 + 4 * 3] = (g.m).to_bytes(4, "little")  # row 1 ends at m, row 2 ends lower
+    (tmp_path / "r.bin").write_bytes(bad_ro)
+    with pytest.raises(sg._lib.SygraphError, match="row_offsets decrease"):
+        sg.io.fromBinary(tmp_path / "r.bin")

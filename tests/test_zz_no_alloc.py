@@ -4,8 +4,11 @@ allocator, or a plug-in whose host application owns all device memory).
 
 Its working memory is a static device array inside the library, so the
 test checks that two calls in a row, sharing that array, give the same
-depths as the allocating entry point (sg_run_bfs); depths are integers, so
-the comparison is exact.  The file is collected last on purpose."""
+depths as the allocating entry point (sg_run_bfs) and as the oracle's BFS;
+depths are integers, so the comparison is exact.  Two graphs at the entry
+point's vertex limit (2^22) fill its heavy-vertex lists (directed: 2^19
+vertices of out-degree 256, the list's capacity; undirected: 2^18 hubs).
+The file is collected last on purpose."""
 import ctypes as C
 
 import numpy as np
@@ -31,8 +34,17 @@ def _reference_depths(sg, G, source, direction):
     return out, int(d.iterations)
 
 
+def _call(fn, sg, G, g, directed, src, direction, depth, m=None):
+    fwd, inv = G.device_view(False), G.device_view(True)
+    it = C.c_uint64()
+    st = fn(fwd.row_offsets, fwd.column_indices, inv.row_offsets if directed else None,
+            inv.column_indices if directed else None, g.n, g.m if m is None else m, src, direction, 15.0, 24.0,
+            C.cast(depth.ptr, C.POINTER(C.c_uint32)), C.byref(it), None)
+    return st, it.value
+
+
 @pytest.mark.parametrize("directed", [False, True])
-def test_noalloc_matches_allocating_bfs_twice(sg, rmat, directed):
+def test_noalloc_matches_allocating_bfs_twice(sg, rmat, oracle, directed):
     fn = _bind(sg)
     if directed:
         rng = np.random.default_rng(4)
@@ -56,6 +68,66 @@ def test_noalloc_matches_allocating_bfs_twice(sg, rmat, directed):
         want, want_it = _reference_depths(sg, G, src, direction)
         assert np.array_equal(depth.numpy(), want)
         assert it.value == want_it
+        assert np.array_equal(want, oracle.bfs_levels(g, src))
+
+
+def _hub_tree_directed(sg):
+    """n = 2^22: hubs 0..2^19-1 of out-degree exactly 256 (tree edges to hubs
+    2h+1, 2h+2, the rest to leaves), leaves without out-edges; m = 2^27."""
+    n, H = 1 << 22, 1 << 19
+    L = n - H
+    h = np.arange(H, dtype=np.int64)[:, None]
+    j = np.arange(256, dtype=np.int64)[None, :]
+    col = H + (h * 256 + j) % L
+    for k in (0, 1):
+        child = 2 * h[:, 0] + 1 + k
+        col[:, k] = np.where(child < H, child, col[:, k])
+    ro = np.concatenate([np.arange(H + 1, dtype=np.int64) * 256, np.full(L, H * 256, np.int64)])
+    return sg.CSR(ro.astype(np.uint32), col.reshape(-1).astype(np.uint32), properties=sg.Properties(directed=True))
+
+
+def _hub_tree_undirected(sg):
+    """n = 2^22: 2^18 hubs linked as a binary tree, each joined to 255 leaves;
+    every leaf is joined to exactly 17 hubs; m = 134,217,726."""
+    n, H = 1 << 22, 1 << 18
+    L = n - H
+    assert H * 255 == 17 * L
+    h = np.arange(H, dtype=np.int64)
+    tree = np.stack([np.where(h > 0, (h - 1) // 2, -1), np.where(2 * h + 1 < H, 2 * h + 1, -1),
+                     np.where(2 * h + 2 < H, 2 * h + 2, -1)], axis=1)
+    leaves = H + (h[:, None] * 255 + np.arange(255, dtype=np.int64)[None, :]) % L
+    hub_rows = np.concatenate([tree, leaves], axis=1)
+    keep = hub_rows >= 0
+    hub_deg = keep.sum(axis=1)
+    r = np.arange(L, dtype=np.int64)[:, None]
+    leaf_rows = (r + np.arange(17, dtype=np.int64)[None, :] * L) // 255
+    deg = np.concatenate([hub_deg, np.full(L, 17, np.int64)])
+    ro = np.zeros(n + 1, np.int64)
+    np.cumsum(deg, out=ro[1:])
+    col = np.concatenate([hub_rows[keep], leaf_rows.reshape(-1)])
+    return sg.CSR(ro.astype(np.uint32), col.astype(np.uint32))
+
+
+@pytest.mark.parametrize("directed", [True, False])
+def test_noalloc_at_its_vertex_limit(sg, oracle, directed):
+    fn = _bind(sg)
+    g = _hub_tree_directed(sg) if directed else _hub_tree_undirected(sg)
+    assert g.n == 1 << 22 and g.m <= 1 << 27
+    assert int((g.degrees() >= 256).sum()) == (1 << 19 if directed else 1 << 18)
+    G = sg.graph.build.fromCSR(g, sg.Properties(directed=directed))
+    depth = sg.DeviceArray(shape=g.n, dtype=np.uint32)
+    for direction, src in ((2, 0), (0, 5)):  # hybrid from the root hub, then push from another hub
+        st, it = _call(fn, sg, G, g, directed, src, direction, depth)
+        assert st == 0, sg._lib.lib.sg_last_error().decode()
+        want, want_it = _reference_depths(sg, G, src, direction)
+        got = depth.numpy()
+        assert np.array_equal(got, want)
+        assert it == want_it
+        assert np.array_equal(got, oracle.bfs_levels(g, src))
+    # an edge count that is not row_offsets[n] would undersize the heavy lists
+    st, _ = _call(fn, sg, G, g, directed, 0, 2, depth, m=g.m // 2)
+    assert st == sg._lib.SG_ERR_INVALID
+    assert "row_offsets[n]" in sg._lib.lib.sg_last_error().decode()
 
 
 def test_noalloc_rejects_graphs_over_its_limit(sg):
