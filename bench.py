@@ -153,27 +153,37 @@ def make_graph(sg):
     return g, time.time() - t
 
 
+def bench_config(n: int, m: int) -> dict:
+    """The workload as both arms report it (identical keys and values)."""
+    return {"workload": f"DO-BFS (hybrid, alpha {ALPHA:g}, beta {BETA:g}) from {N_SOURCES} random sources per GPU, "
+                        f"RMAT-{SCALE} ef{EDGE_FACTOR} (0.57,0.19,0.19,0.05) seed 1",
+            "n": n, "m": m, "sources_per_step": N_SOURCES, "source_seed": SOURCE_SEED,
+            "l2": "inputs larger than L2 (CSR %.2f GB > 126 MB)" % ((4 * (n + 1) + 8 * m) / 1e9)}
+
+
 def run_reference(args, world, rank):
-    """CPU arm: the oracle's OpenMP restatement of BFS::run on the host cores."""
+    """CPU arm: the oracle's OpenMP restatement of BFS::run (the reference is
+    SYCL and cannot be compiled here) on all host cores, on the same workload
+    as the GPU arm: the same RMAT-22 graph (built by the oracle's copy of the
+    generator, so this process loads nothing of sygraph_b200) and the same 64
+    sources per step."""
     if rank != 0:
         return
-    import sygraph_b200 as sg  # graph generator only (host code)
     import oracle
-    g, _ = make_graph(sg)
-    srcs = sg.io.sample_sources(g, N_SOURCES, seed=SOURCE_SEED)
+    t0 = time.time()
+    g = oracle.rmat(SCALE, EDGE_FACTOR, A, B, C, seed=GRAPH_SEED, weight_seed=WEIGHT_SEED, perm_seed=0, value_type=1)
+    gen_s = time.time() - t0
+    srcs = oracle.sample_sources(g, N_SOURCES, seed=SOURCE_SEED)
     cores = os.cpu_count() or 1
-    per_step = 2  # bounded sample: two traversals per step
-    k = 0
+    reached = {}
 
     def step():
-        nonlocal k
         edges = 0
         t = time.perf_counter()
-        for _ in range(per_step):
-            s = int(srcs[k % len(srcs)])
-            k += 1
-            d, _, _ = oracle.bfs_frontier(g, s, 2, ALPHA, BETA, nthreads=cores)
-            edges += oracle.visited_edges(g, d, g.n + 1)
+        for s in srcs:
+            d, _, _ = oracle.bfs_frontier(g, int(s), 2, ALPHA, BETA, nthreads=cores)
+            reached[int(s)] = oracle.visited_edges(g, d, g.n + 1)
+            edges += reached[int(s)]
         return edges, time.perf_counter() - t
 
     for _ in range(args.warmup):
@@ -187,14 +197,14 @@ def run_reference(args, world, rank):
     line = {"metric": METRIC, "value": val, "unit": "GTEPS", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_t / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "uint32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"DO-BFS RMAT-{SCALE} ef{EDGE_FACTOR}, {per_step} sources per step",
-                       "n": g.n, "m": g.m, "alpha": ALPHA, "beta": BETA},
+            "impl": "reference", "config": bench_config(g.n, g.m),
+            "graph": {"generate_s": round(gen_s, 2), "generator": "oracle.rmat (the product generator restated)"},
             "cpu_baseline": {"value": val, "unit": "GTEPS", "cores": cores, "kind": "port",
-                             "sample": f"{per_step} hybrid BFS traversals per step on RMAT-{SCALE}"},
+                             "sample": f"the whole workload: {N_SOURCES} hybrid BFS traversals per step on "
+                                       f"RMAT-{SCALE}, OpenMP oracle with {cores} threads"},
             "e2e": {"value": val, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference is SYCL and cannot be compiled here; the oracle's OpenMP restatement "
-                    "of its BFS::run is timed instead"}
+            "note": "the reference is SYCL and cannot be compiled here (no SYCL compiler); the oracle's OpenMP "
+                    "restatement of its BFS::run (algorithms/bfs.hpp:153-350) is timed instead"}
     print(json.dumps(line), flush=True)
 
 
@@ -234,20 +244,46 @@ def _launch_ms(torch, fn) -> float:
     return a.elapsed_time(b)
 
 
-def cpu_baseline(g, srcs, sg):
+def cpu_baseline(g, srcs):
+    """The oracle's OpenMP frontier BFS on the host cores over a bounded
+    sample of the bench's sources (about 15 s); returns the baseline object
+    and the oracle's depths per source (the bench's parity check)."""
     import oracle
     cores = os.cpu_count() or 1
     edges, t0 = 0, time.perf_counter()
-    used = 0
+    depths = {}
     for s in srcs:
         d, _, _ = oracle.bfs_frontier(g, int(s), 2, ALPHA, BETA, nthreads=cores)
         edges += oracle.visited_edges(g, d, g.n + 1)
-        used += 1
+        depths[int(s)] = d
         if time.perf_counter() - t0 > 15.0:
             break
     dt = time.perf_counter() - t0
     return {"value": edges / dt / 1e9, "unit": "GTEPS", "cores": cores, "kind": "port",
-            "sample": f"{used} hybrid BFS traversals (alpha 15, beta 24) on RMAT-{SCALE}, OpenMP oracle"}
+            "sample": f"{len(depths)} hybrid BFS traversals (alpha 15, beta 24) on RMAT-{SCALE}, OpenMP oracle"}, depths
+
+
+PARITY_SOURCES = 8
+
+
+def bench_parity(sg, g, bfs, srcs, ref_depths, mb_rows, sssp_first) -> dict:
+    """The GPU results of this run against the oracle on the bench's own graph
+    and sources: the single-source depths and the batched launch's rows for
+    every source the CPU baseline traversed, and the first source's SSSP
+    distances (delta-stepping, fp32 bits) against Dijkstra."""
+    import oracle
+    bfs_ok = True
+    for s, want in ref_depths.items():
+        bfs.init(s)
+        bfs.run(2, ALPHA, BETA)
+        bfs_ok &= bool(np.array_equal(bfs.getDistances(), want))
+    rows_ok = all(bool(np.array_equal(mb_rows[i], ref_depths[int(s)]))
+                  for i, s in enumerate(srcs[:len(mb_rows)]) if int(s) in ref_depths)
+    dref = oracle.sssp_dijkstra(g, int(srcs[0]))
+    sssp_ok = bool(np.array_equal(sssp_first.view(np.uint32), dref.view(np.uint32)))
+    return {"ok": bool(bfs_ok and rows_ok and sssp_ok), "bfs_sources": len(ref_depths), "bfs_depths_equal": bfs_ok,
+            "batched_rows_equal": rows_ok, "sssp_sources": 1, "sssp_bits_equal": sssp_ok,
+            "oracle": "oracle.bfs_frontier (alpha 15, beta 24) and oracle.sssp_dijkstra"}
 
 
 def profile_case(kind: str) -> None:
@@ -386,7 +422,7 @@ def main():
     ap.add_argument("--impl", default="sygraph_b200", choices=["sygraph_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sub-benchmark")
-    ap.add_argument("--sssp-sources", type=int, default=8)
+    ap.add_argument("--sssp-sources", type=int, default=64)
     ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs", "bc", "tc", "cc"], default=None,
                     help="profiling case: build the graph, run 2 traversals of one kind and exit (few launches)")
     args = ap.parse_args()
@@ -578,6 +614,7 @@ def main():
         b.synchronize()
         mb_ms.append(a.elapsed_time(b))
     mb_det = mbfs.run(srcs, 2, MS_ALPHA, MS_BETA)
+    mb_rows = mbfs.getDistances()[:PARITY_SOURCES].copy()  # checked against the oracle below
     batched_ms = float(np.median(mb_ms))
     batched_gteps = mb_det["reached_edges"] / (batched_ms * 1e-3) / 1e9
     ms_bytes = 4 * (n + 1) + 4 * m + 4 * n * len(srcs)
@@ -601,7 +638,9 @@ def main():
                "workload": f"Brandes BC, {BC_SOURCES} sources, RMAT-{BC_SCALE} ef{EDGE_FACTOR}",
                "launch_ms": bc_ms, "per_source_ms": bc1_ms, "speedup_vs_per_source": bc1_ms / bc_ms,
                "max_rel_diff_vs_per_source": bc_rel, "forward_levels": bc_det["iterations"]}
-    bc_bytes = 2 * (4 * (gbc.n + 1) + 4 * gbc.m) + 2 * 256 * gbc.n
+    # forward and backward sweeps each read the CSR once; per vertex and
+    # source, sigma and delta are written once and read once (4 bytes each)
+    bc_bytes = 2 * (4 * (gbc.n + 1) + 4 * gbc.m) + 16 * gbc.n * BC_SOURCES
     bc_line["roofline"] = {"bound": "hbm", "achieved": bc_bytes / (bc_ms * 1e-3) / 1e9, "unit": "GB/s",
                            "frac": bc_bytes / (bc_ms * 1e-3) / 1e9 / peaks()[0],
                            "bytes_per_launch": bc_bytes, "traffic": ncu_traffic("bc_batch_kernel")}
@@ -677,10 +716,13 @@ def main():
     sssp.set_pull(SSSP_PULL)
     sssp.set_delta(SSSP_DELTA)
     nf_ms, nf_same = 0.0, True
+    d_first = None
     for s in srcs[:k_ss]:
         sssp.init(int(s))
         sssp.run_async()
         d_nf = sssp.getDistances()
+        if d_first is None:
+            d_first = d_nf
         sssp.set_delta(0.0)
         sssp.init(int(s))
         sssp.run()
@@ -693,17 +735,16 @@ def main():
     serve = None if (args.no_serving or world > 1) else serving_bench(sg, torch)
 
     if rank == 0:
-        base = None if (args.no_cpu_baseline or world > 1) else cpu_baseline(g, srcs[:8], sg)
+        base, parity = None, None
+        if not (args.no_cpu_baseline or world > 1):
+            base, ref_depths = cpu_baseline(g, srcs[:PARITY_SOURCES])
+            parity = bench_parity(sg, g, bfs, srcs, ref_depths, mb_rows, d_first)
         line = {
             "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "uint32", "data": "synthetic",
-            "config": {"workload": f"DO-BFS (hybrid, alpha {ALPHA:g}, beta {BETA:g}) from {N_SOURCES} random "
-                                   f"sources per GPU, RMAT-{SCALE} ef{EDGE_FACTOR} (0.57,0.19,0.19,0.05) seed 1",
-                       "n": n, "m": m, "sources_per_step": N_SOURCES, "source_seed": SOURCE_SEED,
-                       "graph_bytes": G.memory_bytes(), "l2": "inputs larger than L2 (CSR %.2f GB > 126 MB)"
-                                                             % ((4 * (n + 1) + 8 * m) / 1e9),
-                       "generate_s": round(gen_s, 2)},
+            "config": bench_config(n, m),
+            "graph": {"generate_s": round(gen_s, 2), "device_bytes": G.memory_bytes()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "bfs_kernel", "bytes_per_launch": algo_bytes, "launch_ms": kern_ms},
@@ -712,6 +753,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": base,
+            "parity": parity,
             "batched": {"value": batched_gteps, "unit": "GTEPS", "sources_per_launch": len(srcs),
                         "launch_ms": batched_ms, "speedup_vs_single_source": batched_gteps / value,
                         "reached_edges": mb_det["reached_edges"], "reached_edges_single": step_edges,

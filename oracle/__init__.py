@@ -49,6 +49,11 @@ def _load() -> C.CDLL:
         "or_tc_dag": (C.c_uint64, [C.c_uint32, u32p, u32p, u64p, C.c_int]),
         "or_bfs_multi": (None, [C.c_uint32, u32p, u32p, u32p, C.c_uint32, u32p, C.c_int]),
         "or_visited_edges": (C.c_uint64, [C.c_uint32, u32p, u32p, C.c_uint32]),
+        "or_rmat_generate": (C.c_int64, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                         C.c_uint64, C.c_uint64, C.c_int, C.POINTER(u32p), C.POINTER(u32p),
+                                         C.POINTER(u32p)]),
+        "or_sample_sources": (C.c_int, [C.c_uint32, u32p, C.c_uint32, C.c_uint64, u32p]),
+        "or_free": (None, [C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -166,3 +171,57 @@ def visited_edges(csr, depth, unreached: int) -> int:
     n, ro, _ = _csr(csr)
     d = np.ascontiguousarray(depth, np.uint32)
     return int(_lib.or_visited_edges(n, _p(ro), _p(d), unreached))
+
+
+class Csr:
+    """A host CSR of the oracle's own (uint32 offsets and columns, uint32 or
+    float32 values), so that the CPU baseline needs nothing of the product."""
+
+    def __init__(self, row_offsets, column_indices, values=None):
+        self.row_offsets = row_offsets
+        self.column_indices = column_indices
+        self.values = values
+
+    @property
+    def n(self) -> int:
+        return int(self.row_offsets.size - 1)
+
+    @property
+    def m(self) -> int:
+        return int(self.column_indices.size)
+
+
+def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 1,
+         weight_seed: int = 2, perm_seed: int = 0, value_type: int = 1) -> Csr:
+    """The benchmarks' seeded RMAT graph (value_type 0 none, 1 float32 on
+    (0,1], 2 uint32 on [1,64]); the same CSR as sygraph_b200.io.rmat."""
+    u32p = C.POINTER(C.c_uint32)
+    ro, col, val = u32p(), u32p(), u32p()
+    m = _lib.or_rmat_generate(scale, edge_factor, a, b, c, seed, weight_seed, perm_seed, value_type, C.byref(ro),
+                              C.byref(col), C.byref(val))
+    if m < 0:
+        raise ValueError("or_rmat_generate failed")
+    n = 1 << scale
+    try:
+        out_ro = np.ctypeslib.as_array(ro, shape=(n + 1,)).copy()
+        out_col = np.ctypeslib.as_array(col, shape=(max(m, 1),))[:m].copy()
+        out_val = None
+        if value_type:
+            out_val = np.ctypeslib.as_array(val, shape=(max(m, 1),))[:m].copy()
+            if value_type == 1:
+                out_val = out_val.view(np.float32)
+    finally:
+        for p in (ro, col, val):
+            if p:
+                _lib.or_free(C.cast(p, C.c_void_p))
+    return Csr(out_ro, out_col, out_val)
+
+
+def sample_sources(csr, k: int, seed: int = 3) -> np.ndarray:
+    """k distinct vertices with degree > 0 (the benchmarks' source draw; the
+    same vertices as sygraph_b200.io.sample_sources)."""
+    n, ro, _ = _csr(csr)
+    out = np.zeros(k, np.uint32)
+    if _lib.or_sample_sources(n, _p(ro), k, seed, _p(out)) != 0:
+        raise ValueError("fewer vertices with edges than requested sources")
+    return out

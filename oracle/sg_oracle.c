@@ -487,3 +487,200 @@ uint64_t or_visited_edges(uint32_t n, const uint32_t* ro, const uint32_t* depth,
     if (depth[v] != unreached) s += ro[v + 1] - ro[v];
   return s;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Benchmark inputs without the product library                              */
+/* ------------------------------------------------------------------------- */
+
+/* The seeded RMAT graph of the benchmarks, restated so the CPU baseline arm
+ * builds its input without loading the product library: the same draws, so
+ * the same CSR bit for bit (tested against sg_rmat_generate).  Every random
+ * number is the splitmix64 finaliser (Steele, Lea, Flood 2014) of a counter:
+ *   hash2(seed, i) = mix64(mix64(seed) ^ i).
+ * Pair i draws its quadrant at level l (most significant bit first) from the
+ * high 32 bits of mix64(hash2(seed, i) + l) at even l and the low 32 bits of
+ * the same word at the odd l after it, as a fraction of 2^32 against the
+ * cumulative probabilities a, a+b, a+b+c: quadrant 0 keeps both bits, 1 sets
+ * the column bit, 2 the row bit, 3 both.  Ids are relabelled by a
+ * Fisher-Yates shuffle (i from n-1 down to 1 swaps perm[i] with
+ * perm[hash2(perm_seed, i) % (i+1)]; perm_seed 0 = identity).  Self-loops are
+ * dropped, both directions kept, duplicates removed, rows sorted.  The weight
+ * of the unordered pair {lo, hi} is h = hash2(weight_seed, lo << 32 | hi):
+ * float32 ((h >> 40) + 1) * 2^-24 on (0, 1], or uint32 (h >> 58) + 1 on
+ * [1, 64]. */
+static inline uint64_t or_mix64(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+static inline uint64_t or_hash2(uint64_t seed, uint64_t i) { return or_mix64(or_mix64(seed) ^ i); }
+
+static uint32_t or_pair_weight_bits(uint64_t seed, uint32_t u, uint32_t v, int value_type) {
+  const uint32_t lo = u < v ? u : v, hi = u < v ? v : u;
+  const uint64_t h = or_hash2(seed, ((uint64_t)lo << 32) | hi);
+  if (value_type == 1) {
+    float w = (float)((h >> 40) + 1) * (1.0f / 16777216.0f);
+    uint32_t bits;
+    memcpy(&bits, &w, 4);
+    return bits;
+  }
+  return (uint32_t)(h >> 58) + 1u;
+}
+
+/* LSD radix sort of n keys on their low key_bits bits, 11-bit digits, each
+ * thread counting and scattering its own contiguous range (stable). */
+static int or_radix_sort(uint64_t* keys, size_t n, int key_bits) {
+  if (n < 2) return 0;
+  uint64_t* tmp = (uint64_t*)malloc(sizeof(uint64_t) * n);
+  if (!tmp) return -1;
+  const int digit = 11, nb = 1 << 11;
+  const int nt = omp_get_max_threads();
+  size_t* hist = (size_t*)malloc(sizeof(size_t) * (size_t)nt * nb);
+  if (!hist) {
+    free(tmp);
+    return -1;
+  }
+  uint64_t *src = keys, *dst = tmp;
+  int passes = 0;
+  for (int shift = 0; shift < key_bits; shift += digit, passes++) {
+    memset(hist, 0, sizeof(size_t) * (size_t)nt * nb);
+#pragma omp parallel num_threads(nt)
+    {
+      const int t = omp_get_thread_num();
+      const size_t lo = n * t / nt, hi = n * (t + 1) / nt;
+      size_t* h = hist + (size_t)t * nb;
+      for (size_t i = lo; i < hi; i++) h[(src[i] >> shift) & (nb - 1)]++;
+#pragma omp barrier
+#pragma omp single
+      {
+        size_t sum = 0;
+        for (int b = 0; b < nb; b++)
+          for (int tt = 0; tt < nt; tt++) {
+            const size_t c = hist[(size_t)tt * nb + b];
+            hist[(size_t)tt * nb + b] = sum;
+            sum += c;
+          }
+      }
+      for (size_t i = lo; i < hi; i++) dst[h[(src[i] >> shift) & (nb - 1)]++] = src[i];
+    }
+    uint64_t* sw = src;
+    src = dst;
+    dst = sw;
+  }
+  if (passes & 1) memcpy(keys, src, sizeof(uint64_t) * n);
+  free(tmp);
+  free(hist);
+  return 0;
+}
+
+/* Returns m, or -1 on failure; *ro (n+1), *col (m) and *val (m, or NULL for
+ * value_type 0) are malloc'd and released with or_free. */
+int64_t or_rmat_generate(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
+                         uint64_t weight_seed, uint64_t perm_seed, int value_type, uint32_t** ro_out,
+                         uint32_t** col_out, uint32_t** val_out) {
+  if (scale < 1 || scale > 30) return -1;
+  const uint32_t n = 1u << scale;
+  const uint64_t pairs = (uint64_t)edge_factor * n;
+  const double ab = a + b, abc = a + b + c;
+  uint32_t* perm = (uint32_t*)malloc(sizeof(uint32_t) * n);
+  uint64_t* keys = (uint64_t*)malloc(sizeof(uint64_t) * 2 * (pairs ? pairs : 1));
+  if (!perm || !keys) {
+    free(perm);
+    free(keys);
+    return -1;
+  }
+  for (uint32_t i = 0; i < n; i++) perm[i] = i;
+  if (perm_seed)
+    for (uint32_t i = n - 1; i > 0; i--) {
+      const uint32_t j = (uint32_t)(or_hash2(perm_seed, i) % ((uint64_t)i + 1));
+      const uint32_t t = perm[i];
+      perm[i] = perm[j];
+      perm[j] = t;
+    }
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)pairs; i++) {
+    const uint64_t st = or_hash2(seed, (uint64_t)i);
+    uint32_t u = 0, v = 0;
+    uint64_t r = 0;
+    for (uint32_t l = 0; l < scale; l++) {
+      if ((l & 1) == 0) r = or_mix64(st + l);
+      const double x = (double)((l & 1) ? (r & 0xffffffffu) : (r >> 32)) * (1.0 / 4294967296.0);
+      const uint32_t bit = 1u << (scale - 1 - l);
+      if (x < a) {
+      } else if (x < ab) {
+        v |= bit;
+      } else if (x < abc) {
+        u |= bit;
+      } else {
+        u |= bit;
+        v |= bit;
+      }
+    }
+    u = perm[u];
+    v = perm[v];
+    if (u == v) {
+      keys[2 * i] = keys[2 * i + 1] = ~0ull;
+    } else {
+      keys[2 * i] = ((uint64_t)u << scale) | v;
+      keys[2 * i + 1] = ((uint64_t)v << scale) | u;
+    }
+  }
+  free(perm);
+  size_t k = 0;
+  for (size_t i = 0; i < 2 * pairs; i++)
+    if (keys[i] != ~0ull) keys[k++] = keys[i];
+  if (or_radix_sort(keys, k, 2 * (int)scale) != 0) {
+    free(keys);
+    return -1;
+  }
+  size_t m = 0;
+  for (size_t i = 0; i < k; i++)
+    if (m == 0 || keys[i] != keys[m - 1]) keys[m++] = keys[i];
+  uint32_t* ro = (uint32_t*)calloc((size_t)n + 1, sizeof(uint32_t));
+  uint32_t* col = (uint32_t*)malloc(sizeof(uint32_t) * (m ? m : 1));
+  uint32_t* val = value_type ? (uint32_t*)malloc(sizeof(uint32_t) * (m ? m : 1)) : NULL;
+  if (!ro || !col || (value_type && !val)) {
+    free(keys);
+    free(ro);
+    free(col);
+    free(val);
+    return -1;
+  }
+  const uint64_t low = (1ull << scale) - 1;
+  for (size_t i = 0; i < m; i++) ro[(keys[i] >> scale) + 1]++;
+  for (uint32_t v = 0; v < n; v++) ro[v + 1] += ro[v];
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < (int64_t)m; i++) {
+    const uint32_t s = (uint32_t)(keys[i] >> scale), d = (uint32_t)(keys[i] & low);
+    col[i] = d;
+    if (val) val[i] = or_pair_weight_bits(weight_seed, s, d, value_type);
+  }
+  free(keys);
+  *ro_out = ro;
+  *col_out = col;
+  *val_out = val;
+  return (int64_t)m;
+}
+
+/* k distinct vertices with degree > 0: candidate i is hash2(seed, i) % n,
+ * skipped when taken or isolated (the benchmarks' source draw).  Returns 0,
+ * or -1 when fewer than k vertices have edges. */
+int or_sample_sources(uint32_t n, const uint32_t* ro, uint32_t k, uint64_t seed, uint32_t* out) {
+  uint64_t nonzero = 0;
+  for (uint32_t v = 0; v < n; v++) nonzero += ro[v + 1] > ro[v];
+  if (nonzero < k) return -1;
+  uint8_t* taken = (uint8_t*)calloc(n ? n : 1, 1);
+  if (!taken) return -1;
+  uint32_t got = 0;
+  for (uint64_t i = 0; got < k; i++) {
+    const uint32_t v = (uint32_t)(or_hash2(seed, i) % n);
+    if (taken[v] || ro[v + 1] == ro[v]) continue;
+    taken[v] = 1;
+    out[got++] = v;
+  }
+  free(taken);
+  return 0;
+}
+
+void or_free(void* p) { free(p); }

@@ -1,6 +1,7 @@
 """The CPU reference arm of bench.py keeps the bench's JSON contract: one
 line with the headline metric, impl "reference", a cpu_baseline describing
-the run and an e2e object without host-device copies."""
+the run and an e2e object without host-device copies.  It runs the GPU arm's
+workload (same config object) and loads nothing of sygraph_b200."""
 import json
 import subprocess
 import sys
@@ -9,12 +10,21 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parents[1]
 
 
+RUNNER = """
+import runpy, sys
+sys.argv = ["bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1"]
+runpy.run_path("bench.py", run_name="__main__")
+maps = open("/proc/self/maps").read()
+print("LOADED_PRODUCT", "libsygraph_b200" in maps or "sygraph_b200" in sys.modules)
+"""
+
+
 def test_reference_arm_json_line():
-    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "1"],
-                       cwd=ROOT, capture_output=True, text=True, timeout=600)
+    r = subprocess.run([sys.executable, "-c", RUNNER], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.strip().startswith("{")]
     assert len(lines) == 1
+    assert "LOADED_PRODUCT False" in r.stdout
     d = json.loads(lines[0])
     assert d["impl"] == "reference"
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
@@ -27,3 +37,7 @@ def test_reference_arm_json_line():
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert d["config"] == bench.bench_config(1 << bench.SCALE, d["config"]["m"])
+    assert d["config"]["sources_per_step"] == 64 and d["config"]["m"] == 128301086

@@ -122,3 +122,21 @@ def test_bc_matches_networkx_style_definition(rmat, oracle):
                 if dist[s, v] + dist[v, t] == dist[s, t]:
                     expect[v] += sigma[s, v] * sigma[v, t] / sigma[s, t]
     np.testing.assert_allclose(oracle.bc(g, srcs), expect, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("scale,kw", [(10, {}), (12, {"perm_seed": 7}), (14, {"seed": 5, "weight_seed": 9}),
+                                      (11, {"value_type": 2}), (9, {"value_type": 0, "a": 0.45, "b": 0.25,
+                                                                     "c": 0.15})])
+def test_oracle_rmat_equals_the_product_generator(sg, oracle, scale, kw):
+    """The CPU baseline arm builds its graph with the oracle's generator, so
+    that it loads nothing of the product: the two generators agree bit for bit."""
+    o = oracle.rmat(scale, **kw)
+    vt = kw.get("value_type", 1)
+    p = sg.io.rmat(scale, **{**kw, "value_type": vt})
+    assert np.array_equal(o.row_offsets, p.row_offsets)
+    assert np.array_equal(o.column_indices, p.column_indices)
+    if vt:
+        assert np.array_equal(o.values.view(np.uint32), p.values.view(np.uint32))
+    else:
+        assert o.values is None
+    assert np.array_equal(oracle.sample_sources(o, 64, seed=3), sg.io.sample_sources(p, 64, seed=3))
