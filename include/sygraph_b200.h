@@ -187,6 +187,14 @@ sg_status sg_graph_copy_csr(sg_graph g, int inverse, uint32_t* host_row_offsets,
 /* GraphCSRDevice::getDegree (graph_csr.hpp:64), host query. */
 sg_status sg_graph_degree(sg_graph g, uint32_t v, uint32_t* degree);
 sg_status sg_graph_memory_bytes(sg_graph g, uint64_t* bytes);
+/* The rows of the forward CSR sorted by weight (equal weights keep their
+ * column order), the adjacency delta-stepping SSSP reads; built on the
+ * device on first use and kept with the graph.  *symmetric = 1 when every
+ * row is strictly increasing in column and every edge's reverse carries the
+ * same weight (the pull phases of delta-stepping need it).  Output arrays are
+ * host arrays of m entries (either may be NULL).  No counterpart in the
+ * reference, which has no delta-stepping. */
+sg_status sg_graph_weight_sorted(sg_graph g, uint32_t* host_column_indices, void* host_values, int* symmetric);
 
 /* ------------------------------------------------------------- frontier -- */
 typedef struct sg_frontier_s* sg_frontier;
@@ -442,14 +450,22 @@ sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed);
  * list (the parents of late-level vertices tend to have high ids).  Any
  * parent gives the same depth; only the work changes. */
 sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels);
-/* Bitmap words a warp takes per step of a short-circuit pull (2 or 4, the
- * default): more words put more first-neighbour probes in flight. */
+/* Form of the short-circuit pull: 0 (the default) ranks the unvisited
+ * vertices of 32 of a warp's bitmap words across its lanes, four candidates
+ * per lane in flight; 2 or 4 take that many words per warp step, one lane per
+ * vertex of a word.  Every form gives the same depths. */
 sg_status sg_bfs_set_pull_words(sg_bfs b, uint32_t words);
 sg_status sg_bfs_set_selector_margin(sg_bfs b, float margin);
 /* Learned mode: a frontier smaller than fraction * n keeps the heuristic's
  * choice without an inference (when that choice is allowed).  Default 1e-3;
  * 0 asks the MLP on every level. */
 sg_status sg_bfs_set_selector_min_frontier(sg_bfs b, float fraction);
+/* Learned mode: the MLP is consulted only on graphs whose mean-degree feature
+ * log2(1 + m/n) / 8 lies in [lo, hi]; on other graphs the launch carries no
+ * MLP (no parameter staging, no inference) and the heuristic decides every
+ * level.  The model file stores the range of the training graphs on which
+ * the model overruled the heuristic.  Default: every graph. */
+sg_status sg_bfs_set_selector_graph_range(sg_bfs b, float lo, float hi);
 sg_status sg_bfs_log_features(sg_bfs b, int enable);
 sg_status sg_bfs_level_features(sg_bfs b, float* host_features, uint32_t cap_levels, uint32_t* count);
 

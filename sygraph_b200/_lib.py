@@ -127,6 +127,7 @@ SIGNATURES = {
     "sg_graph_copy_csr": (st, [vp, C.c_int, u32p, u32p, vp]),
     "sg_graph_degree": (st, [vp, C.c_uint32, u32p]),
     "sg_graph_memory_bytes": (st, [vp, u64p]),
+    "sg_graph_weight_sorted": (st, [vp, u32p, vp, C.POINTER(C.c_int)]),
     # frontier
     "sg_frontier_create": (st, [C.c_uint32, vp, C.POINTER(vp)]),
     "sg_frontier_destroy": (st, [vp]),
@@ -171,6 +172,7 @@ SIGNATURES = {
     "sg_bfs_set_selector_margin": (st, [vp, C.c_float]),
     "sg_bfs_set_pull_order": (st, [vp, C.c_uint64]),
     "sg_bfs_set_pull_words": (st, [vp, C.c_uint32]),
+    "sg_bfs_set_selector_graph_range": (st, [vp, C.c_float, C.c_float]),
     "sg_bfs_log_features": (st, [vp, C.c_int]),
     "sg_bfs_level_features": (st, [vp, f32p, C.c_uint32, u32p]),
     "sg_mlp_param_count": (C.c_uint32, []),

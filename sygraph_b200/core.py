@@ -220,6 +220,16 @@ class Graph:
         call("sg_graph_memory_bytes", self.handle, C.byref(b))
         return b.value
 
+    def weight_sorted(self):
+        """(columns, values, symmetric): the forward rows sorted by weight, as
+        delta-stepping SSSP reads them (sg_graph_weight_sorted)."""
+        m = self.getEdgeCount()
+        col = np.empty(m, np.uint32)
+        val = np.empty(m, _NP_OF_WT[self.value_type])
+        sym = C.c_int()
+        call("sg_graph_weight_sorted", self.handle, _ptr(col), C.c_void_p(val.ctypes.data), C.byref(sym))
+        return col, val, bool(sym.value)
+
     def __del__(self):
         h = getattr(self, "handle", None)
         if h and lib is not None:  # module globals are gone at interpreter exit

@@ -18,6 +18,7 @@
 //         forced schedule, or the learned selector (bfs_engine.cuh).
 // One grid barrier per level; no host round trip until the traversal ends.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -39,20 +40,12 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
   const uint32_t n = P.n, w0 = P.w0, w1 = P.w1, src = P.source, inf = n + 1;
   const uint32_t deg_src = P.ro[src + 1] - P.ro[src];
 
-  // ---- init: depth = n+1 except the source; F_0 = {source}; vertices that no
-  // edge reaches are pre-marked visited so pull never scans them.
-  if ((reinterpret_cast<uintptr_t>(P.depth) & 15) == 0) {  // 16-byte stores
-    const uint32_t n4 = n / 4;
-    for (uint32_t i = gtid; i < n4; i += nthreads) {
-      const uint32_t b0 = 4 * i;
-      const uint4 v = make_uint4(b0 == src ? 0u : inf, b0 + 1 == src ? 0u : inf, b0 + 2 == src ? 0u : inf,
-                                 b0 + 3 == src ? 0u : inf);
-      st_cg(reinterpret_cast<uint4*>(P.depth) + i, v);
-    }
-    for (uint32_t i = 4 * n4 + gtid; i < n; i += nthreads) st_cg(P.depth + i, i == src ? 0u : inf);
-  } else {
-    for (uint32_t i = gtid; i < n; i += nthreads) st_cg(P.depth + i, i == src ? 0u : inf);
-  }
+  // ---- init: F_0 = {source}; vertices that no edge reaches are pre-marked
+  // visited so pull never scans them.  Depths are write-only in the
+  // traversal: a vertex's depth is stored when it is discovered, and the
+  // unreached ones get n+1 after the last level (the same time as filling all
+  // n depths first on RMAT-22, with less traffic).
+  if (gtid == 0) st_cg(P.depth + src, 0u);
   for (uint32_t i = gtid; i < w0; i += nthreads) {
     const uint32_t b = (i == (src >> 5)) ? (1u << (src & 31)) : 0u;
     st_cg(P.visited + i, P.no_in_edges[i] | b);
@@ -222,6 +215,27 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     P.result[3] = visited_vertices;
     P.result[4] = P.m - unexplored;
   }
+  {
+    // n+1 for every vertex not reached: reached = visited, minus the vertices
+    // pre-marked for having no in-edge, plus the source.  Four vertices per
+    // thread (one 16-byte store when none of them was reached).
+    const bool vec = (reinterpret_cast<uintptr_t>(P.depth) & 15) == 0;
+    const uint32_t nq = (n + 3) / 4;
+    for (uint32_t q = gtid; q < nq; q += nthreads) {
+      const uint32_t wi = q >> 3;
+      uint32_t reached = ld_cg(P.visited + wi) & ~P.no_in_edges[wi];
+      if (wi == (src >> 5)) reached |= 1u << (src & 31);
+      const uint32_t nib = (reached >> ((q & 7) * 4)) & 0xfu;
+      if (nib == 0xfu) continue;
+      const uint32_t v0 = 4 * q;
+      if (vec && nib == 0 && v0 + 3 < n) {
+        st_cg(reinterpret_cast<uint4*>(P.depth) + q, make_uint4(inf, inf, inf, inf));
+        continue;
+      }
+      for (uint32_t k = 0; k < 4 && v0 + k < n; k++)
+        if (!((nib >> k) & 1u)) st_cg(P.depth + v0 + k, inf);
+    }
+  }
   sygraph::detail::grid_exit(P.bar);
 }
 
@@ -273,8 +287,11 @@ struct sg_bfs_s {
   uint32_t allowed = 0x3f;
   float margin = 0.05f;
   float min_frontier = 1e-3f;  // learned mode: frontiers below this fraction of n keep the heuristic
+  // learned mode: the MLP is consulted only on graphs whose mean-degree
+  // feature log2(1 + m/n) / 8 lies in [graph_lo, graph_hi]
+  float graph_lo = -INFINITY, graph_hi = INFINITY;
   unsigned long long pull_reverse = 0;  // levels whose pull probes in-neighbours from the back
-  uint32_t pull_words = 4;              // bitmap words per warp step of a short-circuit pull
+  uint32_t pull_words = bfs::kDefaultPullWords;  // short-circuit pull form (bfs_engine.cuh)
   float* features = nullptr;
   uint32_t last_iterations = 0;
   bool fresh = false;  // initialised but not run: depths not written yet
@@ -325,7 +342,11 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.mode = direction;
   P.alpha = alpha;
   P.beta = beta;
-  P.mlp = b->mlp;
+  // outside the model's graph range the launch runs without the MLP (no
+  // staging, no inference: the heuristic decides every level), as on graphs
+  // where the model never overruled the heuristic in training
+  const float f9 = log2f(1.f + (float)(g->m ? g->m : 1) / (float)g->n) / 8.f;
+  P.mlp = (b->mlp && f9 >= b->graph_lo && f9 <= b->graph_hi) ? b->mlp : nullptr;
   P.allowed = b->allowed;
   P.margin = b->margin;
   P.min_frontier = b->min_frontier;
@@ -503,8 +524,18 @@ sg_status sg_bfs_set_pull_order(sg_bfs b, uint64_t reverse_levels) {
 sg_status sg_bfs_set_pull_words(sg_bfs b, uint32_t words) {
   clear_error();
   SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
-  SG_REQUIRE(words == 2 || words == 4, SG_ERR_INVALID, "2 or 4 words per warp step");
+  SG_REQUIRE(words == 0 || words == 2 || words == 4, SG_ERR_INVALID,
+             "0 (ranked candidates) or 2 or 4 words per warp step");
   b->pull_words = words;
+  return SG_OK;
+}
+
+sg_status sg_bfs_set_selector_graph_range(sg_bfs b, float lo, float hi) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_REQUIRE(!(lo != lo) && !(hi != hi), SG_ERR_INVALID, "graph range bounds must be numbers");
+  b->graph_lo = lo;
+  b->graph_hi = hi;
   return SG_OK;
 }
 
@@ -719,7 +750,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.margin = 0.f;
   P.min_frontier = 0.f;
   P.pull_reverse = 0;
-  P.pull_words = 4;  // the instance default of sg_bfs_create
+  P.pull_words = bfs::kDefaultPullWords;  // the instance default of sg_bfs_create
   P.features = nullptr;
   P.alpha = alpha;
   P.beta = beta;

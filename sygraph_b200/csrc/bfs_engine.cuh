@@ -24,6 +24,9 @@ constexpr unsigned long long kDirectClaimDeg = 1u << 16;  // push frontier degre
 // halves the barrier arrivals but was within 1% on RMAT-22, and whole-SM CTAs
 // cannot share SMs with the half-SM CTAs of concurrent launches (serving).
 constexpr uint32_t kBfsThreads = 512;
+// Short-circuit pull of the engine: 0 = candidates ranked across each warp
+// (pull_ranked); 2 or 4 = the older form, that many bitmap words per warp step.
+constexpr uint32_t kDefaultPullWords = 0;
 
 __device__ __forceinline__ uint32_t bfs_chunks(uint32_t deg) { return (deg + kBfsChunk - 1) / kBfsChunk; }
 
@@ -63,7 +66,7 @@ struct Params {
   float margin;                           // log-time gain the MLP must predict to overrule the heuristic
   float min_frontier;                     // smallest frontier (fraction of n) the MLP is asked about
   unsigned long long pull_reverse;        // bit L: level L's pull probes in-neighbours from the back
-  uint32_t pull_words;                    // bitmap words per warp step of a short-circuit pull (2 or 4)
+  uint32_t pull_words;                    // short-circuit pull: 0 ranked candidates, or 2 / 4 words per warp step
   float* features;                        // optional log: 12 floats per level decision
 };
 
@@ -75,6 +78,7 @@ struct FeatureConst {
 };
 
 struct Shared {
+  uint32_t pull_found[kBfsThreads / 32][32];  // ranked pull: hits per owned word, per warp
   uint32_t scan[32];
   unsigned long long red[32][4];
   unsigned long long acc[2];  // per-level totals of the CTA (new vertices, their degree)

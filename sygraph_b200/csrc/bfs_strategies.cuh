@@ -218,9 +218,12 @@ __device__ __forceinline__ uint32_t* old_frontier(const Level& L) {
 }
 
 // Also clears F_{L-1}: every word is visited once, and the store needs no
-// load of the old summary.
-template <int U>
+// load of the old summary.  PB in-neighbours of each candidate are probed per
+// round (2 and 4 measured no faster than 1 on RMAT-22: after the first probe
+// the columns come from L1).
+template <int U, int PB = 1>
 __device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, bool reverse) {
+  static_assert(kPullProbes % PB == 0, "the probe batch must divide the serial probes");
   const Params& P = *L.P;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -247,19 +250,27 @@ __device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, boo
       e[k] = m ? P.iro[v + 1] : 0u;
       f[k] = false;
     }
-    for (uint32_t j = 0; j < kPullProbes; j++) {
-      uint32_t x[U];
-      bool a[U];
+    for (uint32_t j = 0; j < kPullProbes; j += PB) {
+      uint32_t x[U][PB];
+      bool a[U][PB];
 #pragma unroll
-      for (int k = 0; k < U; k++) {
-        a[k] = !f[k] && b[k] + j < e[k];
-        x[k] = a[k] ? P.icol[probe_pos(b[k], e[k], j, reverse)] : 0u;
-      }
+      for (int k = 0; k < U; k++)
+#pragma unroll
+        for (int q = 0; q < PB; q++) {
+          a[k][q] = !f[k] && b[k] + j + q < e[k];
+          x[k][q] = a[k][q] ? P.icol[probe_pos(b[k], e[k], j + q, reverse)] : 0u;
+        }
+      uint32_t w[U][PB];
+#pragma unroll
+      for (int k = 0; k < U; k++)
+#pragma unroll
+        for (int q = 0; q < PB; q++) w[k][q] = a[k][q] ? fb_cur[x[k][q] >> 5] : 0u;  // as bit_test_ro
       bool more = false;
 #pragma unroll
       for (int k = 0; k < U; k++) {
-        if (a[k]) f[k] = bit_test_ro(fb_cur, x[k]);
-        more |= !f[k] && b[k] + j + 1 < e[k];
+#pragma unroll
+        for (int q = 0; q < PB; q++) f[k] = f[k] || (a[k][q] && ((w[k][q] >> (x[k][q] & 31)) & 1u));
+        more |= !f[k] && b[k] + j + PB < e[k];
       }
       if (!__any_sync(kFullMask, more)) break;
     }
@@ -279,6 +290,120 @@ __device__ __forceinline__ void pull_words(Level& L, const uint32_t* fb_cur, boo
   }
 }
 
+// Short-circuit pull with the candidates ranked across the warp (the
+// default).  A warp owns the bitmap words gwarp + k * nwarps; it loads 32 of
+// them at once (one per lane), ranks their unvisited vertices and hands them
+// to its lanes kRanked at a time, so every lane has kRanked candidates in
+// flight whatever the density of the words: a level whose candidates are
+// sparse costs the warp a few round trips, not one chain of round trips per
+// group of words.  Each candidate probes its first kPullProbes in-neighbours
+// serially (after the first, the columns mostly come from the same sector,
+// in L1); a list still open after that -- no frontier neighbour yet and more
+// in-neighbours left -- is scanned by the whole warp, kPullWin windows of 32
+// edges at a time, until a hit or its end.  (Ranking the open lists' edges
+// across the warp after one or two serial probes measured slower: 0.198
+// against 0.157 ms per RMAT-22 traversal.)  Hits are gathered per word in
+// shared memory and each lane publishes its own word (the owner of a word is
+// its only writer in a pull level).  Also clears F_{L-1}.
+constexpr int kRanked = 4;
+
+__device__ __forceinline__ void pull_ranked(Level& L, const uint32_t* fb_cur, bool reverse) {
+  const Params& P = *L.P;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool same = P.iro == P.ro;
+  uint32_t* found = L.S->pull_found[threadIdx.x >> 5];
+  uint32_t* oldf = old_frontier(L);
+  for (uint64_t k0 = 0; gwarp + k0 * nwarps < P.w0; k0 += 32) {
+    const uint64_t w64 = gwarp + (k0 + lane) * nwarps;
+    const bool wok = w64 < P.w0;
+    const uint32_t w = wok ? (uint32_t)w64 : 0u;
+    const uint32_t vw = wok ? ld_cg(P.visited + w) : 0xffffffffu;
+    if (wok) st_cg(oldf + w, 0u);
+    const uint32_t cand = wok ? (~vw & valid_bits(w, P.w0, P.n)) : 0u;
+    found[lane] = 0u;
+    __syncwarp();
+    const uint32_t incl = warp_inclusive_scan((uint32_t)__popc(cand));
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    const uint32_t excl = incl - (uint32_t)__popc(cand);
+    for (uint32_t r0 = 0; r0 < total; r0 += 32 * kRanked) {
+      uint32_t v[kRanked], b[kRanked], e[kRanked], own[kRanked];
+      bool act[kRanked], f[kRanked];
+#pragma unroll
+      for (int k = 0; k < kRanked; k++) {
+        const uint32_t r = r0 + k * 32 + lane;
+        act[k] = r < total;
+        const uint32_t o = warp_owner_of_rank(incl, act[k] ? r : total - 1);
+        const uint32_t ob = __shfl_sync(kFullMask, cand, o);
+        const uint32_t oe = __shfl_sync(kFullMask, excl, o);
+        const uint32_t ow = __shfl_sync(kFullMask, w, o);
+        own[k] = o;
+        v[k] = ow * 32 + select_bit(ob, act[k] ? r - oe : 0u);
+      }
+#pragma unroll
+      for (int k = 0; k < kRanked; k++) {
+        b[k] = act[k] ? P.iro[v[k]] : 0u;
+        e[k] = act[k] ? P.iro[v[k] + 1] : 0u;
+        f[k] = false;
+      }
+      for (uint32_t j = 0; j < kPullProbes; j++) {
+        uint32_t x[kRanked], fw[kRanked];
+        bool a[kRanked];
+#pragma unroll
+        for (int k = 0; k < kRanked; k++) {
+          a[k] = !f[k] && b[k] + j < e[k];
+          x[k] = a[k] ? P.icol[probe_pos(b[k], e[k], j, reverse)] : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < kRanked; k++) fw[k] = a[k] ? fb_cur[x[k] >> 5] : 0u;  // as bit_test_ro
+        bool more = false;
+#pragma unroll
+        for (int k = 0; k < kRanked; k++) {
+          f[k] = f[k] || (a[k] && ((fw[k] >> (x[k] & 31)) & 1u));
+          more |= !f[k] && b[k] + j + 1 < e[k];
+        }
+        if (!__any_sync(kFullMask, more)) break;
+      }
+      // lists still open after the serial probes: the whole warp, one at a time
+#pragma unroll
+      for (int k = 0; k < kRanked; k++) {
+        for (uint32_t om = __ballot_sync(kFullMask, act[k] && !f[k] && e[k] - b[k] > kPullProbes); om;
+             om &= om - 1) {
+          const uint32_t o = __ffs(om) - 1;
+          const uint32_t ob = __shfl_sync(kFullMask, b[k], o), oe = __shfl_sync(kFullMask, e[k], o);
+          bool hit = false;
+          for (uint32_t x0 = ob + kPullProbes; x0 < oe && !hit; x0 += 32 * kPullWin) {
+            uint32_t cc[kPullWin];
+            bool ca[kPullWin];
+#pragma unroll
+            for (int q = 0; q < kPullWin; q++) {
+              const uint32_t x = x0 + q * 32 + lane;
+              ca[q] = x < oe;
+              cc[q] = ca[q] ? P.icol[probe_pos(ob, oe, x - ob, reverse)] : 0u;
+            }
+            bool h = false;
+#pragma unroll
+            for (int q = 0; q < kPullWin; q++) h |= ca[q] && bit_test_ro(fb_cur, cc[q]);
+            hit = __any_sync(kFullMask, h);
+          }
+          if (lane == o) f[k] = hit;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kRanked; k++)
+        if (act[k] && f[k]) {
+          atomicOr(found + own[k], 1u << (v[k] & 31));
+          L.discovered(v[k], same ? e[k] - b[k] : (P.ro[v[k] + 1] - P.ro[v[k]]));
+        }
+    }
+    __syncwarp();
+    const uint32_t fm = found[lane];
+    __syncwarp();  // found[] is cleared again by the next chunk
+    if (fm) L.publish_word(w, vw, fm);
+  }
+}
+
 __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool short_circuit, bool reverse) {
   const Params& P = *L.P;
   const uint32_t lane = threadIdx.x & 31;
@@ -288,8 +413,10 @@ __device__ __forceinline__ void pull_warp(Level& L, const uint32_t* fb_cur, bool
   if (short_circuit) {
     if (P.pull_words == 4)
       pull_words<4>(L, fb_cur, reverse);
-    else
+    else if (P.pull_words == 2)
       pull_words<2>(L, fb_cur, reverse);
+    else
+      pull_ranked(L, fb_cur, reverse);
     return;
   }
   // pull_all: every in-neighbour of every unvisited vertex is scanned

@@ -22,6 +22,7 @@
 // the first of equal keys).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "engine_common.cuh"
@@ -87,50 +88,28 @@ __device__ __forceinline__ uint32_t block_suffix_min(uint32_t x, Shared& S) {
   return min(x, later);
 }
 
-__global__ void __launch_bounds__(kThreads, 2) build_kernel(BuildParams P) {
-  __shared__ Shared S;
+// LSD radix sort of (key, value) pairs, `passes` digits of 8 bits from bit
+// `shift0` up.  CTA c owns [lo, hi) of the array in every pass: it counts its
+// digits, and after a grid barrier scatters its range in order, one thread
+// per entry and blockDim entries per round, equal digits ranked by warp match
+// groups -- a stable sort.  On return kin / vin hold the sorted pairs (the
+// pointers are swapped after every pass).  False when a barrier wait ran out.
+__device__ __forceinline__ bool radix_sort_pairs(Shared& S, GridBarrier* bar, uint32_t* ghist, u64*& kin,
+                                                 u64*& kout, uint32_t*& vin, uint32_t*& vout, uint64_t lo,
+                                                 uint64_t hi, uint32_t shift0, uint32_t passes) {
   const uint32_t G = gridDim.x, c = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const uint64_t nth = (uint64_t)G * blockDim.x;
-  const uint64_t gtid = (uint64_t)c * blockDim.x + t;
-  const uint64_t E = P.entries;
-  const uint64_t per = (E + G - 1) / G;
-  const uint64_t lo = min(E, (uint64_t)c * per), hi = min(E, lo + per);
-  const uint32_t bmask = (1u << P.b) - 1u;
-
-  // ---- fill
-  for (uint64_t i = gtid; i < E; i += nth) {
-    const uint64_t j = P.symmetrize ? i >> 1 : i;
-    const bool rev = P.symmetrize && (i & 1);
-    const uint32_t u = P.src[j], v = P.dst[j];
-    bool drop = (P.drop_self_loops && u == v) || (rev && u == v);
-    if (u >= P.n || v >= P.n) {
-      atomicOr(P.bad, 1u);
-      drop = true;
-    }
-    const uint32_t a = rev ? v : u, z = rev ? u : v;
-    P.k0[i] = drop ? kNone : (((u64)a << P.b) | z);
-    P.v0[i] = P.val ? P.val[j] : P.one;
-  }
-  for (uint64_t v = gtid; v <= P.n; v += nth) P.ro[v] = 0xffffffffu;
-  if (!grid_sync(P.bar)) return;
-
-  // ---- sort
-  u64* kin = P.k0;
-  u64* kout = P.k1;
-  uint32_t* vin = P.v0;
-  uint32_t* vout = P.v1;
-  for (uint32_t p = 0; p < P.passes; p++) {
-    const uint32_t sh = 8 * p;
+  for (uint32_t p = 0; p < passes; p++) {
+    const uint32_t sh = shift0 + 8 * p;
     if (t < 256) S.hist[t] = 0;
     __syncthreads();
     for (uint64_t i = lo + t; i < hi; i += blockDim.x) atomicAdd(&S.hist[(uint32_t)(kin[i] >> sh) & 255u], 1u);
     __syncthreads();
-    if (t < 256) P.hist[(size_t)t * G + c] = S.hist[t];
-    if (!grid_sync(P.bar)) return;
+    if (t < 256) ghist[(size_t)t * G + c] = S.hist[t];
+    if (!grid_sync(bar)) return false;
     uint32_t tot = 0, before = 0;
     if (t < 256) {
       for (uint32_t cc = 0; cc < G; cc++) {
-        const uint32_t x = ld_cg(P.hist + (size_t)t * G + cc);
+        const uint32_t x = ld_cg(ghist + (size_t)t * G + cc);
         tot += x;
         if (cc < c) before += x;
       }
@@ -175,8 +154,44 @@ __global__ void __launch_bounds__(kThreads, 2) build_kernel(BuildParams P) {
     uint32_t* tv = vin;
     vin = vout;
     vout = tv;
-    if (!grid_sync(P.bar)) return;
+    if (!grid_sync(bar)) return false;
   }
+  return true;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) build_kernel(BuildParams P) {
+  __shared__ Shared S;
+  const uint32_t G = gridDim.x, c = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint64_t nth = (uint64_t)G * blockDim.x;
+  const uint64_t gtid = (uint64_t)c * blockDim.x + t;
+  const uint64_t E = P.entries;
+  const uint64_t per = (E + G - 1) / G;
+  const uint64_t lo = min(E, (uint64_t)c * per), hi = min(E, lo + per);
+  const uint32_t bmask = (1u << P.b) - 1u;
+
+  // ---- fill
+  for (uint64_t i = gtid; i < E; i += nth) {
+    const uint64_t j = P.symmetrize ? i >> 1 : i;
+    const bool rev = P.symmetrize && (i & 1);
+    const uint32_t u = P.src[j], v = P.dst[j];
+    bool drop = (P.drop_self_loops && u == v) || (rev && u == v);
+    if (u >= P.n || v >= P.n) {
+      atomicOr(P.bad, 1u);
+      drop = true;
+    }
+    const uint32_t a = rev ? v : u, z = rev ? u : v;
+    P.k0[i] = drop ? kNone : (((u64)a << P.b) | z);
+    P.v0[i] = P.val ? P.val[j] : P.one;
+  }
+  for (uint64_t v = gtid; v <= P.n; v += nth) P.ro[v] = 0xffffffffu;
+  if (!grid_sync(P.bar)) return;
+
+  // ---- sort
+  u64* kin = P.k0;
+  u64* kout = P.k1;
+  uint32_t* vin = P.v0;
+  uint32_t* vout = P.v1;
+  if (!radix_sort_pairs(S, P.bar, P.hist, kin, kout, vin, vout, lo, hi, 0, P.passes)) return;
 
   // ---- compact: kept entries in order, and the row start of each non-empty row
   auto keep = [&](uint64_t i, u64 k) {
@@ -246,11 +261,170 @@ __global__ void __launch_bounds__(kThreads, 2) build_kernel(BuildParams P) {
   }
 }
 
+
+// ---- weight-sorted adjacency (delta-stepping SSSP) ---------------------------
+//
+// Every row of the forward CSR sorted by weight, on the device: the pairs
+// (row << 32 | weight bits, column) of all edges, filled in row order, are
+// radix-sorted on the weight digits and then the row digits (stable, so equal
+// weights keep their column order); weights are non-negative float32 or
+// uint32, whose bit patterns order like the values.  The same pass checks
+// whether the weighted adjacency is symmetric (each row strictly increasing
+// in column, every edge's reverse present with the same weight), which the
+// pull phases of delta-stepping need.
+constexpr uint32_t kWsBig = 256;  // rows at least this long are filled by a whole warp
+
+struct WsortParams {
+  const uint32_t* ro;
+  const uint32_t* col;
+  const uint32_t* val;
+  uint32_t n;
+  uint64_t m;
+  uint32_t passes;  // 4 weight digits + the row digits
+  u64* k0;
+  u64* k1;
+  uint32_t* v0;
+  uint32_t* v1;
+  uint32_t* hist;       // 256 * gridDim.x
+  uint32_t* big;        // rows of at least kWsBig edges (n entries)
+  uint32_t* big_count;
+  uint32_t* asym;       // set when the adjacency is not symmetric with sorted rows
+  uint32_t* wval;       // out: sorted weights (m)
+  GridBarrier* bar;
+};
+
+// Edge i of row v: its sort pair, and whether it breaks symmetry.
+__device__ __forceinline__ bool ws_edge(const WsortParams& P, uint32_t v, uint64_t i, uint64_t e) {
+  const uint32_t u = P.col[i], w = P.val[i];
+  P.k0[i] = ((u64)v << 32) | w;
+  P.v0[i] = u;
+  if (i + 1 < e && u >= P.col[i + 1]) return true;
+  uint32_t lo = P.ro[u], hi = P.ro[u + 1];  // v in row u (sorted): lower bound
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (P.col[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo == P.ro[u + 1] || P.col[lo] != v || P.val[lo] != w;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) wsort_kernel(WsortParams P) {
+  __shared__ Shared S;
+  const uint32_t G = gridDim.x, c = blockIdx.x, lane = threadIdx.x & 31;
+  const uint64_t nth = (uint64_t)G * blockDim.x;
+  const uint64_t gtid = (uint64_t)c * blockDim.x + threadIdx.x;
+  bool bad = false;
+  // ---- fill: short rows one thread each, long rows listed for whole warps
+  for (uint64_t v = gtid; v < P.n; v += nth) {
+    const uint32_t b = P.ro[v], e = P.ro[v + 1];
+    if (e - b >= kWsBig) {
+      P.big[atomicAdd(P.big_count, 1u)] = (uint32_t)v;
+      continue;
+    }
+    for (uint32_t i = b; i < e; i++) bad |= ws_edge(P, (uint32_t)v, i, e);
+  }
+  if (!grid_sync(P.bar)) return;
+  const uint32_t nbig = ld_cg(P.big_count);
+  for (uint64_t j = gtid >> 5; j < nbig; j += nth >> 5) {
+    const uint32_t v = ld_cg(P.big + j);
+    const uint32_t b = P.ro[v], e = P.ro[v + 1];
+    for (uint32_t i = b + lane; i < e; i += 32) bad |= ws_edge(P, v, i, e);
+  }
+  if (__any_sync(kFullMask, bad) && lane == 0) atomicOr(P.asym, 1u);
+  if (!grid_sync(P.bar)) return;
+  // ---- sort: weight digits (bits 0-31), then row digits
+  const uint64_t per = (P.m + G - 1) / G;
+  const uint64_t lo = min(P.m, (uint64_t)c * per), hi = min(P.m, lo + per);
+  u64* kin = P.k0;
+  u64* kout = P.k1;
+  uint32_t* vin = P.v0;
+  uint32_t* vout = P.v1;
+  if (!radix_sort_pairs(S, P.bar, P.hist, kin, kout, vin, vout, lo, hi, 0, P.passes)) return;
+  // ---- the sorted weights (the sorted columns stay in vin)
+  for (uint64_t i = gtid; i < P.m; i += nth) P.wval[i] = (uint32_t)kin[i];
+}
+
 }  // namespace gb
 
 namespace {
 
 uint32_t bit_length(uint32_t x) { return x ? 32u - (uint32_t)__builtin_clz(x) : 1u; }
+
+}  // namespace
+
+// Builds g->wcol / g->wval (rows of the forward CSR sorted by weight) and
+// g->wsym once per graph, on the device (wsort_kernel).
+sg_status graph_weight_sorted(sg_graph g) {
+  std::lock_guard<std::mutex> lk(g->wsort_mu);
+  if (g->wcol) return SG_OK;
+  SG_REQUIRE(g->fwd.val && g->value_type != SG_WEIGHT_NONE, SG_ERR_INVALID, "the graph has no weights");
+  const uint32_t n = g->n;
+  const uint64_t m = g->m;
+  cudaStream_t st = g->stream;
+  gb::WsortParams P = {};
+  P.ro = g->fwd.ro;
+  P.col = g->fwd.col;
+  P.val = reinterpret_cast<const uint32_t*>(g->fwd.val);
+  P.n = n;
+  P.m = m;
+  P.passes = 4 + (bit_length(n - 1) + 7) / 8;
+  const uint64_t grid = 2ull * device_props().sm_count;
+  const uint64_t ma = m ? m : 1;
+  uint32_t* wv = nullptr;
+  uint32_t* flags = nullptr;  // big_count, asym
+  sg_status s = SG_OK;
+  do {
+    if ((s = dev_alloc(&P.k0, ma)) || (s = dev_alloc(&P.k1, ma)) || (s = dev_alloc(&P.v0, ma)) ||
+        (s = dev_alloc(&P.v1, ma)) || (s = dev_alloc(&P.hist, 256 * grid)) || (s = dev_alloc(&P.big, (uint64_t)n)) ||
+        (s = dev_alloc(&flags, 2)) || (s = dev_alloc(&P.bar, 1)) || (s = dev_alloc(&wv, ma)))
+      break;
+    P.big_count = flags;
+    P.asym = flags + 1;
+    P.wval = wv;
+    cudaError_t e = cudaMemsetAsync(P.bar, 0, sizeof(*P.bar), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) {
+      s = cuda_fail(e, "memset", __FILE__, __LINE__);
+      break;
+    }
+    if ((s = eng::launch_persistent(gb::wsort_kernel, P, 2, st)) != SG_OK) break;
+    uint32_t hf[2] = {0, 0};
+    sygraph::detail::GridBarrier hb;
+    e = cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, P.bar, sizeof(hb), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      s = cuda_fail(e, "weight sort", __FILE__, __LINE__);
+      break;
+    }
+    if (hb.error) {
+      s = fail(SG_ERR_TIMEOUT, "weight sort: a grid barrier wait ran out");
+      break;
+    }
+    // after an even number of passes the sorted columns are in v0, else v1
+    uint32_t*& sorted_col = P.passes % 2 == 0 ? P.v0 : P.v1;
+    g->wcol = sorted_col;
+    sorted_col = nullptr;
+    g->wval = wv;
+    wv = nullptr;
+    g->wsym = hf[1] == 0;
+    g->bytes += 8ull * m;
+  } while (0);
+  dev_free(P.k0);
+  dev_free(P.k1);
+  dev_free(P.v0);
+  dev_free(P.v1);
+  dev_free(P.hist);
+  dev_free(P.big);
+  dev_free(flags);
+  dev_free(P.bar);
+  dev_free(wv);
+  return s;
+}
+
+namespace {
 
 // One direction (forward, or with src / dst swapped the inverse) of a build;
 // out gets device arrays ro (n+1), col and val (m each).
@@ -427,6 +601,19 @@ sg_status sg_graph_create_coo(const uint32_t* src, const uint32_t* dst, const vo
     return s;
   }
   *out = g;
+  return SG_OK;
+}
+
+sg_status sg_graph_weight_sorted(sg_graph g, uint32_t* host_column_indices, void* host_values, int* symmetric) {
+  clear_error();
+  SG_REQUIRE(g, SG_ERR_INVALID, "graph is NULL");
+  SG_TRY(graph_weight_sorted(g));
+  if (host_column_indices && g->m)
+    SG_CUDA(cudaMemcpyAsync(host_column_indices, g->wcol, sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost, g->stream));
+  if (host_values && g->m)
+    SG_CUDA(cudaMemcpyAsync(host_values, g->wval, sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost, g->stream));
+  SG_CUDA(cudaStreamSynchronize(g->stream));
+  if (symmetric) *symmetric = g->wsym ? 1 : 0;
   return SG_OK;
 }
 

@@ -58,78 +58,6 @@ __global__ void k_indegree(const uint32_t* __restrict__ col, uint64_t m, uint32_
     atomicAdd(cnt + col[e], 1u);
 }
 
-// Each row of the forward CSR sorted by (weight, column) on the host: weights
-// are float32 or uint32, non-negative, so their bit patterns order like them.
-sg_status graph_weight_sorted(sg_graph g) {
-  std::lock_guard<std::mutex> lk(g->wsort_mu);
-  if (g->wcol) return SG_OK;
-  SG_REQUIRE(g->fwd.val && g->value_type != SG_WEIGHT_NONE, SG_ERR_INVALID, "the graph has no weights");
-  const uint32_t n = g->n;
-  const uint64_t m = g->m;
-  std::vector<uint32_t> ro((size_t)n + 1), col(m ? m : 1), val(m ? m : 1);
-  SG_CUDA(cudaStreamSynchronize(g->stream));
-  SG_CUDA(cudaMemcpy(ro.data(), g->fwd.ro, sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost));
-  SG_CUDA(cudaMemcpy(col.data(), g->fwd.col, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
-  SG_CUDA(cudaMemcpy(val.data(), g->fwd.val, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
-  // symmetric weighted adjacency: each row sorted by column and every edge's
-  // reverse present with the same weight (binary search in the other row)
-  bool sym = true;
-#pragma omp parallel for schedule(dynamic, 4096) reduction(&& : sym)
-  for (int64_t v = 0; v < (int64_t)n; v++) {
-    if (!sym) continue;
-    for (uint32_t i = ro[v]; i < ro[v + 1]; i++) {
-      if (i + 1 < ro[v + 1] && col[i] >= col[i + 1]) {
-        sym = false;
-        break;
-      }
-      const uint32_t u = col[i];
-      const uint32_t* b = col.data() + ro[u];
-      const uint32_t* e = col.data() + ro[u + 1];
-      const uint32_t* f = std::lower_bound(b, e, (uint32_t)v);
-      if (f == e || *f != (uint32_t)v || val[f - col.data()] != val[i]) {
-        sym = false;
-        break;
-      }
-    }
-  }
-#pragma omp parallel
-  {
-    std::vector<uint64_t> key;
-#pragma omp for schedule(dynamic, 4096)
-    for (int64_t v = 0; v < (int64_t)n; v++) {
-      const uint32_t b = ro[v], e = ro[v + 1];
-      if (e - b < 2) continue;
-      key.resize(e - b);
-      for (uint32_t i = b; i < e; i++) key[i - b] = ((uint64_t)val[i] << 32) | col[i];
-      std::sort(key.begin(), key.end());
-      for (uint32_t i = b; i < e; i++) {
-        val[i] = (uint32_t)(key[i - b] >> 32);
-        col[i] = (uint32_t)key[i - b];
-      }
-    }
-  }
-  uint32_t* wc = nullptr;
-  uint32_t* wv = nullptr;
-  SG_TRY(dev_alloc(&wc, m));
-  sg_status s = dev_alloc(&wv, m);
-  if (s != SG_OK) {
-    dev_free(wc);
-    return s;
-  }
-  if (cudaMemcpy(wc, col.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(wv, val.data(), sizeof(uint32_t) * m, cudaMemcpyHostToDevice) != cudaSuccess) {
-    cudaGetLastError();
-    dev_free(wc);
-    dev_free(wv);
-    return fail(SG_ERR_CUDA, "uploading the weight-sorted adjacency failed");
-  }
-  g->wcol = wc;
-  g->wval = wv;
-  g->wsym = sym;
-  g->bytes += 8ull * m;
-  return SG_OK;
-}
-
 }  // namespace sgb
 
 // Diagnostic of the bounded grid barrier: every block but `skip_block`

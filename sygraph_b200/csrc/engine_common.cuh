@@ -278,12 +278,25 @@ __device__ __forceinline__ uint32_t valid_bits(uint32_t wi, uint32_t w0, uint32_
 template <typename Params>
 inline sg_status launch_persistent(void (*kernel)(Params), const Params& p, int blocks_per_sm, cudaStream_t stream,
                                    unsigned max_grid = 0, unsigned* grid_out = nullptr, unsigned threads = kThreads) {
-  int dev = 0, coop = 0;
+  // the cooperative-launch attribute and the kernel's occupancy are queried
+  // once per (kernel, device, block size) and thread, so a launch costs the
+  // host one cudaGetDevice and the launch itself
+  static thread_local int cached_dev = -1, cached_occ = 0;
+  static thread_local unsigned cached_threads = 0;
+  static thread_local void (*cached_kernel)(Params) = nullptr;
+  int dev = 0;
   SG_CUDA(cudaGetDevice(&dev));
-  SG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-  SG_REQUIRE(coop, SG_ERR_UNSUPPORTED, "device does not support cooperative launch");
-  int occ = 0;
-  SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, (int)threads, 0));
+  if (dev != cached_dev || threads != cached_threads || kernel != cached_kernel) {
+    int coop = 0, o = 0;
+    SG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    SG_REQUIRE(coop, SG_ERR_UNSUPPORTED, "device does not support cooperative launch");
+    SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, (int)threads, 0));
+    cached_dev = dev;
+    cached_threads = threads;
+    cached_kernel = kernel;
+    cached_occ = o;
+  }
+  const int occ = cached_occ;
   SG_REQUIRE(occ > 0, SG_ERR_CUDA, "engine kernel does not fit on an SM");
   const int per_sm = occ < blocks_per_sm ? occ : blocks_per_sm;
   unsigned grid = (unsigned)(per_sm * device_props().sm_count);

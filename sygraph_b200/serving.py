@@ -156,21 +156,31 @@ def run_open_loop(srv: Server, gids, wl: Workload, outs=None) -> dict:
 def run_one_at_a_time(graphs, wl: Workload, sssp_delta: float = 0.0) -> dict:
     """The same queries through BFS / SSSP instances, one after another on
     the default stream (each waits for the previous): service time per query
-    and the throughput that gives."""
+    and the throughput that gives.  Every instance the stream needs is
+    created, and has run one query (which builds its graph's weight-sorted
+    adjacency for delta-stepping), before the clock starts, as the server's
+    workspaces are before its timed runs."""
     from . import algorithms
     inst = {}
+    for i in range(wl.arrivals.size):
+        gi, kind = int(wl.graph[i]), wl.kind[i]
+        key = (gi, kind)
+        if key in inst:
+            continue
+        if kind == "bfs":
+            inst[key] = algorithms.BFS(graphs[gi])
+            inst[key].init(0)
+            inst[key].run(2, 15.0, 24.0)
+        else:
+            inst[key] = algorithms.SSSP(graphs[gi])
+            inst[key].set_delta(sssp_delta)
+            inst[key].init(0)
+            inst[key].run()
     times = []
     t0 = time.perf_counter()
     for i in range(wl.arrivals.size):
         gi, kind, s = int(wl.graph[i]), wl.kind[i], int(wl.source[i])
-        key = (gi, kind)
-        if key not in inst:
-            if kind == "bfs":
-                inst[key] = algorithms.BFS(graphs[gi])
-            else:
-                inst[key] = algorithms.SSSP(graphs[gi])
-                inst[key].set_delta(sssp_delta)
-        a = inst[key]
+        a = inst[(gi, kind)]
         t = time.perf_counter()
         a.init(s)
         if kind == "bfs":

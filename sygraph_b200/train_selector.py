@@ -147,12 +147,17 @@ def traversals(data: dict):
 
 
 def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.ndarray,
-                     allowed: int = 0x3F, margin: float = MARGIN, min_frontier: float = MIN_FRONTIER) -> np.ndarray:
+                     allowed: int = 0x3F, margin: float = MARGIN, min_frontier: float = MIN_FRONTIER,
+                     graph_range=None) -> np.ndarray:
     """The learned mode's schedule on a traversal: the MLP's argmin per level
     (`forward` maps a feature batch to predicted log-times) with the
     current-direction feature following its own previous choice, and the
     heuristic where a feature leaves the trusted range or the frontier is
-    below `min_frontier` of the vertices, as the engine does."""
+    below `min_frontier` of the vertices, as the engine does; on a graph
+    whose mean-degree feature (9) is outside `graph_range` the heuristic
+    decides every level."""
+    if graph_range is not None and len(F) and not (graph_range[0] <= F[0][9] <= graph_range[1]):
+        return np.asarray(heuristic, np.int32).copy()
     t0 = params.size - 4 * IN
     lo, hi = params[t0 + 2 * IN:t0 + 3 * IN], params[t0 + 3 * IN:t0 + 4 * IN]
     banned = [j for j in range(OUT) if not (allowed >> j) & 1]
@@ -179,7 +184,7 @@ def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F) -> dict:
     rows = []
     params = mlp.params
     for name, T, H, F in traversals(data):
-        c = simulate_choices(params, mlp.forward, F, H, allowed)
+        c = simulate_choices(params, mlp.forward, F, H, allowed, graph_range=mlp.graph_range)
         idx = np.arange(len(T))
         rows.append({"traversal": name, "levels": len(T), "heuristic_us": float(T[idx, H].sum()),
                      "learned_us": float(T[idx, c].sum()), "best_us": float(T.min(1).sum()),
@@ -189,6 +194,18 @@ def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F) -> dict:
     tot["regret_learned"] = tot["learned_us"] / max(tot["best_us"], 1e-9) - 1.0
     tot["regret_heuristic"] = tot["heuristic_us"] / max(tot["best_us"], 1e-9) - 1.0
     return {"total": tot, "traversals": rows}
+
+
+def graph_range(mlp: Mlp, data: dict, widen: float = 0.05):
+    """The range of the mean-degree feature (9, constant per graph) over the
+    training traversals on which the model overrules the heuristic at least
+    once, widened by `widen`: the engine consults the model only there, so
+    graphs on which it only ever agreed with the heuristic pay no inference.
+    (1, 0), an empty range, when it never overrules it."""
+    params = mlp.params
+    f9 = [float(F[0][9]) for _, _, H, F in traversals(data)
+          if len(F) and np.any(simulate_choices(params, mlp.forward, F, H) != H)]
+    return (min(f9) - widen, max(f9) + widen) if f9 else (1.0, 0.0)
 
 
 def level_weights(Y: np.ndarray, lo: float = 0.25, hi: float = 8.0) -> np.ndarray:
@@ -252,6 +269,7 @@ def main(argv=None) -> int:
     elif a.cmd == "train":
         data = _load(a.data)
         mlp = train(data, a.steps, a.lr)
+        mlp.graph_range = graph_range(mlp, data)
         rep = evaluate(mlp, data)
         mlp.save(a.model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
         print(json.dumps(rep["total"]))
