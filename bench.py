@@ -608,20 +608,25 @@ def main():
     bfs.set_selector(None)
     del bg, Gg, gg
 
-    # the same 64 sources as one bit-parallel batch (one launch); identical depths
+    # the same 64 sources as one bit-parallel batch (one launch); identical
+    # depths.  Grid size and direction threshold from the autotuner, timed on
+    # these sources before the measurement.
+    from sygraph_b200 import autotune
     mbfs = sg.algorithms.MultiBFS(G, len(srcs))
+    ms_tuned = autotune.tune_batched_bfs(mbfs, srcs, reps=2, use_cache=False)
+    ms_alpha = float(ms_tuned["alpha"])
     for _ in range(2):
-        mbfs.run_async(srcs, 2, MS_ALPHA, MS_BETA)
+        mbfs.run_async(srcs, 2, ms_alpha, MS_BETA)
     torch.cuda.synchronize()
     mb_ms = []
     for _ in range(max(3, args.steps // 2)):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        mbfs.run_async(srcs, 2, MS_ALPHA, MS_BETA)
+        mbfs.run_async(srcs, 2, ms_alpha, MS_BETA)
         b.record()
         b.synchronize()
         mb_ms.append(a.elapsed_time(b))
-    mb_det = mbfs.run(srcs, 2, MS_ALPHA, MS_BETA)
+    mb_det = mbfs.run(srcs, 2, ms_alpha, MS_BETA)
     mb_rows = mbfs.getDistances()[:PARITY_SOURCES].copy()  # checked against the oracle below
     batched_ms = float(np.median(mb_ms))
     batched_gteps = mb_det["reached_edges"] / (batched_ms * 1e-3) / 1e9
@@ -634,6 +639,7 @@ def main():
     Gbc = sg.graph.build.fromCSR(gbc)
     sbc = sg.io.sample_sources(gbc, BC_SOURCES, seed=SOURCE_SEED)
     bcb = sg.algorithms.BatchedBC(Gbc)
+    bc_tuned = autotune.tune_batched_bc(bcb, sbc, reps=1, use_cache=False)
     bc_det = bcb.run(sbc)
     bc_ms = float(np.median([_launch_ms(torch, lambda: bcb.run_async(sbc)) for _ in range(3)]))
     x_bc = bcb.getBC()
@@ -642,7 +648,7 @@ def main():
     bc1_ms = float(np.median([_launch_ms(torch, bc1.run) for _ in range(3)]))  # single runs vary up to 1.7x
     y_bc = bc1.getBC().astype(np.float64)
     bc_rel = float(np.max(np.abs(x_bc - y_bc) / np.maximum(1.0, np.abs(y_bc))))
-    bc_line = {"value": bc_det["reached_edges"] / (bc_ms * 1e-3) / 1e9, "unit": "GTEPS",
+    bc_line = {"value": bc_det["reached_edges"] / (bc_ms * 1e-3) / 1e9, "unit": "GTEPS", "autotuned": bc_tuned,
                "workload": f"Brandes BC, {BC_SOURCES} sources, RMAT-{BC_SCALE} ef{EDGE_FACTOR}",
                "launch_ms": bc_ms, "per_source_ms": bc1_ms, "speedup_vs_per_source": bc1_ms / bc_ms,
                "max_rel_diff_vs_per_source": bc_rel, "forward_levels": bc_det["iterations"]}
@@ -720,9 +726,12 @@ def main():
     sssp_gteps = ss_edges / (ss_ms * 1e-3) / 1e9
     sssp_kern = ss_ms / k_ss
     sssp_achieved = sssp_bytes / (sssp_kern * 1e-3) / 1e9
-    # delta-stepping on the same sources: the same distances (checked), less work
+    # delta-stepping on the same sources: the same distances (checked), less
+    # work; the bucket width from the autotuner (timed on two other sources)
     sssp.set_pull(SSSP_PULL)
-    sssp.set_delta(SSSP_DELTA)
+    sssp_delta = float(autotune.tune_sssp(sssp, srcs[-2:], autotune.mean_weight(g), reps=1,
+                                          use_cache=False)["delta"]) or SSSP_DELTA
+    sssp.set_delta(sssp_delta)
     nf_ms, nf_same = 0.0, True
     d_first = None
     for s in srcs[:k_ss]:
@@ -735,7 +744,7 @@ def main():
         sssp.init(int(s))
         sssp.run()
         nf_same &= bool(np.array_equal(d_nf.view(np.uint32), sssp.getDistances().view(np.uint32)))
-        sssp.set_delta(SSSP_DELTA)
+        sssp.set_delta(sssp_delta)
         sssp.init(int(s))
         nf_ms += _launch_ms(torch, sssp.run_async)
     nf_kern = nf_ms / k_ss
@@ -763,6 +772,7 @@ def main():
             "cpu_baseline": base,
             "parity": parity,
             "batched": {"value": batched_gteps, "unit": "GTEPS", "sources_per_launch": len(srcs),
+                        "autotuned": ms_tuned,
                         "launch_ms": batched_ms, "speedup_vs_single_source": batched_gteps / value,
                         "reached_edges": mb_det["reached_edges"], "reached_edges_single": step_edges,
                         "roofline": {"bound": "hbm", "achieved": ms_bytes / (batched_ms * 1e-3) / 1e9,
@@ -777,7 +787,8 @@ def main():
             "serving": serve,
             "sssp": {"value": sssp_gteps, "unit": "GTEPS", "sources": k_ss, "launch_ms": sssp_kern,
                      "schedule": "frontier Bellman-Ford (the reference's)",
-                     "delta_stepping": {"delta": SSSP_DELTA, "launch_ms": nf_kern,
+                     "delta_stepping": {"delta": sssp_delta, "delta_source": "autotune.tune_sssp",
+                                        "launch_ms": nf_kern,
                                   "value": ss_edges / (nf_ms * 1e-3) / 1e9, "unit": "GTEPS",
                                   "speedup": sssp_kern / nf_kern, "identical_distances": nf_same,
                                   "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s",

@@ -41,7 +41,7 @@ static_assert(kMlpParamCount == kMlpTrainableCount + 4 * kMlpIn, "MlpParams must
 // Shared-memory copy of the parameters for inference inside the traversal
 // engines: the two hidden-layer matrices transposed, so that lane j reads
 // element j of a row (no bank conflicts), and no global load on the path.
-struct MlpStaged {
+struct __align__(16) MlpStaged {
   float w1t[kMlpIn][kMlpHidden];
   float b1[kMlpHidden];
   float w2t[kMlpHidden][kMlpHidden];
@@ -52,9 +52,13 @@ struct MlpStaged {
   float inv_std[kMlpIn];
   float lo[kMlpIn];
   float hi[kMlpIn];
+  float pad[2];  // a whole number of 16-byte chunks
 };
+constexpr int kMlpStagedChunks = (int)(sizeof(MlpStaged) / 16);
+static_assert(sizeof(MlpStaged) % 16 == 0, "the staged image is copied in 16-byte chunks");
 
-// Block-cooperative copy; the caller synchronises the block afterwards.
+// Block-cooperative copy from the parameters; the caller synchronises the
+// block afterwards.  (Also builds the staged image in global memory.)
 __device__ __forceinline__ void mlp_stage(const MlpParams* __restrict__ g, MlpStaged* s) {
   for (int t = threadIdx.x; t < kMlpIn * kMlpHidden; t += blockDim.x)
     s->w1t[t / kMlpHidden][t % kMlpHidden] = g->w1[t % kMlpHidden][t / kMlpHidden];
@@ -73,7 +77,22 @@ __device__ __forceinline__ void mlp_stage(const MlpParams* __restrict__ g, MlpSt
     s->hi[t] = g->hi[t];
   }
   for (int t = threadIdx.x; t < kMlpOut; t += blockDim.x) s->b3[t] = g->b3[t];
+  if (threadIdx.x < 2) s->pad[threadIdx.x] = 0.f;
 }
+
+// Asynchronous copy of a staged image (already in the MlpStaged layout in
+// global memory) into shared memory: every thread issues at most one or two
+// 16-byte cp.async copies and goes on; mlp_stage_wait() completes them.
+__device__ __forceinline__ void mlp_stage_async(const MlpStaged* __restrict__ image, MlpStaged* s) {
+  const char* src = reinterpret_cast<const char*>(image);
+  const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(s));
+  for (int t = threadIdx.x; t < kMlpStagedChunks; t += blockDim.x)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * t), "l"(src + 16 * t) : "memory");
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// Waits for this thread's copies; the block must synchronise before any
+// thread reads the staged parameters.
+__device__ __forceinline__ void mlp_stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Forward pass by one full warp: lane j computes hidden unit j; the hidden
 // activations go through `scratch` (64 floats of shared memory) so that every

@@ -460,6 +460,10 @@ sg_status sg_bfs_set_selector_margin(sg_bfs b, float margin);
  * choice without an inference (when that choice is allowed).  Default 1e-3;
  * 0 asks the MLP on every level. */
 sg_status sg_bfs_set_selector_min_frontier(sg_bfs b, float fraction);
+/* Learned mode: a frontier larger than fraction * n keeps the heuristic's
+ * choice without an inference (when that choice is allowed).  Default 1
+ * (no limit); the model file stores the range chosen in training. */
+sg_status sg_bfs_set_selector_max_frontier(sg_bfs b, float fraction);
 /* Learned mode: the MLP is consulted only on graphs whose mean-degree feature
  * log2(1 + m/n) / 8 lies in [lo, hi]; on other graphs the launch carries no
  * MLP (no parameter staging, no inference) and the heuristic decides every

@@ -169,6 +169,7 @@ SIGNATURES = {
     "sg_bfs_set_schedule": (st, [vp, C.POINTER(C.c_int), C.c_uint32]),
     "sg_bfs_set_selector": (st, [vp, vp, C.c_uint32]),
     "sg_bfs_set_selector_min_frontier": (st, [vp, C.c_float]),
+    "sg_bfs_set_selector_max_frontier": (st, [vp, C.c_float]),
     "sg_bfs_set_selector_margin": (st, [vp, C.c_float]),
     "sg_bfs_set_pull_order": (st, [vp, C.c_uint64]),
     "sg_bfs_set_pull_words": (st, [vp, C.c_uint32]),

@@ -83,13 +83,18 @@ class BFS:
         """The MLP of bfs_direction.learned (None detaches it); `margin` is the
         predicted log-time gain it needs to overrule the heuristic, and
         frontiers below `min_frontier` of the vertices keep the heuristic's
-        choice without an inference; the model's graph range (mlp.graph_range)
-        limits it to the graphs it was trained to overrule the heuristic on."""
+        choice without an inference; the model's graph and frontier ranges
+        (mlp.graph_range, mlp.frontier_range) limit it to the graphs and
+        levels on which it pays for its inferences in training."""
         self._mlp = mlp  # keep the device parameters alive
         call("sg_bfs_set_selector", self.handle, mlp.handle if mlp is not None else None, allowed)
         rng = getattr(mlp, "graph_range", None) if mlp is not None else None
         lo, hi = rng if rng is not None else (-np.inf, np.inf)
         call("sg_bfs_set_selector_graph_range", self.handle, float(lo), float(hi))
+        fr = getattr(mlp, "frontier_range", None) if mlp is not None else None
+        if fr is not None:
+            call("sg_bfs_set_selector_min_frontier", self.handle, float(fr[0]))
+            call("sg_bfs_set_selector_max_frontier", self.handle, float(fr[1]))
         if margin is not None:
             call("sg_bfs_set_selector_margin", self.handle, float(margin))
         if min_frontier is not None:

@@ -79,7 +79,7 @@ def _key(kind: str, G) -> str:
     return f"{kind}:n={G.getVertexCount()}:m={G.getEdgeCount()}"
 
 
-def tune_batched_bfs(mb, sources, alphas=(0.5, 1.0, 2.0), **kw) -> dict:
+def tune_batched_bfs(mb, sources, alphas=(1.0, 2.0, 4.0, 8.0), **kw) -> dict:
     """Grid size and direction threshold of a MultiBFS on its graph; applies
     and returns {"max_ctas", "alpha"}."""
     cands = [{"max_ctas": g, "alpha": a} for g in grid_candidates() for a in alphas]

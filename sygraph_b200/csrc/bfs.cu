@@ -45,6 +45,10 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
   // traversal: a vertex's depth is stored when it is discovered, and the
   // unreached ones get n+1 after the last level (the same time as filling all
   // n depths first on RMAT-22, with less traffic).
+  // learned mode: the staged parameters arrive by asynchronous copies while
+  // the bitmaps are initialised; the init barrier publishes them
+  const bool learned = P.mode == kLearned && P.mlp;
+  if (learned) sygraph::detail::mlp_stage_async(P.mlp_image, &S.mlp);
   if (gtid == 0) st_cg(P.depth + src, 0u);
   for (uint32_t i = gtid; i < w0; i += nthreads) {
     const uint32_t b = (i == (src >> 5)) ? (1u << (src & 31)) : 0u;
@@ -71,8 +75,8 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     S.hn = 0;
     S.acc[0] = S.acc[1] = 0ull;
   }
-  if (P.mode == kLearned && P.mlp) sygraph::detail::mlp_stage(P.mlp, &S.mlp);
   if (threadIdx.x == 0) S.fk = feature_const(P);
+  if (learned) sygraph::detail::mlp_stage_wait();
   if (!grid_sync(P.bar)) return;
 
   // heavy list of the frontier being expanded, read with the level's other
@@ -287,6 +291,8 @@ struct sg_bfs_s {
   uint32_t allowed = 0x3f;
   float margin = 0.05f;
   float min_frontier = 1e-3f;  // learned mode: frontiers below this fraction of n keep the heuristic
+  float max_frontier = 1.0f;   // ... and frontiers above this one
+  const void* mlp_image = nullptr;  // the MLP's staged image
   // learned mode: the MLP is consulted only on graphs whose mean-degree
   // feature log2(1 + m/n) / 8 lies in [graph_lo, graph_hi]
   float graph_lo = -INFINITY, graph_hi = INFINITY;
@@ -350,6 +356,8 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.allowed = b->allowed;
   P.margin = b->margin;
   P.min_frontier = b->min_frontier;
+  P.max_frontier = b->max_frontier;
+  P.mlp_image = static_cast<const sygraph::detail::MlpStaged*>(b->mlp_image);
   P.pull_reverse = b->pull_reverse;
   P.pull_words = b->pull_words;
   P.features = b->features;
@@ -539,6 +547,14 @@ sg_status sg_bfs_set_selector_graph_range(sg_bfs b, float lo, float hi) {
   return SG_OK;
 }
 
+sg_status sg_bfs_set_selector_max_frontier(sg_bfs b, float fraction) {
+  clear_error();
+  SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
+  SG_REQUIRE(fraction >= 0.f && fraction <= 1.f, SG_ERR_INVALID, "fraction must be in [0, 1]");
+  b->max_frontier = fraction;
+  return SG_OK;
+}
+
 sg_status sg_bfs_set_selector_min_frontier(sg_bfs b, float fraction) {
   clear_error();
   SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
@@ -560,6 +576,7 @@ sg_status sg_bfs_set_selector(sg_bfs b, sg_mlp mlp, uint32_t allowed) {
   SG_REQUIRE(b, SG_ERR_INVALID, "bfs is NULL");
   SG_REQUIRE(!mlp || (allowed & 0x3fu), SG_ERR_INVALID, "no strategy allowed");
   b->mlp = mlp ? static_cast<const sygraph::detail::MlpParams*>(mlp_device_params(mlp)) : nullptr;
+  b->mlp_image = mlp ? mlp_device_image(mlp) : nullptr;
   b->allowed = allowed & 0x3fu;
   return SG_OK;
 }
@@ -749,6 +766,8 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.allowed = 0x3f;
   P.margin = 0.f;
   P.min_frontier = 0.f;
+  P.max_frontier = 1.f;
+  P.mlp_image = nullptr;
   P.pull_reverse = 0;
   P.pull_words = bfs::kDefaultPullWords;  // the instance default of sg_bfs_create
   P.features = nullptr;

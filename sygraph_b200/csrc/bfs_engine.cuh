@@ -62,9 +62,11 @@ struct Params {
   const int* schedule;         // optional strategy per level (0..5), -1 = the mode decides
   uint32_t schedule_len;
   const sygraph::detail::MlpParams* mlp;  // learned mode
+  const sygraph::detail::MlpStaged* mlp_image;  // its staged image (copied to shared memory per launch)
   uint32_t allowed;                       // strategies the MLP may pick (bit mask)
   float margin;                           // log-time gain the MLP must predict to overrule the heuristic
   float min_frontier;                     // smallest frontier (fraction of n) the MLP is asked about
+  float max_frontier;                     // largest frontier (fraction of n) the MLP is asked about
   unsigned long long pull_reverse;        // bit L: level L's pull probes in-neighbours from the back
   uint32_t pull_words;                    // short-circuit pull: 0 ranked candidates, or 2 / 4 words per warp step
   float* features;                        // optional log: 12 floats per level decision
@@ -258,13 +260,15 @@ __device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const
   }
   int h = P.mode == SG_BFS_PUSH ? 0 : P.mode == SG_BFS_PULL ? 2 : (pull ? 2 : 0);
   const bool log = P.features && blockIdx.x == 0 && level < kMaxLog;
-  // frontiers below min_frontier * n keep the heuristic's choice without an
-  // inference when that choice is allowed: on them the model and the
-  // heuristic agree (the held-out tables keep 1.15x of the 1.17x grid gain),
+  // frontiers outside [min_frontier, max_frontier] * n keep the heuristic's
+  // choice without an inference when that choice is allowed: there the model
+  // rarely overrules the heuristic (the range is chosen on the training
+  // tables, gain of the model's choices against the cost of the inferences),
   // and the inference is a latency of about a microsecond on every level's
   // critical path
   const bool infer = P.mode == kLearned && P.mlp &&
-                     ((float)x.ns >= P.min_frontier * (float)P.n || !((P.allowed >> h) & 1u));
+                     (((float)x.ns >= P.min_frontier * (float)P.n && (float)x.ns <= P.max_frontier * (float)P.n) ||
+                      !((P.allowed >> h) & 1u));
   if (infer || log) {
     if (threadIdx.x < 32) {
       float f[12];

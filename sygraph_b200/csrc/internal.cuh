@@ -95,6 +95,9 @@ inline unsigned grid_for(uint64_t work_items, unsigned block, unsigned per_sm = 
 
 // Device address of an sg_mlp's parameter block (selector.cu).
 const void* mlp_device_params(sg_mlp h);
+// The parameters in the engines' shared-memory layout (MlpStaged), kept in
+// device memory and rebuilt whenever the parameters change.
+const void* mlp_device_image(sg_mlp h);
 // Frees a graph and every device array it owns.
 void release_graph(sg_graph g);
 // Builds g->wcol / g->wval once (weighted graphs only).

@@ -141,6 +141,9 @@ using sygraph::detail::kMlpOut;
 
 struct sg_mlp_s {
   float* params = nullptr;  // kMlpParamCount
+  // the parameters in the layout the traversal engines read them in (hidden
+  // matrices transposed), rebuilt after every change of the parameters
+  sygraph::detail::MlpStaged* image = nullptr;
   float* grad = nullptr;
   float* m1 = nullptr;
   float* m2 = nullptr;
@@ -150,11 +153,26 @@ struct sg_mlp_s {
 
 namespace sgb {
 const void* mlp_device_params(sg_mlp h) { return h ? h->params : nullptr; }
+const void* mlp_device_image(sg_mlp h) { return h ? h->image : nullptr; }
 }  // namespace sgb
+
+__global__ void mlp_image_kernel(const sygraph::detail::MlpParams* __restrict__ p, sygraph::detail::MlpStaged* image) {
+  sygraph::detail::mlp_stage(p, image);
+}
+
+// Rebuilds the staged image from the parameters and waits for it (the
+// engines read it from any stream).
+static sg_status mlp_refresh_image(sg_mlp h) {
+  mlp_image_kernel<<<1, 256>>>(reinterpret_cast<const sygraph::detail::MlpParams*>(h->params), h->image);
+  SG_CHECK_LAUNCH();
+  SG_CUDA(cudaStreamSynchronize(0));
+  return SG_OK;
+}
 
 static void mlp_release(sg_mlp h) {
   if (!h) return;
   dev_free(h->params);
+  dev_free(h->image);
   dev_free(h->grad);
   dev_free(h->m1);
   dev_free(h->m2);
@@ -174,7 +192,7 @@ sg_status sg_mlp_create(const float* host_params, sg_mlp* out) {
   const uint32_t P = sygraph::detail::kMlpParamCount;
   sg_status s;
   if ((s = dev_alloc(&h->params, P)) || (s = dev_alloc(&h->grad, P)) || (s = dev_alloc(&h->m1, P)) ||
-      (s = dev_alloc(&h->m2, P)) || (s = dev_alloc(&h->loss, 1))) {
+      (s = dev_alloc(&h->m2, P)) || (s = dev_alloc(&h->loss, 1)) || (s = dev_alloc(&h->image, 1))) {
     mlp_release(h);
     return s;
   }
@@ -211,6 +229,10 @@ sg_status sg_mlp_create(const float* host_params, sg_mlp* out) {
     mlp_release(h);
     return cuda_fail(e, "mlp init", __FILE__, __LINE__);
   }
+  if ((s = mlp_refresh_image(h)) != SG_OK) {
+    mlp_release(h);
+    return s;
+  }
   *out = h;
   return SG_OK;
 }
@@ -229,7 +251,7 @@ sg_status sg_mlp_get_params(sg_mlp h, float* host_params) {
 sg_status sg_mlp_set_params(sg_mlp h, const float* host_params) {
   SG_REQUIRE(h && host_params, SG_ERR_INVALID, "NULL argument");
   SG_CUDA(cudaMemcpy(h->params, host_params, sizeof(float) * sygraph::detail::kMlpParamCount, cudaMemcpyHostToDevice));
-  return SG_OK;
+  return mlp_refresh_image(h);
 }
 
 sg_status sg_mlp_forward(sg_mlp h, const float* dev_x, uint32_t n, float* dev_y) {
@@ -277,7 +299,7 @@ sg_status sg_mlp_train(sg_mlp h, const float* dev_x, const float* dev_t, const f
   }
   if (host_final_loss) SG_CUDA(cudaMemcpy(host_final_loss, h->loss, sizeof(float), cudaMemcpyDeviceToHost));
   SG_CUDA(cudaDeviceSynchronize());
-  return SG_OK;
+  return mlp_refresh_image(h);
 }
 
 }  // extern "C"

@@ -33,6 +33,10 @@ MARGIN = 0.05
 # the engine skips the inference on frontiers below this fraction of n (the
 # heuristic's choice stands there), as kLearnedMinFrontier in the engine
 MIN_FRONTIER = 1e-3
+# device time of one inference between two levels (features, three layers,
+# the block barrier that publishes the choice), measured from the level
+# timestamps; the consulted frontier range trades it against the model's gains
+INFERENCE_US = 1.25
 MAX_LEVELS = 4096
 
 # (name, generator, kwargs): RMAT skews and scales, grids with and without
@@ -148,7 +152,7 @@ def traversals(data: dict):
 
 def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.ndarray,
                      allowed: int = 0x3F, margin: float = MARGIN, min_frontier: float = MIN_FRONTIER,
-                     graph_range=None) -> np.ndarray:
+                     graph_range=None, max_frontier: float = 1.0) -> np.ndarray:
     """The learned mode's schedule on a traversal: the MLP's argmin per level
     (`forward` maps a feature batch to predicted log-times) with the
     current-direction feature following its own previous choice, and the
@@ -167,7 +171,7 @@ def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.n
         f = np.array(F[L], np.float32)
         if L > 0:
             f[10] = 1.0 if prev >= 2 else 0.0
-        if f[1] < min_frontier or np.any(f < lo) or np.any(f > hi):
+        if f[1] < min_frontier or f[1] > max_frontier or np.any(f < lo) or np.any(f > hi):
             out[L] = heuristic[L]
         else:
             y = np.array(forward(f[None, :]), np.float64)[0]
@@ -183,8 +187,10 @@ def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F) -> dict:
     the MLP's schedule and the per-level best; totals and regret."""
     rows = []
     params = mlp.params
+    fr = mlp.frontier_range or (MIN_FRONTIER, 1.0)
     for name, T, H, F in traversals(data):
-        c = simulate_choices(params, mlp.forward, F, H, allowed, graph_range=mlp.graph_range)
+        c = simulate_choices(params, mlp.forward, F, H, allowed, graph_range=mlp.graph_range,
+                             min_frontier=fr[0], max_frontier=fr[1])
         idx = np.arange(len(T))
         rows.append({"traversal": name, "levels": len(T), "heuristic_us": float(T[idx, H].sum()),
                      "learned_us": float(T[idx, c].sum()), "best_us": float(T.min(1).sum()),
@@ -203,9 +209,37 @@ def graph_range(mlp: Mlp, data: dict, widen: float = 0.05):
     graphs on which it only ever agreed with the heuristic pay no inference.
     (1, 0), an empty range, when it never overrules it."""
     params = mlp.params
+    fr = getattr(mlp, "frontier_range", None) or (MIN_FRONTIER, 1.0)
     f9 = [float(F[0][9]) for _, _, H, F in traversals(data)
-          if len(F) and np.any(simulate_choices(params, mlp.forward, F, H) != H)]
+          if len(F) and np.any(simulate_choices(params, mlp.forward, F, H, min_frontier=fr[0],
+                                                max_frontier=fr[1]) != H)]
     return (min(f9) - widen, max(f9) + widen) if f9 else (1.0, 0.0)
+
+
+def frontier_range(mlp: Mlp, data: dict, cost_us: float = INFERENCE_US):
+    """The frontier-size range (fraction of n) on which consulting the model
+    pays on the training traversals: over a grid of bounds, the summed time
+    its choices save against the heuristic's, minus cost_us per inference
+    made; the best range."""
+    params = mlp.params
+    f1, dev, gain = [], [], []
+    for _, T, H, F in traversals(data):
+        c = simulate_choices(params, mlp.forward, F, H, min_frontier=0.0)
+        for L in range(len(F)):
+            f1.append(float(F[L][1]))
+            dev.append(bool(c[L] != H[L]))
+            gain.append(float(T[L, H[L]] - T[L, c[L]]))
+    f1, dev, gain = np.array(f1), np.array(dev), np.array(gain)
+    best = None
+    for lo in (0.0, 1e-4, 3e-4, 1e-3, 3e-3, 1e-2, 2e-2, 3e-2, 5e-2):
+        for hi in (0.05, 0.1, 0.2, 0.3, 0.5, 1.0):
+            if hi <= lo:
+                continue
+            sel = (f1 >= lo) & (f1 <= hi)
+            net = gain[sel & dev].sum() - cost_us * sel.sum()
+            if best is None or net > best[0]:
+                best = (net, lo, hi)
+    return (best[1], best[2])
 
 
 def level_weights(Y: np.ndarray, lo: float = 0.25, hi: float = 8.0) -> np.ndarray:
@@ -269,6 +303,7 @@ def main(argv=None) -> int:
     elif a.cmd == "train":
         data = _load(a.data)
         mlp = train(data, a.steps, a.lr)
+        mlp.frontier_range = frontier_range(mlp, data)
         mlp.graph_range = graph_range(mlp, data)
         rep = evaluate(mlp, data)
         mlp.save(a.model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))

@@ -64,6 +64,13 @@ def test_mixed_results_equal_alone(sg, graphs):
         want = cache[key]
         assert np.array_equal(out.array.view(np.uint32), want.view(np.uint32)), key
         assert r["end_ns"] >= r["start_ns"] >= r["submit_ns"]
+    # launches of different slots were in flight together: a query's launch
+    # is (start_ns, end_ns) -- the queries of one batched launch share it --
+    # and some two launches overlap in time
+    launches = sorted({(r["start_ns"], r["end_ns"]) for r in res})
+    assert len(launches) > 1
+    overlapping = sum(1 for (s0, e0), (s1, e1) in zip(launches, launches[1:]) if s1 < e0)
+    assert overlapping > 0, launches[:8]
 
 
 def test_tight_budget_evicts_and_still_matches(sg, graphs):
