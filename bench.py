@@ -244,6 +244,28 @@ def _launch_ms(torch, fn) -> float:
     return a.elapsed_time(b)
 
 
+def _alternating_ms(torch, runs, sources, reps: int = 6):
+    """Median device time per launch of each of `runs` (functions of a
+    source that enqueue one launch), their launches alternating back to back
+    on the current stream, each between two CUDA events, with one host wait
+    at the end: every mode sees the same clocks and caches."""
+    times = [[] for _ in runs]
+    for rep in range(reps + 1):  # the first round warms up
+        pairs = []
+        for s in sources:
+            for k, run in enumerate(runs):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                run(int(s))
+                b.record()
+                pairs.append((k, a, b))
+        torch.cuda.synchronize()
+        if rep:
+            for k, a, b in pairs:
+                times[k].append(a.elapsed_time(b))
+    return [float(np.median(t)) for t in times]
+
+
 def cpu_baseline(g, srcs):
     """The oracle's OpenMP frontier BFS on the host cores over a bounded
     sample of the bench's sources (about 15 s); returns the baseline object
@@ -580,18 +602,27 @@ def main():
     from sygraph_b200 import selector
     mlp = selector.Mlp.load()
     learned = {"model": "sygraph_b200/models/selector_b200.npz"}
-    bfs.set_selector(mlp)
-    learned_ms = float(np.mean([_launch_ms(torch, lambda s=s: (bfs.init(int(s)), bfs.run_async(3, ALPHA, BETA)))
-                                for s in srcs]))
-    learned.update({"rmat_launch_ms": learned_ms, "rmat_heuristic_launch_ms": kern_ms,
-                    "rmat_speedup_vs_heuristic": kern_ms / learned_ms})
+    bl = sg.algorithms.BFS(G)
+    bl.set_selector(mlp)
+    rm_h, rm_l = _alternating_ms(torch, [lambda s: (bfs.init(s), bfs.run_async(2, ALPHA, BETA)),
+                                         lambda s: (bl.init(s), bl.run_async(3, ALPHA, BETA))], srcs)
+    same_rmat = True
+    for s in srcs[:8]:
+        bfs.init(int(s))
+        bfs.run(2, ALPHA, BETA)
+        bl.init(int(s))
+        bl.run(3, ALPHA, BETA)
+        same_rmat &= bool(np.array_equal(bfs.getDistances(), bl.getDistances()))
+    del bl
+    learned.update({"rmat_launch_ms": rm_l, "rmat_heuristic_launch_ms": rm_h,
+                    "rmat_speedup_vs_heuristic": rm_h / rm_l, "timing": "median per launch, the two modes "
+                    "alternating back to back on one stream (6 rounds of the 64 sources)"})
     gg = sg.io.grid(4096, long_range_frac=0.02, seed=103)
     Gg = sg.graph.build.fromCSR(gg)
     bg = sg.algorithms.BFS(Gg)
     bg.set_selector(mlp)
     gsrc = sg.io.sample_sources(gg, 4, seed=SOURCE_SEED)
-    same = True
-    t_h, t_l = [], []
+    same = same_rmat
     for s in gsrc:
         bg.init(int(s))
         bg.run(2, ALPHA, BETA)
@@ -599,13 +630,10 @@ def main():
         bg.init(int(s))
         bg.run(3, ALPHA, BETA)
         same &= bool(np.array_equal(d_h, bg.getDistances()))
-        for _ in range(3):
-            t_h.append(_launch_ms(torch, lambda s=s: (bg.init(int(s)), bg.run_async(2, ALPHA, BETA))))
-            t_l.append(_launch_ms(torch, lambda s=s: (bg.init(int(s)), bg.run_async(3, ALPHA, BETA))))
-    learned.update({"grid4096_heuristic_ms": float(np.median(t_h)), "grid4096_learned_ms": float(np.median(t_l)),
-                    "grid4096_speedup_vs_heuristic": float(np.median(t_h) / np.median(t_l)),
-                    "identical_depths": same})
-    bfs.set_selector(None)
+    g_h, g_l = _alternating_ms(torch, [lambda s: (bg.init(s), bg.run_async(2, ALPHA, BETA)),
+                                       lambda s: (bg.init(s), bg.run_async(3, ALPHA, BETA))], gsrc)
+    learned.update({"grid4096_heuristic_ms": g_h, "grid4096_learned_ms": g_l,
+                    "grid4096_speedup_vs_heuristic": g_h / g_l, "identical_depths": same})
     del bg, Gg, gg
 
     # the same 64 sources as one bit-parallel batch (one launch); identical
