@@ -94,31 +94,33 @@ __device__ __forceinline__ void mlp_stage_async(const MlpStaged* __restrict__ im
 // thread reads the staged parameters.
 __device__ __forceinline__ void mlp_stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Forward pass by one full warp: lane j computes hidden unit j; the hidden
-// activations go through `scratch` (64 floats of shared memory) so that every
-// lane reads them with independent broadcast loads, and lanes 0-5 compute the
-// six outputs.  Returns, in every lane, the strategy with the smallest
-// predicted time among the set bits of `allowed` (lowest index on ties) --
-// unless `fallback` (the heuristic's choice, when allowed) is predicted within
-// `margin` of it in log-time, which keeps the fallback -- or -1 when a
-// feature lies outside the trusted range.
-__device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const float* f, uint32_t allowed,
-                                          float* scratch, int fallback = -1, float margin = 0.f) {
+// Forward pass by one full warp, laid out for latency (it sits between a grid
+// barrier and the next level): lane i < 12 holds feature i and checks and
+// standardises it; lane j computes hidden unit j of both hidden layers (the
+// inputs of layer 1 come by shuffles, the layer-1 activations through
+// `scratch`, 32 floats of shared memory); the six outputs are butterfly sums
+// over the lanes, so every lane ends with all six and picks locally.  Returns
+// the strategy with the smallest predicted time among the set bits of
+// `allowed` (lowest index on ties) -- unless `fallback` (the heuristic's
+// choice, when allowed) is predicted within `margin` of it in log-time, which
+// keeps the fallback -- or -1 when a feature lies outside the trusted range.
+// Lanes may differ in the last bit of an output (each sums in its own order);
+// callers take lane 0's answer, which is the same in every CTA.
+__device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, float f, uint32_t allowed, float* scratch,
+                                          int fallback = -1, float margin = 0.f) {
+  constexpr uint32_t kAll = 0xffffffffu;
   const uint32_t lane = threadIdx.x & 31;
-  bool out_of_range = false;
-  float x[kMlpIn];
-#pragma unroll
-  for (int i = 0; i < kMlpIn; i++) {
-    out_of_range |= f[i] < P->lo[i] || f[i] > P->hi[i];
-    x[i] = (f[i] - P->mean[i]) * P->inv_std[i];
-  }
-  if (out_of_range) return -1;
-  // independent partial sums break the dependent FMA chains
+  const bool mine = lane < (uint32_t)kMlpIn;
+  const uint32_t li = mine ? lane : 0u;
+  const bool out_of_range = mine && (f < P->lo[li] || f > P->hi[li]);
+  if (__any_sync(kAll, out_of_range)) return -1;
+  const float x = mine ? (f - P->mean[li]) * P->inv_std[li] : 0.f;
+  // layer 1; independent partial sums break the dependent FMA chains
   float a0 = P->b1[lane], a1 = 0.f;
 #pragma unroll
   for (int i = 0; i < kMlpIn; i += 2) {
-    a0 += P->w1t[i][lane] * x[i];
-    a1 += P->w1t[i + 1][lane] * x[i + 1];
+    a0 += P->w1t[i][lane] * __shfl_sync(kAll, x, i);
+    a1 += P->w1t[i + 1][lane] * __shfl_sync(kAll, x, i + 1);
   }
   const float h1 = a0 + a1;
   scratch[lane] = h1 > 0.f ? h1 : 0.f;
@@ -129,34 +131,28 @@ __device__ __forceinline__ int mlp_choose(const MlpStaged* __restrict__ P, const
 #pragma unroll
     for (int k = 0; k < 4; k++) c[k] += P->w2t[i + k][lane] * scratch[i + k];
   const float h2 = (c[0] + c[1]) + (c[2] + c[3]);
-  scratch[kMlpHidden + lane] = h2 > 0.f ? h2 : 0.f;
-  __syncwarp();
-  float y = 3.4e38f;
-  if (lane < (uint32_t)kMlpOut) {
-    float d[4] = {P->b3[lane], 0.f, 0.f, 0.f};
+  const float r2 = h2 > 0.f ? h2 : 0.f;
+  __syncwarp();  // scratch is rewritten by the next call
+  // layer 3: the products of this lane's hidden unit, summed over the warp
+  float y[kMlpOut];
 #pragma unroll
-    for (int i = 0; i < kMlpHidden; i += 4)
+  for (int o = 0; o < kMlpOut; o++) y[o] = P->w3[o][lane] * r2;
 #pragma unroll
-      for (int k = 0; k < 4; k++) d[k] += P->w3[lane][i + k] * scratch[kMlpHidden + i + k];
-    y = (d[0] + d[1]) + (d[2] + d[3]);
-  }
-  __syncwarp();
-  const float y_fallback = __shfl_sync(0xffffffffu, y, fallback >= 0 ? fallback : 0);
-  // argmin over lanes 0-7 (the six outputs; the others hold +inf)
-  float best = (lane < (uint32_t)kMlpOut && ((allowed >> lane) & 1u)) ? y : 3.4e38f;
-  int arg = best < 3.4e38f ? (int)lane : 32;
+  for (int d = 16; d > 0; d >>= 1)
 #pragma unroll
-  for (int dd = 4; dd > 0; dd >>= 1) {
-    const float ob = __shfl_xor_sync(0xffffffffu, best, dd);
-    const int oa = __shfl_xor_sync(0xffffffffu, arg, dd);
-    if (ob < best || (ob == best && oa < arg)) {
-      best = ob;
-      arg = oa;
+    for (int o = 0; o < kMlpOut; o++) y[o] += __shfl_xor_sync(kAll, y[o], d);
+  float best = 3.4e38f, y_fallback = 3.4e38f;
+  int arg = -1;
+#pragma unroll
+  for (int o = 0; o < kMlpOut; o++) {
+    y[o] += P->b3[o];
+    if (((allowed >> o) & 1u) && y[o] < best) {
+      best = y[o];
+      arg = o;
     }
+    if (o == fallback) y_fallback = y[o];
   }
-  best = __shfl_sync(0xffffffffu, best, 0);
-  arg = __shfl_sync(0xffffffffu, arg, 0);
-  if (arg >= kMlpOut) return -1;
+  if (arg < 0) return -1;
   if (fallback >= 0 && ((allowed >> fallback) & 1u) && y_fallback - best <= margin) arg = fallback;
   return arg;
 }

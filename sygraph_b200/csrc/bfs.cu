@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kBfsThreads, 2) bfs_kernel(Params P) {
     S.hn = 0;
     S.acc[0] = S.acc[1] = 0ull;
   }
-  if (threadIdx.x == 0) S.fk = feature_const(P);
+  if (threadIdx.x == 0) S.fk = feature_const(P.n, P.m, P.w0, P.w1);
   if (learned) sygraph::detail::mlp_stage_wait();
   if (!grid_sync(P.bar)) return;
 

@@ -8,6 +8,7 @@
 #pragma once
 
 #include "engine_common.cuh"
+#include "selector_features.cuh"
 #include "sygraph/detail/selector_mlp.cuh"
 
 namespace sgb {
@@ -72,13 +73,6 @@ struct Params {
   float* features;                        // optional log: 12 floats per level decision
 };
 
-// Per-launch constants of the features (reciprocals and logarithms of the
-// graph's sizes), computed once so a level's features need no division by
-// them.
-struct FeatureConst {
-  float inv_log_n, inv_n, inv_log_m, inv_m, inv_w0, inv_sw1, f9;
-};
-
 struct Shared {
   uint32_t pull_found[kBfsThreads / 32][32];  // ranked pull: hits per owned word, per warp
   uint32_t scan[32];
@@ -93,7 +87,7 @@ struct Shared {
   uint32_t flag[kBfsThreads];
   int choice;
   sygraph::detail::MlpStaged mlp;  // learned mode: parameters staged once per launch
-  float mlp_scratch[2 * sygraph::detail::kMlpHidden];
+  float mlp_scratch[sygraph::detail::kMlpHidden];
   FeatureConst fk;  // set once per launch
 };
 
@@ -206,43 +200,6 @@ __device__ __forceinline__ void block_sum4(unsigned long long v[4], Shared& S) {
   __syncthreads();
 }
 
-// The twelve selector features of the frontier about to be expanded.
-struct FeatureInputs {
-  double ns;     // frontier size
-  double nd;     // frontier degree sum
-  double ud;     // unexplored degree (unvisited vertices)
-  double vis;    // visited vertices
-  double prev;   // previous frontier size
-  int cur_pull;  // direction of the level that produced this frontier
-};
-
-__device__ __forceinline__ FeatureConst feature_const(const Params& P) {
-  const float n = (float)P.n, m = (float)(P.m ? P.m : 1);
-  return FeatureConst{1.f / log2f(1.f + n), 1.f / n, 1.f / log2f(1.f + m), 1.f / m, 1.f / (float)P.w0,
-                      1.f / (32.f * (float)P.w1), log2f(1.f + m / n) / 8.f};
-}
-
-__device__ __forceinline__ void compute_features(const Params& P, const FeatureConst& k, const FeatureInputs& x,
-                                                 float f[12]) {
-  const float ns = (float)x.ns, nd = (float)x.nd;
-  const float lns = log2f(1.f + ns);
-  f[0] = lns * k.inv_log_n;
-  f[1] = ns * k.inv_n;
-  f[2] = log2f(1.f + nd) * k.inv_log_m;
-  f[3] = nd * k.inv_m;
-  f[4] = (float)x.ud * k.inv_m;
-  f[5] = ((float)P.n - (float)x.vis) * k.inv_n;
-  // expected occupancy of the frontier bitmap and of its summary for a
-  // frontier of this size spread at random (the words are not counted: that
-  // would make every bitmap atomic wait for its old value)
-  f[6] = 1.f - expf(-ns * k.inv_w0);
-  f[7] = 1.f - expf(-ns * k.inv_sw1);
-  f[8] = log2f(1.f + nd / fmaxf(1.f, ns)) / 16.f;
-  f[9] = k.f9;
-  f[10] = x.cur_pull ? 1.f : 0.f;
-  f[11] = fminf(16.f, fmaxf(-16.f, lns - log2f(1.f + (float)x.prev))) / 16.f;
-}
-
 // Strategy of the next level, identical in every CTA (same inputs, same
 // arithmetic).  Heuristic: BFS::evaluateHeuristic (bfs.hpp:325-350), with the
 // reference's float arithmetic; the learned mode asks the MLP (warp 0) and
@@ -260,21 +217,21 @@ __device__ __forceinline__ int decide(const Params& P, Shared& S, int cur, const
   }
   int h = P.mode == SG_BFS_PUSH ? 0 : P.mode == SG_BFS_PULL ? 2 : (pull ? 2 : 0);
   const bool log = P.features && blockIdx.x == 0 && level < kMaxLog;
-  // frontiers outside [min_frontier, max_frontier] * n keep the heuristic's
-  // choice without an inference when that choice is allowed: there the model
-  // rarely overrules the heuristic (the range is chosen on the training
-  // tables, gain of the model's choices against the cost of the inferences),
-  // and the inference is a latency of about a microsecond on every level's
-  // critical path
+  // The model is asked where the heuristic would switch direction, on a
+  // frontier inside [min_frontier, max_frontier] * n, and wherever the
+  // heuristic's choice is not allowed.  An inference is a latency of about a
+  // microsecond on the critical path between two levels; away from the
+  // switch points the model rarely overrules the heuristic, and the
+  // frontier range is the one where, on the training tables, its choices
+  // saved more than its inferences cost.
   const bool infer = P.mode == kLearned && P.mlp &&
-                     (((float)x.ns >= P.min_frontier * (float)P.n && (float)x.ns <= P.max_frontier * (float)P.n) ||
+                     ((((h >= 2) != cur_pull) && (float)x.ns >= P.min_frontier * (float)P.n &&
+                       (float)x.ns <= P.max_frontier * (float)P.n) ||
                       !((P.allowed >> h) & 1u));
   if (infer || log) {
     if (threadIdx.x < 32) {
-      float f[12];
-      compute_features(P, S.fk, x, f);
-      if (log && threadIdx.x == 0)
-        for (int i = 0; i < 12; i++) P.features[(size_t)level * 12 + i] = f[i];
+      const float f = feature_of_lane(threadIdx.x, P.n, S.fk, x);
+      if (log && threadIdx.x < 12) P.features[(size_t)level * 12 + threadIdx.x] = f;
       if (infer) {
         const int c = sygraph::detail::mlp_choose(&S.mlp, f, P.allowed, S.mlp_scratch, h, P.margin);
         if (threadIdx.x == 0) S.choice = c;

@@ -33,10 +33,13 @@ MARGIN = 0.05
 # the engine skips the inference on frontiers below this fraction of n (the
 # heuristic's choice stands there), as kLearnedMinFrontier in the engine
 MIN_FRONTIER = 1e-3
-# device time of one inference between two levels (features, three layers,
-# the block barrier that publishes the choice), measured from the level
-# timestamps; the consulted frontier range trades it against the model's gains
-INFERENCE_US = 1.25
+# device time one inference adds between two levels (features, three layers,
+# the block barrier that publishes the choice, and the slower start of the
+# level after it), measured from the level timestamps of RMAT-22 traversals:
+# the gap before a consulted level grows by about 1.7 us, the next one by
+# about 0.5 us; the consulted frontier and graph ranges trade it against the
+# model's gains
+INFERENCE_US = 2.2
 MAX_LEVELS = 4096
 
 # (name, generator, kwargs): RMAT skews and scales, grids with and without
@@ -150,96 +153,141 @@ def traversals(data: dict):
         yield str(data["names"][i]), data["T"][a:b], data["H"][a:b], data["F0"][a:b]
 
 
+def heuristic_choice(f, cur: int, alpha: float = HYBRID_ALPHA, beta: float = HYBRID_BETA) -> int:
+    """The reference heuristic (bfs.hpp:325-350) from a level's features and
+    the direction `cur` of the level just run: push turns to pull when the
+    frontier's degree exceeds the unexplored degree / alpha (features 3 and
+    4), pull returns to push below n / beta vertices (feature 1)."""
+    if cur < 2:
+        return 2 if f[3] > f[4] / alpha else 0
+    return 0 if f[1] < 1.0 / beta else 2
+
+
 def simulate_choices(params: np.ndarray, forward, F: np.ndarray, heuristic: np.ndarray,
                      allowed: int = 0x3F, margin: float = MARGIN, min_frontier: float = MIN_FRONTIER,
-                     graph_range=None, max_frontier: float = 1.0) -> np.ndarray:
-    """The learned mode's schedule on a traversal: the MLP's argmin per level
-    (`forward` maps a feature batch to predicted log-times) with the
-    current-direction feature following its own previous choice, and the
-    heuristic where a feature leaves the trusted range or the frontier is
-    below `min_frontier` of the vertices, as the engine does; on a graph
-    whose mean-degree feature (9) is outside `graph_range` the heuristic
-    decides every level."""
-    if graph_range is not None and len(F) and not (graph_range[0] <= F[0][9] <= graph_range[1]):
-        return np.asarray(heuristic, np.int32).copy()
+                     graph_range=None, max_frontier: float = 1.0, alpha: float = HYBRID_ALPHA,
+                     beta: float = HYBRID_BETA) -> np.ndarray:
+    """The learned mode's schedule on a traversal, as the engine makes it:
+    after each level the heuristic's choice given the direction actually run
+    (level 0: the recorded one); the MLP (`forward` maps a feature batch to
+    predicted log-times; the current-direction feature follows the schedule)
+    is asked only where that choice switches direction, the frontier lies in
+    [min_frontier, max_frontier] of the vertices and every feature in the
+    trusted range, and overrules the heuristic when it predicts the
+    heuristic's choice more than `margin` slower; on a graph whose
+    mean-degree feature (9) is outside `graph_range` the heuristic decides
+    every level."""
     t0 = params.size - 4 * IN
     lo, hi = params[t0 + 2 * IN:t0 + 3 * IN], params[t0 + 3 * IN:t0 + 4 * IN]
     banned = [j for j in range(OUT) if not (allowed >> j) & 1]
+    use_model = graph_range is None or not len(F) or graph_range[0] <= F[0][9] <= graph_range[1]
     out = np.empty(len(F), np.int32)
     prev = 0
     for L in range(len(F)):
         f = np.array(F[L], np.float32)
         if L > 0:
             f[10] = 1.0 if prev >= 2 else 0.0
-        if f[1] < min_frontier or f[1] > max_frontier or np.any(f < lo) or np.any(f > hi):
-            out[L] = heuristic[L]
+        h = int(heuristic[0]) if L == 0 else heuristic_choice(F[L], prev, alpha, beta)
+        switch = L > 0 and (h >= 2) != (prev >= 2)
+        if (not use_model or not switch or f[1] < min_frontier or f[1] > max_frontier or np.any(f < lo)
+                or np.any(f > hi)):
+            out[L] = h
         else:
             y = np.array(forward(f[None, :]), np.float64)[0]
             y[banned] = np.inf
-            best, h = int(np.argmin(y)), int(heuristic[L])
+            best = int(np.argmin(y))
             out[L] = h if np.isfinite(y[h]) and y[h] - y[best] <= margin else best
         prev = out[L]
     return out
 
 
-def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F) -> dict:
+def heuristic_along(F, H, c, alpha: float = HYBRID_ALPHA, beta: float = HYBRID_BETA) -> np.ndarray:
+    """The heuristic's choice at each level given the schedule `c` run so far."""
+    return np.array([int(H[0]) if L == 0 else heuristic_choice(F[L], int(c[L - 1]), alpha, beta)
+                     for L in range(len(F))], np.int32)
+
+
+def consulted(F, c, lo: float, hi: float, alpha: float = HYBRID_ALPHA, beta: float = HYBRID_BETA) -> np.ndarray:
+    """Levels at which the engine asks the model along schedule `c`: the
+    heuristic switches direction there and the frontier is inside [lo, hi]."""
+    h = heuristic_along(F, np.zeros(len(F), np.int32), c, alpha, beta)
+    return np.array([L > 0 and (h[L] >= 2) != (c[L - 1] >= 2) and lo <= F[L][1] <= hi
+                     for L in range(len(F))], bool)
+
+
+def evaluate(mlp: Mlp, data: dict, allowed: int = 0x3F, alpha: float = HYBRID_ALPHA,
+             beta: float = HYBRID_BETA, cost_us: float = 0.0) -> dict:
     """Summed level time (us) per traversal under the heuristic's schedule,
-    the MLP's schedule and the per-level best; totals and regret."""
+    the MLP's schedule (plus cost_us per inference it makes) and the
+    per-level best; totals and regret."""
     rows = []
     params = mlp.params
     fr = mlp.frontier_range or (MIN_FRONTIER, 1.0)
+    g = mlp.graph_range
     for name, T, H, F in traversals(data):
-        c = simulate_choices(params, mlp.forward, F, H, allowed, graph_range=mlp.graph_range,
-                             min_frontier=fr[0], max_frontier=fr[1])
+        c = simulate_choices(params, mlp.forward, F, H, allowed, graph_range=g, min_frontier=fr[0],
+                             max_frontier=fr[1], alpha=alpha, beta=beta)
+        use = g is None or not len(F) or g[0] <= F[0][9] <= g[1]
+        asked = int(consulted(F, c, fr[0], fr[1], alpha, beta).sum()) if use else 0
         idx = np.arange(len(T))
         rows.append({"traversal": name, "levels": len(T), "heuristic_us": float(T[idx, H].sum()),
-                     "learned_us": float(T[idx, c].sum()), "best_us": float(T.min(1).sum()),
-                     "learned_schedule": "".join(map(str, c)), "heuristic_schedule": "".join(map(str, H))})
-    tot = {k: sum(r[k] for r in rows) for k in ("heuristic_us", "learned_us", "best_us")}
+                     "learned_us": float(T[idx, c].sum()) + cost_us * asked, "best_us": float(T.min(1).sum()),
+                     "inferences": asked, "learned_schedule": "".join(map(str, c)),
+                     "heuristic_schedule": "".join(map(str, H))})
+    tot = {k: sum(r[k] for r in rows) for k in ("heuristic_us", "learned_us", "best_us", "inferences")}
     tot["speedup_vs_heuristic"] = tot["heuristic_us"] / max(tot["learned_us"], 1e-9)
     tot["regret_learned"] = tot["learned_us"] / max(tot["best_us"], 1e-9) - 1.0
     tot["regret_heuristic"] = tot["heuristic_us"] / max(tot["best_us"], 1e-9) - 1.0
     return {"total": tot, "traversals": rows}
 
 
-def graph_range(mlp: Mlp, data: dict, widen: float = 0.05):
-    """The range of the mean-degree feature (9, constant per graph) over the
-    training traversals on which the model overrules the heuristic at least
-    once, widened by `widen`: the engine consults the model only there, so
-    graphs on which it only ever agreed with the heuristic pay no inference.
-    (1, 0), an empty range, when it never overrules it."""
-    params = mlp.params
-    fr = getattr(mlp, "frontier_range", None) or (MIN_FRONTIER, 1.0)
-    f9 = [float(F[0][9]) for _, _, H, F in traversals(data)
-          if len(F) and np.any(simulate_choices(params, mlp.forward, F, H, min_frontier=fr[0],
-                                                max_frontier=fr[1]) != H)]
-    return (min(f9) - widen, max(f9) + widen) if f9 else (1.0, 0.0)
+def _net_gain(params, forward, T, H, F, lo, hi, allowed, alpha, beta, cost_us) -> float:
+    """Time the model's schedule saves on one traversal against the
+    heuristic's, minus cost_us per inference."""
+    c = simulate_choices(params, forward, F, H, allowed, min_frontier=lo, max_frontier=hi, alpha=alpha, beta=beta)
+    h = heuristic_along(F, H, c, alpha, beta)
+    idx = np.arange(len(T))
+    return float((T[idx, h] - T[idx, c]).sum()) - cost_us * int(consulted(F, c, lo, hi, alpha, beta).sum())
 
 
-def frontier_range(mlp: Mlp, data: dict, cost_us: float = INFERENCE_US):
+def frontier_range(mlp: Mlp, data: dict, cost_us: float = INFERENCE_US, allowed: int = 0x3F,
+                   alpha: float = HYBRID_ALPHA, beta: float = HYBRID_BETA):
     """The frontier-size range (fraction of n) on which consulting the model
     pays on the training traversals: over a grid of bounds, the summed time
     its choices save against the heuristic's, minus cost_us per inference
     made; the best range."""
     params = mlp.params
-    f1, dev, gain = [], [], []
-    for _, T, H, F in traversals(data):
-        c = simulate_choices(params, mlp.forward, F, H, min_frontier=0.0)
-        for L in range(len(F)):
-            f1.append(float(F[L][1]))
-            dev.append(bool(c[L] != H[L]))
-            gain.append(float(T[L, H[L]] - T[L, c[L]]))
-    f1, dev, gain = np.array(f1), np.array(dev), np.array(gain)
     best = None
     for lo in (0.0, 1e-4, 3e-4, 1e-3, 3e-3, 1e-2, 2e-2, 3e-2, 5e-2):
         for hi in (0.05, 0.1, 0.2, 0.3, 0.5, 1.0):
             if hi <= lo:
                 continue
-            sel = (f1 >= lo) & (f1 <= hi)
-            net = gain[sel & dev].sum() - cost_us * sel.sum()
+            net = sum(_net_gain(params, mlp.forward, T, H, F, lo, hi, allowed, alpha, beta, cost_us)
+                      for _, T, H, F in traversals(data))
             if best is None or net > best[0]:
                 best = (net, lo, hi)
     return (best[1], best[2])
+
+
+def graph_range(mlp: Mlp, data: dict, widen: float = 0.05, cost_us: float = INFERENCE_US, allowed: int = 0x3F,
+                alpha: float = HYBRID_ALPHA, beta: float = HYBRID_BETA):
+    """The range of the mean-degree feature (9, constant per graph) over the
+    training graphs on which consulting the model pays (its schedules save
+    more than cost_us per inference, summed over the graph's traversals),
+    widened by `widen`: elsewhere the engine never asks it and stages
+    nothing.  (1, 0), an empty range, when it pays on no graph."""
+    params = mlp.params
+    fr = getattr(mlp, "frontier_range", None) or (MIN_FRONTIER, 1.0)
+    per_graph = {}
+    for name, T, H, F in traversals(data):
+        if not len(F):
+            continue
+        key = name.split(":")[0]
+        net = _net_gain(params, mlp.forward, T, H, F, fr[0], fr[1], allowed, alpha, beta, cost_us)
+        f9, tot = per_graph.get(key, (float(F[0][9]), 0.0))
+        per_graph[key] = (f9, tot + net)
+    f9 = [v[0] for v in per_graph.values() if v[1] > 0.0]
+    return (min(f9) - widen, max(f9) + widen) if f9 else (1.0, 0.0)
 
 
 def level_weights(Y: np.ndarray, lo: float = 0.25, hi: float = 8.0) -> np.ndarray:
@@ -293,10 +341,15 @@ def main(argv=None) -> int:
     t.add_argument("--model", default=str(MODEL_PATH))
     t.add_argument("--steps", type=int, default=6000)
     t.add_argument("--lr", type=float, default=3e-3)
+    r = sub.add_parser("regate", help="recompute a model's frontier and graph ranges on training tables")
+    r.add_argument("--data", required=True)
+    r.add_argument("--model", default=str(MODEL_PATH))
+    r.add_argument("--cost-us", type=float, default=INFERENCE_US)
     e = sub.add_parser("evaluate")
     e.add_argument("--data", required=True)
     e.add_argument("--model", default=str(MODEL_PATH))
     e.add_argument("--json", default=None)
+    e.add_argument("--cost-us", type=float, default=INFERENCE_US)
     a = ap.parse_args(argv)
     if a.cmd == "collect":
         _save(collect(TRAIN_GRAPHS if a.set == "train" else EVAL_GRAPHS, a.sources, a.reps), a.out)
@@ -305,11 +358,19 @@ def main(argv=None) -> int:
         mlp = train(data, a.steps, a.lr)
         mlp.frontier_range = frontier_range(mlp, data)
         mlp.graph_range = graph_range(mlp, data)
-        rep = evaluate(mlp, data)
+        rep = evaluate(mlp, data, cost_us=INFERENCE_US)
         mlp.save(a.model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
         print(json.dumps(rep["total"]))
+    elif a.cmd == "regate":
+        data = _load(a.data)
+        mlp = Mlp.load(a.model)
+        mlp.frontier_range = frontier_range(mlp, data, a.cost_us)
+        mlp.graph_range = graph_range(mlp, data, cost_us=a.cost_us)
+        rep = evaluate(mlp, data, cost_us=a.cost_us)
+        mlp.save(a.model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
+        print(json.dumps({"frontier_range": mlp.frontier_range, "graph_range": mlp.graph_range, **rep["total"]}))
     else:
-        rep = evaluate(Mlp.load(a.model), _load(a.data))
+        rep = evaluate(Mlp.load(a.model), _load(a.data), cost_us=a.cost_us)
         print(json.dumps(rep["total"]))
         if a.json:
             with open(a.json, "w") as f:

@@ -14,6 +14,9 @@ from conftest import ROOT
 
 EVAL = ROOT / "tests" / "golden" / "selector_eval_b200.npz"
 MODEL = ROOT / "sygraph_b200" / "models" / "selector_b200.npz"
+# level-time tables of the training graphs (`train_selector collect --set
+# train`, kept without the per-sample arrays: T, H, F0, offsets, names)
+TRAIN_TABLES = ROOT / "tests" / "golden" / "selector_train_tables_b200.npz"
 
 
 @pytest.fixture(scope="module")
@@ -84,3 +87,38 @@ def test_regret_bookkeeping_matches_tables(tables):
         assert T.shape[1] == 6 and len(H) == len(T) == len(F)
         assert set(np.unique(H)) <= {0, 2}
         assert np.all(T > 0)
+
+
+class _CpuModel:
+    """The committed parameters with the FP64 oracle forward pass, in the
+    shape the trainer's gate functions read."""
+
+    def __init__(self, params, graph_range=None, frontier_range=None):
+        self.params = params
+        self.graph_range = graph_range
+        self.frontier_range = frontier_range
+
+    def forward(self, X):
+        from oracle import mlp as omlp
+        return omlp.forward(self.params.astype(np.float64), np.asarray(X, np.float64))[0]
+
+
+def test_gates_follow_from_training_tables(tables):
+    """The committed frontier and graph ranges are the ones the trainer
+    derives from the training tables at the measured inference cost: the
+    model is consulted on the grids with long-range pairs, where its choices
+    save more than the inferences cost, and on no RMAT graph, where the
+    heuristic's switch points were already as good."""
+    ts, _, params, gates = tables
+    with np.load(TRAIN_TABLES) as d:
+        data = {k: d[k] for k in d.files}
+    m = _CpuModel(params)
+    fr = ts.frontier_range(m, data)
+    m.frontier_range = fr
+    gr = ts.graph_range(m, data)
+    assert np.allclose(fr, gates["frontier_range"], atol=1e-6), (fr, gates)
+    assert np.allclose(gr, gates["graph_range"], atol=1e-6), (gr, gates)
+    lo, hi = gr
+    f9 = {str(n).split(":")[0]: float(F[0][9]) for n, _, _, F in ts.traversals(data)}
+    assert all(lo <= v <= hi for k, v in f9.items() if k.startswith("grid") and k != "grid512")
+    assert not any(lo <= v <= hi for k, v in f9.items() if k.startswith(("rmat", "uniform")))

@@ -110,15 +110,35 @@ def _trusting_mlp(selector, seed):
     return m
 
 
+def _heuristic_levels(recs, n, alpha, beta):
+    """The reference heuristic's choice (0 push, 2 pull) for every level, from
+    the level records of the run and the strategy each level actually took,
+    in the engine's float arithmetic (bfs.hpp:325-350)."""
+    f32 = np.float32
+    out = [0]  # level 0 starts in push
+    for prev in recs[:-1]:
+        if prev["strategy"] < 2:
+            pull = f32(np.uint32(prev["next_degree"] & 0xFFFFFFFF)) > \
+                f32(np.uint32(prev["unexplored_degree"] & 0xFFFFFFFF)) / f32(alpha)
+        else:
+            pull = not f32(prev["next_size"]) < f32(n) / f32(beta)
+        out.append(2 if pull else 0)
+    return out
+
+
 def test_learned_mode_parity_and_mask(sg, oracle, graphs):
+    """The model is asked where the heuristic switches direction and where
+    the heuristic's choice is not allowed; there the device takes the MLP's
+    argmin over the allowed strategies, elsewhere the heuristic's choice."""
     from sygraph_b200 import selector
+    asked = 0
     for name in ("rmat14", "grid", "star"):
         g = graphs[name]
         G = sg.graph.build.fromCSR(g)
         bfs = sg.algorithms.BFS(G)
         for seed, allowed in ((1, 0x3F), (2, 0x03), (3, 0x0C), (4, 0x30), (5, 0x21)):
             m = _trusting_mlp(selector, seed)
-            bfs.set_selector(m, allowed, margin=0.0, min_frontier=0.0)  # plain argmin on every level, checked below
+            bfs.set_selector(m, allowed, margin=0.0, min_frontier=0.0)  # plain argmin where asked
             bfs.log_features(True)
             for s in _sources(sg, g)[:2]:
                 bfs.init(s)
@@ -128,13 +148,21 @@ def test_learned_mode_parity_and_mask(sg, oracle, graphs):
                 assert all((allowed >> r["strategy"]) & 1 for r in recs)
                 F = bfs.level_features()
                 assert F.shape == (det.iterations, 12) and np.all(np.isfinite(F))
-                # the device's choice is the MLP's argmin on the logged features
-                # (up to float summation order between the two forward passes)
+                got = np.array([r["strategy"] for r in recs])
+                heur = np.array(_heuristic_levels(recs, g.n, 15.0, 24.0))
+                cur = np.concatenate([[0], got[:-1]])
+                ask = np.array([(h >= 2) != (c >= 2) or not (allowed >> int(h)) & 1 for h, c in zip(heur, cur)])
+                assert np.array_equal(got[~ask], heur[~ask]), (name, seed, s)
+                # where asked, the device's choice is the MLP's argmin on the
+                # logged features (up to float summation order between the two
+                # forward passes)
                 y = m.forward(F)
                 y[:, [j for j in range(6) if not (allowed >> j) & 1]] = np.inf
-                got = np.array([r["strategy"] for r in recs])
                 best = y.min(1)
-                assert np.all(y[np.arange(len(got)), got] <= best + 1e-4 * (1 + np.abs(best)))
+                ok = y[np.arange(len(got)), got] <= best + 1e-4 * (1 + np.abs(best))
+                assert np.all(ok[ask]), (name, seed, s)
+                asked += int(ask.sum())
+    assert asked >= 30
 
 
 def test_learned_mode_small_frontiers_keep_the_heuristic(sg, oracle, rmat):
