@@ -430,6 +430,25 @@ sg_status sg_mlp_gradient(sg_mlp h, const float* dev_x, const float* dev_t, cons
 sg_status sg_mlp_train(sg_mlp h, const float* dev_x, const float* dev_t, const float* dev_mask, uint32_t n,
                        uint32_t steps, float lr, float weight_decay, float* host_final_loss);
 
+/* Scheduling controls of the batched BFS (no counterpart in the reference,
+ * whose batch of traversals does not exist; none changes any depth):
+ *   sg_msbfs_set_schedule  forces the direction of level i (0 push, 2 pull,
+ *                          -1 the mode decides) for i < len; len 0 clears it
+ *   sg_msbfs_set_selector  the MLP of SG_BFS_LEARNED (NULL detaches it): it
+ *                          is asked, between push/warp and pull/warp, where
+ *                          the hybrid heuristic would switch direction on a
+ *                          frontier of min_frontier..max_frontier * n vertices,
+ *                          and overrules the heuristic when it predicts the
+ *                          heuristic's choice `margin` slower in log-time
+ *   sg_msbfs_log_features  records the twelve selector features of each
+ *                          level decision (frontier = the union over the
+ *                          sources, visited = vertices every source reached);
+ *                          sg_msbfs_level_features reads them. */
+sg_status sg_msbfs_set_schedule(sg_msbfs h, const int* host_directions, uint32_t len);
+sg_status sg_msbfs_set_selector(sg_msbfs h, sg_mlp mlp, float margin, float min_frontier, float max_frontier);
+sg_status sg_msbfs_log_features(sg_msbfs h, int enable);
+sg_status sg_msbfs_level_features(sg_msbfs h, float* host_features, uint32_t cap_levels, uint32_t* count);
+
 /* Scheduling controls of the fused BFS engine (no counterpart in the
  * reference; none changes any depth):
  *   sg_bfs_set_schedule  forces the strategy of level i (SG_STRATEGY_*, or -1

@@ -169,6 +169,36 @@ class MultiBFS:
     def set_launch(self, max_ctas: int = 0, stream=None) -> None:
         call("sg_msbfs_set_launch", self.handle, stream, int(max_ctas))
 
+    def set_schedule(self, directions) -> None:
+        """Forced direction per level (0 push, 2 pull, -1 the mode decides);
+        an empty sequence clears it."""
+        d = np.ascontiguousarray(list(directions), np.int32)
+        call("sg_msbfs_set_schedule", self.handle, d.ctypes.data_as(C.POINTER(C.c_int)) if d.size else None, d.size)
+
+    def set_selector(self, mlp, margin: float = 0.05) -> None:
+        """The MLP of bfs_direction.learned (None detaches it), asked where
+        the heuristic would switch direction on frontiers inside the model's
+        frontier range (mlp.frontier_range, else every size); `margin` is the
+        predicted log-time gain it needs to overrule the heuristic."""
+        self._mlp = mlp  # keep the device parameters alive
+        fr = getattr(mlp, "frontier_range", None) if mlp is not None else None
+        lo, hi = fr if fr is not None else (0.0, 1.0)
+        call("sg_msbfs_set_selector", self.handle, mlp.handle if mlp is not None else None, float(margin),
+             float(lo), float(hi))
+
+    def log_features(self, enable: bool = True) -> None:
+        call("sg_msbfs_log_features", self.handle, int(enable))
+
+    def level_features(self) -> np.ndarray:
+        out = np.zeros((_lib.SG_MAX_LOGGED_LEVELS, 12), np.float32)
+        cnt = C.c_uint32()
+        call("sg_msbfs_level_features", self.handle, out.ctypes.data_as(C.POINTER(C.c_float)),
+             _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
+        return out[:cnt.value]
+
+    def level_times_us(self) -> np.ndarray:
+        return np.array([(r["t_end_ns"] - r["t_start_ns"]) / 1000.0 for r in self.level_records()])
+
     def getDistances(self) -> np.ndarray:
         """k x n depths (row s: depths from sources[s])."""
         out = np.empty((self.k, self.G.getVertexCount()), np.uint32)

@@ -28,6 +28,8 @@
 #include <vector>
 
 #include "engine_common.cuh"
+#include "selector_features.cuh"
+#include "sygraph/detail/selector_mlp.cuh"
 
 namespace sgb {
 namespace ms {
@@ -53,7 +55,7 @@ struct LevelCounters {
   u64 reached_edges; // sum over (source, newly reached vertex) of the vertex degree
   u64 done_deg;      // degree of vertices every source reached at this level
   uint32_t grab[kGrabDomains];  // words handed out by each domain's counter
-  u64 pad[1];
+  u64 done_count;    // vertices every source reached at this level
 };
 
 // Each warp's first word is its own (word = its warp index); the later ones
@@ -103,6 +105,13 @@ struct Params {
   uint32_t* depth;   // k * n, source-major, written after the last level
   sg_level_record* log;
   u64* result;       // [iterations, push, pull, reached_edges]
+  const int* schedule;    // optional direction per level: 0 push, 2 pull, -1 the mode decides
+  uint32_t schedule_len;
+  const sygraph::detail::MlpStaged* mlp_image;  // learned mode: the selector, staged per launch
+  float margin;           // log-time gain the MLP must predict to overrule the heuristic
+  float min_frontier;     // frontier sizes (fraction of n) the MLP is asked about
+  float max_frontier;
+  float* features;        // optional log: 12 floats per level decision
 };
 
 struct Shared {
@@ -113,6 +122,10 @@ struct Shared {
   uint32_t hd[kHeavyBuf];
   uint32_t hn;
   uint32_t base_e, base_c;
+  int choice;
+  sygraph::detail::MlpStaged mlp;  // learned mode: parameters staged once per launch
+  float mlp_scratch[sygraph::detail::kMlpHidden];
+  eng::FeatureConst fk;
 };
 
 struct Level {
@@ -126,7 +139,7 @@ struct Level {
   uint32_t* hs_next;
   uint32_t next_depth;
   uint32_t n_new = 0;
-  u64 deg_new = 0, reached = 0, done_deg = 0;
+  u64 deg_new = 0, reached = 0, done_deg = 0, done_count = 0;
 
   __device__ __forceinline__ void add_heavy(uint32_t u, uint32_t du) {
     const uint32_t i = atomicAdd(&S->hn, 1u);
@@ -151,6 +164,7 @@ struct Level {
     reached += (u64)__popcll(nw) * du;
     if ((old | nw) == P->all) {
       done_deg += du;
+      done_count++;
       atomicOr(P->done + (u >> 5), 1u << (u & 31));
     }
     if (atomicOr(F_next + u, nw) == 0) {
@@ -194,6 +208,7 @@ struct Level {
       reached += (u64)__popcll(nw[k]) * du;
       if ((old[k] | nw[k]) == P->all) {
         done_deg += du;
+        done_count++;
         atomicOr(P->done + (u[k] >> 5), 1u << (u[k] & 31));
       }
       if (fo[k] == 0) {  // first sources to reach u this level: u joins the frontier
@@ -267,6 +282,38 @@ __device__ __forceinline__ void materialise(const Params& P, const u64* F_last, 
   }
 }
 
+constexpr int kLearnedMode = SG_BFS_LEARNED;
+constexpr uint32_t kMsAllowed = (1u << 0) | (1u << 2);  // the model's push/warp and pull/warp outputs
+
+// Direction of level `level` (1 = pull), identical in every CTA (same inputs,
+// same arithmetic): a forced direction from the schedule, else in learned
+// mode the MLP's choice between push and pull where the heuristic would
+// switch direction on a frontier inside [min_frontier, max_frontier] * n
+// (warp 0 of each CTA; the heuristic's choice `h_pull` stands unless the
+// model predicts it `margin` slower in log-time, and outside the trusted
+// feature range), else the heuristic's.  Logs the features when asked.
+__device__ __forceinline__ int ms_decide(const Params& P, Shared& S, int h_pull, const eng::FeatureInputs& x,
+                                         uint32_t level) {
+  const int forced = (P.schedule && level < P.schedule_len) ? P.schedule[level] : -1;
+  const bool log = P.features && blockIdx.x == 0 && level < kMaxLog;
+  const bool infer = forced < 0 && P.mode == kLearnedMode && P.mlp_image && (h_pull != 0) != (x.cur_pull != 0) &&
+                     (float)x.ns >= P.min_frontier * (float)P.n && (float)x.ns <= P.max_frontier * (float)P.n;
+  if (infer || log) {
+    if (threadIdx.x < 32) {
+      const float f = eng::feature_of_lane(threadIdx.x, P.n, S.fk, x);
+      if (log && threadIdx.x < 12) P.features[(size_t)level * 12 + threadIdx.x] = f;
+      if (infer) {
+        const int c = sygraph::detail::mlp_choose(&S.mlp, f, kMsAllowed, S.mlp_scratch, h_pull ? 2 : 0, P.margin);
+        if (threadIdx.x == 0) S.choice = c;
+      }
+    }
+    __syncthreads();  // S.choice is written again only after the next grid barrier
+  }
+  if (forced >= 0) return forced >= 2;
+  if (infer && S.choice >= 0) return S.choice >= 2;
+  return h_pull;
+}
+
 __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
   __shared__ Shared S;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,6 +321,12 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t gwarp = gtid >> 5, nwarps = nthreads >> 5;
   const uint32_t n = P.n, w0 = P.w0, w1 = P.w1;
+
+  // learned mode: the staged MLP parameters arrive by asynchronous copies
+  // while the state is cleared; the first barrier publishes them
+  const bool learned = P.mode == kLearnedMode && P.mlp_image;
+  if (learned) sygraph::detail::mlp_stage_async(P.mlp_image, &S.mlp);
+  if (threadIdx.x == 0) S.fk = eng::feature_const(n, P.m, w0, w1);
 
   // ---- clear state
   for (uint32_t i = gtid; i < n; i += nthreads) {
@@ -294,6 +347,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
     P.cnt[gtid] = z;
   }
   if (threadIdx.x == 0) S.hn = 0;
+  if (learned) sygraph::detail::mlp_stage_wait();
   if (!grid_sync(P.bar)) return;
   // ---- sources: F_0, seen, depth 0, and the level-0 heavy list
   if (gtid == 0) {
@@ -336,7 +390,14 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
     reached_total += P.ro[s + 1] - P.ro[s];
   }
   u64 n_push = 0, n_pull = 0;
+  // vertices every source has reached (the sources themselves when k == 1)
+  u64 done_total = P.k == 1 ? 1 : 0;
   int pull = P.mode == SG_BFS_PULL;
+  {
+    const eng::FeatureInputs x{(double)frontier_size, (double)frontier_deg, (double)unexplored, (double)done_total,
+                               (double)frontier_size, 0};
+    pull = ms_decide(P, S, pull, x, 0);
+  }
   uint32_t level = 0;
   for (;; level++) {
     LevelCounters* C = P.cnt + (level % 3);
@@ -485,7 +546,10 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
           L.n_new++;
           L.deg_new += du;
           L.reached += (u64)__popcll(nw) * du;
-          if ((su | nw) == P.all) L.done_deg += du;
+          if ((su | nw) == P.all) {
+            L.done_deg += du;
+            L.done_count++;
+          }
           if (du >= kHeavy) L.add_heavy(u, du);
         }
         // heavy vertices of the same word update these words by atomics too
@@ -568,11 +632,13 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
       const u64 d = block_sum<u64>(L.deg_new, S.red);
       const u64 r = block_sum<u64>(L.reached, S.red);
       const u64 dd = block_sum<u64>(L.done_deg, S.red);
+      const u64 dc = block_sum<u64>(L.done_count, S.red);
       if (threadIdx.x == 0) {
         if (c) atomicAdd(&C->new_count, c);
         if (d) atomicAdd(&C->new_deg, d);
         if (r) atomicAdd(&C->reached_edges, r);
         if (dd) atomicAdd(&C->done_deg, dd);
+        if (dc) atomicAdd(&C->done_count, dc);
       }
     }
     if (!grid_sync(P.bar)) return;
@@ -580,6 +646,7 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
     const u64 next_deg = ld_cg(&C->new_deg);
     reached_total += ld_cg(&C->reached_edges);
     unexplored -= ld_cg(&C->done_deg);
+    done_total += ld_cg(&C->done_count);
     if (gtid == 0 && level < kMaxLog) {
       sg_level_record rr;
       rr.level = level;
@@ -593,16 +660,20 @@ __global__ void __launch_bounds__(kThreads, 2) msbfs_kernel(Params P) {
       rr.t_end_ns = sygraph::detail::global_timer_ns();
       P.log[level] = rr;
     }
-    if (P.mode == SG_BFS_HYBRID) {
+    if (next_size == 0) break;
+    int h_pull = pull;
+    if (P.mode == SG_BFS_HYBRID || P.mode == kLearnedMode) {
       if (!pull) {
-        if ((float)next_deg > (float)unexplored / P.alpha) pull = 1;
+        if ((float)next_deg > (float)unexplored / P.alpha) h_pull = 1;
       } else {
-        if ((float)next_size < (float)n / P.beta) pull = 0;
+        if ((float)next_size < (float)n / P.beta) h_pull = 0;
       }
     }
+    const eng::FeatureInputs x{(double)next_size, (double)next_deg, (double)unexplored, (double)done_total,
+                               (double)frontier_size, pull};
+    pull = ms_decide(P, S, h_pull, x, level + 1);
     frontier_size = next_size;
     frontier_deg = next_deg;
-    if (next_size == 0) break;
   }
   // depths from the planes; F of the last level (depth `level`) is folded in registers
   {
@@ -661,6 +732,11 @@ struct sg_msbfs_s {
   sg_level_record* log = nullptr;
   unsigned long long* result = nullptr;
   uint32_t last_k = 0;
+  int* schedule = nullptr;  // forced direction per level (device)
+  uint32_t schedule_len = 0;
+  const void* mlp_image = nullptr;  // the selector's staged image (owned by the sg_mlp)
+  float margin = 0.05f, min_frontier = 0.f, max_frontier = 1.f;
+  float* features = nullptr;  // feature log, 12 floats per level
 };
 
 static void msbfs_release(sg_msbfs h) {
@@ -682,6 +758,8 @@ static void msbfs_release(sg_msbfs h) {
   dev_free(h->bar);
   dev_free(h->log);
   dev_free(h->result);
+  dev_free(h->schedule);
+  dev_free(h->features);
   delete h;
 }
 
@@ -765,7 +843,9 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
   clear_error();
   SG_REQUIRE(h && host_sources, SG_ERR_INVALID, "NULL argument");
   SG_REQUIRE(k >= 1 && k <= h->k, SG_ERR_INVALID, "source count exceeds the batch capacity");
-  SG_REQUIRE(direction >= SG_BFS_PUSH && direction <= SG_BFS_HYBRID, SG_ERR_INVALID, "unknown BFS direction");
+  SG_REQUIRE(direction >= SG_BFS_PUSH && direction <= SG_BFS_LEARNED, SG_ERR_INVALID, "unknown BFS direction");
+  SG_REQUIRE(direction != SG_BFS_LEARNED || h->mlp_image, SG_ERR_INVALID,
+             "learned mode needs a selector (sg_msbfs_set_selector)");
   for (uint32_t i = 0; i < k; i++) SG_REQUIRE(host_sources[i] < h->g->n, SG_ERR_INVALID, "source out of range");
   sg_graph g = h->g;
   SG_CUDA(cudaMemcpyAsync(h->sources, host_sources, sizeof(uint32_t) * k, cudaMemcpyHostToDevice, h->stream));
@@ -804,6 +884,13 @@ sg_status sg_msbfs_run_async(sg_msbfs h, const uint32_t* host_sources, uint32_t 
   P.depth = h->depth;
   P.log = h->log;
   P.result = h->result;
+  P.schedule = h->schedule;
+  P.schedule_len = h->schedule_len;
+  P.mlp_image = static_cast<const sygraph::detail::MlpStaged*>(h->mlp_image);
+  P.margin = h->margin;
+  P.min_frontier = h->min_frontier;
+  P.max_frontier = h->max_frontier;
+  P.features = h->features;
   h->last_k = k;
   return eng::launch_persistent(ms::msbfs_kernel, P, 2, h->stream, h->max_ctas);
 }
@@ -870,6 +957,59 @@ sg_status sg_msbfs_level_records(sg_msbfs h, sg_level_record* host_records, uint
 sg_status sg_msbfs_depths_device(sg_msbfs h, const uint32_t** dev_depth) {
   SG_REQUIRE(h && dev_depth, SG_ERR_INVALID, "NULL argument");
   *dev_depth = h->depth;
+  return SG_OK;
+}
+
+sg_status sg_msbfs_set_schedule(sg_msbfs h, const int* host_directions, uint32_t len) {
+  clear_error();
+  SG_REQUIRE(h, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(len == 0 || host_directions, SG_ERR_INVALID, "directions is NULL");
+  for (uint32_t i = 0; i < len; i++)
+    SG_REQUIRE(host_directions[i] == -1 || host_directions[i] == 0 || host_directions[i] == 2, SG_ERR_INVALID,
+               "batched directions are 0 (push), 2 (pull) or -1 (the mode decides)");
+  SG_CUDA(cudaStreamSynchronize(h->stream));  // a queued launch may still read the old schedule
+  dev_free(h->schedule);
+  h->schedule_len = 0;
+  if (len) {
+    SG_TRY(dev_alloc(&h->schedule, len));
+    SG_CUDA(cudaMemcpy(h->schedule, host_directions, sizeof(int) * len, cudaMemcpyHostToDevice));
+    h->schedule_len = len;
+  }
+  return SG_OK;
+}
+
+sg_status sg_msbfs_set_selector(sg_msbfs h, sg_mlp mlp, float margin, float min_frontier, float max_frontier) {
+  clear_error();
+  SG_REQUIRE(h, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(margin >= 0.f && min_frontier >= 0.f && min_frontier <= max_frontier, SG_ERR_INVALID,
+             "margin >= 0 and 0 <= min_frontier <= max_frontier");
+  h->mlp_image = mlp ? mlp_device_image(mlp) : nullptr;
+  h->margin = margin;
+  h->min_frontier = min_frontier;
+  h->max_frontier = max_frontier;
+  return SG_OK;
+}
+
+sg_status sg_msbfs_log_features(sg_msbfs h, int enable) {
+  clear_error();
+  SG_REQUIRE(h, SG_ERR_INVALID, "NULL argument");
+  SG_CUDA(cudaStreamSynchronize(h->stream));
+  if (enable && !h->features) SG_TRY(dev_alloc(&h->features, 12ull * SG_MAX_LOGGED_LEVELS));
+  if (!enable) dev_free(h->features);
+  return SG_OK;
+}
+
+sg_status sg_msbfs_level_features(sg_msbfs h, float* host_features, uint32_t cap_levels, uint32_t* count) {
+  SG_REQUIRE(h && count, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(h->features, SG_ERR_NOT_INITIALIZED, "feature logging is off (sg_msbfs_log_features)");
+  SG_CUDA(cudaStreamSynchronize(h->stream));
+  unsigned long long it = 0;
+  if (h->last_k) SG_CUDA(cudaMemcpy(&it, h->result, sizeof(it), cudaMemcpyDeviceToHost));
+  uint32_t k = (uint32_t)(it < SG_MAX_LOGGED_LEVELS ? it : SG_MAX_LOGGED_LEVELS);
+  if (k > cap_levels) k = cap_levels;
+  if (host_features && k)
+    SG_CUDA(cudaMemcpy(host_features, h->features, sizeof(float) * 12 * k, cudaMemcpyDeviceToHost));
+  *count = k;
   return SG_OK;
 }
 

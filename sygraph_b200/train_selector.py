@@ -145,6 +145,78 @@ def collect(graphs, sources_per_graph: int = 6, reps: int = 5, log=print) -> dic
     }
 
 
+# The batched (64-source) BFS's selector: push or pull per level (the
+# model's outputs 0 and 2), the batched heuristic (alpha 4, beta 24) as the
+# fallback; its own model file.  The cost of an inference is negligible
+# against a batched level, so it has no graph range.
+BATCHED_MODEL_PATH = MODEL_PATH.parent / "selector_msbfs_b200.npz"
+BATCH_ALPHA, BATCH_BETA = 4.0, 24.0
+BATCH_ALLOWED = (1 << 0) | (1 << 2)
+BATCH_SOURCES = 64
+
+
+def _forced_batch(mb, srcs, direction: int, reps: int):
+    """Median level times (us) and logged features of batched runs with every
+    level forced to `direction` (0 push, 2 pull)."""
+    mb.set_schedule([direction] * MAX_LEVELS)
+    times, feats = [], None
+    for _ in range(reps):
+        mb.run(srcs, algorithms.bfs_direction.hybrid, BATCH_ALPHA, BATCH_BETA)
+        times.append(mb.level_times_us())
+        if feats is None:
+            feats = mb.level_features()
+    mb.set_schedule([])
+    return np.median(np.stack(times), 0), feats
+
+
+def collect_batched(graphs, batches_per_graph: int = 3, reps: int = 5, log=print) -> dict:
+    """Cost tables of the batched BFS, in the layout of collect(): per batch
+    of BATCH_SOURCES sources the level times under forced push and forced
+    pull (strategy columns 0 and 2; the other columns repeat the slower of
+    the two and are masked out of the loss), the features of both runs as
+    samples, and the batched heuristic's schedule."""
+    X, Y, M, group, H, TT, F0 = [], [], [], [], [], [], []
+    names = []
+    gid = 0
+    mask = np.array([(BATCH_ALLOWED >> j) & 1 for j in range(OUT)], np.float32)
+    for name, kind, kw in graphs:
+        t0 = time.time()
+        csr = make_graph(kind, kw)
+        G = build.fromCSR(csr)
+        mb = algorithms.MultiBFS(G, BATCH_SOURCES)
+        mb.log_features(True)
+        for b in range(batches_per_graph):
+            srcs = io.sample_sources(csr, BATCH_SOURCES, seed=1000 + 17 * gid + b)
+            tp, fp = _forced_batch(mb, srcs, 0, reps)
+            tq, fq = _forced_batch(mb, srcs, 2, reps)
+            levels = min(len(tp), len(tq))
+            T = np.empty((levels, OUT), np.float32)
+            T[:] = np.maximum(tp[:levels], tq[:levels])[:, None]
+            T[:, 0], T[:, 2] = tp[:levels], tq[:levels]
+            logT = np.log(np.maximum(T, 0.05))
+            for Fx in (fp, fq):
+                for L in range(levels):
+                    X.append(Fx[L])
+                    Y.append(logT[L])
+                    M.append(mask)
+                    group.append(gid)
+            mb.run(srcs, algorithms.bfs_direction.hybrid, BATCH_ALPHA, BATCH_BETA)
+            H.append(np.array([r["strategy"] for r in mb.level_records()][:levels], np.int32))
+            TT.append(T)
+            F0.append(fp[:levels])
+            names.append(f"{name}:batch{b}")
+            gid += 1
+        log(f"{name}: n={csr.n} m={csr.m} batches={batches_per_graph} {time.time() - t0:.1f}s")
+        del mb, G
+    lens = [len(t) for t in TT]
+    return {
+        "X": np.asarray(X, np.float32), "Y": np.asarray(Y, np.float32), "M": np.asarray(M, np.float32),
+        "group": np.asarray(group, np.int32), "names": np.asarray(names),
+        "T": np.concatenate(TT).astype(np.float32), "H": np.concatenate(H).astype(np.int32),
+        "F0": np.concatenate(F0).astype(np.float32), "offsets": np.concatenate([[0], np.cumsum(lens)]).astype(np.int64),
+    }
+
+
 def traversals(data: dict):
     """(name, T[levels,6], heuristic[levels], features[levels,12]) per traversal."""
     o = data["offsets"]
@@ -334,43 +406,47 @@ def main(argv=None) -> int:
     c = sub.add_parser("collect")
     c.add_argument("--out", required=True)
     c.add_argument("--set", choices=["train", "eval"], default="train")
+    c.add_argument("--batched", action="store_true", help="the 64-source batched BFS (push / pull per level)")
     c.add_argument("--sources", type=int, default=6)
     c.add_argument("--reps", type=int, default=5)
     t = sub.add_parser("train")
     t.add_argument("--data", required=True)
-    t.add_argument("--model", default=str(MODEL_PATH))
+    t.add_argument("--model", default=None)
+    t.add_argument("--batched", action="store_true")
     t.add_argument("--steps", type=int, default=6000)
     t.add_argument("--lr", type=float, default=3e-3)
     r = sub.add_parser("regate", help="recompute a model's frontier and graph ranges on training tables")
     r.add_argument("--data", required=True)
-    r.add_argument("--model", default=str(MODEL_PATH))
+    r.add_argument("--model", default=None)
+    r.add_argument("--batched", action="store_true")
     r.add_argument("--cost-us", type=float, default=INFERENCE_US)
     e = sub.add_parser("evaluate")
     e.add_argument("--data", required=True)
-    e.add_argument("--model", default=str(MODEL_PATH))
+    e.add_argument("--model", default=None)
+    e.add_argument("--batched", action="store_true")
     e.add_argument("--json", default=None)
     e.add_argument("--cost-us", type=float, default=INFERENCE_US)
     a = ap.parse_args(argv)
     if a.cmd == "collect":
-        _save(collect(TRAIN_GRAPHS if a.set == "train" else EVAL_GRAPHS, a.sources, a.reps), a.out)
-    elif a.cmd == "train":
-        data = _load(a.data)
-        mlp = train(data, a.steps, a.lr)
-        mlp.frontier_range = frontier_range(mlp, data)
-        mlp.graph_range = graph_range(mlp, data)
-        rep = evaluate(mlp, data, cost_us=INFERENCE_US)
-        mlp.save(a.model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
-        print(json.dumps(rep["total"]))
-    elif a.cmd == "regate":
-        data = _load(a.data)
-        mlp = Mlp.load(a.model)
-        mlp.frontier_range = frontier_range(mlp, data, a.cost_us)
-        mlp.graph_range = graph_range(mlp, data, cost_us=a.cost_us)
-        rep = evaluate(mlp, data, cost_us=a.cost_us)
-        mlp.save(a.model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
+        graphs = TRAIN_GRAPHS if a.set == "train" else EVAL_GRAPHS
+        if a.batched:
+            _save(collect_batched(graphs, reps=a.reps), a.out)
+        else:
+            _save(collect(graphs, a.sources, a.reps), a.out)
+        return 0
+    model = a.model or str(BATCHED_MODEL_PATH if a.batched else MODEL_PATH)
+    kw = dict(allowed=BATCH_ALLOWED, alpha=BATCH_ALPHA, beta=BATCH_BETA) if a.batched else {}
+    data = _load(a.data)
+    if a.cmd in ("train", "regate"):
+        mlp = train(data, a.steps, a.lr) if a.cmd == "train" else Mlp.load(model)
+        cost = getattr(a, "cost_us", INFERENCE_US)
+        mlp.frontier_range = frontier_range(mlp, data, cost, **kw)
+        mlp.graph_range = None if a.batched else graph_range(mlp, data, cost_us=cost, **kw)
+        rep = evaluate(mlp, data, cost_us=cost, **kw)
+        mlp.save(model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
         print(json.dumps({"frontier_range": mlp.frontier_range, "graph_range": mlp.graph_range, **rep["total"]}))
     else:
-        rep = evaluate(Mlp.load(a.model), _load(a.data), cost_us=a.cost_us)
+        rep = evaluate(Mlp.load(model), data, cost_us=a.cost_us, **kw)
         print(json.dumps(rep["total"]))
         if a.json:
             with open(a.json, "w") as f:

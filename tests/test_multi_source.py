@@ -68,3 +68,84 @@ def test_msbfs_long_diameter_depth_planes(sg, oracle, n):
     shallow = np.array([n // 2, n // 2 + 1], np.uint32)
     mb.run(shallow)
     assert np.array_equal(mb.getDistances(), oracle.bfs_multi(path, shallow))
+
+
+def _trusting_mlp(selector, seed):
+    """A random MLP whose trusted range covers every feature value."""
+    rng = np.random.default_rng(seed)
+    m = selector.Mlp()
+    p = m.params
+    t, I = selector.TRAINABLE_COUNT, selector.IN
+    p[:t] = rng.normal(scale=0.5, size=t).astype(np.float32)
+    p[t:t + I] = 0.0
+    p[t + I:t + 2 * I] = 1.0
+    p[t + 2 * I:t + 3 * I] = -1e9
+    p[t + 3 * I:t + 4 * I] = 1e9
+    m.params = p
+    return m
+
+
+def _batched_heuristic(recs, n, alpha, beta):
+    """The batched engine's heuristic choice (0 push, 2 pull) for every level
+    after the first, given the direction each level actually took."""
+    f32 = np.float32
+    out = [0]
+    for r in recs[:-1]:
+        if r["strategy"] < 2:
+            pull = f32(r["next_degree"]) > f32(r["unexplored_degree"]) / f32(alpha)
+        else:
+            pull = not f32(r["next_size"]) < f32(n) / f32(beta)
+        out.append(2 if pull else 0)
+    return np.array(out)
+
+
+@pytest.mark.parametrize("scale,perm", [(12, 0), (15, 3)])
+def test_msbfs_forced_and_learned_schedules_keep_depths(sg, oracle, rmat, scale, perm):
+    """Forced per-level directions and the learned mode change the work, not
+    the depths; the learned mode asks the model where the heuristic switches
+    direction and takes its argmin over push and pull there, the heuristic's
+    choice elsewhere; the feature log covers every level."""
+    from sygraph_b200 import selector
+    g = rmat(scale, perm_seed=perm)
+    G = sg.graph.build.fromCSR(g)
+    srcs = sg.io.sample_sources(g, 64, seed=5)
+    ref = oracle.bfs_multi(g, srcs)
+    mb = sg.algorithms.MultiBFS(G, 64)
+    rng = np.random.default_rng(scale)
+    for _ in range(3):
+        sched = rng.choice([0, 2], size=32)
+        mb.set_schedule(sched)
+        mb.run(srcs, 2, 4.0, 24.0)
+        assert np.array_equal(mb.getDistances(), ref)
+        got = [r["strategy"] for r in mb.level_records()]
+        assert got == list(sched[:len(got)])
+    mb.set_schedule([])
+    with pytest.raises(sg._lib.SygraphError):
+        mb.set_schedule([1])
+    with pytest.raises(sg._lib.SygraphError):
+        mb.run(srcs, sg.algorithms.bfs_direction.learned, 4.0, 24.0)  # no selector yet
+    asked = 0
+    for seed in range(4):
+        m = _trusting_mlp(selector, seed)
+        mb.set_selector(m, margin=0.0)
+        mb.log_features(True)
+        det = mb.run(srcs, sg.algorithms.bfs_direction.learned, 4.0, 24.0)
+        assert np.array_equal(mb.getDistances(), ref)
+        recs = mb.level_records()
+        F = mb.level_features()
+        assert F.shape == (det["iterations"], 12) and np.all(np.isfinite(F))
+        got = np.array([r["strategy"] for r in recs])
+        assert set(np.unique(got)) <= {0, 2}
+        heur = _batched_heuristic(recs, g.n, 4.0, 24.0)
+        cur = np.concatenate([[0], got[:-1]])
+        ask = (heur >= 2) != (cur >= 2)
+        assert np.array_equal(got[~ask], heur[~ask])
+        y = m.forward(F)[:, [0, 2]]
+        pick = np.where(got == 2, 1, 0)
+        best = y.min(1)
+        ok = y[np.arange(len(got)), pick] <= best + 1e-4 * (1 + np.abs(best))
+        assert np.all(ok[ask])
+        asked += int(ask.sum())
+    assert asked >= 2
+    mb.set_selector(None)
+    mb.log_features(False)

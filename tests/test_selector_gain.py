@@ -122,3 +122,49 @@ def test_gates_follow_from_training_tables(tables):
     f9 = {str(n).split(":")[0]: float(F[0][9]) for n, _, _, F in ts.traversals(data)}
     assert all(lo <= v <= hi for k, v in f9.items() if k.startswith("grid") and k != "grid512")
     assert not any(lo <= v <= hi for k, v in f9.items() if k.startswith(("rmat", "uniform")))
+
+
+# The batched (64-source) BFS's selector: push or pull per level, measured on
+# batches of 64 sources of the same held-out graphs
+# (`train_selector collect --batched --set eval`), the batched heuristic
+# (alpha 4, beta 24) as its fallback.
+BATCH_EVAL = ROOT / "tests" / "golden" / "selector_msbfs_eval_b200.npz"
+BATCH_TRAIN_TABLES = ROOT / "tests" / "golden" / "selector_msbfs_train_tables_b200.npz"
+BATCH_MODEL = ROOT / "sygraph_b200" / "models" / "selector_msbfs_b200.npz"
+
+
+def _batched_model():
+    with np.load(BATCH_MODEL) as m:
+        return m["params"].astype(np.float32), tuple(float(x) for x in m["frontier_range"])
+
+
+def test_batched_learned_schedule_on_held_out_graphs():
+    from sygraph_b200 import train_selector as ts
+    with np.load(BATCH_EVAL) as d:
+        data = {k: d[k] for k in d.files}
+    params, (lo, hi) = _batched_model()
+    m = _CpuModel(params, None, (lo, hi))
+    heur = learned = 0.0
+    for name, T, H, F in ts.traversals(data):
+        assert set(np.unique(H)) <= {0, 2}
+        c = ts.simulate_choices(params, m.forward, F, H, ts.BATCH_ALLOWED, min_frontier=lo, max_frontier=hi,
+                                alpha=ts.BATCH_ALPHA, beta=ts.BATCH_BETA)
+        assert set(np.unique(c)) <= {0, 2}  # push or pull only
+        idx = np.arange(len(T))
+        h = float(T[idx, H].sum())
+        l = float(T[idx, c].sum()) + ts.INFERENCE_US * int(ts.consulted(F, c, lo, hi, ts.BATCH_ALPHA,
+                                                                           ts.BATCH_BETA).sum())
+        assert l <= 1.01 * h, (name, l, h)  # no batch more than 1% slower
+        heur += h
+        learned += l
+    assert learned <= heur / 1.02, (learned, heur)  # at least 2% less time over the held-out batches
+
+
+def test_batched_frontier_range_follows_from_training_tables():
+    from sygraph_b200 import train_selector as ts
+    with np.load(BATCH_TRAIN_TABLES) as d:
+        data = {k: d[k] for k in d.files}
+    params, fr = _batched_model()
+    got = ts.frontier_range(_CpuModel(params), data, allowed=ts.BATCH_ALLOWED, alpha=ts.BATCH_ALPHA,
+                            beta=ts.BATCH_BETA)
+    assert np.allclose(got, fr, atol=1e-6), (got, fr)

@@ -76,3 +76,38 @@ def test_learned_faster_on_grid4096(sg):
     g = sg.io.grid(4096, long_range_frac=0.02, seed=103, weight_seed=2, value_type=sg.WEIGHT_U32)
     ratio = _timed_ratio(sg, g, sg.io.sample_sources(g, 4, seed=3))
     assert ratio >= 1.10, ratio
+
+
+def _batched_ratio(sg, g, alpha):
+    """Heuristic / learned launch time of the batched BFS (64 sources), both
+    modes on one instance alternating on one stream; identical depths."""
+    import torch
+    from sygraph_b200 import selector, train_selector
+    G = sg.graph.build.fromCSR(g)
+    srcs = sg.io.sample_sources(g, 64, seed=3)
+    mb = sg.algorithms.MultiBFS(G, 64)
+    mb.set_selector(selector.Mlp.load(train_selector.BATCHED_MODEL_PATH))
+    mb.run(srcs, HYBRID, alpha, 24.0)
+    ref = mb.getDistances()
+    mb.run(srcs, LEARNED, alpha, 24.0)
+    assert np.array_equal(ref, mb.getDistances())
+
+    def launch(mode, a, b):
+        a.record()
+        mb.run_async(srcs, mode, alpha, 24.0)
+        b.record()
+
+    m = _alternating(torch, launch, [HYBRID, LEARNED])
+    return m[HYBRID] / m[LEARNED]
+
+
+def test_learned_batched_no_slower_on_rmat22(sg):
+    g = sg.io.rmat(22, 16, 0.57, 0.19, 0.19, seed=1, weight_seed=2, perm_seed=0, value_type=sg.WEIGHT_F32)
+    ratio = _batched_ratio(sg, g, 4.0)
+    assert ratio >= 0.99, ratio
+
+
+def test_learned_batched_faster_on_grid4096(sg):
+    g = sg.io.grid(4096, long_range_frac=0.02, seed=103, weight_seed=2, value_type=sg.WEIGHT_U32)
+    ratio = _batched_ratio(sg, g, 4.0)
+    assert ratio >= 1.02, ratio
