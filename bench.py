@@ -245,25 +245,28 @@ def _launch_ms(torch, fn) -> float:
 
 
 def _alternating_ms(torch, runs, sources, reps: int = 6):
-    """Median device time per launch of each of `runs` (functions of a
-    source that enqueue one launch), their launches alternating back to back
-    on the current stream, each between two CUDA events, with one host wait
-    at the end: every mode sees the same clocks and caches."""
-    times = [[] for _ in runs]
+    """Device time per launch of each of `runs` (functions of a source that
+    enqueue one launch): each source's median over `reps` rounds, averaged
+    over the sources.  The runs' launches of a source go back to back on the
+    current stream, each between two CUDA events, in reversed order every
+    other round, with one host wait per round: every mode sees the same
+    clocks and caches."""
+    times = [[[] for _ in sources] for _ in runs]
     for rep in range(reps + 1):  # the first round warms up
         pairs = []
-        for s in sources:
-            for k, run in enumerate(runs):
+        order = list(enumerate(runs)) if rep % 2 == 0 else list(enumerate(runs))[::-1]
+        for i, s in enumerate(sources):
+            for k, run in order:
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record()
                 run(int(s))
                 b.record()
-                pairs.append((k, a, b))
+                pairs.append((k, i, a, b))
         torch.cuda.synchronize()
         if rep:
-            for k, a, b in pairs:
-                times[k].append(a.elapsed_time(b))
-    return [float(np.median(t)) for t in times]
+            for k, i, a, b in pairs:
+                times[k][i].append(a.elapsed_time(b))
+    return [float(np.mean([np.median(t) for t in per_src])) for per_src in times]
 
 
 def cpu_baseline(g, srcs):
@@ -604,7 +607,8 @@ def main():
     learned = {"model": "sygraph_b200/models/selector_b200.npz"}
     bl = sg.algorithms.BFS(G)
     bl.set_selector(mlp)
-    rm_h, rm_l = _alternating_ms(torch, [lambda s: (bfs.init(s), bfs.run_async(2, ALPHA, BETA)),
+    # both modes on the one instance (same buffers), alternating per source
+    rm_h, rm_l = _alternating_ms(torch, [lambda s: (bl.init(s), bl.run_async(2, ALPHA, BETA)),
                                          lambda s: (bl.init(s), bl.run_async(3, ALPHA, BETA))], srcs)
     same_rmat = True
     for s in srcs[:8]:
@@ -615,8 +619,9 @@ def main():
         same_rmat &= bool(np.array_equal(bfs.getDistances(), bl.getDistances()))
     del bl
     learned.update({"rmat_launch_ms": rm_l, "rmat_heuristic_launch_ms": rm_h,
-                    "rmat_speedup_vs_heuristic": rm_h / rm_l, "timing": "median per launch, the two modes "
-                    "alternating back to back on one stream (6 rounds of the 64 sources)"})
+                    "rmat_speedup_vs_heuristic": rm_h / rm_l, "timing": "per-source median over 6 rounds, "
+                    "averaged over the sources; both modes on one instance, alternating back to back on one "
+                    "stream", "graph_range": mlp.graph_range, "frontier_range": mlp.frontier_range})
     gg = sg.io.grid(4096, long_range_frac=0.02, seed=103)
     Gg = sg.graph.build.fromCSR(gg)
     bg = sg.algorithms.BFS(Gg)
@@ -659,7 +664,36 @@ def main():
     batched_ms = float(np.median(mb_ms))
     batched_gteps = mb_det["reached_edges"] / (batched_ms * 1e-3) / 1e9
     ms_bytes = 4 * (n + 1) + 4 * m + 4 * n * len(srcs)
+    # learned + batched: the batched selector against the batched heuristic,
+    # both on this instance, alternating; then on the 4096 x 4096 grid
+    from sygraph_b200 import train_selector
+    bmlp = selector.Mlp.load(train_selector.BATCHED_MODEL_PATH)
+    mbfs.set_selector(bmlp)
+    mbfs.run(srcs, 3, ms_alpha, MS_BETA)
+    b_same = bool(np.array_equal(mbfs.getDistances()[:PARITY_SOURCES], mb_rows))
+    bh, bl_ms = _alternating_ms(torch, [lambda _: mbfs.run_async(srcs, 2, ms_alpha, MS_BETA),
+                                        lambda _: mbfs.run_async(srcs, 3, ms_alpha, MS_BETA)], [0], reps=8)
+    mbfs.set_selector(None)
     del mbfs
+    gg = sg.io.grid(4096, long_range_frac=0.02, seed=103)
+    Gg = sg.graph.build.fromCSR(gg)
+    mg = sg.algorithms.MultiBFS(Gg, 64)
+    mg.set_selector(bmlp)
+    gsrc64 = sg.io.sample_sources(gg, 64, seed=SOURCE_SEED)
+    mg.run(gsrc64, 2, train_selector.BATCH_ALPHA, MS_BETA)
+    d_h = mg.getDistances()
+    mg.run(gsrc64, 3, train_selector.BATCH_ALPHA, MS_BETA)
+    b_same &= bool(np.array_equal(d_h, mg.getDistances()))
+    del d_h
+    gh, gl = _alternating_ms(torch, [lambda _: mg.run_async(gsrc64, 2, train_selector.BATCH_ALPHA, MS_BETA),
+                                     lambda _: mg.run_async(gsrc64, 3, train_selector.BATCH_ALPHA, MS_BETA)],
+                             [0], reps=4)
+    del mg, Gg, gg
+    batched_learned = {"model": "sygraph_b200/models/selector_msbfs_b200.npz", "rmat_heuristic_ms": bh,
+                       "rmat_learned_ms": bl_ms, "rmat_speedup_vs_heuristic": bh / bl_ms,
+                       "grid4096_heuristic_ms": gh, "grid4096_learned_ms": gl,
+                       "grid4096_speedup_vs_heuristic": gh / gl, "identical_depths": b_same,
+                       "frontier_range": bmlp.frontier_range}
 
     # batched Brandes BC: 64 sources per launch on RMAT-20 against the
     # per-source engine on the same sources (float32, both checked equal within 1e-4)
@@ -806,7 +840,8 @@ def main():
                         "roofline": {"bound": "hbm", "achieved": ms_bytes / (batched_ms * 1e-3) / 1e9,
                                      "peak": peak, "unit": "GB/s",
                                      "frac": ms_bytes / (batched_ms * 1e-3) / 1e9 / peak,
-                                     "bytes_per_launch": ms_bytes, "traffic": ncu_traffic("msbfs_kernel")}},
+                                     "bytes_per_launch": ms_bytes, "traffic": ncu_traffic("msbfs_kernel")},
+                        "learned": batched_learned},
             "learned": learned,
             "bc_batched": bc_line,
             "construction": construction,
