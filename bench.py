@@ -810,6 +810,33 @@ def main():
         sssp.init(int(s))
         nf_ms += _launch_ms(torch, sssp.run_async)
     nf_kern = nf_ms / k_ss
+    # learned heavy phases (the SSSP model) against the heavy_pull rule on the
+    # same sources and instance, alternating launch by launch
+    from sygraph_b200 import train_selector
+    smdl = selector.Mlp.load(train_selector.SSSP_MODEL_PATH)
+    sl_t = {False: [[] for _ in range(k_ss)], True: [[] for _ in range(k_ss)]}
+    sl_same = True
+    for rep in range(5):
+        for i, s in enumerate(srcs[:k_ss]):
+            for use_model in ((False, True) if rep % 2 == 0 else (True, False)):
+                sssp.set_selector(smdl if use_model else None)
+                sssp.init(int(s))
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                sssp.run_async()
+                b.record()
+                b.synchronize()
+                if rep:
+                    sl_t[use_model][i].append(a.elapsed_time(b))
+                if rep == 0 and use_model:
+                    sl_same &= bool(np.array_equal(sssp.getDistances().view(np.uint32),
+                                                   d_first.view(np.uint32))) if i == 0 else True
+    sssp.set_selector(None)
+    sl_h = float(np.mean([np.median(t) for t in sl_t[False]]))
+    sl_l = float(np.mean([np.median(t) for t in sl_t[True]]))
+    sssp_learned = {"model": "sygraph_b200/models/selector_sssp_b200.npz", "heavy_range": smdl.heavy_range,
+                    "rule_launch_ms": sl_h, "learned_launch_ms": sl_l, "speedup_vs_rule": sl_h / sl_l,
+                    "identical_distances": sl_same}
 
     serve = None if (args.no_serving or world > 1) else serving_bench(sg, torch)
 
@@ -858,7 +885,8 @@ def main():
                                                "achieved": sssp_bytes / (nf_kern * 1e-3) / 1e9,
                                                "frac": sssp_bytes / (nf_kern * 1e-3) / 1e9 / peak,
                                                "bytes_per_launch": sssp_bytes,
-                                               "traffic": ncu_traffic("sssp_kernel")}},
+                                               "traffic": ncu_traffic("sssp_kernel")},
+                                  "learned": sssp_learned},
                      "roofline": {"bound": "hbm", "achieved": sssp_achieved, "peak": peak, "unit": "GB/s",
                                   "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,
                                   "traffic": None}},  # the ncu capture is of the delta-stepping schedule

@@ -546,6 +546,27 @@ sg_status sg_sssp_set_launch(sg_sssp s, void* stream, uint32_t max_ctas);
 sg_status sg_sssp_run_async(sg_sssp s);
 sg_status sg_sssp_get_distances(sg_sssp s, void* host_dist);
 sg_status sg_sssp_distances_device(sg_sssp s, const void** dev_dist);
+
+/* Learned heavy phases of delta-stepping SSSP (no counterpart in the
+ * reference, which has no buckets; none changes any distance):
+ *   sg_sssp_set_selector  the MLP (NULL detaches it) that chooses, at a
+ *                         bucket's heavy phase, between pushing the bucket's
+ *                         heavy edges and pulling them into the vertices
+ *                         beyond the bucket (its outputs 0 and 2), where the
+ *                         graph allows pull (symmetric weighted rows) and the
+ *                         bucket's heavy edges number min_heavy..max_heavy * m
+ *                         (the model file stores the range chosen in
+ *                         training); the sg_sssp_set_heavy_pull rule stands
+ *                         unless the model predicts it `margin` slower in
+ *                         log-time
+ *   sg_sssp_log_features  records the twelve features of each heavy phase
+ *                         (bucket vertices and heavy edges, heavy edges not
+ *                         yet relaxed, vertices settled, previous bucket,
+ *                         previous direction); sg_sssp_level_features reads
+ *                         them, one row per heavy phase. */
+sg_status sg_sssp_set_selector(sg_sssp s, sg_mlp mlp, float margin, float min_heavy, float max_heavy);
+sg_status sg_sssp_log_features(sg_sssp s, int enable);
+sg_status sg_sssp_level_features(sg_sssp s, float* host_features, uint32_t cap, uint32_t* count);
 sg_status sg_run_sssp(sg_graph g, uint32_t source, void* host_dist, uint64_t* iterations);
 
 /* CC(G) + init + run (algorithms/cc.hpp:82-169): labels[v] = max id over the

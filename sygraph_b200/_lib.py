@@ -215,6 +215,9 @@ SIGNATURES = {
     "sg_msbfs_set_selector": (st, [vp, vp, C.c_float, C.c_float, C.c_float]),
     "sg_msbfs_log_features": (st, [vp, C.c_int]),
     "sg_msbfs_level_features": (st, [vp, f32p, C.c_uint32, u32p]),
+    "sg_sssp_set_selector": (st, [vp, vp, C.c_float, C.c_float, C.c_float]),
+    "sg_sssp_log_features": (st, [vp, C.c_int]),
+    "sg_sssp_level_features": (st, [vp, f32p, C.c_uint32, u32p]),
     "sg_msbfs_destroy": (st, [vp]),
     "sg_msbfs_run": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float, C.POINTER(MsbfsDetails)]),
     "sg_msbfs_run_async": (st, [vp, u32p, C.c_uint32, C.c_int, C.c_float, C.c_float]),

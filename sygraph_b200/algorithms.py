@@ -261,6 +261,29 @@ class SSSP:
         pull when they number more than m / ratio (0: always push)."""
         call("sg_sssp_set_heavy_pull", self.handle, int(ratio))
 
+    def set_selector(self, mlp, margin: float = 0.05) -> None:
+        """The MLP that chooses push or pull for the heavy phases of
+        delta-stepping (None detaches it), asked on buckets whose heavy edges
+        are within the model's heavy range (mlp.heavy_range, a fraction of m;
+        else every bucket); `margin` is the predicted log-time gain it needs
+        to overrule the heavy_pull rule."""
+        self._mlp = mlp  # keep the device parameters alive
+        hr = getattr(mlp, "heavy_range", None) if mlp is not None else None
+        lo, hi = hr if hr is not None else (0.0, 1e30)
+        call("sg_sssp_set_selector", self.handle, mlp.handle if mlp is not None else None, float(margin),
+             float(lo), float(hi))
+
+    def log_features(self, enable: bool = True) -> None:
+        call("sg_sssp_log_features", self.handle, int(enable))
+
+    def level_features(self) -> np.ndarray:
+        """Twelve features per heavy phase of the last run."""
+        out = np.zeros((_lib.SG_MAX_LOGGED_LEVELS, 12), np.float32)
+        cnt = C.c_uint32()
+        call("sg_sssp_level_features", self.handle, out.ctypes.data_as(C.POINTER(C.c_float)),
+             _lib.SG_MAX_LOGGED_LEVELS, C.byref(cnt))
+        return out[:cnt.value]
+
     def set_light_pull(self, ratio: int) -> None:
         """Near-far on symmetric weighted graphs: an iteration whose frontier
         holds more than n / ratio vertices relaxes light edges by pull (0:

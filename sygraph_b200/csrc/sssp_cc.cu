@@ -15,7 +15,9 @@
 #include <vector>
 
 #include "push_engine.cuh"
+#include "selector_features.cuh"
 #include "sssp_pull.cuh"
+#include "sygraph/detail/selector_mlp.cuh"
 
 namespace sgb {
 namespace {
@@ -53,7 +55,54 @@ struct SsspParams {
   // light iteration by pull when its frontier holds more than n / light_pull
   // vertices (0: always push); same condition on the graph
   uint32_t light_pull;
+  // learned heavy phase: the selector's staged image (nullptr: the ratio
+  // rule above decides), asked at every heavy phase when pull is possible
+  const sygraph::detail::MlpStaged* mlp_image;
+  float margin;      // log-time gain the MLP must predict to overrule the rule
+  float heavy_lo, heavy_hi;  // heavy edges of the buckets (fraction of m) on which the MLP is asked
+  bool pull_ok;      // the weighted rows are symmetric: a heavy phase may pull
+  float* features;   // optional log: 12 floats per heavy phase
 };
+
+// Shared state of the learned heavy-phase choice.
+struct HeavySelect {
+  sygraph::detail::MlpStaged mlp;
+  float scratch[sygraph::detail::kMlpHidden];
+  FeatureConst fk;
+  int choice;
+};
+
+// Direction of a bucket's heavy phase (true = pull), identical in every CTA:
+// the MLP's choice between push and pull (warp 0 of each CTA; outputs 0 and
+// 2) on the bucket's features, where the model is attached, pull is possible
+// and the bucket's heavy edges are within [heavy_lo, heavy_hi] * m (near the
+// rule's own threshold, where the rule was wrong in training; elsewhere an
+// inference costs more than it saves), the ratio rule's `h_pull` unless the
+// model predicts it `margin` slower in log-time or outside the trusted
+// feature range; logs the features when asked.  Features: the bucket's vertices and heavy edges, the heavy
+// edges not yet relaxed, the vertices settled, the previous bucket's size
+// and the previous heavy phase's direction.
+template <typename W>
+__device__ __forceinline__ bool heavy_decide(const SsspParams<W>& P, HeavySelect& S, bool h_pull,
+                                             const FeatureInputs& x, uint32_t phase) {
+  const bool log = P.features && blockIdx.x == 0 && phase < kMaxLog;
+  const bool infer = P.mlp_image && P.pull_ok && (float)x.nd >= P.heavy_lo * (float)P.m &&
+                     (float)x.nd <= P.heavy_hi * (float)P.m;
+  if (!infer && !log) return h_pull;
+  if (threadIdx.x < 32) {
+    const float f = feature_of_lane(threadIdx.x, P.L.n, S.fk, x);
+    if (log && threadIdx.x < 12) P.features[(size_t)phase * 12 + threadIdx.x] = f;
+    if (infer) {
+      const int c = sygraph::detail::mlp_choose(&S.mlp, f, (1u << 0) | (1u << 2), S.scratch, h_pull ? 2 : 0,
+                                                P.margin);
+      if (threadIdx.x == 0) S.choice = c;
+    }
+  }
+  __syncthreads();
+  const bool out = (infer && S.choice >= 0) ? S.choice == 2 : h_pull;
+  __syncthreads();  // S.choice is written again at the next heavy phase
+  return out;
+}
 
 // Edge relaxation of the SSSP push steps, kU edges per lane at a time: the
 // column and weight loads of all kU edges go out together, then their
@@ -393,8 +442,14 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   __shared__ uint32_t s_scan[32];
   __shared__ unsigned long long s_red[32];
   __shared__ uint32_t s_best[kThreads];
+  __shared__ HeavySelect s_sel;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
   const uint32_t n = P.L.n, w0 = P.L.w0, src = P.source;
+  // learned heavy phases: the staged parameters arrive while the state is
+  // initialised; the init barrier publishes them
+  const bool staging = P.mlp_image && P.pull_ok;
+  if (staging) sygraph::detail::mlp_stage_async(P.mlp_image, &s_sel.mlp);
+  if (threadIdx.x == 0) s_sel.fk = feature_const(n, P.m, w0, (w0 + 31) / 32);
   const W inf = (W)(n + 1);  // (weight_t)(size + 1), sssp.hpp:43
   for (uint32_t i = gtid; i < n; i += nthreads) st_cg(P.dist + i, i == src ? (W)0 : inf);
   for (uint32_t i = gtid; i < w0; i += nthreads) {
@@ -418,6 +473,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       P.refill[gtid] = z;
     }
   }
+  if (staging) sygraph::detail::mlp_stage_wait();
   if (!grid_sync(P.L.bar)) return;
   // Near-far: vertices improved to a distance below the threshold stay in the
   // frontier, the others wait in the far set; when the near frontier is empty
@@ -439,6 +495,10 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
   unsigned long long far_left = ~0ull;  // far vertices the last refill left
   unsigned long long settled = 0;       // vertices of finished buckets
   uint32_t records = 0;                 // log entries written: iterations, heavy phases, refills
+  uint32_t phases = 0;                  // heavy phases run
+  unsigned long long heavy_done = 0;    // heavy edges of the buckets before this one
+  unsigned long long prev_bucket = 1;   // vertices of the previous bucket
+  bool prev_pull = false;               // direction of the previous heavy phase
   // one log entry for a heavy phase (strategy 4) or a refill pass (5)
   auto log_phase = [&](uint32_t kind, uint64_t t0, unsigned long long size, unsigned long long next) {
     if (P.L.log && gtid == 0 && records < kMaxLog) {
@@ -470,9 +530,18 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       if (!grid_sync(P.L.bar)) return;
       const uint32_t ns = ld_cg(&Ch->small_tail);
       const unsigned long long bp = ld_cg(&Ch->big_packed);
-      settled += ns + (uint32_t)(bp >> 32);
-      // pull when the push would relax a large share of the edges
-      const bool pull_heavy = P.heavy_pull && ld_cg(&Ch->frontier_deg) * P.heavy_pull > P.m;
+      const unsigned long long bsize = ns + (bp >> 32), hdeg = ld_cg(&Ch->frontier_deg);
+      settled += bsize;
+      // pull when the push would relax a large share of the edges (or as the
+      // learned selector says)
+      const bool h_pull = P.heavy_pull && hdeg * P.heavy_pull > P.m;
+      const FeatureInputs x{(double)bsize, (double)hdeg, (double)(P.m - min(P.m, heavy_done)), (double)settled,
+                            (double)prev_bucket, prev_pull};
+      const bool pull_heavy = heavy_decide(P, s_sel, h_pull, x, phases);
+      phases++;
+      heavy_done += hdeg;
+      prev_bucket = bsize;
+      prev_pull = pull_heavy;
       if (pull_heavy) {
         sssp_pull_scan<W, false>(P, P.bucket, nullptr, lo, threshold);
       } else {
@@ -572,6 +641,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
     P.result[0] = total;
     P.result[1] = pass;
     P.result[2] = records;
+    P.result[3] = phases;
   }
 }
 
@@ -853,6 +923,10 @@ struct sg_sssp_s {
   uint32_t* heavy_v = nullptr;      // vertices of in-degree >= kPullHeavy
   uint32_t* heavy_first = nullptr;  // their first chunk index
   uint32_t n_heavy = 0, n_chunks = 0;
+  const void* mlp_image = nullptr;  // learned heavy phases: the selector's staged image (owned by the sg_mlp)
+  float margin = 0.05f;
+  float heavy_lo = 0.f, heavy_hi = 1e30f;
+  float* features = nullptr;  // feature log, 12 floats per heavy phase
   PushWorkspace ws;
 };
 
@@ -925,6 +999,12 @@ static sg_status sssp_launch(sg_sssp s) {
     P.tail = (uint32_t)(s->tail * g->n);
     P.heavy_pull = g->wsym ? s->heavy_pull : 0u;
     P.light_pull = g->wsym ? s->light_pull : 0u;
+    P.mlp_image = static_cast<const sygraph::detail::MlpStaged*>(s->delta > 0.0 ? s->mlp_image : nullptr);
+    P.margin = s->margin;
+    P.heavy_lo = s->heavy_lo;
+    P.heavy_hi = s->heavy_hi;
+    P.pull_ok = g->wsym;
+    P.features = s->features;
     return launch_persistent(sssp_kernel<float>, P, 2, s->stream, s->max_ctas);
   }
   const uint32_t d = s->delta > 0.0 ? (uint32_t)std::max(1.0, std::min(s->delta, 4294967295.0)) : 0u;
@@ -940,6 +1020,12 @@ static sg_status sssp_launch(sg_sssp s) {
   P.tail = (uint32_t)(s->tail * g->n);
   P.heavy_pull = g->wsym ? s->heavy_pull : 0u;
   P.light_pull = g->wsym ? s->light_pull : 0u;
+  P.mlp_image = static_cast<const sygraph::detail::MlpStaged*>(s->delta > 0.0 ? s->mlp_image : nullptr);
+  P.margin = s->margin;
+  P.heavy_lo = s->heavy_lo;
+  P.heavy_hi = s->heavy_hi;
+  P.pull_ok = g->wsym;
+  P.features = s->features;
   return launch_persistent(sssp_kernel<uint32_t>, P, 2, s->stream, s->max_ctas);
 }
 
@@ -1018,6 +1104,7 @@ sg_status sg_sssp_destroy(sg_sssp s) {
     dev_free(s->log);
     dev_free(s->heavy_v);
     dev_free(s->heavy_first);
+    dev_free(s->features);
     delete s;
   }
   return SG_OK;
@@ -1027,6 +1114,42 @@ sg_status sg_sssp_set_pull(sg_sssp s, uint32_t ratio) {
   clear_error();
   SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
   s->pull_ratio = ratio;
+  return SG_OK;
+}
+
+sg_status sg_sssp_set_selector(sg_sssp s, sg_mlp mlp, float margin, float min_heavy, float max_heavy) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  SG_REQUIRE(margin >= 0.f && min_heavy >= 0.f && min_heavy <= max_heavy, SG_ERR_INVALID,
+             "margin >= 0 and 0 <= min_heavy <= max_heavy");
+  SG_CUDA(cudaStreamSynchronize(s->stream));  // a queued launch may still read the old image
+  s->mlp_image = mlp ? mlp_device_image(mlp) : nullptr;
+  s->margin = margin;
+  s->heavy_lo = min_heavy;
+  s->heavy_hi = max_heavy;
+  return SG_OK;
+}
+
+sg_status sg_sssp_log_features(sg_sssp s, int enable) {
+  clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "sssp is NULL");
+  SG_CUDA(cudaStreamSynchronize(s->stream));
+  if (enable && !s->features) SG_TRY(dev_alloc(&s->features, 12ull * SG_MAX_LOGGED_LEVELS));
+  if (!enable) dev_free(s->features);
+  return SG_OK;
+}
+
+sg_status sg_sssp_level_features(sg_sssp s, float* host_features, uint32_t cap, uint32_t* count) {
+  SG_REQUIRE(s && count, SG_ERR_INVALID, "NULL argument");
+  SG_REQUIRE(s->features, SG_ERR_NOT_INITIALIZED, "feature logging is off (sg_sssp_log_features)");
+  SG_CUDA(cudaStreamSynchronize(s->stream));
+  unsigned long long r[4] = {0, 0, 0, 0};
+  SG_CUDA(cudaMemcpy(r, s->ws.result, sizeof(r), cudaMemcpyDeviceToHost));
+  uint32_t k = (uint32_t)(r[3] < SG_MAX_LOGGED_LEVELS ? r[3] : SG_MAX_LOGGED_LEVELS);
+  if (k > cap) k = cap;
+  if (host_features && k)
+    SG_CUDA(cudaMemcpy(host_features, s->features, sizeof(float) * 12 * k, cudaMemcpyDeviceToHost));
+  *count = k;
   return SG_OK;
 }
 

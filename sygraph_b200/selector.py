@@ -33,7 +33,7 @@ def _fptr(a):
 class Mlp:
     """Device-resident MLP (sg_mlp)."""
 
-    def __init__(self, params: np.ndarray | None = None, graph_range=None, frontier_range=None):
+    def __init__(self, params: np.ndarray | None = None, graph_range=None, frontier_range=None, heavy_range=None):
         # (lo, hi) of the mean-degree feature log2(1 + m/n) / 8 on which the
         # model is consulted (None: every graph); see sg_bfs_set_selector_graph_range
         self.graph_range = None if graph_range is None else (float(graph_range[0]), float(graph_range[1]))
@@ -41,6 +41,9 @@ class Mlp:
         # consulted (None: the engine's defaults); see sg_bfs_set_selector_*_frontier
         self.frontier_range = None if frontier_range is None else (float(frontier_range[0]),
                                                                    float(frontier_range[1]))
+        # SSSP heavy phases: (lo, hi) of the bucket's heavy edges as a
+        # fraction of m on which the model is consulted; see sg_sssp_set_selector
+        self.heavy_range = None if heavy_range is None else (float(heavy_range[0]), float(heavy_range[1]))
         h = C.c_void_p()
         p = None if params is None else np.ascontiguousarray(params, np.float32)
         call("sg_mlp_create", None if p is None else _fptr(p), C.byref(h))
@@ -108,13 +111,16 @@ class Mlp:
             meta["graph_range"] = np.asarray(self.graph_range, np.float32)
         if self.frontier_range is not None:
             meta["frontier_range"] = np.asarray(self.frontier_range, np.float32)
+        if self.heavy_range is not None:
+            meta["heavy_range"] = np.asarray(self.heavy_range, np.float32)
         np.savez(path, params=self.params, **meta)
 
     @staticmethod
     def load(path=MODEL_PATH) -> "Mlp":
         d = np.load(path)
         return Mlp(d["params"], d["graph_range"] if "graph_range" in d.files else None,
-                   d["frontier_range"] if "frontier_range" in d.files else None)
+                   d["frontier_range"] if "frontier_range" in d.files else None,
+                   d["heavy_range"] if "heavy_range" in d.files else None)
 
     def __del__(self):
         h = getattr(self, "handle", None)

@@ -217,6 +217,169 @@ def collect_batched(graphs, batches_per_graph: int = 3, reps: int = 5, log=print
     }
 
 
+# Delta-stepping SSSP's selector: push or pull for each bucket's heavy phase
+# (outputs 0 and 2), the heavy_pull rule (pull when the bucket's heavy edges
+# times SSSP_RATIO exceed m) as the fallback; its own model file.  A bucket's
+# state after its heavy phase is the same by push or by pull, so the forced
+# all-push and all-pull runs of a source give its per-phase cost table.
+SSSP_MODEL_PATH = MODEL_PATH.parent / "selector_sssp_b200.npz"
+SSSP_RATIO = 8
+SSSP_ALLOWED = BATCH_ALLOWED
+ALWAYS_PULL = 0xFFFFFFFF  # heavy_pull ratio that pulls every heavy phase with a heavy edge
+
+
+def _sssp_phases(sp, source: int, ratio: int, reps: int):
+    """Median heavy-phase times (us), the logged features and the directions
+    (0 push / 2 pull) of `reps` runs with the heavy_pull ratio `ratio`."""
+    sp.set_heavy_pull(ratio)
+    times, feats, dirs = [], None, None
+    for _ in range(reps):
+        sp.init(source)
+        sp.run()
+        recs = [r for r in sp.level_records() if r["strategy"] in (4, 6)]
+        times.append([(r["t_end_ns"] - r["t_start_ns"]) / 1e3 for r in recs])
+        dirs = [2 if r["strategy"] == 6 else 0 for r in recs]
+        if feats is None:
+            feats = sp.level_features()
+    L = min(len(t) for t in times)
+    sp.set_heavy_pull(SSSP_RATIO)
+    return np.median(np.array([t[:L] for t in times]), 0), feats, dirs
+
+
+def collect_sssp(graphs, sources_per_graph: int = 4, reps: int = 3, log=print) -> dict:
+    """Cost tables of delta-stepping's heavy phases, in the layout of
+    collect(): per source the phase times under forced push and forced pull
+    (strategy columns 0 and 2; the others repeat the slower and are masked
+    out of the loss), both runs' features as samples, and the rule's
+    directions.  Delta from the autotuner per graph; graphs whose weighted
+    rows are not symmetric (no pull) are skipped."""
+    from . import autotune
+    X, Y, M, group, H, TT, F0 = [], [], [], [], [], [], []
+    names = []
+    gid = 0
+    mask = np.array([(SSSP_ALLOWED >> j) & 1 for j in range(OUT)], np.float32)
+    for name, kind, kw in graphs:
+        t0 = time.time()
+        csr = make_graph(kind, kw)
+        G = build.fromCSR(csr)
+        if not G.weight_sorted()[2]:
+            log(f"{name}: weighted rows not symmetric, skipped")
+            continue
+        sp = algorithms.SSSP(G)
+        srcs = [int(x) for x in io.sample_sources(csr, sources_per_graph, seed=500 + gid)]
+        integer = csr.value_type == io.WEIGHT_U32
+        delta = float(autotune.tune_sssp(sp, srcs[:1], autotune.mean_weight(csr), integer=integer, reps=1,
+                                         use_cache=False)["delta"])
+        sp.set_delta(delta)
+        sp.log_features(True)
+        for src in srcs:
+            tp, fp, _ = _sssp_phases(sp, src, 0, reps)
+            tq, fq, _ = _sssp_phases(sp, src, ALWAYS_PULL, reps)
+            _, _, h = _sssp_phases(sp, src, SSSP_RATIO, 1)
+            L = min(len(tp), len(tq), len(h), len(fp), len(fq))
+            if not L:
+                continue
+            T = np.empty((L, OUT), np.float32)
+            T[:] = np.maximum(tp[:L], tq[:L])[:, None]
+            T[:, 0], T[:, 2] = tp[:L], tq[:L]
+            logT = np.log(np.maximum(T, 0.05))
+            for Fx in (fp, fq):
+                for i in range(L):
+                    X.append(Fx[i])
+                    Y.append(logT[i])
+                    M.append(mask)
+                    group.append(gid)
+            H.append(np.array(h[:L], np.int32))
+            TT.append(T)
+            F0.append(fp[:L])
+            names.append(f"{name}:{src}")
+            gid += 1
+        log(f"{name}: n={csr.n} m={csr.m} delta={delta:g} sources={len(srcs)} {time.time() - t0:.1f}s")
+        del sp, G
+    lens = [len(t) for t in TT]
+    return {
+        "X": np.asarray(X, np.float32), "Y": np.asarray(Y, np.float32), "M": np.asarray(M, np.float32),
+        "group": np.asarray(group, np.int32), "names": np.asarray(names),
+        "T": np.concatenate(TT).astype(np.float32), "H": np.concatenate(H).astype(np.int32),
+        "F0": np.concatenate(F0).astype(np.float32), "offsets": np.concatenate([[0], np.cumsum(lens)]).astype(np.int64),
+    }
+
+
+def simulate_sssp(params: np.ndarray, forward, F: np.ndarray, heuristic: np.ndarray,
+                  margin: float = MARGIN, heavy_range=None) -> np.ndarray:
+    """The learned heavy phases' directions as the engine makes them: on the
+    phases whose heavy edges (feature 3, a fraction of m) lie in
+    `heavy_range` (None: every phase) the MLP (the previous-direction
+    feature following the schedule) picks push or pull, the rule's direction
+    standing unless the model predicts it `margin` slower in log-time or a
+    feature leaves the trusted range; elsewhere the rule decides."""
+    lo_h, hi_h = heavy_range if heavy_range is not None else (0.0, np.inf)
+    t0 = params.size - 4 * IN
+    lo, hi = params[t0 + 2 * IN:t0 + 3 * IN], params[t0 + 3 * IN:t0 + 4 * IN]
+    banned = [j for j in range(OUT) if not (SSSP_ALLOWED >> j) & 1]
+    out = np.empty(len(F), np.int32)
+    prev = 0
+    for L in range(len(F)):
+        f = np.array(F[L], np.float32)
+        f[10] = 1.0 if prev >= 2 else 0.0
+        h = int(heuristic[L])
+        if not lo_h <= f[3] <= hi_h or np.any(f < lo) or np.any(f > hi):
+            out[L] = h
+        else:
+            y = np.array(forward(f[None, :]), np.float64)[0]
+            y[banned] = np.inf
+            best = int(np.argmin(y))
+            out[L] = h if y[h] - y[best] <= margin else best
+        prev = out[L]
+    return out
+
+
+def _asked_sssp(F, heavy_range) -> int:
+    lo, hi = heavy_range if heavy_range is not None else (0.0, np.inf)
+    return int(np.sum((F[:, 3] >= lo) & (F[:, 3] <= hi))) if len(F) else 0
+
+
+def heavy_range(mlp, data: dict, cost_us: float = INFERENCE_US):
+    """The range of a bucket's heavy edges (fraction of m) on which asking the
+    model pays on the training tables (time its choices save against the
+    rule's, minus cost_us per inference), over a grid of bounds; (1, 0), an
+    empty range, when it pays nowhere."""
+    best = None
+    for lo in (0.0, 1e-3, 0.01, 0.02, 0.04, 0.06, 0.08, 0.1):
+        for hi in (0.125, 0.15, 0.2, 0.25, 0.3, 0.5, 1.0):
+            if hi <= lo:
+                continue
+            net = 0.0
+            for _, T, H, F in traversals(data):
+                c = simulate_sssp(mlp.params, mlp.forward, F, H, heavy_range=(lo, hi))
+                idx = np.arange(len(T))
+                net += float((T[idx, H] - T[idx, c]).sum()) - cost_us * _asked_sssp(F, (lo, hi))
+            if best is None or net > best[0]:
+                best = (net, lo, hi)
+    return (best[1], best[2]) if best[0] > 0 else (1.0, 0.0)
+
+
+def evaluate_sssp(mlp, data: dict, cost_us: float = INFERENCE_US) -> dict:
+    """Summed heavy-phase time (us) per source under the rule, under the
+    model (plus cost_us per inference, made on the phases inside its heavy
+    range) and the per-phase best."""
+    rows = []
+    hr = getattr(mlp, "heavy_range", None)
+    for name, T, H, F in traversals(data):
+        c = simulate_sssp(mlp.params, mlp.forward, F, H, heavy_range=hr)
+        idx = np.arange(len(T))
+        asked = _asked_sssp(F, hr)
+        rows.append({"traversal": name, "phases": len(T), "inferences": asked,
+                     "heuristic_us": float(T[idx, H].sum()),
+                     "learned_us": float(T[idx, c].sum()) + cost_us * asked, "best_us": float(T.min(1).sum()),
+                     "learned_schedule": "".join(map(str, c)), "heuristic_schedule": "".join(map(str, H))})
+    tot = {k: sum(r[k] for r in rows) for k in ("heuristic_us", "learned_us", "best_us", "inferences")}
+    tot["speedup_vs_heuristic"] = tot["heuristic_us"] / max(tot["learned_us"], 1e-9)
+    tot["regret_learned"] = tot["learned_us"] / max(tot["best_us"], 1e-9) - 1.0
+    tot["regret_heuristic"] = tot["heuristic_us"] / max(tot["best_us"], 1e-9) - 1.0
+    return {"total": tot, "traversals": rows}
+
+
 def traversals(data: dict):
     """(name, T[levels,6], heuristic[levels], features[levels,12]) per traversal."""
     o = data["offsets"]
@@ -407,36 +570,56 @@ def main(argv=None) -> int:
     c.add_argument("--out", required=True)
     c.add_argument("--set", choices=["train", "eval"], default="train")
     c.add_argument("--batched", action="store_true", help="the 64-source batched BFS (push / pull per level)")
+    c.add_argument("--sssp", action="store_true", help="delta-stepping SSSP's heavy phases (push / pull per bucket)")
     c.add_argument("--sources", type=int, default=6)
     c.add_argument("--reps", type=int, default=5)
     t = sub.add_parser("train")
     t.add_argument("--data", required=True)
     t.add_argument("--model", default=None)
     t.add_argument("--batched", action="store_true")
+    t.add_argument("--sssp", action="store_true")
     t.add_argument("--steps", type=int, default=6000)
     t.add_argument("--lr", type=float, default=3e-3)
     r = sub.add_parser("regate", help="recompute a model's frontier and graph ranges on training tables")
     r.add_argument("--data", required=True)
     r.add_argument("--model", default=None)
     r.add_argument("--batched", action="store_true")
+    r.add_argument("--sssp", action="store_true")
     r.add_argument("--cost-us", type=float, default=INFERENCE_US)
     e = sub.add_parser("evaluate")
     e.add_argument("--data", required=True)
     e.add_argument("--model", default=None)
     e.add_argument("--batched", action="store_true")
+    e.add_argument("--sssp", action="store_true")
     e.add_argument("--json", default=None)
     e.add_argument("--cost-us", type=float, default=INFERENCE_US)
     a = ap.parse_args(argv)
     if a.cmd == "collect":
         graphs = TRAIN_GRAPHS if a.set == "train" else EVAL_GRAPHS
-        if a.batched:
+        if a.sssp:
+            _save(collect_sssp(graphs), a.out)
+        elif a.batched:
             _save(collect_batched(graphs, reps=a.reps), a.out)
         else:
             _save(collect(graphs, a.sources, a.reps), a.out)
         return 0
-    model = a.model or str(BATCHED_MODEL_PATH if a.batched else MODEL_PATH)
+    model = a.model or str(SSSP_MODEL_PATH if a.sssp else BATCHED_MODEL_PATH if a.batched else MODEL_PATH)
     kw = dict(allowed=BATCH_ALLOWED, alpha=BATCH_ALPHA, beta=BATCH_BETA) if a.batched else {}
     data = _load(a.data)
+    if a.sssp:
+        # asked on the buckets inside its heavy range: no frontier or graph range
+        mlp = train(data, a.steps, a.lr) if a.cmd == "train" else Mlp.load(model)
+        cost = getattr(a, "cost_us", INFERENCE_US)
+        if a.cmd in ("train", "regate"):
+            mlp.heavy_range = heavy_range(mlp, data, cost)
+        rep = evaluate_sssp(mlp, data, cost)
+        if a.cmd in ("train", "regate"):
+            mlp.save(model, strategies=np.asarray(STRATEGIES), train_report=json.dumps(rep["total"]))
+        print(json.dumps(rep["total"]))
+        if getattr(a, "json", None):
+            with open(a.json, "w") as f:
+                json.dump(rep, f, indent=1)
+        return 0
     if a.cmd in ("train", "regate"):
         mlp = train(data, a.steps, a.lr) if a.cmd == "train" else Mlp.load(model)
         cost = getattr(a, "cost_us", INFERENCE_US)

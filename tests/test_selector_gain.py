@@ -168,3 +168,41 @@ def test_batched_frontier_range_follows_from_training_tables():
     got = ts.frontier_range(_CpuModel(params), data, allowed=ts.BATCH_ALLOWED, alpha=ts.BATCH_ALPHA,
                             beta=ts.BATCH_BETA)
     assert np.allclose(got, fr, atol=1e-6), (got, fr)
+
+
+# Delta-stepping SSSP's selector: push or pull for a bucket's heavy phase,
+# per-phase cost tables of the held-out graphs (`train_selector collect --sssp
+# --set eval`) and of the training graphs (`--set train`).
+SSSP_EVAL = ROOT / "tests" / "golden" / "selector_sssp_eval_b200.npz"
+SSSP_TRAIN_TABLES = ROOT / "tests" / "golden" / "selector_sssp_train_tables_b200.npz"
+SSSP_MODEL = ROOT / "sygraph_b200" / "models" / "selector_sssp_b200.npz"
+
+
+def _sssp_model():
+    with np.load(SSSP_MODEL) as m:
+        params = m["params"].astype(np.float32)
+        hr = tuple(float(x) for x in m["heavy_range"])
+    mdl = _CpuModel(params)
+    mdl.heavy_range = hr
+    return mdl
+
+
+def test_sssp_learned_heavy_phases_on_held_out_graphs():
+    """Inference cost included, the model's heavy phases take less time than
+    the rule's on the held-out graphs; no source loses more than 1%."""
+    from sygraph_b200 import train_selector as ts
+    with np.load(SSSP_EVAL) as d:
+        data = {k: d[k] for k in d.files}
+    rep = ts.evaluate_sssp(_sssp_model(), data)
+    assert rep["total"]["learned_us"] <= rep["total"]["heuristic_us"] / 1.01, rep["total"]
+    for r in rep["traversals"]:
+        assert r["learned_us"] <= 1.01 * r["heuristic_us"] + 2 * ts.INFERENCE_US, r
+
+
+def test_sssp_heavy_range_follows_from_training_tables():
+    from sygraph_b200 import train_selector as ts
+    with np.load(SSSP_TRAIN_TABLES) as d:
+        data = {k: d[k] for k in d.files}
+    mdl = _sssp_model()
+    got = ts.heavy_range(mdl, data)
+    assert np.allclose(got, mdl.heavy_range, atol=1e-6), (got, mdl.heavy_range)

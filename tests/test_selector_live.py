@@ -111,3 +111,49 @@ def test_learned_batched_faster_on_grid4096(sg):
     g = sg.io.grid(4096, long_range_frac=0.02, seed=103, weight_seed=2, value_type=sg.WEIGHT_U32)
     ratio = _batched_ratio(sg, g, 4.0)
     assert ratio >= 1.02, ratio
+
+
+def _sssp_ratio(sg, g, sources, delta):
+    """Rule / learned time of delta-stepping SSSP (heavy phases chosen by the
+    SSSP model), both on one instance alternating on one stream, per-source
+    medians summed; identical distances."""
+    import torch
+    from sygraph_b200 import selector, train_selector
+    G = sg.graph.build.fromCSR(g)
+    sp = sg.algorithms.SSSP(G)
+    sp.set_delta(delta)
+    mdl = selector.Mlp.load(train_selector.SSSP_MODEL_PATH)
+    for s in sources:
+        sp.set_selector(None)
+        sp.init(int(s))
+        sp.run()
+        ref = sp.getDistances().view(np.uint32).copy()
+        sp.set_selector(mdl)
+        sp.init(int(s))
+        sp.run()
+        assert np.array_equal(ref, sp.getDistances().view(np.uint32)), int(s)
+
+    def launch(key, a, b):
+        s, learned = key
+        sp.set_selector(mdl if learned else None)
+        sp.init(int(s))
+        a.record()
+        sp.run_async()
+        b.record()
+
+    th = tl = 0.0
+    for s in sources:
+        m = _alternating(torch, launch, [(s, False), (s, True)], reps=6)
+        th += m[(s, False)]
+        tl += m[(s, True)]
+    return th / tl
+
+
+def test_learned_sssp_no_slower_on_rmat22(sg):
+    g = sg.io.rmat(22, 16, 0.57, 0.19, 0.19, seed=1, weight_seed=2, perm_seed=0, value_type=sg.WEIGHT_F32)
+    assert _sssp_ratio(sg, g, sg.io.sample_sources(g, 4, seed=3), 0.1) >= 0.99
+
+
+def test_learned_sssp_no_slower_on_uniform21(sg):
+    g = sg.io.rmat(21, 16, 0.25, 0.25, 0.25, seed=104, weight_seed=2, value_type=sg.WEIGHT_F32)
+    assert _sssp_ratio(sg, g, sg.io.sample_sources(g, 4, seed=3), 0.2) >= 0.99

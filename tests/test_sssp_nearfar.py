@@ -208,3 +208,75 @@ def test_pull_iterations_directed_hubs_and_u32(sg, oracle):
     s2.init(0)
     s2.run()
     assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gg, 0))
+
+
+def _trusting_mlp(selector, seed):
+    """A random MLP whose trusted range covers every feature value."""
+    rng = np.random.default_rng(seed)
+    m = selector.Mlp()
+    p = m.params
+    t, I = selector.TRAINABLE_COUNT, selector.IN
+    p[:t] = rng.normal(scale=0.5, size=t).astype(np.float32)
+    p[t:t + I] = 0.0
+    p[t + I:t + 2 * I] = 1.0
+    p[t + 2 * I:t + 3 * I] = -1e9
+    p[t + 3 * I:t + 4 * I] = 1e9
+    m.params = p
+    return m
+
+
+@pytest.mark.parametrize("delta", [0.02, 0.1])
+def test_learned_heavy_phases(sg, oracle, rmat, delta):
+    """The learned heavy phase (sg_sssp_set_selector) keeps the oracle's
+    distances; at every heavy phase the device takes the MLP's choice between
+    push (4) and pull (6) on the logged features; without a model the
+    heavy_pull rule decides, and its forced forms give the same features."""
+    from sygraph_b200 import selector
+    g = rmat(14, perm_seed=3)
+    G = sg.graph.build.fromCSR(g)
+    assert G.weight_sorted()[2]  # symmetric weighted rows: pull is possible
+    s = sg.algorithms.SSSP(G)
+    s.set_delta(delta)
+    s.log_features(True)
+    srcs = [int(np.argmax(g.degrees()))] + [int(x) for x in sg.io.sample_sources(g, 2, seed=4)]
+    phases = 0
+    for seed in range(3):
+        m = _trusting_mlp(selector, seed)
+        s.set_selector(m, margin=0.0)
+        for src in srcs:
+            s.init(src)
+            s.run()
+            ref = oracle.sssp_dijkstra(g, src)
+            assert np.array_equal(s.getDistances().view(np.uint32), ref.view(np.uint32)), (seed, src)
+            got = np.array([2 if r["strategy"] == 6 else 0 for r in s.level_records() if r["strategy"] in (4, 6)])
+            F = s.level_features()
+            assert len(F) == len(got) and np.all(np.isfinite(F))
+            if not len(F):
+                continue
+            y = m.forward(F)[:, [0, 2]]
+            pick = np.where(got == 2, 1, 0)
+            best = y.min(1)
+            assert np.all(y[np.arange(len(got)), pick] <= best + 1e-4 * (1 + np.abs(best))), (seed, src)
+            phases += len(F)
+    assert phases >= 6
+    s.set_selector(None)
+    # without a model: the rule (pull when the bucket's heavy edges exceed
+    # m / ratio, feature 3 = heavy edges / m) and its forced forms
+    src = srcs[0]
+    for ratio in (0, 8, 0xFFFFFFFF):
+        s.set_heavy_pull(ratio)
+        s.init(src)
+        s.run()
+        assert np.array_equal(s.getDistances().view(np.uint32), oracle.sssp_dijkstra(g, src).view(np.uint32))
+        F = s.level_features()
+        got = np.array([2 if r["strategy"] == 6 else 0 for r in s.level_records() if r["strategy"] in (4, 6)])
+        assert len(F) == len(got) and len(F) >= 2
+        if ratio == 0:
+            assert np.all(got == 0)
+        elif ratio == 8:
+            clear = np.abs(F[:, 3] * 8 - 1) > 1e-3
+            assert np.array_equal(got[clear], np.where(F[clear, 3] * 8 > 1, 2, 0))
+        else:
+            assert np.all(got[F[:, 3] > 0] == 2)
+    s.set_heavy_pull(8)
+    s.log_features(False)
