@@ -693,6 +693,14 @@ typedef struct {
 sg_status sg_server_create(const sg_server_config* cfg, sg_server* out);
 sg_status sg_server_destroy(sg_server s);
 sg_status sg_server_add_graph(sg_server s, sg_graph g, uint32_t* graph_id);
+/* Creates now, on every slot, each workspace the graph's queries can use (the
+ * single and batched BFS and, on a weighted graph, the SSSP instance) that
+ * is not there yet and fits in the memory budget without evicting another
+ * workspace; SG_ERR_NOMEM when some did not fit.  A workspace is otherwise
+ * created by the first query that needs it, and its creation (allocations,
+ * host passes over the in-edge offsets for the pull chunk lists) then holds
+ * up every query queued behind it. */
+sg_status sg_server_prepare(sg_server s, uint32_t graph_id);
 sg_status sg_server_submit(sg_server s, uint32_t graph_id, int kind, uint32_t source, void* host_out,
                            uint64_t* ticket);
 /* Blocks until the query completes (SG_ERR_TIMEOUT after timeout_s; <= 0 waits without limit). */

@@ -188,6 +188,7 @@ SIGNATURES = {
     "sg_server_create": (st, [C.POINTER(ServerConfig), C.POINTER(vp)]),
     "sg_server_destroy": (st, [vp]),
     "sg_server_add_graph": (st, [vp, vp, u32p]),
+    "sg_server_prepare": (st, [vp, C.c_uint32]),
     "sg_server_submit": (st, [vp, C.c_uint32, C.c_int, C.c_uint32, vp, u64p]),
     "sg_server_wait": (st, [vp, C.c_uint64, C.c_double, C.POINTER(QueryResult)]),
     "sg_server_drain": (st, [vp, C.c_double]),

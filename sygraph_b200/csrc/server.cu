@@ -446,6 +446,29 @@ sg_status sg_server_add_graph(sg_server s, sg_graph g, uint32_t* graph_id) {
   return SG_OK;
 }
 
+sg_status sg_server_prepare(sg_server s, uint32_t graph_id) {
+  sgb::clear_error();
+  SG_REQUIRE(s, SG_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  SG_REQUIRE(graph_id < s->graphs.size(), SG_ERR_INVALID, "unknown graph id");
+  const sg_graph g = s->graphs[graph_id];
+  bool short_of_memory = false;
+  for (uint32_t si = 0; si < s->slots.size(); si++)
+    for (int kind : {kWsBfs, kWsBatch, kWsSssp}) {
+      if (kind == kWsSssp && g->value_type == SG_WEIGHT_NONE) continue;
+      if (s->slots[si].ws.count(ws_key(graph_id, kind))) continue;
+      if (s->ws_bytes + ws_estimate(g, kind, s->cfg.max_batch) > s->cfg.memory_budget) {
+        short_of_memory = true;  // (no eviction for a prepared workspace)
+        continue;
+      }
+      Workspace* w = nullptr;
+      bool never = false;
+      SG_TRY(get_workspace(s, si, graph_id, kind, &w, &never));
+    }
+  if (short_of_memory) return sgb::fail(SG_ERR_NOMEM, "server: some workspaces do not fit in the memory budget");
+  return SG_OK;
+}
+
 sg_status sg_server_submit(sg_server s, uint32_t graph_id, int kind, uint32_t source, void* host_out,
                            uint64_t* ticket) {
   sgb::clear_error();

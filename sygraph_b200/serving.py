@@ -58,6 +58,12 @@ class Server:
         self.graphs.append(G)
         return gid.value
 
+    def prepare(self, graph_id: int) -> None:
+        """Creates every workspace the graph's queries can use on every slot
+        now (within the memory budget, without evicting), so that no query
+        waits for one to be built."""
+        call("sg_server_prepare", self.handle, graph_id)
+
     def submit(self, graph_id: int, kind: str, source: int, out=None) -> int:
         t = C.c_uint64()
         ptr = None if out is None else C.c_void_p(out.ptr.value if isinstance(out, PinnedBuffer) else out.ctypes.data)

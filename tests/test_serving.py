@@ -99,3 +99,41 @@ def test_workspace_that_never_fits_is_refused(sg, graphs):
         srv.wait(99)  # unknown ticket
     assert srv.stats()["failed"] == 1
     srv.close()
+
+
+def test_prepare_builds_every_workspace_before_queries(sg, graphs):
+    """After prepare, queries of every kind run without building a workspace
+    (the workspace bytes do not grow) and match the single-query results; a
+    budget too small for them all is reported, without evicting."""
+    from sygraph_b200 import serving
+    Gs = [sg.graph.build.fromCSR(g) for g in graphs[:2]]
+    srv = serving.Server(slots=2, sssp_delta=0.1)
+    gids = [srv.add_graph(G) for G in Gs]
+    for gi in gids:
+        srv.prepare(gi)
+        srv.prepare(gi)  # a second call finds them all
+    before = srv.stats()["workspace_bytes"]
+    assert before > 0
+    rng = np.random.default_rng(4)
+    qs, outs, tickets = [], [], []
+    for k in range(80):
+        gi = k % 2
+        kind = "bfs" if k % 3 else "sssp"
+        src = int(rng.integers(0, graphs[gi].n))
+        out = serving.PinnedBuffer(graphs[gi].n, np.uint32 if kind == "bfs" else np.float32)
+        qs.append((gi, kind, src))
+        outs.append(out)
+        tickets.append(srv.submit(gids[gi], kind, src, out))
+    res = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert all(r["status"] == 0 for r in res)
+    assert st["workspace_bytes"] == before and st["evictions"] == 0
+    for (gi, kind, src), out in zip(qs, outs):
+        assert np.array_equal(out.array.view(np.uint32), _alone(sg, Gs[gi], kind, src, 0.1).view(np.uint32))
+    small = serving.Server(slots=2, memory_budget=1 << 20)
+    gid = small.add_graph(Gs[1])
+    with pytest.raises(sg._lib.SygraphError):
+        small.prepare(gid)
+    assert small.stats()["evictions"] == 0
+    small.close()
