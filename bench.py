@@ -861,7 +861,9 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "bfs_kernel", "bytes_per_launch": algo_bytes, "launch_ms": kern_ms},
             "e2e": {"value": e2e_val, "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
-                    "d2h_bytes_per_step": 4 * n * len(srcs), "ms_per_step": e2e_ms / e_steps},
+                    "d2h_bytes_per_step": 4 * n * len(srcs), "ms_per_step": e2e_ms / e_steps,
+                    # the depth rows' copy to the host bounds it: the host link's rate
+                    "d2h_gbs": 4 * n * len(srcs) / (e2e_ms / e_steps * 1e-3) / 1e9},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": base,

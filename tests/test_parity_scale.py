@@ -107,13 +107,25 @@ def _selector_graphs(sg):
 
 
 def test_learned_selector_graphs(sg, oracle):
-    from sygraph_b200 import selector
+    """The three learned modes on the selector's evaluation graphs against the
+    oracle: single-source BFS, delta-stepping SSSP with the learned heavy
+    phases, and the batched BFS (8 sources) with its model."""
+    from sygraph_b200 import selector, train_selector
     mlp = selector.Mlp.load()
+    sssp_mlp = selector.Mlp.load(train_selector.SSSP_MODEL_PATH)
+    batch_mlp = selector.Mlp.load(train_selector.BATCHED_MODEL_PATH)
     for name, g in _selector_graphs(sg):
         G = sg.graph.build.fromCSR(g)
         bfs = sg.algorithms.BFS(G)
         bfs.set_selector(mlp)
         sssp = sg.algorithms.SSSP(G)
+        sssp.set_selector(sssp_mlp)
+        mb = sg.algorithms.MultiBFS(G, 8)
+        mb.set_selector(batch_mlp)
+        ms = sg.io.sample_sources(g, 8, seed=5)
+        mb.run(ms, sg.algorithms.bfs_direction.learned, train_selector.BATCH_ALPHA, train_selector.BATCH_BETA)
+        assert np.array_equal(mb.getDistances(), oracle.bfs_multi(g, ms)), name
+        del mb
         srcs = sg.io.sample_sources(g, 2, seed=3)
         for s in srcs:
             want, it, _ = oracle.bfs_frontier(g, int(s), 2, ALPHA, BETA)
