@@ -248,6 +248,16 @@ __global__ void fill_depth_kernel(uint32_t* depth, uint32_t n, uint32_t src) {
     depth[i] = i == src ? 0u : n + 1;
 }
 
+// First in-neighbour of every vertex (0 for a vertex with none, which is
+// never a pull candidate).
+__global__ void first_in_kernel(const uint32_t* __restrict__ iro, const uint32_t* __restrict__ icol, uint32_t n,
+                                uint32_t* __restrict__ out) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t b = iro[v];
+    out[v] = b < iro[v + 1] ? icol[b] : 0u;
+  }
+}
+
 // Bitmap of the vertices with no incoming edge (inverse degree 0).
 __global__ void no_in_edges_kernel(const uint32_t* __restrict__ iro, uint32_t n, uint32_t w0, uint32_t* out) {
   const uint32_t lane = threadIdx.x & 31;
@@ -278,6 +288,7 @@ struct sg_bfs_s {
   uint32_t* fb = nullptr;
   uint32_t* sm = nullptr;
   uint32_t* no_in = nullptr;
+  uint32_t* first_in = nullptr;  // first in-neighbour of each vertex (the pull's first probe)
   uint32_t* heavy_v = nullptr;
   uint32_t* heavy_s = nullptr;
   uint32_t heavy_cap = 0;
@@ -322,6 +333,7 @@ static void bfs_release(sg_bfs b) {
   dev_free(b->fb);
   dev_free(b->sm);
   dev_free(b->no_in);
+  dev_free(b->first_in);
   dev_free(b->heavy_v);
   dev_free(b->heavy_s);
   dev_free(b->cnt);
@@ -364,6 +376,7 @@ static sg_status bfs_launch(sg_bfs b, int direction, float alpha, float beta) {
   P.depth = b->depth;
   P.visited = b->visited;
   P.no_in_edges = b->no_in;
+  P.first_in = b->first_in;
   P.fb = b->fb;
   P.sm = b->sm;
   P.heavy_v = b->heavy_v;
@@ -429,7 +442,7 @@ sg_status sg_bfs_create(sg_graph g, sg_bfs* out) {
   b->heavy_cap = (uint32_t)std::min<uint64_t>(n, g->m / bfs::kHeavy + 1);
   sg_status s = SG_OK;
   if ((s = dev_alloc(&b->depth, n)) || (s = dev_alloc(&b->visited, b->w0)) || (s = dev_alloc(&b->fb, 3ull * b->w0)) ||
-      (s = dev_alloc(&b->sm, 3ull * b->w1)) || (s = dev_alloc(&b->no_in, b->w0)) ||
+      (s = dev_alloc(&b->sm, 3ull * b->w1)) || (s = dev_alloc(&b->no_in, b->w0)) || (s = dev_alloc(&b->first_in, n)) ||
       (s = dev_alloc(&b->heavy_v, 2ull * b->heavy_cap)) || (s = dev_alloc(&b->heavy_s, 2ull * b->heavy_cap)) ||
       (s = dev_alloc(&b->cnt, 3)) || (s = dev_alloc(&b->bar, 1)) || (s = dev_alloc(&b->log, SG_MAX_LOGGED_LEVELS)) ||
       (s = dev_alloc(&b->result, 8))) {
@@ -438,6 +451,7 @@ sg_status sg_bfs_create(sg_graph g, sg_bfs* out) {
   }
   bfs::no_in_edges_kernel<<<grid_for((uint64_t)b->w0 * 32, 256), 256, 0, g->stream>>>(g->inv.ro, g->n, b->w0,
                                                                                        b->no_in);
+  bfs::first_in_kernel<<<grid_for(n, 256), 256, 0, g->stream>>>(g->inv.ro, g->inv.col, g->n, b->first_in);
   if (cudaGetLastError() != cudaSuccess) {
     bfs_release(b);
     return fail(SG_ERR_CUDA, "BFS set-up kernel failed to launch");
@@ -777,6 +791,7 @@ sg_status sg_bfs_noalloc(const uint32_t* dev_row_offsets, const uint32_t* dev_co
   P.visited = reinterpret_cast<uint32_t*>(base + kOffVisited);
   uint32_t* no_in = reinterpret_cast<uint32_t*>(base + kOffNoIn);
   P.no_in_edges = no_in;
+  P.first_in = nullptr;  // (no room in the static workspace: read through the offsets)
   P.fb = reinterpret_cast<uint32_t*>(base + kOffFb);
   P.sm = reinterpret_cast<uint32_t*>(base + kOffSm);
   P.heavy_cap = (uint32_t)std::min<uint64_t>(n, m / bfs::kHeavy + 1);

@@ -51,6 +51,10 @@ struct Params {
   uint32_t* depth;
   uint32_t* visited;
   const uint32_t* no_in_edges;  // bitmap of vertices no edge reaches: never candidates
+  // first in-neighbour of every vertex with one (nullptr: read through the
+  // in-edge offsets): the short-circuit pull's first probe without the
+  // dependent offset load and the random column read
+  const uint32_t* first_in;
   uint32_t* fb;                 // 3 * w0
   uint32_t* sm;                 // 3 * w1
   uint32_t* heavy_v;            // 2 * heavy_cap

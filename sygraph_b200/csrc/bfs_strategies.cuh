@@ -341,13 +341,27 @@ __device__ __forceinline__ void pull_ranked(Level& L, const uint32_t* fb_cur, bo
         own[k] = o;
         v[k] = ow * 32 + select_bit(ob, act[k] ? r - oe : 0u);
       }
+      // the first probe from the first-in-neighbour array when there is one
+      // (every candidate has an in-edge: the others are pre-marked visited),
+      // its load issued with the offsets' and not after them
+      const bool first = P.first_in && !reverse;
+      uint32_t x0[kRanked];
+#pragma unroll
+      for (int k = 0; k < kRanked; k++) x0[k] = (first && act[k]) ? P.first_in[v[k]] : 0u;
 #pragma unroll
       for (int k = 0; k < kRanked; k++) {
         b[k] = act[k] ? P.iro[v[k]] : 0u;
         e[k] = act[k] ? P.iro[v[k] + 1] : 0u;
         f[k] = false;
       }
-      for (uint32_t j = 0; j < kPullProbes; j++) {
+      if (first) {
+        uint32_t fw0[kRanked];
+#pragma unroll
+        for (int k = 0; k < kRanked; k++) fw0[k] = act[k] ? fb_cur[x0[k] >> 5] : 0u;  // as bit_test_ro
+#pragma unroll
+        for (int k = 0; k < kRanked; k++) f[k] = act[k] && ((fw0[k] >> (x0[k] & 31)) & 1u);
+      }
+      for (uint32_t j = first ? 1u : 0u; j < kPullProbes; j++) {
         uint32_t x[kRanked], fw[kRanked];
         bool a[kRanked];
 #pragma unroll
