@@ -112,3 +112,31 @@ def test_bfs_star_hub(sg, oracle):
         for direction in (0, 1, 2):
             d, _ = run_bfs(sg, g, s, direction, 15.0, 24.0)
             assert np.array_equal(d, oracle.bfs_levels(g, s))
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_bfs_consecutive_runs_across_components(sg, oracle, directed):
+    """One instance, sources in components of different sizes and on an
+    isolated vertex, in turn, with distances read before a run in between:
+    every run gives the oracle's depths (the engine rewrites only the depths
+    that the previous run reached and this one does not)."""
+    rng = np.random.default_rng(11)
+    n = 40_000
+    # a big random component on [0, 30000), a path on [30000, 30500), a star
+    # on [31000, 31200), the rest isolated
+    a = rng.integers(0, 30_000, 150_000)
+    b = rng.integers(0, 30_000, 150_000)
+    p = np.arange(30_000, 30_499)
+    s = np.full(199, 31_000)
+    src = np.concatenate([a, p, s])
+    dst = np.concatenate([b, p + 1, np.arange(31_001, 31_200)])
+    g = sg.io.fromCOO(n, src, dst, symmetrize=not directed, dedupe=True, drop_self_loops=True)
+    G = sg.graph.build.fromCSR(g, sg.Properties(directed=True)) if directed else sg.graph.build.fromCSR(g)
+    bfs = sg.algorithms.BFS(G)
+    order = [5, 30_000, 123, 31_000, 39_999, 30_250, 7, 31_100, 77, 39_000]
+    for k, s0 in enumerate(order):
+        bfs.init(s0)
+        if k == 4:
+            bfs.getDistances()  # the initial state, written before the run
+        bfs.run(sg.algorithms.bfs_direction.hybrid, 15.0, 24.0)
+        assert np.array_equal(bfs.getDistances(), oracle.bfs_levels(g, s0)), (directed, s0)
