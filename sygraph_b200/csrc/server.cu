@@ -103,8 +103,8 @@ uint64_t ws_estimate(const sg_graph g, int kind, uint32_t max_batch) {
   const uint64_t n = g->n, m = g->m, w0 = (n + 31) / 32;
   const uint64_t fixed = 512 * 1024;  // counters, barrier, level log
   switch (kind) {
-    case kWsBfs:
-      return fixed + 4 * n + 4 * 6 * w0 + 16 * (m / 256 + 1);
+    case kWsBfs:  // depths and first in-neighbours, bitmaps, heavy lists
+      return fixed + 8 * n + 4 * 6 * w0 + 16 * (m / 256 + 1);
     case kWsBatch:
       return fixed + 8 * n * (4 + bits_of(n ? n - 1 : 0)) + 4 * n * max_batch + 4 * 8 * w0 + 16 * (m / 256 + 1);
     default:
