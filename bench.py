@@ -269,6 +269,34 @@ def _alternating_ms(torch, runs, sources, reps: int = 6):
     return [float(np.mean([np.median(t) for t in per_src])) for per_src in times]
 
 
+def _summary(line: dict) -> dict:
+    """The sub-benchmarks' headline figures in one short object, printed as
+    the line's last key (the full objects above hold the details)."""
+    r3 = lambda x: None if x is None else round(float(x), 3)  # noqa: E731
+    b, ss, bc, ln = line["batched"], line["sssp"], line["bc_batched"], line["learned"]
+    dl = ss["delta_stepping"]
+    out = {
+        "bfs_gteps": r3(line["value"]), "bfs_frac": r3(line["roofline"]["frac"]), "e2e_gteps": r3(line["e2e"]["value"]),
+        "learned_bfs_rmat22": r3(ln.get("rmat_speedup_vs_heuristic")),
+        "learned_bfs_grid4096": r3(ln.get("grid4096_speedup_vs_heuristic")),
+        "batched_gteps": r3(b["value"]), "batched_frac": r3(b["roofline"]["frac"]),
+        "learned_batched_rmat22": r3(b["learned"]["rmat_speedup_vs_heuristic"]),
+        "learned_batched_grid4096": r3(b["learned"]["grid4096_speedup_vs_heuristic"]),
+        "sssp_bf_gteps": r3(ss["value"]), "sssp_bf_frac": r3(ss["roofline"]["frac"]),
+        "sssp_delta_gteps": r3(dl["value"]), "sssp_delta_frac": r3(dl["roofline"]["frac"]),
+        "learned_sssp_rmat22": r3(dl["learned"]["speedup_vs_rule"]),
+        "bc_batched_ms": r3(bc.get("launch_ms")), "bc_vs_per_source": r3(bc.get("speedup_vs_per_source")),
+        "parity_ok": (line.get("parity") or {}).get("ok"),
+    }
+    sv = line.get("serving")
+    if sv:
+        r = sv["runs"][0]
+        out.update({"serve_qps": r3(r["qps_served"]), "serve_p99_ms": r3(r["p99_ms"]),
+                    "serve_bfs_p99_ms": r3(r["bfs"]["p99_ms"]),
+                    "serve_vs_one_at_a_time": r3(sv["served_qps_vs_one_at_a_time"])})
+    return out
+
+
 def cpu_baseline(g, srcs):
     """The oracle's OpenMP frontier BFS on the host cores over a bounded
     sample of the bench's sources (about 15 s); returns the baseline object
@@ -899,6 +927,7 @@ def main():
                                   "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,
                                   "traffic": None}},  # the ncu capture is of the delta-stepping schedule
         }
+        line["summary"] = _summary(line)  # last key: the tail of the line stays readable
         print(json.dumps(line), flush=True)
     del bfs, sssp, G
     if world > 1:
