@@ -49,7 +49,8 @@ struct Queues {
   uint32_t* big_start;  // first chunk index of big[i]; increasing in i
 };
 
-__device__ __forceinline__ uint32_t chunks_of(uint32_t deg) { return (deg + kChunk - 1) / kChunk; }
+template <uint32_t kC = kChunk>
+__device__ __forceinline__ uint32_t chunks_of(uint32_t deg) { return (deg + kC - 1) / kC; }
 
 // Position of the k-th (0-based) set bit of x.
 __device__ __forceinline__ uint32_t select_bit(uint32_t x, uint32_t k) {
@@ -87,6 +88,7 @@ struct RowRange {
 // the slots; a second pass repeats the same rank walk and writes them.  When
 // `accumulate` is given, each word is also OR-ed into it (one thread per
 // word).
+template <uint32_t kC = kChunk>  // edges per chunk of a big vertex
 __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb, uint32_t w0, RowRange R,
                                                  Counters* C, Queues q, uint32_t* s_scan,
                                                  uint32_t* accumulate = nullptr) {
@@ -123,7 +125,7 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
           n_small++;
         } else {
           n_big++;
-          n_chunk += chunks_of(d);
+          n_chunk += chunks_of<kC>(d);
         }
       }
     }
@@ -156,7 +158,7 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
           q.big[pb] = v;
           q.big_start[pb] = pc;
           pb++;
-          pc += chunks_of(d);
+          pc += chunks_of<kC>(d);
         }
       }
     }

@@ -112,6 +112,12 @@ __device__ __forceinline__ bool heavy_decide(const SsspParams<W>& P, HeavySelect
 // order as their bit patterns); an improved u joins the next frontier, or,
 // under near-far bucketing with nd at or beyond the threshold, the far set.
 constexpr int kU = 4;
+// Edges per chunk of a big vertex in SSSP push steps: half the push
+// engines' (more warps share a hub's edges; a step with few frontier
+// vertices is a few dependent round trips per chunk): on RMAT-22 the
+// reference schedule 5.40 -> 5.04 ms per source, delta-stepping 1.99 ->
+// 1.95 ms; 64-edge chunks lose on the reference schedule (6.0 ms).
+constexpr uint32_t kSsspChunk = 128;
 
 template <typename W>
 struct SsspRelax {
@@ -174,7 +180,7 @@ struct SsspRelax {
 
 // Push expansion of one SSSP step over the compacted queues.  Small vertices
 // (row range < kSmallDeg) go 32 per warp, their edges ranked across the warp;
-// big vertices are cut in kChunk-edge chunks, and each warp takes a
+// big vertices are cut in kSsspChunk-edge chunks, and each warp takes a
 // contiguous run of chunks: one owner search, then the owners advance.
 template <typename W>
 __device__ __forceinline__ void sssp_expand(RowRange R, Queues q, uint32_t n_small, uint32_t n_big, uint32_t n_chunks,
@@ -232,8 +238,8 @@ __device__ __forceinline__ void sssp_expand(RowRange R, Queues q, uint32_t n_sma
       ve = R.end(v);
       dv = ld_cg(X.dist + v);
     }
-    const uint32_t cb = vb + (c - first) * kChunk;
-    const uint32_t ce = min(ve, cb + kChunk);
+    const uint32_t cb = vb + (c - first) * kSsspChunk;
+    const uint32_t ce = min(ve, cb + kSsspChunk);
     for (uint32_t eb = cb; eb < ce; eb += 32 * kU) {
       uint32_t e[kU];
       W d[kU];
@@ -394,7 +400,7 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
     } else if (!pull) {
       // bucketed: light edges only, the prefix of each weight-sorted row
       const RowRange R = bucketed ? RowRange{S.ro, P.split, 0} : RowRange{S.ro, S.ro, 1};
-      compact_frontier(fb_cur, S.w0, R, C, S.q, s_scan, bucketed ? P.bucket : nullptr);
+      compact_frontier<kSsspChunk>(fb_cur, S.w0, R, C, S.q, s_scan, bucketed ? P.bucket : nullptr);
       if (!grid_sync(S.bar)) return 0;
       ns = ld_cg(&C->small_tail);
       bp = ld_cg(&C->big_packed);
@@ -526,7 +532,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
       // their final distances: they land at or beyond the threshold (far)
       Counters* Ch = P.L.cnt + (levels % 3);  // zeroed by the last level, unused since
       const RowRange Rh{P.split, P.L.ro, 1};   // the suffix of each weight-sorted row
-      compact_frontier(P.bucket, w0, Rh, Ch, P.L.q, s_scan);
+      compact_frontier<kSsspChunk>(P.bucket, w0, Rh, Ch, P.L.q, s_scan);
       if (!grid_sync(P.L.bar)) return;
       const uint32_t ns = ld_cg(&Ch->small_tail);
       const unsigned long long bp = ld_cg(&Ch->big_packed);
