@@ -218,8 +218,12 @@ __device__ __forceinline__ void sssp_expand(RowRange R, Queues q, uint32_t n_sma
     }
   }
   if (!n_chunks) return;
+  // the chunk runs start at the first warp without a small group, so that
+  // on a small frontier no warp walks a group and then a chunk (two chains
+  // of dependent loads one after the other)
+  const uint32_t bw = (gwarp + nwarps - (n_groups % nwarps)) % nwarps;
   const uint32_t per = (n_chunks + nwarps - 1) / nwarps;
-  const uint32_t c_lo = gwarp * per;
+  const uint32_t c_lo = bw * per;
   const uint32_t c_hi = min(n_chunks, c_lo + per);
   if (c_lo >= c_hi) return;
   uint32_t ent = warp_find_owner(q.big_start, n_big, c_lo);
