@@ -825,7 +825,7 @@ def main():
     # delta-stepping on the same sources: the same distances (checked), less
     # work; the bucket width from the autotuner (timed on two other sources)
     sssp.set_pull(SSSP_PULL)
-    sssp_delta = float(autotune.tune_sssp(sssp, srcs[-2:], autotune.mean_weight(g), reps=1,
+    sssp_delta = float(autotune.tune_sssp(sssp, srcs[-2:], autotune.mean_weight(g), reps=3,
                                           use_cache=False)["delta"]) or SSSP_DELTA
     sssp.set_delta(sssp_delta)
     nf_ms, nf_same = 0.0, True

@@ -535,7 +535,9 @@ sg_status sg_sssp_set_pull(sg_sssp s, uint32_t ratio);
  * iteration, 2 pull sweep; with near-far bucketing also 4, the heavy-edge
  * phase of a bucket (frontier_size = the bucket's vertices), and 5, a refill
  * pass (frontier_size = vertices moved to the frontier, next_size = vertices
- * left beyond the threshold). */
+ * left beyond the threshold).  In the push iterations of near-far bucketing
+ * without light pulls, next_size counts frontier marks, an upper bound on the
+ * vertices of the next frontier (zero exactly when it is empty). */
 sg_status sg_sssp_level_records(sg_sssp s, sg_level_record* host_records, uint32_t cap, uint32_t* count);
 /* Stream of this instance's launches and copies (NULL: the graph's stream)
  * and a cap on its persistent grid in CTAs of 512 threads (0: two per SM on

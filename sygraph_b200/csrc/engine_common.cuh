@@ -101,6 +101,9 @@ __device__ __forceinline__ void compact_frontier(const uint32_t* __restrict__ fb
     const uint32_t wi = base + threadIdx.x;
     const uint32_t bits = wi < wend ? ld_cg(fb + wi) : 0u;
     if (accumulate && bits) st_cg(accumulate + wi, ld_cg(accumulate + wi) | bits);
+    // words all empty across the block (most blocks of a small frontier):
+    // nothing to rank, count or reserve, so one barrier instead of the scans
+    if (!__syncthreads_or(bits != 0u)) continue;
     const uint32_t c = __popc(bits);
     const uint32_t incl = warp_inclusive_scan(c);
     const uint32_t total = __shfl_sync(kFullMask, incl, 31);

@@ -130,6 +130,10 @@ struct SsspRelax {
   W threshold;
   bool bucketed;
   bool want_deg;  // sum the out-degree of new frontier vertices (only a pull decision reads it)
+  // count each newly set frontier bit once; otherwise the marks do not wait
+  // for the old bitmap word and n_new counts marks (zero exactly when no bit
+  // was set, which is all that termination reads)
+  bool exact = true;
   uint32_t n_new = 0;
   unsigned long long deg_new = 0;
 
@@ -154,6 +158,20 @@ struct SsspRelax {
     if (!imp) return;
 #pragma unroll
     for (int k = 0; k < kU; k++) old[k] = ((imp >> k) & 1u) ? sygraph::detail::atomic_min_nonneg(dist + u[k], nd[k]) : W(0);
+    if (!exact) {
+#pragma unroll
+      for (int k = 0; k < kU; k++)
+        if (((imp >> k) & 1u) && nd[k] < old[k]) {
+          const uint32_t b = 1u << (u[k] & 31);
+          if (bucketed && !(nd[k] < threshold)) {
+            atomicOr(far + (u[k] >> 5), b);
+          } else {
+            atomicOr(fb_next + (u[k] >> 5), b);
+            n_new++;
+          }
+        }
+      return;
+    }
     uint32_t prev[kU];
     uint32_t marked = 0;
 #pragma unroll
@@ -418,6 +436,11 @@ __device__ __forceinline__ uint32_t sssp_levels(const SsspParams<W>& P, const Pu
       X.threshold = threshold;
       X.bucketed = bucketed;
       X.want_deg = !bucketed && P.pull_ratio;
+      // delta-stepping's light iterations need only termination from the
+      // count, unless a light pull decision reads the frontier size (the
+      // frontier Bellman-Ford ran slower without the returned word: RMAT-22
+      // 4.97 -> 5.11 ms, delta 0.1 1.89 -> 1.85 ms)
+      X.exact = !bucketed || X.want_deg || P.light_pull;
       sssp_expand(R, S.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, X);
       n_new = X.n_new;
       deg_new = X.deg_new;
@@ -565,6 +588,7 @@ __global__ void __launch_bounds__(kThreads, 2) sssp_kernel(SsspParams<W> P) {
         X.threshold = threshold;
         X.bucketed = true;
         X.want_deg = false;
+        X.exact = false;
         sssp_expand(Rh, P.L.q, ns, (uint32_t)(bp >> 32), (uint32_t)bp, X);
       }
       // the bucket bitmap is cleared by the refill (the pull reads it until the barrier)

@@ -31,7 +31,8 @@ def test_tune_picks_fastest_and_caches(tmp_path):
 
 def test_delta_candidates():
     f = autotune.delta_candidates(0.5, integer=False)
-    assert len(f) == 7 and abs(f[0] - 0.1) < 1e-12 and abs(f[-1] - 6.4) < 1e-12
+    assert len(f) == 15 and abs(f[0] - 0.05) < 1e-12 and abs(f[-1] - 6.4) < 1e-9
+    assert all(abs(b / a - 2 ** 0.5) < 1e-9 for a, b in zip(f, f[1:]))
     u = autotune.delta_candidates(32.5, integer=True)
     assert u == sorted(set(u)) and u[0] >= 1 and all(float(x).is_integer() for x in u)
 
