@@ -378,13 +378,16 @@ def profile_case(kind: str) -> None:
             det = a.run(sbc)
         print(json.dumps({"profile": "bc", "sources": BC_SOURCES, **det}))
     else:
+        # "sssp": delta-stepping at the bucket width the autotuner picks on
+        # this graph; "sssp_bf": the reference's frontier Bellman-Ford
         a = sg.algorithms.SSSP(G)
+        delta = SSSP_PROFILE_DELTA if kind == "sssp" else 0.0
         a.set_pull(SSSP_PULL)
-        a.set_delta(SSSP_DELTA)
+        a.set_delta(delta)
         for _ in range(2):
             a.init(src)
             it = a.run()
-        print(json.dumps({"profile": "sssp", "source": src, "iterations": it}))
+        print(json.dumps({"profile": kind, "source": src, "delta": delta, "iterations": it}))
 
 
 SERVE_SCALES = (14, 16, 18, 20, 21, 22, 22, 23)
@@ -393,6 +396,9 @@ SERVE_SECONDS = 2.0
 SERVE_SLOTS = 4
 SSSP_DELTA = 0.1
 SSSP_PULL = 0  # pull iterations off: on RMAT they cost more than the pushes they replace
+# delta-stepping bucket width of the ncu capture: the autotuner's pick on the
+# RMAT-22 bench graph (its candidates are a factor sqrt(2) apart)
+SSSP_PROFILE_DELTA = 0.1 * 2 ** -0.5
 
 
 def _edge_list(g, seed: int = 5):
@@ -482,7 +488,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving sub-benchmark")
     ap.add_argument("--sssp-sources", type=int, default=64)
-    ap.add_argument("--profile", choices=["bfs", "sssp", "msbfs", "bc", "tc", "cc"], default=None,
+    ap.add_argument("--profile", choices=["bfs", "sssp", "sssp_bf", "msbfs", "bc", "tc", "cc"], default=None,
                     help="profiling case: build the graph, run 2 traversals of one kind and exit (few launches)")
     args = ap.parse_args()
     world, rank, local = dist_init()
@@ -925,7 +931,7 @@ def main():
                                   "learned": sssp_learned},
                      "roofline": {"bound": "hbm", "achieved": sssp_achieved, "peak": peak, "unit": "GB/s",
                                   "frac": sssp_achieved / peak, "bytes_per_launch": sssp_bytes,
-                                  "traffic": None}},  # the ncu capture is of the delta-stepping schedule
+                                  "traffic": ncu_traffic("sssp_kernel_bf")}},
         }
         line["summary"] = _summary(line)  # last key: the tail of the line stays readable
         print(json.dumps(line), flush=True)
