@@ -68,6 +68,35 @@ def test_nearfar_bellman_ford_tail(sg, oracle, rmat, delta, tail):
     assert np.array_equal(s2.getDistances(), oracle.sssp_dijkstra(gg, 100))
 
 
+@pytest.mark.parametrize("delta", [0.0, 0.05, 0.1])
+def test_push_step_counts_in_the_log(sg, oracle, rmat, delta):
+    """A push step's next_size against the frontier the next step expands:
+    equal in the frontier Bellman-Ford (each newly set bit counted once), an
+    upper bound in delta-stepping's push steps (marks are counted without
+    waiting for the old bitmap word), and zero only where the run of push
+    steps ends.  A refill's count is the next step's frontier exactly."""
+    g = rmat(14, perm_seed=3)
+    s = sg.algorithms.SSSP(sg.graph.build.fromCSR(g))
+    s.set_delta(delta)
+    for src in [int(np.argmax(g.degrees()))] + [int(x) for x in sg.io.sample_sources(g, 2, seed=8)]:
+        s.init(src)
+        it = s.run()
+        assert np.array_equal(s.getDistances().view(np.uint32), oracle.sssp_dijkstra(g, src).view(np.uint32))
+        recs = s.level_records()
+        assert 0 < len(recs) < 4096 and sum(r["strategy"] == 0 for r in recs) == it
+        assert recs[0]["strategy"] == 0 and recs[0]["frontier_size"] == 1
+        for a, b in zip(recs, recs[1:]):
+            if a["strategy"] == 0 and b["strategy"] == 0:
+                assert a["next_size"] >= b["frontier_size"] > 0, (delta, src, a, b)
+                if delta == 0.0:
+                    assert a["next_size"] == b["frontier_size"], (src, a, b)
+            if a["strategy"] == 0 and a["next_size"] == 0:
+                assert b["strategy"] != 0, (delta, src, a, b)
+            if a["strategy"] == 5 and b["strategy"] == 0:
+                assert a["frontier_size"] == b["frontier_size"], (delta, src, a, b)
+        assert recs[-1]["next_size"] == 0 or recs[-1]["strategy"] == 5
+
+
 @pytest.mark.parametrize("light", [0, 16, 1 << 30])
 @pytest.mark.parametrize("ratio", [0, 1, 8, 1 << 30])
 def test_nearfar_heavy_pull(sg, oracle, rmat, ratio, light):
