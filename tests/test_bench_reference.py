@@ -41,3 +41,20 @@ def test_reference_arm_json_line():
     import bench
     assert d["config"] == bench.bench_config(1 << bench.SCALE, d["config"]["m"])
     assert d["config"]["sources_per_step"] == 64 and d["config"]["m"] == 128301086
+
+
+def test_every_traffic_key_of_the_bench_has_a_capture():
+    """Each kernel whose `traffic` the bench line reports has its ncu DRAM
+    bytes in profiles/traffic.json and a summary in profiles/ naming the
+    profiling case that captured it."""
+    import re
+
+    src = (ROOT / "bench.py").read_text()
+    keys = set(re.findall(r'ncu_traffic\("([a-z_0-9]+)"\)', src))
+    traffic = json.loads((ROOT / "profiles" / "traffic.json").read_text())
+    assert keys and keys <= set(traffic), keys - set(traffic)
+    assert all(isinstance(traffic[k], int) and traffic[k] > 0 for k in keys)
+    summaries = " ".join(p.read_text() for p in (ROOT / "profiles").glob("*.md"))
+    cases = set(re.search(r'"--profile", choices=\[([^\]]*)\]', src).group(1).replace('"', "").replace(" ", "").split(","))
+    for case in cases:
+        assert f"--profile {case}" in summaries, case
